@@ -1,0 +1,193 @@
+/*
+ * libgs_cuda — the C ABI of the B200 (sm_100a) 3D Gaussian Splatting training step.
+ *
+ * It replaces the reference engine's private pass recorders and their Vulkan dispatch:
+ * gs::Trainer::record_project / record_sort / record_rasterize / record_loss /
+ * record_backward / record_optimize / record_scan, densify and reset_opacity
+ * (engine/include/gs/trainer.h:429-443, engine/src/trainer.cpp:576-586, 665-776,
+ * 1083-1128), which bind std430 buffers and call VkContext::dispatch
+ * (engine/include/gs/vk_context.h:172-184). The caller keeps the reference's host code
+ * above this line (gs::Trainer's public API, gs_train, gs_render).
+ *
+ * Conventions (the reference throws std::runtime_error / VulkanError with a message,
+ * engine/include/gs/vk_context.h:18-29; here every function returns a status):
+ *  - 0 is success; nonzero is one of GS_ERR_*; gs_last_error() gives the message of the
+ *    calling thread's latest failure.
+ *  - No device pointers cross this boundary: host pointers are copied before return.
+ *  - The library owns all device memory and grows its pair buffers itself, as the
+ *    reference grows them on overflow (engine/src/trainer.cpp:588-624).
+ *  - One context per device and caller thread; calls on a context are serialised on its
+ *    own CUDA stream and are synchronous unless stated otherwise.
+ *
+ * Layouts crossing the boundary are the reference's: 16 floats of parameters per slot
+ * (train_common.glsl:3-8: position xyz + opacity logit, log scale xyz + alive flag,
+ * quaternion w x y z, SH DC rgb + unused), `sh_stride` floats of SH beyond DC per slot
+ * ([coeff][rgb]), RGBA8 images, and FrameData (train_common.glsl:15-37) per view.
+ */
+#ifndef GS_CUDA_H
+#define GS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_ERR_INVALID 1   /* invalid argument */
+#define GS_ERR_NO_MEMORY 2 /* device or host allocation failed */
+#define GS_ERR_CAPACITY 3  /* more pairs than the largest buffer the library will allocate */
+#define GS_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (the sort's look-back) */
+#define GS_ERR_CUDA 5      /* any other CUDA error */
+
+#define GS_MAX_VIEWS 16
+
+/* Flags in gs_frame_data.model[3] (train_common.glsl:50-57). */
+#define GS_FLAG_MASKED_TARGET 1u /* composite the target over the background by its alpha */
+#define GS_FLAG_SSIM 4u          /* measure SSIM (and its gradient when training) */
+#define GS_FLAG_SPARSE_ADAM 128u /* gaussians that drew nothing keep their values and moments */
+
+/* Per-view step constants: FrameData of train_common.glsl:15-37, filled as
+   Trainer::write_frame fills it (engine/src/trainer.cpp:440-547). 288 bytes. */
+typedef struct gs_frame_data {
+  float rot[3][4];     /* world -> camera rotation rows (OpenCV axes); [r][3] = translation */
+  float cam_pos[4];    /* camera centre, world */
+  float intrinsics[4]; /* fx, fy, cx, cy */
+  uint32_t image[4];   /* width, height, tiles_x, tiles_y (16x16 tiles) */
+  uint32_t model[4];   /* slots in use, active SH degree, sh_stride (floats), flags */
+  float background[4]; /* rgb, loss scale 1 / (3 W H) */
+  float lr0[4];        /* position (x camera extent, decayed), log scale, rotation, opacity */
+  float lr1[4];        /* SH DC, SH rest */
+  float adam[4];       /* beta1, beta2, epsilon */
+  float bias[4];       /* 1 / (1 - beta1^t), 1 / (1 - beta2^t) */
+  float densify0[4];   /* grad threshold, clone max scale, prune min opacity, prune max world scale */
+  float densify1[4];   /* prune max screen radius, seed (uint bits), split scale divisor */
+  uint32_t limits[4];  /* set by the library: pair capacity, 0, 0, most pairs the update accepts */
+  float loss[4];       /* D-SSIM weight lambda, C1, C2 */
+  float head[4];       /* head region centre x, y, radius (px; 0: none), loss weight */
+  float exposure[4];   /* rgb: the photo's colour times this is compared (1 / gain) */
+} gs_frame_data;
+
+typedef struct gs_context gs_context;
+
+/* Per-view outcome of a step. losses: the per-tile sums of train_forward.comp:18-23 and
+   train_ssim.comp summed over the view (Trainer::read_slot, trainer.cpp:778-795):
+   [0] sum |e|, [1] sum e^2, [2] SSIM sum, [3] sum w |e|, [4] sum w SSIM, [5] sum 3 w,
+   [6] head sum e^2, [7] head pixels. */
+typedef struct gs_step_result {
+  uint32_t n_views;
+  uint32_t overflow;      /* the pairs did not fit and no retry was allowed: no update */
+  uint32_t retries;       /* the step ran again after growing the pair buffers */
+  uint32_t tile_mismatch; /* gaussians whose emitted tiles differed from the count (whole run) */
+  uint64_t pairs[GS_MAX_VIEWS];
+  double losses[GS_MAX_VIEWS][8];
+  float gpu_ms; /* device time of the step (CUDA events) */
+  uint32_t kernels; /* kernel launches of the step */
+  /* With GS_STEP_PROFILE, device milliseconds per pass (Trainer's PassTimes,
+     trainer.h:173-185): [0] project, [1] sort (depth sort, scan, emit, pair sort,
+     ranges), [2] rasterize, [3] loss (SSIM and its gradient), [4] backward,
+     [5] optimize (pair sum + projection backward + Adam). */
+  float pass_ms[6];
+} gs_step_result;
+
+/* Which intermediate buffer gs_snapshot copies (Trainer::DebugSnapshot, trainer.h:302-313). */
+typedef enum gs_snapshot_kind {
+  GS_SNAP_PIXEL_COUNT = 0,  /* uint32 per pixel: pairs up to the last contributor */
+  GS_SNAP_PIXEL_GRAD = 1,   /* 4 floats per pixel: dL/dC rgb, final transmittance */
+  GS_SNAP_PROJECTED = 2,    /* 16 floats per slot (train_common.glsl:9-13) */
+  GS_SNAP_TILES = 3,        /* uint32 per slot: tiles touched */
+  GS_SNAP_OFFSETS = 4,      /* uint32 per slot: first pair (pre-sort order) */
+  GS_SNAP_PAIR_GRADS = 5,   /* 12 floats per pair, pre-sort order (deterministic mode) */
+  GS_SNAP_PAIR_TILE = 6,    /* uint32 per pair, pre-sort order: the view's tile */
+  GS_SNAP_RENDER_ORDER = 7, /* uint32 per pair: pre-sort index in render order */
+  GS_SNAP_DEPTH_KEY = 8,    /* uint32 per slot: 16-bit depth key */
+  GS_SNAP_IMAGE = 9,        /* RGBA8 per pixel */
+  GS_SNAP_RANGES = 10,      /* 2 uint32 per tile: [start, end) in render order, view-local */
+  GS_SNAP_TILE_LOSS = 11,   /* 16 floats per tile */
+  GS_SNAP_PIXEL_DOT = 12,   /* float per pixel: dL/dC . colour */
+  GS_SNAP_STATS = 13,       /* 4 floats per slot: densification statistics */
+  GS_SNAP_PAIR_GAUSSIAN = 14, /* uint32 per pair, pre-sort order: the slot */
+  GS_SNAP_PIXEL_OUT = 15,     /* 4 floats per pixel: rendered rgb over the background, loss weight */
+  GS_SNAP_SPAWN = 16          /* uint32 per slot after gs_densify: 0 none, 1 clone, 2 split */
+} gs_snapshot_kind;
+
+/* Tuning knobs (Trainer options that shape buffers and kernels; trainer.h:150-165). */
+typedef struct gs_tuning {
+  uint32_t min_pair_capacity; /* smallest pair buffer (TrainOptions::min_pair_capacity) */
+  uint64_t initial_pairs;     /* pairs to allocate before the first count (0: 4 per slot and view) */
+  uint32_t deterministic;     /* 1: per-pair gradients + fixed-order sum (bit-stable); 0: atomics */
+  uint32_t raster_batch;      /* splats staged per block in the backward pass: 32 or 64 (0: auto) */
+  uint32_t sort_digit_bits;   /* radix digit width: 8 (0: auto) */
+  uint32_t retry;             /* 1 (default): grow the pair buffers and run again on overflow */
+} gs_tuning;
+
+typedef struct gs_model_info {
+  uint32_t capacity, slots, sh_stride;
+  uint64_t pair_capacity;
+  uint64_t device_bytes;
+} gs_model_info;
+
+/* Message of the calling thread's latest failure ("" if none). */
+const char* gs_last_error(void);
+
+/* Context on CUDA device `device`: the role of the VkContext& the reference's Trainer
+   takes (trainer.h:253), device + stream owner. */
+int gs_create(int device, gs_context** out);
+int gs_destroy(gs_context* ctx);
+
+/* Parameters and Adam state: the Trainer constructor's upload (trainer.cpp:388-417).
+   capacity slots are allocated; `count` are initialised from params16 (16 floats per
+   slot) and sh (sh_stride floats per slot, may be NULL when sh_stride is 0). Moments and
+   statistics start at zero. */
+int gs_model_init(gs_context* ctx, uint32_t capacity, uint32_t sh_stride, const float* params16, const float* sh,
+                  uint32_t count);
+int gs_model_info_get(gs_context* ctx, gs_model_info* out);
+/* The slots in use, in the reference layout (Trainer::export_scene, trainer.cpp:1773-1800
+   reads the same buffers). Either pointer may be NULL. */
+int gs_model_export(gs_context* ctx, float* params16, float* sh, uint32_t max_slots, uint32_t* slots);
+/* Adam moments of the slots in use (Trainer::first_step_gradients, trainer.cpp:1802-1811,
+   divides m by 1 - beta1). Any pointer may be NULL. */
+int gs_model_moments(gs_context* ctx, float* m16, float* v16, float* m_sh, float* v_sh);
+
+/* The views of the next step: one FrameData each, with its own resolution, and each
+   view's target image (RGBA8, width x height x 4 bytes; NULL: no loss). Replaces
+   Trainer::write_frame's host-visible uploads (trainer.cpp:440-547, 1024-1031). */
+int gs_set_views(gs_context* ctx, uint32_t n_views, const gs_frame_data* frames, const uint8_t* const* rgba_targets);
+
+#define GS_STEP_TRAIN 1u   /* backward pass and Adam (else: forward and loss only) */
+#define GS_STEP_PROFILE 2u /* time each pass with CUDA events (pass_ms) */
+
+/* One step over the views set by gs_set_views: project -> key build + sort -> tile ranges
+   -> rasterise -> L1 + SSIM -> backward -> Adam (trainer.cpp:825-831). With more than one
+   view, the views' gradients are summed and one Adam step is taken. Overflowing pair
+   buffers are grown and the step re-run (trainer.cpp:814-836) unless tuning.retry is 0. */
+int gs_step(gs_context* ctx, uint32_t flags, gs_step_result* out);
+
+/* Forward only: `frame`'s view of the model as RGBA8 (alpha = coverage) into rgba_out
+   (Trainer::render_with, trainer.cpp:1140-1153). */
+int gs_render(gs_context* ctx, const gs_frame_data* frame, uint8_t* rgba_out);
+
+/* Adaptive density control with `frame`'s thresholds (Trainer::densify,
+   trainer.cpp:1083-1119; train_densify_mark.comp, train_densify_spawn.comp). Slots are
+   placed deterministically (free list in slot order, spawners in slot order). counters:
+   [0] free slots, [1] gaussians that asked to spawn, [2] pruned, [3] slots in use after. */
+int gs_densify(gs_context* ctx, const gs_frame_data* frame, uint32_t counters_out[4]);
+
+/* Caps every opacity logit at max_logit and clears its moments
+   (Trainer::reset_opacity, trainer.cpp:1121-1128). */
+int gs_reset_opacity(gs_context* ctx, float max_logit);
+
+/* Copies an intermediate buffer of the latest step's view `view` to host (the reference's
+   Trainer::debug_snapshot, trainer.cpp:1813-1852). `needed` receives the byte size;
+   host may be NULL to query it. */
+int gs_snapshot(gs_context* ctx, uint32_t view, gs_snapshot_kind which, void* host, size_t bytes, size_t* needed);
+
+int gs_set_tuning(gs_context* ctx, const gs_tuning* tuning);
+int gs_get_tuning(gs_context* ctx, gs_tuning* tuning);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

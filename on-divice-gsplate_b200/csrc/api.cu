@@ -1,0 +1,890 @@
+// The C ABI of libgs_cuda (include/gs_cuda.h): device memory, the step's launch sequence
+// and the overflow protocol. Replaces Trainer::record_* and VkContext::run
+// (engine/src/trainer.cpp:576-776, engine/src/vk_context.cpp:583-632).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gs_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure {
+  int code;
+  std::string message;
+};
+
+#define GS_CUDA_TRY(expr)                                                                                  \
+  do {                                                                                                     \
+    const cudaError_t e_ = (expr);                                                                         \
+    if (e_ != cudaSuccess)                                                                                 \
+      throw Failure{e_ == cudaErrorMemoryAllocation ? GS_ERR_NO_MEMORY : GS_ERR_CUDA,                     \
+                    std::string(#expr) + ": " + cudaGetErrorString(e_)};                                   \
+  } while (0)
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return GS_OK;
+  } catch (const Failure& e) {
+    g_last_error = e.message;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return GS_ERR_INVALID;
+  }
+}
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Failure{code, msg}; }
+
+template <typename T>
+void dev_alloc(T*& p, size_t count) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (count == 0) count = 1;
+  GS_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)));
+}
+template <typename T>
+void dev_free(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+uint32_t bits_for(uint32_t n) {
+  uint32_t bits = 0;
+  while (bits < 32u && (1ull << bits) < n) ++bits;
+  return bits;
+}
+
+constexpr uint64_t kMaxPairs = (1ull << 30) - 1ull;  // look-back words carry 30-bit counts
+
+}  // namespace
+
+struct gs_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t marks[7] = {};  // pass boundaries when profiling
+  bool profile = false;
+  gsk::Model model;
+  gs_tuning tuning{};
+  // views of the step
+  uint32_t n_views = 0;
+  std::vector<gs_frame_data> frames;
+  gs_frame_data* d_frames = nullptr;
+  gs_frame_data* h_frames = nullptr;  // pinned
+  gsk::ViewTable vt{};
+  uint32_t total_tiles = 0, total_pixels = 0;
+  bool has_target = false;
+  // (view, slot) buffers
+  uint32_t vb_views = 0;
+  gsk::ViewBuffers vb;
+  uint32_t *dkeys = nullptr, *dvals = nullptr, *dkeys_alt = nullptr, *dvals_alt = nullptr;
+  uint32_t* sorted_offsets = nullptr;
+  const uint32_t* depth_sorted_keys = nullptr;
+  const uint32_t* depth_sorted_vals = nullptr;
+  // pixels and tiles
+  size_t pixel_cap = 0, tile_cap = 0;
+  uint32_t* target = nullptr;
+  float4 *pixel_grad = nullptr, *pixel_out = nullptr, *ssim_maps = nullptr;
+  uint32_t *pixel_count = nullptr, *image = nullptr;
+  float* pixel_dot = nullptr;
+  uint2* ranges = nullptr;
+  float* tile_loss = nullptr;
+  uint32_t* tile_count = nullptr;
+  // pairs
+  uint64_t pair_cap = 0;
+  uint32_t *keys = nullptr, *values = nullptr, *keys_alt = nullptr, *values_alt = nullptr, *pair_gaussian = nullptr;
+  float4* pair_grads = nullptr;
+  const uint32_t* sorted_keys = nullptr;
+  const uint32_t* sorted_values = nullptr;
+  // scalars: [0] pairs (the scan's total), [1] emit mismatches (whole run)
+  uint32_t* d_scalars = nullptr;
+  uint32_t* h_scalars = nullptr;  // pinned
+  double* d_view_sums = nullptr;
+  double* h_view_sums = nullptr;  // pinned
+  gsk::SortScratch sort;
+  gsk::DensifyScratch dens;
+  uint64_t max_pairs_seen = 0;
+  uint64_t last_pairs = 0;
+  bool stepped = false;
+  int launches = 0;
+
+  ~gs_context() { release(); }
+
+  void release() {
+    cudaSetDevice(device);
+    for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &pixel_grad,
+                       &pixel_out, &ssim_maps, &pair_grads})
+      dev_free(*p);
+    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss}) dev_free(*p);
+    for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
+                         &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
+                         &d_scalars, &sort.hist, &sort.lookback, &sort.ticket, &sort.err, &dens.spawn,
+                         &dens.release, &dens.wants, &dens.free_pos, &dens.spawn_pos, &dens.free_list,
+                         &dens.counters})
+      dev_free(*p);
+    dev_free(ranges);
+    dev_free(d_frames);
+    dev_free(d_view_sums);
+    dev_free(sort.scan_lookback);
+    if (h_frames) cudaFreeHost(h_frames);
+    if (h_scalars) cudaFreeHost(h_scalars);
+    if (h_view_sums) cudaFreeHost(h_view_sums);
+    h_frames = nullptr;
+    h_scalars = nullptr;
+    h_view_sums = nullptr;
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t& e : marks) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
+    if (stream) cudaStreamDestroy(stream);
+    ev0 = ev1 = nullptr;
+    stream = nullptr;
+  }
+
+  void check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(GS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+
+  // (view, slot) buffers for `views` views of `cap` slots.
+  void reserve_views(uint32_t views) {
+    if (views <= vb_views) return;
+    const size_t n = size_t(views) * model.cap;
+    dev_alloc(vb.splat, n * 3);
+    dev_alloc(vb.foot, n);
+    dev_alloc(vb.tiles, n);
+    dev_alloc(vb.offsets, n);
+    dev_alloc(vb.grad2d, n * 3);
+    dev_alloc(dkeys, n);
+    dev_alloc(dvals, n);
+    dev_alloc(dkeys_alt, n);
+    dev_alloc(dvals_alt, n);
+    dev_alloc(sorted_offsets, n);
+    GS_CUDA_TRY(cudaMemsetAsync(vb.tiles, 0, n * sizeof(uint32_t), stream));
+    const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
+    if (sort_tiles > sort.lookback_tiles) {
+      dev_alloc(sort.lookback, size_t(sort_tiles) * 256);
+      sort.lookback_tiles = sort_tiles;
+    }
+    const uint32_t scan_tiles = uint32_t((n + gsk::kScanTile - 1) / gsk::kScanTile);
+    if (scan_tiles > sort.scan_tiles) {
+      dev_alloc(sort.scan_lookback, scan_tiles);
+      sort.scan_tiles = scan_tiles;
+    }
+    vb_views = views;
+  }
+
+  void reserve_pixels(size_t pixels, size_t tiles) {
+    if (pixels > pixel_cap) {
+      dev_alloc(target, pixels);
+      dev_alloc(pixel_grad, pixels);
+      dev_alloc(pixel_out, pixels);
+      dev_alloc(ssim_maps, pixels * 3);
+      dev_alloc(pixel_count, pixels);
+      dev_alloc(image, pixels);
+      dev_alloc(pixel_dot, pixels);
+      pixel_cap = pixels;
+    }
+    if (tiles + 1 > tile_cap) {
+      dev_alloc(ranges, tiles + 1);
+      dev_alloc(tile_loss, (tiles + 1) * 16);
+      dev_alloc(tile_count, tiles + 1);
+      tile_cap = tiles + 1;
+    }
+  }
+
+  void reserve_pairs(uint64_t expected) {
+    const uint64_t wanted = expected + expected / 8;
+    if (wanted <= pair_cap && pair_cap > 0) return;
+    if (expected > kMaxPairs) fail(GS_ERR_CAPACITY, "more tile-gaussian pairs than the pair buffers can hold (" +
+                                                        std::to_string(expected) + ")");
+    const uint64_t n = std::min<uint64_t>(kMaxPairs, std::max<uint64_t>(wanted + wanted / 4, tuning.min_pair_capacity));
+    dev_alloc(keys, n);
+    dev_alloc(values, n);
+    dev_alloc(keys_alt, n);
+    dev_alloc(values_alt, n);
+    dev_alloc(pair_gaussian, n);
+    dev_alloc(pair_grads, n * 3);
+    const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
+    if (sort_tiles > sort.lookback_tiles) {
+      dev_alloc(sort.lookback, size_t(sort_tiles) * 256);
+      sort.lookback_tiles = sort_tiles;
+    }
+    pair_cap = n;
+  }
+
+  void mark(int k) {
+    if (profile) GS_CUDA_TRY(cudaEventRecord(marks[k], stream));
+  }
+
+  void run_step(bool train, gs_step_result* out) {
+    if (n_views == 0) fail(GS_ERR_INVALID, "gs_step: no views (gs_set_views first)");
+    if (train && !has_target) fail(GS_ERR_INVALID, "gs_step: training needs target images");
+    const uint32_t degree = frames[0].model[1];
+    uint32_t retries = 0;
+    for (;;) {
+      const uint64_t guess = max_pairs_seen > 0 ? max_pairs_seen
+                             : tuning.initial_pairs ? tuning.initial_pairs
+                                                    : uint64_t(model.slots) * 4u * n_views;
+      reserve_pairs(guess);
+      for (uint32_t v = 0; v < n_views; ++v) {
+        h_frames[v] = frames[v];
+        h_frames[v].model[0] = model.slots;
+        h_frames[v].model[2] = model.sh_stride;
+        h_frames[v].limits[0] = uint32_t(pair_cap);
+        h_frames[v].limits[3] = uint32_t(pair_cap);
+      }
+      GS_CUDA_TRY(cudaMemcpyAsync(d_frames, h_frames, sizeof(gs_frame_data) * n_views, cudaMemcpyHostToDevice, stream));
+      GS_CUDA_TRY(cudaEventRecord(ev0, stream));
+      launches = 0;
+      record(train, degree);
+      GS_CUDA_TRY(cudaEventRecord(ev1, stream));
+      GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+      GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * 8 * n_views, cudaMemcpyDeviceToHost,
+                                  stream));
+      GS_CUDA_TRY(cudaStreamSynchronize(stream));
+      check_launch("step");
+      uint32_t err = 0;
+      GS_CUDA_TRY(cudaMemcpy(&err, sort.err, sizeof(err), cudaMemcpyDeviceToHost));
+      if (err != 0u) {
+        GS_CUDA_TRY(cudaMemset(sort.err, 0, sizeof(uint32_t)));
+        fail(GS_ERR_TIMEOUT, "a bounded device-side wait (sort/scan look-back) gave up; results discarded");
+      }
+      const uint64_t pairs = h_scalars[0];
+      last_pairs = pairs;
+      max_pairs_seen = std::max(max_pairs_seen, pairs);
+      stepped = true;
+      const bool overflow = pairs > pair_cap;
+      if (overflow && tuning.retry && retries < 4) {
+        ++retries;
+        continue;  // the step left the model alone; grow and run it again
+      }
+      if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->n_views = n_views;
+        out->overflow = overflow ? 1u : 0u;
+        out->retries = retries;
+        out->tile_mismatch = h_scalars[1];
+        // Pairs per view: the emitted offsets are global; per-view counts come from the
+        // per-view tile sums, summed on the host.
+        view_pairs(out->pairs);
+        for (uint32_t v = 0; v < n_views; ++v)
+          for (int k = 0; k < 8; ++k) out->losses[v][k] = h_view_sums[v * 8 + k];
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        out->gpu_ms = ms;
+        out->kernels = uint32_t(launches);
+        if (profile) {
+          for (int k = 0; k < 6; ++k) {
+            float t = 0.f;
+            if (train || k < 4) cudaEventElapsedTime(&t, marks[k], marks[k + 1]);
+            out->pass_ms[k] = t;
+          }
+        }
+      }
+      return;
+    }
+  }
+
+  // Pairs of each view: pairs are ordered by view, so the first pair of view v+1 bounds v.
+  void view_pairs(uint64_t* out) {
+    if (n_views == 1) {
+      out[0] = last_pairs;
+      return;
+    }
+    std::vector<uint2> r(total_tiles + 1);
+    cudaMemcpy(r.data(), ranges, sizeof(uint2) * r.size(), cudaMemcpyDeviceToHost);
+    for (uint32_t v = 0; v < n_views; ++v) {
+      uint64_t lo = UINT64_MAX, hi = 0;
+      for (uint32_t t = vt.tile_base[v]; t < vt.tile_base[v + 1]; ++t)
+        if (r[t].y > r[t].x) {
+          lo = std::min<uint64_t>(lo, r[t].x);
+          hi = std::max<uint64_t>(hi, r[t].y);
+        }
+      out[v] = hi > lo ? hi - lo : 0;
+    }
+  }
+
+  gsk::StepPointers step_pointers() const {
+    gsk::StepPointers sp;
+    sp.frames = d_frames;
+    sp.vt = vt;
+    sp.n_views = n_views;
+    sp.total_tiles = total_tiles;
+    sp.total_pixels = total_pixels;
+    return sp;
+  }
+
+  gsk::RasterBuffers raster_buffers() const {
+    gsk::RasterBuffers rb;
+    rb.ranges = ranges;
+    rb.values = sorted_values;
+    rb.pair_gaussian = pair_gaussian;
+    rb.target = has_target ? target : nullptr;
+    rb.pixel_grad = pixel_grad;
+    rb.pixel_out = pixel_out;
+    rb.pixel_count = pixel_count;
+    rb.image = image;
+    rb.pixel_dot = pixel_dot;
+    rb.tile_loss = tile_loss;
+    rb.tile_count = tile_count;
+    rb.ssim_maps = ssim_maps;
+    return rb;
+  }
+
+  // The launch sequence of one step (trainer.cpp:825-831), all on `stream`.
+  void record(bool train, uint32_t degree) {
+    const gsk::StepPointers sp = step_pointers();
+    const uint32_t items = n_views * model.slots;
+    const bool det = tuning.deterministic != 0u;
+    GS_CUDA_TRY(cudaMemsetAsync(d_scalars, 0, sizeof(uint32_t), stream));  // [0] pairs; [1] mismatches accumulate
+    mark(0);
+    gsk::launch_project(sp, model, degree, vb, dkeys, dvals, train && !det, stream);
+    launches += model.slots ? 1 : 0;
+    mark(1);
+    // Depth sort of every (view, slot): key = view << 16 | depth16.
+    const int depth_bits = 16 + int(bits_for(n_views));
+    const bool in_alt = gsk::radix_sort_pairs(sort, dkeys, dvals, dkeys_alt, dvals_alt, nullptr, items, depth_bits,
+                                              stream, &launches);
+    depth_sorted_keys = in_alt ? dkeys_alt : dkeys;
+    depth_sorted_vals = in_alt ? dvals_alt : dvals;
+    // Offsets of each item's pairs in depth order; the total is the step's pair count.
+    gsk::exclusive_scan(sort, vb.tiles, depth_sorted_vals, sorted_offsets, items, d_scalars, stream, &launches);
+    gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, uint32_t(pair_cap), keys, values,
+                     pair_gaussian, pair_grads, d_scalars + 1, stream);
+    launches += items ? 1 : 0;
+    const int tile_bits = int(bits_for(total_tiles + 1));
+    const bool pairs_alt = gsk::radix_sort_pairs(sort, keys, values, keys_alt, values_alt, d_scalars,
+                                                 uint32_t(pair_cap), std::max(tile_bits, 1), stream, &launches);
+    sorted_keys = pairs_alt ? keys_alt : keys;
+    sorted_values = pairs_alt ? values_alt : values;
+    GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (total_tiles + 1), stream));
+    gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, stream);
+    ++launches;
+    mark(2);
+    const gsk::RasterBuffers rb = raster_buffers();
+    gsk::launch_raster_forward(sp, vb, rb, stream);
+    ++launches;
+    mark(3);
+    const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
+    if (ssim) {
+      gsk::launch_ssim(sp, rb, stream);
+      ++launches;
+      if (train) {
+        gsk::launch_ssim_grad(sp, rb, stream);
+        ++launches;
+      }
+    }
+    gsk::launch_loss_reduce(sp, tile_loss, d_view_sums, stream);
+    ++launches;
+    mark(4);
+    if (train) {
+      const int batch = tuning.raster_batch ? int(tuning.raster_batch) : 32;
+      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, batch, d_scalars, uint32_t(pair_cap), stream);
+      ++launches;
+      mark(5);
+      if (det) {
+        gsk::launch_pair_sum(sp, vb, model.cap, model.slots, pair_grads, d_scalars, uint32_t(pair_cap), stream);
+        ++launches;
+      }
+      gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), stream);
+      ++launches;
+      mark(6);
+    }
+    check_launch("launch");
+  }
+
+  void set_views(uint32_t n, const gs_frame_data* fr, const uint8_t* const* targets) {
+    if (n == 0 || n > GS_MAX_VIEWS) fail(GS_ERR_INVALID, "gs_set_views: 1 to 16 views");
+    if (model.cap == 0) fail(GS_ERR_INVALID, "gs_set_views: no model (gs_model_init first)");
+    frames.assign(fr, fr + n);
+    gsk::ViewTable t{};
+    t.n_views = n;
+    uint64_t tiles = 0, pixels = 0;
+    for (uint32_t v = 0; v < n; ++v) {
+      gs_frame_data& f = frames[v];
+      const uint32_t w = f.image[0], h = f.image[1];
+      if (w == 0 || h == 0) fail(GS_ERR_INVALID, "gs_set_views: empty image");
+      f.image[2] = (w + gsk::kTile - 1) / gsk::kTile;
+      f.image[3] = (h + gsk::kTile - 1) / gsk::kTile;
+      if (f.model[1] > 3u || gsk::sh_rest_coeffs(f.model[1]) * 3u > model.sh_stride)
+        fail(GS_ERR_INVALID, "gs_set_views: active SH degree beyond the model's SH storage");
+      if (v > 0 && f.model[1] != frames[0].model[1])
+        fail(GS_ERR_INVALID, "gs_set_views: the views of a step share the active SH degree");
+      t.tile_base[v] = uint32_t(tiles);
+      t.pixel_base[v] = uint32_t(pixels);
+      tiles += uint64_t(f.image[2]) * f.image[3];
+      pixels += uint64_t(w) * h;
+    }
+    t.tile_base[n] = uint32_t(tiles);
+    t.pixel_base[n] = uint32_t(pixels);
+    if (tiles >= (1ull << 24) || pixels >= (1ull << 31)) fail(GS_ERR_INVALID, "gs_set_views: images too large");
+    for (uint32_t v = n + 1; v <= GS_MAX_VIEWS; ++v) {
+      t.tile_base[v] = t.tile_base[n];
+      t.pixel_base[v] = t.pixel_base[n];
+    }
+    reserve_views(n);
+    reserve_pixels(pixels, tiles);
+    vt = t;
+    n_views = n;
+    total_tiles = uint32_t(tiles);
+    total_pixels = uint32_t(pixels);
+    has_target = targets != nullptr;
+    if (targets) {
+      for (uint32_t v = 0; v < n; ++v) {
+        if (targets[v] == nullptr) fail(GS_ERR_INVALID, "gs_set_views: missing target image");
+        const size_t bytes = size_t(frames[v].image[0]) * frames[v].image[1] * 4;
+        GS_CUDA_TRY(cudaMemcpyAsync(target + t.pixel_base[v], targets[v], bytes, cudaMemcpyHostToDevice, stream));
+      }
+    }
+  }
+};
+
+namespace gsk {
+namespace {
+
+__global__ void k_params_to_planes(const float* __restrict__ params16, const float* __restrict__ sh, uint32_t count,
+                                   uint32_t cap, uint32_t stride, float4* P, float* SH) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float4* p = reinterpret_cast<const float4*>(params16) + size_t(i) * 4u;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) P[size_t(k) * cap + i] = p[k];
+  if (sh != nullptr)
+    for (uint32_t k = 0; k < stride; ++k) SH[size_t(k) * cap + i] = sh[size_t(i) * stride + k];
+}
+
+__global__ void k_planes_to_params(const float4* P, const float* SH, uint32_t count, uint32_t cap, uint32_t stride,
+                                   float* params16, float* sh) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  if (params16 != nullptr) {
+    float4* p = reinterpret_cast<float4*>(params16) + size_t(i) * 4u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[k] = P[size_t(k) * cap + i];
+  }
+  if (sh != nullptr)
+    for (uint32_t k = 0; k < stride; ++k) sh[size_t(i) * stride + k] = SH[size_t(k) * cap + i];
+}
+
+__global__ void k_projected_record(const float4* splat, const float4* foot, uint32_t base, uint32_t slots,
+                                   float4* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slots) return;
+  const size_t g = size_t(base) + i;
+  out[size_t(i) * 4u] = splat[g * 3u];
+  out[size_t(i) * 4u + 1u] = splat[g * 3u + 1u];
+  out[size_t(i) * 4u + 2u] = splat[g * 3u + 2u];
+  out[size_t(i) * 4u + 3u] = foot[g];
+}
+
+}  // namespace
+
+void launch_params_to_planes(const float* params16, const float* sh, uint32_t count, const Model& m, cudaStream_t st) {
+  if (count == 0) return;
+  k_params_to_planes<<<(count + 255u) / 256u, 256, 0, st>>>(params16, sh, count, m.cap, m.sh_stride, m.P, m.SH);
+}
+
+void launch_planes_to_params(const Model& m, const float4* P, const float* SH, float* params16, float* sh,
+                             uint32_t count, cudaStream_t st) {
+  if (count == 0) return;
+  k_planes_to_params<<<(count + 255u) / 256u, 256, 0, st>>>(P, SH, count, m.cap, m.sh_stride, params16, sh);
+}
+
+void launch_projected_record(const ViewBuffers& vb, uint32_t view, uint32_t cap, uint32_t slots, float* out16,
+                             cudaStream_t st) {
+  if (slots == 0) return;
+  k_projected_record<<<(slots + 255u) / 256u, 256, 0, st>>>(vb.splat, vb.foot, view * cap, slots,
+                                                            reinterpret_cast<float4*>(out16));
+}
+
+}  // namespace gsk
+
+namespace {
+
+// Copies `count` items of a device array to host through a temporary device buffer
+// produced by `fill` (layout conversions).
+template <typename T, typename F>
+void download_via(gs_context* c, size_t count, T* host, F fill) {
+  T* tmp = nullptr;
+  dev_alloc(tmp, count);
+  fill(tmp);
+  const cudaError_t e1 = cudaMemcpyAsync(host, tmp, count * sizeof(T), cudaMemcpyDeviceToHost, c->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  dev_free(tmp);
+  GS_CUDA_TRY(e1);
+  GS_CUDA_TRY(e2);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gs_last_error(void) { return g_last_error.c_str(); }
+
+int gs_create(int device, gs_context** out) {
+  return guarded([&] {
+    if (out == nullptr) fail(GS_ERR_INVALID, "gs_create: null output");
+    *out = nullptr;
+    int count = 0;
+    GS_CUDA_TRY(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) fail(GS_ERR_INVALID, "gs_create: no CUDA device " + std::to_string(device));
+    cudaDeviceProp prop{};
+    GS_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+      fail(GS_ERR_INVALID, std::string("gs_create: libgs_cuda is built for sm_100a; device is ") + prop.name);
+    GS_CUDA_TRY(cudaSetDevice(device));
+    gs_context* c = new gs_context();
+    c->device = device;
+    c->tuning.min_pair_capacity = 1u << 16;
+    c->tuning.deterministic = 1u;
+    c->tuning.raster_batch = 32u;
+    c->tuning.sort_digit_bits = 8u;
+    c->tuning.retry = 1u;
+    try {
+      GS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      GS_CUDA_TRY(cudaEventCreate(&c->ev0));
+      GS_CUDA_TRY(cudaEventCreate(&c->ev1));
+      for (cudaEvent_t& e : c->marks) GS_CUDA_TRY(cudaEventCreate(&e));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_frames), sizeof(gs_frame_data) * GS_MAX_VIEWS));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), 4 * sizeof(uint32_t)));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_view_sums), 8 * sizeof(double) * GS_MAX_VIEWS));
+      dev_alloc(c->d_frames, GS_MAX_VIEWS);
+      dev_alloc(c->d_scalars, 4);
+      dev_alloc(c->d_view_sums, 8 * GS_MAX_VIEWS);
+      dev_alloc(c->sort.hist, 4 * 256);
+      dev_alloc(c->sort.ticket, 1);
+      dev_alloc(c->sort.err, 1);
+      GS_CUDA_TRY(cudaMemset(c->d_scalars, 0, 4 * sizeof(uint32_t)));
+      GS_CUDA_TRY(cudaMemset(c->sort.err, 0, sizeof(uint32_t)));
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+int gs_destroy(gs_context* ctx) {
+  return guarded([&] { delete ctx; });
+}
+
+int gs_model_init(gs_context* c, uint32_t capacity, uint32_t sh_stride, const float* params16, const float* sh,
+                  uint32_t count) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_model_init: null context");
+    if (capacity == 0 || count > capacity) fail(GS_ERR_INVALID, "gs_model_init: count must be within 1..capacity");
+    if (sh_stride % 3u != 0u || sh_stride > 45u) fail(GS_ERR_INVALID, "gs_model_init: sh_stride must be 0, 9, 24 or 45");
+    if (count > 0 && params16 == nullptr) fail(GS_ERR_INVALID, "gs_model_init: null params");
+    if (count > 0 && sh_stride > 0 && sh == nullptr) fail(GS_ERR_INVALID, "gs_model_init: null sh");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    gsk::Model& m = c->model;
+    dev_free(m.P);
+    dev_free(m.M);
+    dev_free(m.V);
+    dev_free(m.stats);
+    dev_free(m.SH);
+    dev_free(m.MSH);
+    dev_free(m.VSH);
+    c->vb_views = 0;
+    m.cap = capacity;
+    m.slots = count;
+    m.sh_stride = sh_stride;
+    dev_alloc(m.P, size_t(capacity) * 4);
+    dev_alloc(m.M, size_t(capacity) * 4);
+    dev_alloc(m.V, size_t(capacity) * 4);
+    dev_alloc(m.stats, capacity);
+    dev_alloc(m.SH, size_t(capacity) * sh_stride);
+    dev_alloc(m.MSH, size_t(capacity) * sh_stride);
+    dev_alloc(m.VSH, size_t(capacity) * sh_stride);
+    for (float4* p : {m.P, m.M, m.V}) GS_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(float4) * 4 * capacity, c->stream));
+    GS_CUDA_TRY(cudaMemsetAsync(m.stats, 0, sizeof(float4) * capacity, c->stream));
+    for (float* p : {m.SH, m.MSH, m.VSH})
+      GS_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(float) * std::max<size_t>(1, size_t(capacity) * sh_stride), c->stream));
+    dev_alloc(c->dens.spawn, capacity);
+    dev_alloc(c->dens.release, capacity);
+    dev_alloc(c->dens.wants, capacity);
+    dev_alloc(c->dens.free_pos, capacity);
+    dev_alloc(c->dens.spawn_pos, capacity);
+    dev_alloc(c->dens.free_list, capacity);
+    dev_alloc(c->dens.counters, 4);
+    const uint32_t scan_tiles = (capacity + gsk::kScanTile - 1) / gsk::kScanTile;
+    if (scan_tiles > c->sort.scan_tiles) {
+      dev_alloc(c->sort.scan_lookback, scan_tiles);
+      c->sort.scan_tiles = scan_tiles;
+    }
+    if (count > 0) {
+      float* d_params = nullptr;
+      float* d_sh = nullptr;
+      dev_alloc(d_params, size_t(count) * 16);
+      GS_CUDA_TRY(cudaMemcpyAsync(d_params, params16, sizeof(float) * 16 * count, cudaMemcpyHostToDevice, c->stream));
+      if (sh_stride > 0) {
+        dev_alloc(d_sh, size_t(count) * sh_stride);
+        GS_CUDA_TRY(cudaMemcpyAsync(d_sh, sh, sizeof(float) * sh_stride * count, cudaMemcpyHostToDevice, c->stream));
+      }
+      gsk::launch_params_to_planes(d_params, d_sh, count, m, c->stream);
+      GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      dev_free(d_params);
+      dev_free(d_sh);
+    }
+    c->max_pairs_seen = 0;
+    c->stepped = false;
+    c->check_launch("gs_model_init");
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int gs_model_info_get(gs_context* c, gs_model_info* out) {
+  return guarded([&] {
+    if (c == nullptr || out == nullptr) fail(GS_ERR_INVALID, "gs_model_info_get: null argument");
+    out->capacity = c->model.cap;
+    out->slots = c->model.slots;
+    out->sh_stride = c->model.sh_stride;
+    out->pair_capacity = c->pair_cap;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    out->device_bytes = total_b - free_b;
+  });
+}
+
+int gs_model_export(gs_context* c, float* params16, float* sh, uint32_t max_slots, uint32_t* slots) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_model_export: null context");
+    if (slots) *slots = c->model.slots;
+    const uint32_t n = std::min(max_slots, c->model.slots);
+    if (n == 0) return;
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    if (params16)
+      download_via<float>(c, size_t(n) * 16, params16, [&](float* tmp) {
+        gsk::launch_planes_to_params(c->model, c->model.P, c->model.SH, tmp, nullptr, n, c->stream);
+      });
+    if (sh && c->model.sh_stride)
+      download_via<float>(c, size_t(n) * c->model.sh_stride, sh, [&](float* tmp) {
+        gsk::launch_planes_to_params(c->model, c->model.P, c->model.SH, nullptr, tmp, n, c->stream);
+      });
+  });
+}
+
+int gs_model_moments(gs_context* c, float* m16, float* v16, float* m_sh, float* v_sh) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_model_moments: null context");
+    const uint32_t n = c->model.slots;
+    if (n == 0) return;
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    const gsk::Model& m = c->model;
+    if (m16)
+      download_via<float>(c, size_t(n) * 16, m16,
+                          [&](float* t) { gsk::launch_planes_to_params(m, m.M, m.MSH, t, nullptr, n, c->stream); });
+    if (v16)
+      download_via<float>(c, size_t(n) * 16, v16,
+                          [&](float* t) { gsk::launch_planes_to_params(m, m.V, m.VSH, t, nullptr, n, c->stream); });
+    if (m_sh && m.sh_stride)
+      download_via<float>(c, size_t(n) * m.sh_stride, m_sh,
+                          [&](float* t) { gsk::launch_planes_to_params(m, m.M, m.MSH, nullptr, t, n, c->stream); });
+    if (v_sh && m.sh_stride)
+      download_via<float>(c, size_t(n) * m.sh_stride, v_sh,
+                          [&](float* t) { gsk::launch_planes_to_params(m, m.V, m.VSH, nullptr, t, n, c->stream); });
+  });
+}
+
+int gs_set_views(gs_context* c, uint32_t n_views, const gs_frame_data* frames, const uint8_t* const* rgba_targets) {
+  return guarded([&] {
+    if (c == nullptr || frames == nullptr) fail(GS_ERR_INVALID, "gs_set_views: null argument");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    c->set_views(n_views, frames, rgba_targets);
+  });
+}
+
+int gs_step(gs_context* c, uint32_t flags, gs_step_result* out) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_step: null context");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    c->profile = (flags & GS_STEP_PROFILE) != 0u;
+    c->run_step((flags & GS_STEP_TRAIN) != 0u, out);
+    c->profile = false;
+  });
+}
+
+int gs_render(gs_context* c, const gs_frame_data* frame, uint8_t* rgba_out) {
+  return guarded([&] {
+    if (c == nullptr || frame == nullptr || rgba_out == nullptr) fail(GS_ERR_INVALID, "gs_render: null argument");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    gs_frame_data f = *frame;
+    f.model[3] &= ~GS_FLAG_SSIM;
+    c->set_views(1, &f, nullptr);
+    c->profile = false;
+    c->run_step(false, nullptr);
+    GS_CUDA_TRY(cudaMemcpy(rgba_out, c->image, size_t(f.image[0]) * f.image[1] * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+int gs_densify(gs_context* c, const gs_frame_data* frame, uint32_t counters_out[4]) {
+  return guarded([&] {
+    if (c == nullptr || frame == nullptr) fail(GS_ERR_INVALID, "gs_densify: null argument");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    gs_frame_data f = *frame;
+    f.model[0] = c->model.slots;
+    f.model[2] = c->model.sh_stride;
+    *c->h_frames = f;
+    GS_CUDA_TRY(cudaMemcpyAsync(c->d_frames, c->h_frames, sizeof(gs_frame_data), cudaMemcpyHostToDevice, c->stream));
+    int launches = 0;
+    gsk::launch_densify(c->d_frames, c->model, c->dens, c->sort, c->stream, &launches);
+    uint32_t counters[4] = {0, 0, 0, 0};
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    GS_CUDA_TRY(cudaMemcpy(counters, c->dens.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    c->check_launch("gs_densify");
+    const uint32_t free_slots = counters[0], spawned = counters[1];
+    const uint32_t room = free_slots + (c->model.cap - c->model.slots);
+    const uint32_t placed = std::min(spawned, room);
+    if (placed > free_slots) c->model.slots += placed - free_slots;
+    counters[3] = c->model.slots;
+    if (counters_out) std::memcpy(counters_out, counters, sizeof(counters));
+  });
+}
+
+int gs_reset_opacity(gs_context* c, float max_logit) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_reset_opacity: null context");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    gsk::launch_reset_opacity(c->model, max_logit, c->stream);
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->check_launch("gs_reset_opacity");
+  });
+}
+
+int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host, size_t bytes, size_t* needed) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_snapshot: null context");
+    if (which != GS_SNAP_SPAWN && which != GS_SNAP_STATS && (!c->stepped || view >= c->n_views))
+      fail(GS_ERR_INVALID, "gs_snapshot: no such view in the latest step");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const gs_frame_data f = view < c->frames.size() ? c->frames[view] : gs_frame_data{};
+    const size_t pixels = size_t(f.image[0]) * f.image[1];
+    const size_t tiles = size_t(f.image[2]) * f.image[3];
+    const uint32_t slots = c->model.slots, cap = c->model.cap;
+    const uint64_t pairs = std::min<uint64_t>(c->last_pairs, c->pair_cap);
+    const size_t pb = c->vt.pixel_base[view], tb = c->vt.tile_base[view];
+    size_t size = 0;
+    switch (which) {
+      case GS_SNAP_PIXEL_COUNT: case GS_SNAP_IMAGE: case GS_SNAP_PIXEL_DOT: size = pixels * 4; break;
+      case GS_SNAP_PIXEL_GRAD: case GS_SNAP_PIXEL_OUT: size = pixels * 16; break;
+      case GS_SNAP_SPAWN: size = size_t(slots) * 4; break;
+      case GS_SNAP_PROJECTED: size = size_t(slots) * 64; break;
+      case GS_SNAP_TILES: case GS_SNAP_OFFSETS: case GS_SNAP_DEPTH_KEY: size = size_t(slots) * 4; break;
+      case GS_SNAP_STATS: size = size_t(slots) * 16; break;
+      case GS_SNAP_PAIR_GRADS: size = size_t(pairs) * 48; break;
+      case GS_SNAP_PAIR_TILE: case GS_SNAP_RENDER_ORDER: case GS_SNAP_PAIR_GAUSSIAN: size = size_t(pairs) * 4; break;
+      case GS_SNAP_RANGES: size = tiles * 8; break;
+      case GS_SNAP_TILE_LOSS: size = tiles * 64; break;
+      default: fail(GS_ERR_INVALID, "gs_snapshot: unknown buffer");
+    }
+    if (needed) *needed = size;
+    if (host == nullptr) return;
+    if (bytes < size) fail(GS_ERR_INVALID, "gs_snapshot: buffer too small");
+    auto d2h = [&](void* dst, const void* src, size_t n) {
+      if (n) GS_CUDA_TRY(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+    };
+    switch (which) {
+      case GS_SNAP_PIXEL_COUNT: d2h(host, c->pixel_count + pb, size); break;
+      case GS_SNAP_IMAGE: d2h(host, c->image + pb, size); break;
+      case GS_SNAP_PIXEL_DOT: d2h(host, c->pixel_dot + pb, size); break;
+      case GS_SNAP_PIXEL_GRAD: d2h(host, c->pixel_grad + pb, size); break;
+      case GS_SNAP_PIXEL_OUT: d2h(host, c->pixel_out + pb, size); break;
+      case GS_SNAP_SPAWN: d2h(host, c->dens.spawn, size); break;
+      case GS_SNAP_TILES: d2h(host, c->vb.tiles + size_t(view) * cap, size); break;
+      case GS_SNAP_OFFSETS: d2h(host, c->vb.offsets + size_t(view) * cap, size); break;
+      case GS_SNAP_STATS: d2h(host, c->model.stats, size); break;
+      case GS_SNAP_TILE_LOSS: d2h(host, c->tile_loss + tb * 16, size); break;
+      case GS_SNAP_PAIR_GRADS: d2h(host, c->pair_grads, size); break;
+      case GS_SNAP_PAIR_GAUSSIAN: {
+        std::vector<uint32_t> g(pairs);
+        d2h(g.data(), c->pair_gaussian, pairs * 4);
+        for (auto& x : g) x -= view * cap;  // slots of this view
+        std::memcpy(host, g.data(), size);
+        break;
+      }
+      case GS_SNAP_PROJECTED:
+        download_via<float>(c, size_t(slots) * 16, static_cast<float*>(host), [&](float* tmp) {
+          gsk::launch_projected_record(c->vb, view, cap, slots, tmp, c->stream);
+        });
+        break;
+      case GS_SNAP_RANGES: {
+        std::vector<uint2> r(tiles);
+        d2h(r.data(), c->ranges + tb, tiles * 8);
+        // View-local positions: the view's pairs start at its first non-empty tile.
+        uint32_t first = UINT32_MAX;
+        for (const uint2& x : r)
+          if (x.y > x.x) first = std::min(first, x.x);
+        for (uint2& x : r) {
+          if (x.y > x.x) {
+            x.x -= first;
+            x.y -= first;
+          } else {
+            x = make_uint2(0u, 0u);
+          }
+        }
+        std::memcpy(host, r.data(), size);
+        break;
+      }
+      case GS_SNAP_PAIR_TILE: case GS_SNAP_RENDER_ORDER: {
+        std::vector<uint32_t> k(pairs), v(pairs);
+        d2h(k.data(), c->sorted_keys, pairs * 4);
+        d2h(v.data(), c->sorted_values, pairs * 4);
+        uint32_t* o = static_cast<uint32_t*>(host);
+        if (which == GS_SNAP_RENDER_ORDER) {
+          std::memcpy(o, v.data(), size);
+        } else {
+          for (uint64_t p = 0; p < pairs; ++p) o[p] = ~0u;
+          for (uint64_t s = 0; s < pairs; ++s)
+            if (v[s] < pairs) o[v[s]] = k[s] - uint32_t(tb);
+        }
+        break;
+      }
+      case GS_SNAP_DEPTH_KEY: {
+        const size_t n = size_t(c->n_views) * slots;
+        std::vector<uint32_t> k(n), v(n);
+        d2h(k.data(), c->depth_sorted_keys, n * 4);
+        d2h(v.data(), c->depth_sorted_vals, n * 4);
+        uint32_t* o = static_cast<uint32_t*>(host);
+        for (uint32_t i = 0; i < slots; ++i) o[i] = ~0u;
+        for (size_t e = 0; e < n; ++e)
+          if (v[e] / cap == view && v[e] % cap < slots) o[v[e] % cap] = k[e] & 0xffffu;
+        break;
+      }
+      default: break;
+    }
+  });
+}
+
+int gs_set_tuning(gs_context* c, const gs_tuning* t) {
+  return guarded([&] {
+    if (c == nullptr || t == nullptr) fail(GS_ERR_INVALID, "gs_set_tuning: null argument");
+    if (t->raster_batch != 0 && t->raster_batch != 32 && t->raster_batch != 64)
+      fail(GS_ERR_INVALID, "gs_set_tuning: raster_batch must be 32 or 64");
+    if (t->sort_digit_bits != 0 && t->sort_digit_bits != 8)
+      fail(GS_ERR_INVALID, "gs_set_tuning: sort_digit_bits must be 8");
+    c->tuning = *t;
+    if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
+  });
+}
+
+int gs_get_tuning(gs_context* c, gs_tuning* t) {
+  return guarded([&] {
+    if (c == nullptr || t == nullptr) fail(GS_ERR_INVALID, "gs_get_tuning: null argument");
+    *t = c->tuning;
+  });
+}
+
+}  // extern "C"

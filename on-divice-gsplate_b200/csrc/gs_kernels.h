@@ -1,0 +1,126 @@
+// Host-side launchers of the training-step kernels (internal to libgs_cuda).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gs_common.cuh"
+
+namespace gsk {
+
+// ---- model layout in HBM ----
+// Parameters: 4 float4 planes of `cap` slots (P[plane * cap + slot]): position + opacity
+// logit, log scale + alive flag, quaternion (w, x, y, z), SH DC + 0 — the reference's
+// 4 x vec4 per slot (train_common.glsl:3-8) split into planes so every access is a
+// coalesced 16-byte load. SH beyond DC: `sh_stride` float planes (SH[f * cap + slot],
+// f = coeff * 3 + channel). Adam moments mirror both layouts.
+struct Model {
+  uint32_t cap = 0, slots = 0, sh_stride = 0;
+  float4* P = nullptr;
+  float4* M = nullptr;
+  float4* V = nullptr;
+  float* SH = nullptr;
+  float* MSH = nullptr;
+  float* VSH = nullptr;
+  float4* stats = nullptr;  // grad norm sum, visible count, max radius, abs grad sum
+};
+
+// Per (view, slot) buffers: index g = view * cap + slot.
+struct ViewBuffers {
+  float4* splat = nullptr;   // 3 per g: (mean xy, depth, opacity), (conic abc, radius), (rgb, clamp bits)
+  float4* foot = nullptr;    // 1 per g: dilated 2D covariance abc, footprint threshold
+  uint32_t* tiles = nullptr; // tiles touched
+  uint32_t* offsets = nullptr;  // first pair, pre-sort order
+  float4* grad2d = nullptr;  // 3 per g: summed pair gradients (train_pair_sum layout)
+};
+
+struct StepPointers {
+  const gs_frame_data* frames = nullptr;  // device copy, n_views entries
+  ViewTable vt{};
+  uint32_t n_views = 0, total_tiles = 0, total_pixels = 0;
+};
+
+// ---- project.cu ----
+void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                    uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, cudaStream_t st);
+
+// ---- sort.cu ----
+struct SortScratch {
+  uint32_t* hist = nullptr;           // 4 passes x 256
+  uint32_t* lookback = nullptr;       // tiles x 256 status words
+  uint32_t lookback_tiles = 0;
+  unsigned long long* scan_lookback = nullptr;
+  uint32_t scan_tiles = 0;
+  uint32_t* ticket = nullptr;         // 1 word
+  uint32_t* err = nullptr;            // 1 word: a bounded wait gave up
+};
+constexpr uint32_t kSortTile = 256 * 15;
+constexpr uint32_t kScanTile = 256 * 8;
+// Sorts (keys, vals) of min(*d_count, n_max) items by key bits [0, bits), stable. Returns
+// true when the result ended in the alternate buffers.
+bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches);
+// Exclusive scan of in[gather ? gather[k] : k] for k < n; *d_total (if non-null) = the sum.
+void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* gather, uint32_t* out, uint32_t n,
+                    uint32_t* d_total, cudaStream_t st, int* launches);
+
+// ---- pairs.cu ----
+void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
+                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, uint32_t pair_capacity, uint32_t* keys,
+                 uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads, uint32_t* mismatch, cudaStream_t st);
+void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
+                   cudaStream_t st);
+
+// ---- raster.cu ----
+struct RasterBuffers {
+  const uint2* ranges = nullptr;
+  const uint32_t* values = nullptr;         // pre-sort pair index per sorted pair
+  const uint32_t* pair_gaussian = nullptr;  // g per pre-sort pair
+  const uint32_t* target = nullptr;         // RGBA8 per global pixel (nullptr: no loss)
+  float4* pixel_grad = nullptr;             // dL/dC rgb, final T
+  float4* pixel_out = nullptr;              // rendered colour rgb (over the background), loss weight
+  uint32_t* pixel_count = nullptr;
+  uint32_t* image = nullptr;
+  float* pixel_dot = nullptr;
+  float* tile_loss = nullptr;               // 16 per global tile
+  uint32_t* tile_count = nullptr;
+  float4* ssim_maps = nullptr;              // 3 per pixel
+};
+void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, cudaStream_t st);
+// Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
+// vb.grad2d (fast). Skipped on device when *d_pairs > accept.
+void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
+                            float4* pair_grads, bool deterministic, int batch, const uint32_t* d_pairs,
+                            uint32_t accept, cudaStream_t st);
+
+// ---- loss.cu ----
+void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
+void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
+void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, cudaStream_t st);
+
+// ---- step.cu ----
+void launch_pair_sum(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t slots,
+                     const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
+void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                 const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
+struct DensifyScratch {
+  uint32_t* spawn = nullptr;     // action per slot
+  uint32_t* release = nullptr;   // 1 per freed slot
+  uint32_t* wants = nullptr;     // 1 per spawning slot
+  uint32_t* free_pos = nullptr;  // exclusive scans
+  uint32_t* spawn_pos = nullptr;
+  uint32_t* free_list = nullptr;
+  uint32_t* counters = nullptr;  // [0] free, [1] spawned, [2] pruned
+};
+void launch_densify(const gs_frame_data* d_frame, const Model& m, const DensifyScratch& ds, const SortScratch& ss,
+                    cudaStream_t st, int* launches);
+void launch_reset_opacity(const Model& m, float max_logit, cudaStream_t st);
+
+// ---- layout conversions (api.cu) ----
+void launch_params_to_planes(const float* params16, const float* sh, uint32_t count, const Model& m, cudaStream_t st);
+void launch_planes_to_params(const Model& m, const float4* P, const float* SH, float* params16, float* sh,
+                             uint32_t count, cudaStream_t st);
+void launch_projected_record(const ViewBuffers& vb, uint32_t view, uint32_t cap, uint32_t slots, float* out16,
+                             cudaStream_t st);
+
+}  // namespace gsk

@@ -1,0 +1,113 @@
+// Pair emission and tile ranges.
+//
+// launch_emit: train_emit.comp:26-64. Items come in depth order (the depth sort of every
+// (view, slot)); each writes its (tile, gaussian) pairs at its scanned offset, walking
+// the same footprint rows train_project counted (train_common.glsl:185-213) from the
+// stored records. The pair key is the global tile (view tile base + tile), so one stable
+// sort by key leaves every tile's pairs front to back, ties in slot order — the order a
+// (tile, depth16, index) sort gives (test_trainer.cpp:197-233).
+// launch_ranges: train_ranges.comp:14-29 over the sorted keys.
+#include "gs_kernels.h"
+
+namespace gsk {
+namespace {
+
+struct EmitArgs {
+  const gs_frame_data* frames;
+  ViewTable vt;
+  uint32_t cap, n_items, pair_capacity, pad_tile;
+  const uint32_t* sorted_vals;
+  const uint32_t* sorted_offsets;
+  const float4* splat;
+  const float4* foot;
+  const uint32_t* tiles;
+  uint32_t* offsets;
+  uint32_t* keys;
+  uint32_t* values;
+  uint32_t* pair_gaussian;
+  float4* pair_grads;
+  uint32_t* mismatch;
+};
+
+__global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n_items) return;
+  const uint32_t g = a.sorted_vals[k];
+  const uint32_t count = a.tiles[g];
+  if (count == 0u) return;
+  const uint32_t v = g / a.cap;
+  const gs_frame_data& f = a.frames[v];
+  const float4 q0 = a.splat[size_t(g) * 3u];
+  const float4 fp = a.foot[g];
+  uint32_t p = a.sorted_offsets[k];
+  a.offsets[g] = p;
+  const uint32_t end = min(p + count, a.pair_capacity);
+  const uint32_t tile_base = a.vt.tile_base[v];
+  const uint32_t width = f.image[0], height = f.image[1], tiles_x = f.image[2];
+  uint32_t wanted = 0u;
+  const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
+  if (rows.x <= rows.y) {
+    for (uint32_t ty = uint32_t(rows.x) / kTile; ty <= uint32_t(rows.y) / kTile; ++ty) {
+      const uint2 span = footprint_row_tiles(q0.x, q0.y, fp.x, fp.y, fp.z, fp.w, rows, ty, width);
+      wanted += span.y - span.x;
+      for (uint32_t x = span.x; x < span.y && p < end; ++x) {
+        a.keys[p] = tile_base + ty * tiles_x + x;
+        a.values[p] = p;
+        a.pair_gaussian[p] = g;
+        ++p;
+      }
+    }
+  }
+  if (wanted == count) return;
+  // The count and the walk disagree (never expected: same inputs, same arithmetic).
+  // Pad the rest into the unused tile after the last one, with zero gradient.
+  atomicAdd(a.mismatch, 1u);
+  for (; p < end; ++p) {
+    a.keys[p] = a.pad_tile;
+    a.values[p] = p;
+    a.pair_gaussian[p] = g;
+    if (a.pair_grads != nullptr) {
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      a.pair_grads[size_t(p) * 3u] = z;
+      a.pair_grads[size_t(p) * 3u + 1u] = z;
+      a.pair_grads[size_t(p) * 3u + 2u] = z;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count,
+                                                uint32_t capacity, uint2* __restrict__ ranges) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t count = min(*d_count, capacity);
+  if (s >= count) return;
+  const uint32_t tile = keys[s];
+  if (s == 0u) {
+    ranges[tile].x = 0u;
+  } else {
+    const uint32_t prev = keys[s - 1u];
+    if (prev != tile) {
+      ranges[prev].y = s;
+      ranges[tile].x = s;
+    }
+  }
+  if (s == count - 1u) ranges[tile].y = count;
+}
+
+}  // namespace
+
+void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
+                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, uint32_t pair_capacity, uint32_t* keys,
+                 uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads, uint32_t* mismatch, cudaStream_t st) {
+  if (n_items == 0u) return;
+  EmitArgs a{sp.frames, sp.vt, cap, n_items, pair_capacity, sp.total_tiles, sorted_vals, sorted_offsets,
+             vb.splat, vb.foot, vb.tiles, vb.offsets, keys, values, pair_gaussian, pair_grads, mismatch};
+  k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
+}
+
+void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
+                   cudaStream_t st) {
+  if (pair_capacity == 0u) return;
+  k_ranges<<<(pair_capacity + 255u) / 256u, 256, 0, st>>>(sorted_keys, d_count, pair_capacity, ranges);
+}
+
+}  // namespace gsk

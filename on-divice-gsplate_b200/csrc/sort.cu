@@ -1,0 +1,315 @@
+// Device radix sort and exclusive scan.
+//
+// The reference sorts with a 3-kernel LSD radix sort of 4-bit digits (count, single
+// workgroup scan, scatter: engine/src/radix_sort.cpp:57-108, radix_{count,scan,scatter}.comp)
+// and scans with scan_local/blocks/add. Here:
+//  - radix_sort_pairs: onesweep LSD sort, 8-bit digits. One kernel computes every pass's
+//    digit histogram; each pass is then one kernel in which a block ranks its 3840 keys
+//    (warp match + per-warp counters, stable), publishes its digit counts and looks back
+//    over its predecessors' (decoupled look-back) for its global digit offsets, then
+//    scatters through shared memory so each digit run is written contiguously.
+//  - exclusive_scan: single-pass scan with decoupled look-back.
+// Blocks take their tile from an atomic ticket, so every predecessor a block waits on is
+// already running; each wait is still bounded (kSpinLimit polls), after which the block
+// records an error word the host turns into GS_ERR_TIMEOUT, and carries on.
+#include <cuda/atomic>
+
+#include "gs_kernels.h"
+
+namespace gsk {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kIpt = 15;  // keys per thread
+constexpr int kRadix = 256;
+constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint32_t kAgg = 1u << 30, kPrefix = 2u << 30, kValueMask = (1u << 30) - 1u;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  return cuda::atomic_ref<const uint32_t, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+  cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+  return cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_relaxed);
+}
+
+__device__ __forceinline__ uint32_t count_of(const uint32_t* d_count, uint32_t n_max) {
+  return d_count != nullptr ? min(*d_count, n_max) : n_max;
+}
+
+// Exclusive scan of one value per thread over a 256-thread block; returns the block total.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  T warp_prefix = 0, sum = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const T t = s_warp[w];
+    if (w < warp) warp_prefix += t;
+    sum += t;
+  }
+  __syncthreads();
+  total = sum;
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kThreads) k_histogram(const uint32_t* __restrict__ keys, const uint32_t* d_count,
+                                                        uint32_t n_max, int passes, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[4][kRadix];
+  for (int k = threadIdx.x; k < 4 * kRadix; k += kThreads) (&s_hist[0][0])[k] = 0u;
+  __syncthreads();
+  const uint32_t n = count_of(d_count, n_max);
+  for (uint32_t idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
+    const uint32_t key = keys[idx];
+    for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(key >> (8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < passes * kRadix; k += kThreads) {
+    const uint32_t c = (&s_hist[0][0])[k];
+    if (c) atomicAdd(&hist[k], c);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_histogram_scan(uint32_t* hist, int passes) {
+  __shared__ uint32_t s_warp[kWarps];
+  for (int p = 0; p < passes; ++p) {
+    uint32_t total;
+    const uint32_t v = hist[p * kRadix + threadIdx.x];
+    const uint32_t ex = block_exclusive_scan<uint32_t>(v, s_warp, total);
+    hist[p * kRadix + threadIdx.x] = ex;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
+                                                       const uint32_t* __restrict__ vals_in,
+                                                       uint32_t* __restrict__ keys_out,
+                                                       uint32_t* __restrict__ vals_out, const uint32_t* d_count,
+                                                       uint32_t n_max, int shift, uint32_t mask,
+                                                       const uint32_t* __restrict__ pass_offsets, uint32_t* lookback,
+                                                       uint32_t* ticket, uint32_t* err) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_wc[kWarps][kRadix];  // per-warp digit counts, then per-warp exclusive offsets
+  __shared__ uint32_t s_dstart[kRadix];      // block-local start of each digit
+  __shared__ uint32_t s_gbase[kRadix];       // global position of each digit's first key of this block
+  __shared__ uint32_t s_warp[kWarps];
+  __shared__ uint32_t s_keys[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = tid; k < kWarps * kRadix; k += kThreads) (&s_wc[0][0])[k] = 0u;
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t n = count_of(d_count, n_max);
+  const uint32_t base = tile * kSortTile;
+  if (base >= n) return;  // every later tile is empty too: nobody waits on this one
+
+  uint32_t key[kIpt], val[kIpt];
+  uint16_t rank[kIpt];
+  const uint32_t wbase = base + uint32_t(warp) * 32u * kIpt;
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
+    if (idx < n) {
+      key[j] = keys_in[idx];
+      val[j] = vals_in[idx];
+    } else {
+      key[j] = 0xffffffffu;
+      val[j] = 0u;
+    }
+  }
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
+    const bool valid = idx < n;
+    const uint32_t digit = valid ? (key[j] >> shift) & mask : uint32_t(kRadix);
+    const uint32_t peers = __match_any_sync(0xffffffffu, digit);
+    uint32_t before = 0u;
+    if (valid) before = s_wc[warp][digit];
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) s_wc[warp][digit] = before + __popc(peers);
+    __syncwarp();
+    rank[j] = uint16_t(before + __popc(peers & lanemask_lt));
+  }
+  __syncthreads();
+
+  // Digit `tid`: per-warp exclusive offsets, block count, block-local start.
+  uint32_t count = 0u;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const uint32_t c = s_wc[w][tid];
+    s_wc[w][tid] = count;
+    count += c;
+  }
+  uint32_t block_total;
+  s_dstart[tid] = block_exclusive_scan<uint32_t>(count, s_warp, block_total);
+
+  // Decoupled look-back on digit `tid`.
+  uint32_t prefix = 0u;
+  if (tile == 0u) {
+    st_relaxed(&lookback[tid], kPrefix | count);
+  } else {
+    st_relaxed(&lookback[size_t(tile) * kRadix + tid], kAgg | count);
+    uint32_t j = tile - 1u, spins = 0u;
+    for (;;) {
+      const uint32_t w = ld_relaxed(&lookback[size_t(j) * kRadix + tid]);
+      const uint32_t status = w & ~kValueMask;
+      if (status == 0u) {
+        if (++spins > kSpinLimit) {
+          atomicExch(err, 1u);
+          break;
+        }
+        if (spins > 64u) __nanosleep(64);
+        continue;
+      }
+      prefix += w & kValueMask;
+      if (status == kPrefix || j == 0u) break;
+      --j;
+    }
+    st_relaxed(&lookback[size_t(tile) * kRadix + tid], kPrefix | ((prefix + count) & kValueMask));
+  }
+  s_gbase[tid] = pass_offsets[tid] + prefix;
+  __syncthreads();
+
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
+    if (idx < n) {
+      const uint32_t d = (key[j] >> shift) & mask;
+      const uint32_t pos = s_dstart[d] + s_wc[warp][d] + rank[j];
+      s_keys[pos] = key[j];
+      s_vals[pos] = val[j];
+    }
+  }
+  __syncthreads();
+  const uint32_t tile_n = min(kSortTile, n - base);
+  for (uint32_t p = tid; p < tile_n; p += kThreads) {
+    const uint32_t k = s_keys[p];
+    const uint32_t d = (k >> shift) & mask;
+    const uint32_t out = s_gbase[d] + (p - s_dstart[d]);
+    keys_out[out] = k;
+    vals_out[out] = s_vals[p];
+  }
+}
+
+constexpr int kScanIpt = 8;
+
+__global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, const uint32_t* __restrict__ gather,
+                                                   uint32_t* __restrict__ out, uint32_t n, uint32_t* d_total,
+                                                   unsigned long long* lookback, uint32_t* ticket, uint32_t* err) {
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_warp[kWarps];
+  __shared__ unsigned long long s_prefix;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t base = tile * kScanTile;
+  if (base >= n) return;
+  uint32_t x[kScanIpt];
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int j = 0; j < kScanIpt; ++j) {
+    const uint32_t idx = base + uint32_t(tid) * kScanIpt + j;
+    x[j] = idx < n ? in[gather != nullptr ? gather[idx] : idx] : 0u;
+    sum += x[j];
+  }
+  unsigned long long block_total;
+  const unsigned long long ex = block_exclusive_scan<unsigned long long>(sum, s_warp, block_total);
+  constexpr unsigned long long kA = 1ull << 62, kP = 2ull << 62, kM = (1ull << 62) - 1ull;
+  if (tid == 0) {
+    unsigned long long prefix = 0;
+    if (tile == 0u) {
+      st_relaxed64(&lookback[0], kP | block_total);
+    } else {
+      st_relaxed64(&lookback[tile], kA | block_total);
+      uint32_t j = tile - 1u, spins = 0u;
+      for (;;) {
+        const unsigned long long w = ld_relaxed64(&lookback[j]);
+        const unsigned long long status = w & ~kM;
+        if (status == 0ull) {
+          if (++spins > kSpinLimit) {
+            atomicExch(err, 1u);
+            break;
+          }
+          if (spins > 64u) __nanosleep(64);
+          continue;
+        }
+        prefix += w & kM;
+        if (status == kP || j == 0u) break;
+        --j;
+      }
+      st_relaxed64(&lookback[tile], kP | ((prefix + block_total) & kM));
+    }
+    s_prefix = prefix;
+    if (d_total != nullptr && base + kScanTile >= n) *d_total = uint32_t(prefix + block_total);
+  }
+  __syncthreads();
+  unsigned long long run = s_prefix + ex;
+#pragma unroll
+  for (int j = 0; j < kScanIpt; ++j) {
+    const uint32_t idx = base + uint32_t(tid) * kScanIpt + j;
+    if (idx < n) out[idx] = uint32_t(run);
+    run += x[j];
+  }
+}
+
+}  // namespace
+
+bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches) {
+  if (n_max <= 1u || bits <= 0) return false;
+  const int passes = (bits + 7) / 8;
+  const uint32_t tiles = (n_max + kSortTile - 1u) / kSortTile;
+  cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 4 * kRadix, st);
+  const uint32_t hist_blocks = min((n_max + kThreads - 1u) / kThreads, 148u * 8u);
+  k_histogram<<<hist_blocks, kThreads, 0, st>>>(keys, d_count, n_max, passes, s.hist);
+  k_histogram_scan<<<1, kThreads, 0, st>>>(s.hist, passes);
+  if (launches) *launches += 2 + passes;
+  uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_alt, *dst_v = vals_alt;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    const int width = min(8, bits - shift);
+    cudaMemsetAsync(s.ticket, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * size_t(tiles) * kRadix, st);
+    k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, (1u << width) - 1u,
+                                           s.hist + p * kRadix, s.lookback, s.ticket, s.err);
+    uint32_t* t = src_k;
+    src_k = dst_k;
+    dst_k = t;
+    t = src_v;
+    src_v = dst_v;
+    dst_v = t;
+  }
+  return (passes & 1) != 0;
+}
+
+void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* gather, uint32_t* out, uint32_t n,
+                    uint32_t* d_total, cudaStream_t st, int* launches) {
+  if (n == 0u) {
+    if (d_total) cudaMemsetAsync(d_total, 0, sizeof(uint32_t), st);
+    return;
+  }
+  const uint32_t tiles = (n + kScanTile - 1u) / kScanTile;
+  cudaMemsetAsync(s.ticket, 0, sizeof(uint32_t), st);
+  cudaMemsetAsync(s.scan_lookback, 0, sizeof(unsigned long long) * tiles, st);
+  k_scan<<<tiles, kThreads, 0, st>>>(in, gather, out, n, d_total, s.scan_lookback, s.ticket, s.err);
+  if (launches) *launches += 1;
+}
+
+}  // namespace gsk
