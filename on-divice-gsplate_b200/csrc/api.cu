@@ -113,6 +113,7 @@ struct gs_context {
   gsk::DensifyScratch dens;
   uint64_t max_pairs_seen = 0;
   uint64_t last_pairs = 0;
+  uint32_t densify_slots = 0;  // slots the latest densify marked (the spawn mask's length)
   bool stepped = false;
   int launches = 0;
 
@@ -739,6 +740,7 @@ int gs_densify(gs_context* c, const gs_frame_data* frame, uint32_t counters_out[
     *c->h_frames = f;
     GS_CUDA_TRY(cudaMemcpyAsync(c->d_frames, c->h_frames, sizeof(gs_frame_data), cudaMemcpyHostToDevice, c->stream));
     int launches = 0;
+    c->densify_slots = c->model.slots;
     gsk::launch_densify(c->d_frames, c->model, c->dens, c->sort, c->stream, &launches);
     uint32_t counters[4] = {0, 0, 0, 0};
     GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -780,7 +782,7 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
     switch (which) {
       case GS_SNAP_PIXEL_COUNT: case GS_SNAP_IMAGE: case GS_SNAP_PIXEL_DOT: size = pixels * 4; break;
       case GS_SNAP_PIXEL_GRAD: case GS_SNAP_PIXEL_OUT: size = pixels * 16; break;
-      case GS_SNAP_SPAWN: size = size_t(slots) * 4; break;
+      case GS_SNAP_SPAWN: size = size_t(c->densify_slots) * 4; break;
       case GS_SNAP_PROJECTED: size = size_t(slots) * 64; break;
       case GS_SNAP_TILES: case GS_SNAP_OFFSETS: case GS_SNAP_DEPTH_KEY: size = size_t(slots) * 4; break;
       case GS_SNAP_STATS: size = size_t(slots) * 16; break;

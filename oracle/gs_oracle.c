@@ -1267,7 +1267,9 @@ typedef struct {
 
 double gso_reference_loss(const double* camera, uint32_t width, uint32_t height, const double* params,
                           const double* sh, uint32_t n, int stride, int degree, const uint8_t* target,
-                          const float* bg, int masked, double lambda, double* image, const double* head) {
+                          const float* bg, int masked, double lambda, double* image, const double* head,
+                          uint64_t* signature) {
+  uint64_t sig = 1469598103934665603ull; /* FNV-1a over every blend decision */
   const size_t pixels = (size_t)width * height;
   double* render = (double*)malloc(sizeof(double) * pixels * 3u);
   double* truth = (double*)malloc(sizeof(double) * pixels * 3u);
@@ -1301,12 +1303,18 @@ double gso_reference_loss(const double* camera, uint32_t width, uint32_t height,
         const double dx = g->mx - (x + 0.5), dy = g->my - (y + 0.5);
         const double power = -0.5 * (g->con[0] * dx * dx + g->con[2] * dy * dy) - g->con[1] * dx * dy;
         if (power > 0) continue;
-        const double alpha = fmin(0.99, g->opacity * exp(power));
+        const double raw = g->opacity * exp(power);
+        const double alpha = fmin(0.99, raw);
         if (alpha < 1.0 / 255.0) continue;
-        if (T * (1 - alpha) < 1e-4) break;
+        if (T * (1 - alpha) < 1e-4) {
+          sig = (sig ^ (0x100000000ull | order[k])) * 1099511628211ull;
+          break;
+        }
+        sig = (sig ^ ((raw >= 0.99 ? 0x200000000ull : 0ull) | order[k])) * 1099511628211ull;
         for (int c = 0; c < 3; ++c) C[c] += g->color[c] * alpha * T;
         T *= 1 - alpha;
       }
+      sig = (sig ^ 0xffffffffffull) * 1099511628211ull; /* pixel boundary */
       const uint8_t* t = &target[((size_t)y * width + x) * 4u];
       const double a = t[3] / 255.0;
       for (int c = 0; c < 3; ++c) {
@@ -1329,6 +1337,12 @@ double gso_reference_loss(const double* camera, uint32_t width, uint32_t height,
       weight_sum += 3.0 * w;
     }
   if (image) memcpy(image, render, sizeof(double) * pixels * 3u);
+  if (signature) {
+    /* Depth order and colour clamps change the loss discontinuously too. */
+    for (uint32_t k = 0; k < count; ++k) sig = (sig ^ order[k]) * 1099511628211ull;
+    for (uint32_t i = 0; i < n; ++i) sig = (sig ^ (uint64_t)refs[i].visible) * 1099511628211ull;
+    *signature = sig;
+  }
   const double values = 3.0 * (double)width * height;
   double result;
   if (lambda <= 0.0) {

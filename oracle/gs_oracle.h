@@ -140,10 +140,13 @@ void gso_reset_opacity(const gso_frame* f, float* params, float* m, float* v, fl
 /* FP64 forward + loss of train_selftest.cpp:79-283 (project, stable depth sort, blend over
    all gaussians per pixel, L1 + lambda (1 - SSIM)). params: 16 doubles per slot, sh:
    `stride` doubles per slot. camera: rotation[9] row-major, translation[3], position[3],
-   fx, fy, cx, cy. image: optional 3 doubles per pixel. */
+   fx, fy, cx, cy. image: optional 3 doubles per pixel. signature: optional hash of every
+   blend decision (which splats each pixel took, where it stopped, which alphas clamped,
+   the depth order): central differences whose stencil changes it cross a cut-off. */
 double gso_reference_loss(const double* camera, uint32_t width, uint32_t height, const double* params,
                           const double* sh, uint32_t n, int stride, int degree, const uint8_t* target,
-                          const float* bg, int masked, double lambda, double* image, const double* head);
+                          const float* bg, int masked, double lambda, double* image, const double* head,
+                          uint64_t* signature);
 
 /* reference_ssim of train_selftest.cpp:176-217 (x, y: 3 doubles per pixel). */
 double gso_reference_ssim(const double* x, const double* y, uint32_t width, uint32_t height, const double* weights);

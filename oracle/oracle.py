@@ -64,7 +64,7 @@ def lib():
         L.gso_densify_spawn.argtypes = [_vp, _f32p, _vp, _f32p, _f32p, _vp, _vp, _u32p, _u32p, _u32p, u32]
         L.gso_reset_opacity.argtypes = [_vp, _f32p, _f32p, _f32p, ctypes.c_float]
         L.gso_reference_loss.argtypes = [_f64p, u32, u32, _f64p, _vp, u32, ctypes.c_int, ctypes.c_int, _u8p,
-                                         _f32p, ctypes.c_int, ctypes.c_double, _vp, _vp]
+                                         _f32p, ctypes.c_int, ctypes.c_double, _vp, _vp, _vp]
         L.gso_reference_loss.restype = ctypes.c_double
         L.gso_reference_ssim.argtypes = [_f64p, _f64p, u32, u32, _vp]
         L.gso_reference_ssim.restype = ctypes.c_double
@@ -285,8 +285,10 @@ def footprint_tiles(frame: np.ndarray, proj16: np.ndarray) -> np.ndarray:
 
 
 def reference_loss(camera: dict, width: int, height: int, params64: np.ndarray, sh64: np.ndarray, degree: int,
-                   target: np.ndarray, bg, masked: bool, lam: float, want_image: bool = False, head=None):
-    """FP64 forward + loss of train_selftest.cpp:211-283."""
+                   target: np.ndarray, bg, masked: bool, lam: float, want_image: bool = False, head=None,
+                   want_signature: bool = False):
+    """FP64 forward + loss of train_selftest.cpp:211-283. With want_signature, also the hash
+    of its blend decisions (equal hashes: no alpha / transmittance / clamp cut-off crossed)."""
     L = lib()
     cam = np.concatenate([np.asarray(camera["rotation"], np.float64).reshape(9),
                           np.asarray(camera["translation"], np.float64).reshape(3),
@@ -296,10 +298,13 @@ def reference_loss(camera: dict, width: int, height: int, params64: np.ndarray, 
     stride = sh64.shape[1] if sh64.ndim == 2 else 0
     img = np.zeros((width * height, 3), np.float64) if want_image else None
     h = None if head is None else np.asarray(head, np.float64)
+    sig = np.zeros(1, np.uint64) if want_signature else None
     loss = L.gso_reference_loss(cam, width, height, np.ascontiguousarray(params64, np.float64),
                                 _ptr(np.ascontiguousarray(sh64, np.float64)) if stride else None, n, stride,
                                 degree, np.ascontiguousarray(target.reshape(-1), np.uint8),
-                                np.asarray(bg, np.float32), int(masked), float(lam), _ptr(img), _ptr(h))
+                                np.asarray(bg, np.float32), int(masked), float(lam), _ptr(img), _ptr(h), _ptr(sig))
+    if want_signature:
+        return (loss, img, int(sig[0])) if want_image else (loss, int(sig[0]))
     return (loss, img) if want_image else loss
 
 

@@ -23,17 +23,23 @@ GROUPS = {"position": [0, 1, 2], "opacity": [3], "log_scale": [4, 5, 6], "rotati
 
 
 def fd_check(scene: S.Scene, cam: F.Camera, target: np.ndarray, grad16: np.ndarray, grad_sh: np.ndarray,
-             bg, masked: bool, lam: float, eps: float = 1e-5, params: list | None = None) -> dict:
+             bg, masked: bool, lam: float, eps: float = 1e-5, params: list | None = None,
+             skip_crossings: bool = False) -> dict:
     """check_gradients (train_selftest.cpp:418-446): central finite differences of the FP64
     reference loss, |err| <= 5% |fd| + 2e-6, per parameter group. `params`: optional list of
-    (slot, offset) to check (offset < 0: SH coefficient -1 - offset); default all."""
+    (slot, offset) to check (offset < 0: SH coefficient -1 - offset); default all.
+    skip_crossings: leave out parameters whose stencil changes any blend decision of the FP64
+    forward (an alpha or transmittance cut-off, a clamp or the depth order), where central
+    differences measure a jump, not the derivative; they are counted as `skipped`."""
     p64, s64 = params64(scene)
     W, H = cam.width, cam.height
     camd = cam.as_dict()
     stride = scene.sh.shape[1]
 
     def loss():
-        return O.reference_loss(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam)
+        return O.reference_loss(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam, want_signature=True)
+
+    _, sig0 = loss()
 
     todo = params
     if todo is None:
@@ -44,14 +50,17 @@ def fd_check(scene: S.Scene, cam: F.Camera, target: np.ndarray, grad16: np.ndarr
         arr, idx = (p64, (i, off)) if off >= 0 else (s64, (i, -1 - off))
         saved = arr[idx]
         arr[idx] = saved + eps
-        up = loss()
+        up, sig_up = loss()
         arr[idx] = saved - eps
-        down = loss()
+        down, sig_down = loss()
         arr[idx] = saved
         fd = (up - down) / (2 * eps)
         got = float(grad16[i, off]) if off >= 0 else float(grad_sh[i, -1 - off])
         group = next((k for k, v in GROUPS.items() if off in v), "sh_rest") if off >= 0 else "sh_rest"
-        g = report.setdefault(group, {"checked": 0, "bad": 0, "max_err": 0.0, "max_ref": 0.0})
+        g = report.setdefault(group, {"checked": 0, "bad": 0, "max_err": 0.0, "max_ref": 0.0, "skipped": 0})
+        if skip_crossings and (sig_up != sig0 or sig_down != sig0):
+            g["skipped"] += 1
+            continue
         err = abs(got - fd)
         g["checked"] += 1
         g["max_err"] = max(g["max_err"], err)

@@ -183,7 +183,9 @@ def test_adjoint_sh3_against_oracle_and_fd(ctx):
     sample = [(int(i), int(off)) for i, off in zip(rng.integers(0, 512, 120),
                                                     rng.choice([0, 1, 2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 13, 14, -1,
                                                                 -7, -20, -44], 120))]
-    report = fd_check(scene, cam, target, g16, gsh, bg, False, 0.2, eps=1e-4, params=sample)
+    report = fd_check(scene, cam, target, g16, gsh, bg, False, 0.2, eps=1e-4, params=sample, skip_crossings=True)
+    checked = sum(g["checked"] for g in report.values())
+    assert checked >= 40, report
     for name, g in report.items():
         assert g["bad"] <= max(1, g["checked"] // 20), (name, g)
 
