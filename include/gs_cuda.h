@@ -117,8 +117,8 @@ typedef struct gs_tuning {
   uint32_t min_pair_capacity; /* smallest pair buffer (TrainOptions::min_pair_capacity) */
   uint64_t initial_pairs;     /* pairs to allocate before the first count (0: 4 per slot and view) */
   uint32_t deterministic;     /* 1: per-pair gradients + fixed-order sum (bit-stable); 0: atomics */
-  uint32_t raster_batch;      /* splats staged per block in the backward pass: 32 or 64 (0: auto) */
-  uint32_t sort_digit_bits;   /* radix digit width: 8 (0: auto) */
+  uint32_t forward_pixels;    /* pixels per thread in the forward pass: 1, 2 or 4 (0: default) */
+  uint32_t backward_pixels;   /* pixels per thread in the backward pass: 1, 2 or 4 (0: default) */
   uint32_t retry;             /* 1 (default): grow the pair buffers and run again on overflow */
 } gs_tuning;
 

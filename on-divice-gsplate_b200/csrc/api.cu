@@ -121,7 +121,7 @@ struct gs_context {
 
   void release() {
     cudaSetDevice(device);
-    for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &pixel_grad,
+    for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.shin, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
     for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss}) dev_free(*p);
@@ -166,6 +166,7 @@ struct gs_context {
     dev_alloc(vb.tiles, n);
     dev_alloc(vb.offsets, n);
     dev_alloc(vb.grad2d, n * 3);
+    dev_alloc(vb.shin, n * 2);
     dev_alloc(dkeys, n);
     dev_alloc(dvals, n);
     dev_alloc(dkeys_alt, n);
@@ -374,7 +375,7 @@ struct gs_context {
     ++launches;
     mark(2);
     const gsk::RasterBuffers rb = raster_buffers();
-    gsk::launch_raster_forward(sp, vb, rb, stream);
+    gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2, stream);
     ++launches;
     mark(3);
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
@@ -390,8 +391,8 @@ struct gs_context {
     ++launches;
     mark(4);
     if (train) {
-      const int batch = tuning.raster_batch ? int(tuning.raster_batch) : 32;
-      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, batch, d_scalars, uint32_t(pair_cap), stream);
+      const int px = tuning.backward_pixels ? int(tuning.backward_pixels) : 2;
+      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, px, d_scalars, uint32_t(pair_cap), stream);
       ++launches;
       mark(5);
       if (det) {
@@ -549,8 +550,8 @@ int gs_create(int device, gs_context** out) {
     c->device = device;
     c->tuning.min_pair_capacity = 1u << 16;
     c->tuning.deterministic = 1u;
-    c->tuning.raster_batch = 32u;
-    c->tuning.sort_digit_bits = 8u;
+    c->tuning.forward_pixels = 2u;
+    c->tuning.backward_pixels = 2u;
     c->tuning.retry = 1u;
     try {
       GS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -873,10 +874,9 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
 int gs_set_tuning(gs_context* c, const gs_tuning* t) {
   return guarded([&] {
     if (c == nullptr || t == nullptr) fail(GS_ERR_INVALID, "gs_set_tuning: null argument");
-    if (t->raster_batch != 0 && t->raster_batch != 32 && t->raster_batch != 64)
-      fail(GS_ERR_INVALID, "gs_set_tuning: raster_batch must be 32 or 64");
-    if (t->sort_digit_bits != 0 && t->sort_digit_bits != 8)
-      fail(GS_ERR_INVALID, "gs_set_tuning: sort_digit_bits must be 8");
+    for (uint32_t px : {t->forward_pixels, t->backward_pixels})
+      if (px != 0 && px != 1 && px != 2 && px != 4)
+        fail(GS_ERR_INVALID, "gs_set_tuning: pixels per thread must be 1, 2 or 4");
     c->tuning = *t;
     if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
   });

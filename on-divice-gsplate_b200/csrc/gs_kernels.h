@@ -32,6 +32,7 @@ struct ViewBuffers {
   uint32_t* tiles = nullptr; // tiles touched
   uint32_t* offsets = nullptr;  // first pair, pre-sort order
   float4* grad2d = nullptr;  // 3 per g: summed pair gradients (train_pair_sum layout)
+  float4* shin = nullptr;    // 2 per g (several views): colour gradient + flag, view direction
 };
 
 struct StepPointers {
@@ -86,11 +87,13 @@ struct RasterBuffers {
   uint32_t* tile_count = nullptr;
   float4* ssim_maps = nullptr;              // 3 per pixel
 };
-void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, cudaStream_t st);
+// px: pixels per thread (1, 2 or 4).
+void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,
+                           cudaStream_t st);
 // Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
 // vb.grad2d (fast). Skipped on device when *d_pairs > accept.
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
-                            float4* pair_grads, bool deterministic, int batch, const uint32_t* d_pairs,
+                            float4* pair_grads, bool deterministic, int px, const uint32_t* d_pairs,
                             uint32_t accept, cudaStream_t st);
 
 // ---- loss.cu ----

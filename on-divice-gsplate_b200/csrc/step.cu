@@ -3,10 +3,12 @@
 // train_step_sh.comp:21-44), adaptive density control (train_densify_mark.comp,
 // train_densify_spawn.comp) and the opacity reset (train_reset_opacity.comp).
 //
-// k_step reads each slot's parameters, SH and moments once, back-propagates every view's
-// summed 2D gradient through that view's projection (views of one step add up), and
-// takes one Adam step on the 16 parameters and the active SH coefficients. HBM-bound:
-// params, SH and both moment sets are read and written once per step.
+// The step back-propagates every view's summed 2D gradient through that view's projection
+// (views of one step add up) and takes one Adam step on the 16 parameters
+// (k_step_geometry) and on the active SH coefficients (k_step_sh). HBM-bound: parameters,
+// SH and both moment sets are read and written once per step (SH read twice).
+#include <utility>
+
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -58,6 +60,7 @@ struct StepArgs {
   const float4* splat;
   const uint32_t* tiles;
   const float4* grad2d;
+  float4* shin;  // several views: per (view, slot) colour gradient + drew flag, view direction
   const uint32_t* d_pairs;
   uint32_t accept;
 };
@@ -69,264 +72,362 @@ __device__ __forceinline__ float adam1(float p, float g, float& m, float& v, flo
   return p - lr * (m * c1) / (sqrtf(v * c2) + eps);
 }
 
-template <int DEG>
-__global__ void __launch_bounds__(128) k_step(StepArgs a) {
-  __shared__ gs_frame_data s_frames[kMaxViews];
-  {
-    const uint32_t words = a.n_views * uint32_t(sizeof(gs_frame_data) / 4);
-    for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
-      reinterpret_cast<uint32_t*>(s_frames)[k] = reinterpret_cast<const uint32_t*>(a.frames)[k];
+// Basis function k (1..15) of the real SH basis and its gradient w.r.t. the unit
+// direction (train_common.glsl:84-140), one term at a time so unrolled loops keep only
+// what they use in registers.
+template <int K>
+__device__ __forceinline__ float sh_term(float x, float y, float z, float& gx, float& gy, float& gz) {
+  constexpr float C1 = 0.4886025119029199f, A = 1.0925484305920792f, B = 0.31539156525252005f,
+                  C = 0.5462742152960396f, D = -0.5900435899266435f, E = 2.890611442640554f,
+                  F = -0.4570457994644658f, G = 0.3731763325901154f, H = 1.445305721320277f;
+  const float xx = x * x, yy = y * y, zz = z * z;
+  if constexpr (K == 1) { gx = 0.f; gy = -C1; gz = 0.f; return -C1 * y; }
+  if constexpr (K == 2) { gx = 0.f; gy = 0.f; gz = C1; return C1 * z; }
+  if constexpr (K == 3) { gx = -C1; gy = 0.f; gz = 0.f; return -C1 * x; }
+  if constexpr (K == 4) { gx = A * y; gy = A * x; gz = 0.f; return A * x * y; }
+  if constexpr (K == 5) { gx = 0.f; gy = -A * z; gz = -A * y; return -A * y * z; }
+  if constexpr (K == 6) { gx = B * (-2.0f * x); gy = B * (-2.0f * y); gz = B * (4.0f * z); return B * (2.0f * zz - xx - yy); }
+  if constexpr (K == 7) { gx = -A * z; gy = 0.f; gz = -A * x; return -A * x * z; }
+  if constexpr (K == 8) { gx = C * (2.0f * x); gy = C * (-2.0f * y); gz = 0.f; return C * (xx - yy); }
+  if constexpr (K == 9) { gx = D * (6.0f * x * y); gy = D * (3.0f * xx - 3.0f * yy); gz = 0.f; return D * y * (3.0f * xx - yy); }
+  if constexpr (K == 10) { gx = E * (y * z); gy = E * (x * z); gz = E * (x * y); return E * x * y * z; }
+  if constexpr (K == 11) {
+    gx = F * (-2.0f * x * y); gy = F * (4.0f * zz - xx - 3.0f * yy); gz = F * (8.0f * y * z);
+    return F * y * (4.0f * zz - xx - yy);
   }
+  if constexpr (K == 12) {
+    gx = G * (-6.0f * x * z); gy = G * (-6.0f * y * z); gz = G * (6.0f * zz - 3.0f * xx - 3.0f * yy);
+    return G * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+  }
+  if constexpr (K == 13) {
+    gx = F * (4.0f * zz - 3.0f * xx - yy); gy = F * (-2.0f * x * y); gz = F * (8.0f * x * z);
+    return F * x * (4.0f * zz - xx - yy);
+  }
+  if constexpr (K == 14) { gx = H * (2.0f * x * z); gy = H * (-2.0f * y * z); gz = H * (xx - yy); return H * z * (xx - yy); }
+  if constexpr (K == 15) {
+    gx = D * (3.0f * xx - 3.0f * yy); gy = D * (-6.0f * x * y); gz = 0.f;
+    return D * x * (xx - 3.0f * yy);
+  }
+  return 0.0f;
+}
+
+template <int... Ks, typename F>
+__device__ __forceinline__ void for_terms(std::integer_sequence<int, Ks...>, F&& f) {
+  (f(std::integral_constant<int, Ks + 1>{}), ...);
+}
+
+// View-independent quantities of a slot's covariance.
+struct Geometry {
+  float qn[4], qlen, R[3][3], s[3], M[3][3], Sig[3][3], opacity;
+};
+
+__device__ __forceinline__ void slot_geometry(float4 p0, float4 p1, float4 q, Geometry& G) {
+  G.qlen = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-12f);
+  G.qn[0] = q.x / G.qlen;
+  G.qn[1] = q.y / G.qlen;
+  G.qn[2] = q.z / G.qlen;
+  G.qn[3] = q.w / G.qlen;
+  quat_to_matrix(G.qn[0], G.qn[1], G.qn[2], G.qn[3], G.R);
+  G.s[0] = expf(p1.x);
+  G.s[1] = expf(p1.y);
+  G.s[2] = expf(p1.z);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) G.M[r][c] = G.R[r][c] * G.s[c];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) G.Sig[r][c] = G.M[r][0] * G.M[c][0] + G.M[r][1] * G.M[c][1] + G.M[r][2] * G.M[c][2];
+  G.opacity = sigmoidf(p0.w);
+}
+
+// One view's projection backward (train_step.glsl:82-219) of a slot: adds the gradient of
+// the 14 geometry + DC parameters to g16 (without the SH view-direction term, which the
+// caller adds through `dir`/`dir_len`), updates the densification statistics, and returns
+// the clamped colour gradient and the view direction. drew: bit 0 any pair gradient, bit
+// 1 a non-zero colour gradient.
+template <int DEG>
+__device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0, const Geometry& G, float4 a0, float4 a1,
+                                              float4 a2, uint32_t clamped, float radius, float g16[16], float4& st,
+                                              float dcol[3], float dir[3], float& dir_len, uint32_t& drew) {
+  if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f || a0.w != 0.f || a1.x != 0.f || a1.y != 0.f || a1.z != 0.f ||
+      a1.w != 0.f || a2.x != 0.f || a2.y != 0.f || a2.z != 0.f || a2.w != 0.f)
+    drew |= 1u;
+  const float dmx = a0.x, dmy = a0.y;
+  const float ga = a0.z, gb = a0.w, gc = a1.x;
+  const float dop = a1.y;
+  dcol[0] = (clamped & 1u) ? 0.0f : a1.z;
+  dcol[1] = (clamped & 2u) ? 0.0f : a1.w;
+  dcol[2] = (clamped & 4u) ? 0.0f : a2.x;
+  if (dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f) drew |= 2u;
+  const float width = float(f.image[0]), height = float(f.image[1]);
+  const float nx = 0.5f * width, ny = 0.5f * height;
+  // Densification statistics: the view-space positional gradient in NDC units.
+  st.x += sqrtf((dmx * nx) * (dmx * nx) + (dmy * ny) * (dmy * ny));
+  st.y += 1.0f;
+  st.z = fmaxf(st.z, radius);
+  st.w += sqrtf((a2.y * nx) * (a2.y * nx) + (a2.z * ny) * (a2.z * ny));
+
+  float t[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) t[r] = f.rot[r][0] * p0.x + f.rot[r][1] * p0.y + f.rot[r][2] * p0.z + f.rot[r][3];
+  const float fx = f.intrinsics[0], fy = f.intrinsics[1], cx = f.intrinsics[2], cy = f.intrinsics[3];
+  const float inv_z = 1.0f / t[2];
+  const float lim_x = 1.3f * fmaxf(cx, width - cx) / fx;
+  const float lim_y = 1.3f * fmaxf(cy, height - cy) / fy;
+  const float rx = t[0] * inv_z, ry = t[1] * inv_z;
+  const bool clamp_x = rx < -lim_x || rx > lim_x;
+  const bool clamp_y = ry < -lim_y || ry > lim_y;
+  const float tx = clampf(rx, -lim_x, lim_x), ty = clampf(ry, -lim_y, lim_y);
+  const float j00 = fx * inv_z, j02 = -fx * tx * inv_z, j11 = fy * inv_z, j12 = -fy * ty * inv_z;
+  float T[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    T[0][c] = j00 * f.rot[0][c] + j02 * f.rot[2][c];
+    T[1][c] = j11 * f.rot[1][c] + j12 * f.rot[2][c];
+  }
+  float TS[2][3];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) TS[r][c] = T[r][0] * G.Sig[0][c] + T[r][1] * G.Sig[1][c] + T[r][2] * G.Sig[2][c];
+  const float A = TS[0][0] * T[0][0] + TS[0][1] * T[0][1] + TS[0][2] * T[0][2] + kDilation;
+  const float B = TS[1][0] * T[0][0] + TS[1][1] * T[0][1] + TS[1][2] * T[0][2];
+  const float C = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + kDilation;
+  const float D = A * C - B * B;
+
+  const float dr0 = p0.x - f.cam_pos[0], dr1 = p0.y - f.cam_pos[1], dr2 = p0.z - f.cam_pos[2];
+  dir_len = fmaxf(sqrtf(dr0 * dr0 + dr1 * dr1 + dr2 * dr2), 1e-12f);
+  dir[0] = dr0 / dir_len;
+  dir[1] = dr1 / dir_len;
+  dir[2] = dr2 / dir_len;
+  g16[12] += 0.28209479177387814f * dcol[0];
+  g16[13] += 0.28209479177387814f * dcol[1];
+  g16[14] += 0.28209479177387814f * dcol[2];
+
+  g16[3] += dop * G.opacity * (1.0f - G.opacity);
+
+  // Conic -> dilated 2D covariance.
+  const float inv_d2 = 1.0f / (D * D);
+  const float gA = (-C * C * ga + B * C * gb - B * B * gc) * inv_d2;
+  const float gB = (2.0f * B * C * ga - (D + 2.0f * B * B) * gb + 2.0f * A * B * gc) * inv_d2;
+  const float gC = (-B * B * ga + A * B * gb - A * A * gc) * inv_d2;
+  const float G2[2][2] = {{gA, 0.5f * gB}, {0.5f * gB, gC}};
+  // dSigma = T^T G2 T, dT = 2 G2 T Sigma, dJ = dT W^T (J's third row is zero).
+  float G2T[2][3];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) G2T[r][c] = G2[r][0] * T[0][c] + G2[r][1] * T[1][c];
+  float dT[2][3];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dT[r][c] = 2.0f * (G2[r][0] * TS[0][c] + G2[r][1] * TS[1][c]);
+  float dJ[2][3];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dJ[r][c] = dT[r][0] * f.rot[c][0] + dT[r][1] * f.rot[c][1] + dT[r][2] * f.rot[c][2];
+  float dt[3] = {0.f, 0.f, 0.f};
+  const float inv_z2 = inv_z * inv_z;
+  dt[2] += -fx * inv_z2 * dJ[0][0] - fy * inv_z2 * dJ[1][1];
+  if (clamp_x) {
+    dt[2] += fx * tx * inv_z2 * dJ[0][2];
+  } else {
+    dt[0] += -fx * inv_z2 * dJ[0][2];
+    dt[2] += 2.0f * fx * t[0] * inv_z2 * inv_z * dJ[0][2];
+  }
+  if (clamp_y) {
+    dt[2] += fy * ty * inv_z2 * dJ[1][2];
+  } else {
+    dt[1] += -fy * inv_z2 * dJ[1][2];
+    dt[2] += 2.0f * fy * t[1] * inv_z2 * inv_z * dJ[1][2];
+  }
+  dt[0] += dmx * fx * inv_z;
+  dt[1] += dmy * fy * inv_z;
+  dt[2] += -(dmx * fx * t[0] + dmy * fy * t[1]) * inv_z2;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g16[c] += f.rot[0][c] * dt[0] + f.rot[1][c] * dt[1] + f.rot[2][c] * dt[2];
+
+  // 3D covariance -> log scale and rotation; dSigma = T^T G2 T folded into dM = 2 dSigma M.
+  float dM[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    float dS[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dS[c] = T[0][r] * G2T[0][c] + T[1][r] * G2T[1][c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dM[r][c] = 2.0f * (dS[0] * G.M[0][c] + dS[1] * G.M[1][c] + dS[2] * G.M[2][c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    g16[4 + c] += (dM[0][c] * G.R[0][c] + dM[1][c] * G.R[1][c] + dM[2][c] * G.R[2][c]) * G.s[c];
+  float gR[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gR[r][c] = dM[r][c] * G.s[c];
+  const float w = G.qn[0], x = G.qn[1], y = G.qn[2], z = G.qn[3];
+  float dq[4];
+  dq[0] = 2.0f * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
+  dq[1] = 2.0f * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0f * x * gR[1][1] - w * gR[1][2] + z * gR[2][0] +
+                  w * gR[2][1] - 2.0f * x * gR[2][2]);
+  dq[2] = 2.0f * (-2.0f * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] - w * gR[2][0] +
+                  z * gR[2][1] - 2.0f * y * gR[2][2]);
+  dq[3] = 2.0f * (-2.0f * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0f * z * gR[1][1] +
+                  y * gR[1][2] + x * gR[2][0] + y * gR[2][1]);
+  const float qd = G.qn[0] * dq[0] + G.qn[1] * dq[1] + G.qn[2] * dq[2] + G.qn[3] * dq[3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) g16[8 + k] += (dq[k] - G.qn[k] * qd) / G.qlen;
+}
+
+// dL/d(position) through the SH view direction: (dL/ddir - dir (dir . dL/ddir)) / |p - c|.
+__device__ __forceinline__ void add_direction_term(float g16[16], const float dir[3], float dir_len, const float dd[3]) {
+  const float proj = dir[0] * dd[0] + dir[1] * dd[1] + dir[2] * dd[2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g16[c] += (dd[c] - dir[c] * proj) / dir_len;
+}
+
+__device__ __forceinline__ void adam_params(const StepArgs& a, const gs_frame_data& f0, uint32_t i, float4 p0,
+                                            float4 p1, float4 q, float4 p3, const float g16[16]) {
+  const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1];
+  float4 m0 = a.M[i], m1 = a.M[a.cap + i], m2 = a.M[2u * a.cap + i], m3 = a.M[3u * a.cap + i];
+  float4 v0 = a.V[i], v1 = a.V[a.cap + i], v2 = a.V[2u * a.cap + i], v3 = a.V[3u * a.cap + i];
+  const float lp = f0.lr0[0], ls = f0.lr0[1], lq = f0.lr0[2], lo = f0.lr0[3], ld = f0.lr1[0];
+  p0.x = adam1(p0.x, g16[0], m0.x, v0.x, lp, b1, b2, c1, c2, eps);
+  p0.y = adam1(p0.y, g16[1], m0.y, v0.y, lp, b1, b2, c1, c2, eps);
+  p0.z = adam1(p0.z, g16[2], m0.z, v0.z, lp, b1, b2, c1, c2, eps);
+  p0.w = adam1(p0.w, g16[3], m0.w, v0.w, lo, b1, b2, c1, c2, eps);
+  p1.x = adam1(p1.x, g16[4], m1.x, v1.x, ls, b1, b2, c1, c2, eps);
+  p1.y = adam1(p1.y, g16[5], m1.y, v1.y, ls, b1, b2, c1, c2, eps);
+  p1.z = adam1(p1.z, g16[6], m1.z, v1.z, ls, b1, b2, c1, c2, eps);
+  p1.w = adam1(p1.w, 0.0f, m1.w, v1.w, 0.0f, b1, b2, c1, c2, eps);
+  q.x = adam1(q.x, g16[8], m2.x, v2.x, lq, b1, b2, c1, c2, eps);
+  q.y = adam1(q.y, g16[9], m2.y, v2.y, lq, b1, b2, c1, c2, eps);
+  q.z = adam1(q.z, g16[10], m2.z, v2.z, lq, b1, b2, c1, c2, eps);
+  q.w = adam1(q.w, g16[11], m2.w, v2.w, lq, b1, b2, c1, c2, eps);
+  p3.x = adam1(p3.x, g16[12], m3.x, v3.x, ld, b1, b2, c1, c2, eps);
+  p3.y = adam1(p3.y, g16[13], m3.y, v3.y, ld, b1, b2, c1, c2, eps);
+  p3.z = adam1(p3.z, g16[14], m3.z, v3.z, ld, b1, b2, c1, c2, eps);
+  p3.w = adam1(p3.w, 0.0f, m3.w, v3.w, 0.0f, b1, b2, c1, c2, eps);
+  a.P[i] = p0;
+  a.P[a.cap + i] = p1;
+  a.P[2u * a.cap + i] = q;
+  a.P[3u * a.cap + i] = p3;
+  a.M[i] = m0;
+  a.M[a.cap + i] = m1;
+  a.M[2u * a.cap + i] = m2;
+  a.M[3u * a.cap + i] = m3;
+  a.V[i] = v0;
+  a.V[a.cap + i] = v1;
+  a.V[2u * a.cap + i] = v2;
+  a.V[3u * a.cap + i] = v3;
+}
+
+__device__ __forceinline__ void copy_frames(const StepArgs& a, gs_frame_data* s_frames, uint32_t n) {
+  const uint32_t words = n * uint32_t(sizeof(gs_frame_data) / 4);
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
+    reinterpret_cast<uint32_t*>(s_frames)[k] = reinterpret_cast<const uint32_t*>(a.frames)[k];
   __syncthreads();
-  // More pairs than the buffers hold: gradients are incomplete, leave everything as it
-  // was (train_step.glsl:247-251); the host grows the buffers and runs the step again.
+}
+
+// Part 1 (train_step.glsl:72-240): every view's projection backward summed, Adam on the
+// 16 parameters; each view's colour gradient and direction go to `shin` for part 2.
+template <int DEG>
+__global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
+  __shared__ gs_frame_data s_frames[kMaxViews];
+  copy_frames(a, s_frames, a.n_views);
   if (*a.d_pairs > a.accept) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.slots) return;
   constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
-  float4 p0 = a.P[i], p1 = a.P[a.cap + i], q = a.P[2u * a.cap + i], p3 = a.P[3u * a.cap + i];
-  if (p1.w < 0.5f) return;  // free slot
-
+  const float4 p0 = a.P[i], p1 = a.P[a.cap + i], q = a.P[2u * a.cap + i], p3 = a.P[3u * a.cap + i];
+  if (p1.w < 0.5f) return;
   float g16[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) g16[k] = 0.0f;
-  float gsh[K > 0 ? 3 * K : 1];
-#pragma unroll
-  for (int k = 0; k < 3 * K; ++k) gsh[k] = 0.0f;
   uint32_t drew = 0u;
-
-  // View-independent: normalised quaternion, R, scales, M = R S, Sigma = M M^T.
-  const float qlen = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-12f);
-  const float qn[4] = {q.x / qlen, q.y / qlen, q.z / qlen, q.w / qlen};
-  float R[3][3];
-  quat_to_matrix(qn[0], qn[1], qn[2], qn[3], R);
-  const float s[3] = {expf(p1.x), expf(p1.y), expf(p1.z)};
-  float Mm[3][3], Sig[3][3];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) Mm[r][c] = R[r][c] * s[c];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) Sig[r][c] = Mm[r][0] * Mm[c][0] + Mm[r][1] * Mm[c][1] + Mm[r][2] * Mm[c][2];
-  const float opacity = sigmoidf(p0.w);
+  Geometry G;
+  slot_geometry(p0, p1, q, G);
   float4 st = a.stats[i];
   bool seen = false;
-
   for (uint32_t v = 0; v < a.n_views; ++v) {
     const size_t g = size_t(v) * a.cap + i;
-    if (a.tiles[g] == 0u) continue;
+    if (a.tiles[g] == 0u) {
+      a.shin[g * 2u] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
+    }
     seen = true;
-    const gs_frame_data& f = s_frames[v];
-    const float4 a0 = a.grad2d[g * 3u], a1 = a.grad2d[g * 3u + 1u], a2 = a.grad2d[g * 3u + 2u];
-    if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f || a0.w != 0.f || a1.x != 0.f || a1.y != 0.f || a1.z != 0.f ||
-        a1.w != 0.f || a2.x != 0.f || a2.y != 0.f || a2.z != 0.f || a2.w != 0.f)
-      drew |= 1u;
-    const float dmx = a0.x, dmy = a0.y;
-    const float ga = a0.z, gb = a0.w, gc = a1.x;
-    const float dop = a1.y;
-    float dcol[3] = {a1.z, a1.w, a2.x};
-    const float width = float(f.image[0]), height = float(f.image[1]);
-    const float nx = 0.5f * width, ny = 0.5f * height;
-    // Densification statistics: the view-space positional gradient in NDC units.
-    st.x += sqrtf((dmx * nx) * (dmx * nx) + (dmy * ny) * (dmy * ny));
-    st.y += 1.0f;
-    st.z = fmaxf(st.z, a.splat[g * 3u + 1u].w);
-    st.w += sqrtf((a2.y * nx) * (a2.y * nx) + (a2.z * ny) * (a2.z * ny));
-
-    // Recompute the projection.
-    float t[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) t[r] = f.rot[r][0] * p0.x + f.rot[r][1] * p0.y + f.rot[r][2] * p0.z + f.rot[r][3];
-    const float fx = f.intrinsics[0], fy = f.intrinsics[1], cx = f.intrinsics[2], cy = f.intrinsics[3];
-    const float inv_z = 1.0f / t[2];
-    const float lim_x = 1.3f * fmaxf(cx, width - cx) / fx;
-    const float lim_y = 1.3f * fmaxf(cy, height - cy) / fy;
-    const float rx = t[0] * inv_z, ry = t[1] * inv_z;
-    const bool clamp_x = rx < -lim_x || rx > lim_x;
-    const bool clamp_y = ry < -lim_y || ry > lim_y;
-    const float tx = clampf(rx, -lim_x, lim_x), ty = clampf(ry, -lim_y, lim_y);
-    const float j00 = fx * inv_z, j02 = -fx * tx * inv_z, j11 = fy * inv_z, j12 = -fy * ty * inv_z;
-    float T[2][3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      T[0][c] = j00 * f.rot[0][c] + j02 * f.rot[2][c];
-      T[1][c] = j11 * f.rot[1][c] + j12 * f.rot[2][c];
-    }
-    float TS[2][3];  // T Sigma
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) TS[r][c] = T[r][0] * Sig[0][c] + T[r][1] * Sig[1][c] + T[r][2] * Sig[2][c];
-    const float A = TS[0][0] * T[0][0] + TS[0][1] * T[0][1] + TS[0][2] * T[0][2] + kDilation;
-    const float B = TS[1][0] * T[0][0] + TS[1][1] * T[0][1] + TS[1][2] * T[0][2];
-    const float C = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + kDilation;
-    const float D = A * C - B * B;
-
-    // Colour -> SH coefficients and view direction.
-    float dr[3] = {p0.x - f.cam_pos[0], p0.y - f.cam_pos[1], p0.z - f.cam_pos[2]};
-    const float dir_len = fmaxf(sqrtf(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), 1e-12f);
-    const float dir[3] = {dr[0] / dir_len, dr[1] / dir_len, dr[2] / dir_len};
-    const uint32_t clamped = __float_as_uint(a.splat[g * 3u + 2u].w);
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if (clamped & (1u << c)) dcol[c] = 0.0f;
-    if (dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f) drew |= 2u;
-    float basis[16];
-    sh_basis<DEG>(dir[0], dir[1], dir[2], basis);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) g16[12 + c] += basis[0] * dcol[c];
-    float ddir[3] = {0.f, 0.f, 0.f};
+    float dcol[3], dir[3], dir_len;
+    uint32_t vdrew = 0u;
+    view_backward<DEG>(s_frames[v], p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u], a.grad2d[g * 3u + 2u],
+                       __float_as_uint(a.splat[g * 3u + 2u].w), a.splat[g * 3u + 1u].w, g16, st, dcol, dir, dir_len,
+                       vdrew);
+    drew |= vdrew;
     if constexpr (K > 0) {
-      float db[16][3];
-      sh_basis_grad<DEG>(dir[0], dir[1], dir[2], db);
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const float w = a.SH[size_t(3 * k) * a.cap + i] * dcol[0] + a.SH[size_t(3 * k + 1) * a.cap + i] * dcol[1] +
-                        a.SH[size_t(3 * k + 2) * a.cap + i] * dcol[2];
-        ddir[0] += w * db[k + 1][0];
-        ddir[1] += w * db[k + 1][1];
-        ddir[2] += w * db[k + 1][2];
-        gsh[3 * k] += basis[k + 1] * dcol[0];
-        gsh[3 * k + 1] += basis[k + 1] * dcol[1];
-        gsh[3 * k + 2] += basis[k + 1] * dcol[2];
-      }
+      float dd[3] = {0.f, 0.f, 0.f};
+      for_terms(std::make_integer_sequence<int, K>{}, [&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        float gx, gy, gz;
+        sh_term<k>(dir[0], dir[1], dir[2], gx, gy, gz);
+        const float w = a.SH[size_t(3 * (k - 1)) * a.cap + i] * dcol[0] +
+                        a.SH[size_t(3 * (k - 1) + 1) * a.cap + i] * dcol[1] +
+                        a.SH[size_t(3 * (k - 1) + 2) * a.cap + i] * dcol[2];
+        dd[0] += w * gx;
+        dd[1] += w * gy;
+        dd[2] += w * gz;
+      });
+      add_direction_term(g16, dir, dir_len, dd);
     }
-    const float dd = dir[0] * ddir[0] + dir[1] * ddir[1] + dir[2] * ddir[2];
-    float ddir_raw[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) ddir_raw[c] = (ddir[c] - dir[c] * dd) / dir_len;
-
-    g16[3] += dop * opacity * (1.0f - opacity);
-
-    // Conic -> dilated 2D covariance.
-    const float inv_d2 = 1.0f / (D * D);
-    const float gA = (-C * C * ga + B * C * gb - B * B * gc) * inv_d2;
-    const float gB = (2.0f * B * C * ga - (D + 2.0f * B * B) * gb + 2.0f * A * B * gc) * inv_d2;
-    const float gC = (-B * B * ga + A * B * gb - A * A * gc) * inv_d2;
-    const float G2[2][2] = {{gA, 0.5f * gB}, {0.5f * gB, gC}};
-    // dSigma = T^T G2 T, dT = 2 G2 T Sigma, dJ = dT W^T (rows 0, 1; row 2 of J is zero).
-    float G2T[2][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) G2T[r][c] = G2[r][0] * T[0][c] + G2[r][1] * T[1][c];
-    float dSig[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) dSig[r][c] = T[0][r] * G2T[0][c] + T[1][r] * G2T[1][c];
-    float dT[2][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        dT[r][c] = 2.0f * (G2[r][0] * TS[0][c] + G2[r][1] * TS[1][c]);
-    float dJ[2][3];
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) dJ[r][c] = dT[r][0] * f.rot[c][0] + dT[r][1] * f.rot[c][1] + dT[r][2] * f.rot[c][2];
-    float dt[3] = {0.f, 0.f, 0.f};
-    const float inv_z2 = inv_z * inv_z;
-    dt[2] += -fx * inv_z2 * dJ[0][0] - fy * inv_z2 * dJ[1][1];
-    if (clamp_x) {
-      dt[2] += fx * tx * inv_z2 * dJ[0][2];
-    } else {
-      dt[0] += -fx * inv_z2 * dJ[0][2];
-      dt[2] += 2.0f * fx * t[0] * inv_z2 * inv_z * dJ[0][2];
-    }
-    if (clamp_y) {
-      dt[2] += fy * ty * inv_z2 * dJ[1][2];
-    } else {
-      dt[1] += -fy * inv_z2 * dJ[1][2];
-      dt[2] += 2.0f * fy * t[1] * inv_z2 * inv_z * dJ[1][2];
-    }
-    dt[0] += dmx * fx * inv_z;
-    dt[1] += dmy * fy * inv_z;
-    dt[2] += -(dmx * fx * t[0] + dmy * fy * t[1]) * inv_z2;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) g16[c] += f.rot[0][c] * dt[0] + f.rot[1][c] * dt[1] + f.rot[2][c] * dt[2] + ddir_raw[c];
-
-    // 3D covariance -> log scale and rotation.
-    float dM[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) dM[r][c] = 2.0f * (dSig[r][0] * Mm[0][c] + dSig[r][1] * Mm[1][c] + dSig[r][2] * Mm[2][c]);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) g16[4 + c] += (dM[0][c] * R[0][c] + dM[1][c] * R[1][c] + dM[2][c] * R[2][c]) * s[c];
-    float gR[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gR[r][c] = dM[r][c] * s[c];
-    const float w = qn[0], x = qn[1], y = qn[2], z = qn[3];
-    float dq[4];
-    dq[0] = 2.0f * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
-    dq[1] = 2.0f * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0f * x * gR[1][1] - w * gR[1][2] + z * gR[2][0] +
-                    w * gR[2][1] - 2.0f * x * gR[2][2]);
-    dq[2] = 2.0f * (-2.0f * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] - w * gR[2][0] +
-                    z * gR[2][1] - 2.0f * y * gR[2][2]);
-    dq[3] = 2.0f * (-2.0f * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0f * z * gR[1][1] +
-                    y * gR[1][2] + x * gR[2][0] + y * gR[2][1]);
-    const float qd = qn[0] * dq[0] + qn[1] * dq[1] + qn[2] * dq[2] + qn[3] * dq[3];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) g16[8 + k] += (dq[k] - qn[k] * qd) / qlen;
+    a.shin[g * 2u] = make_float4(dcol[0], dcol[1], dcol[2], (vdrew & 2u) ? 1.0f : 0.0f);
+    a.shin[g * 2u + 1u] = make_float4(dir[0], dir[1], dir[2], 0.0f);
   }
   if (seen) a.stats[i] = st;
-
-  // Adam with the step's constants (the first view's frame).
   const gs_frame_data& f0 = s_frames[0];
   const bool sparse = (f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u;
-  const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1];
-  if (!sparse || (drew & 1u)) {
-    float4 m0 = a.M[i], m1 = a.M[a.cap + i], m2 = a.M[2u * a.cap + i], m3 = a.M[3u * a.cap + i];
-    float4 v0 = a.V[i], v1 = a.V[a.cap + i], v2 = a.V[2u * a.cap + i], v3 = a.V[3u * a.cap + i];
-    const float lp = f0.lr0[0], ls = f0.lr0[1], lq = f0.lr0[2], lo = f0.lr0[3], ld = f0.lr1[0];
-    p0.x = adam1(p0.x, g16[0], m0.x, v0.x, lp, b1, b2, c1, c2, eps);
-    p0.y = adam1(p0.y, g16[1], m0.y, v0.y, lp, b1, b2, c1, c2, eps);
-    p0.z = adam1(p0.z, g16[2], m0.z, v0.z, lp, b1, b2, c1, c2, eps);
-    p0.w = adam1(p0.w, g16[3], m0.w, v0.w, lo, b1, b2, c1, c2, eps);
-    p1.x = adam1(p1.x, g16[4], m1.x, v1.x, ls, b1, b2, c1, c2, eps);
-    p1.y = adam1(p1.y, g16[5], m1.y, v1.y, ls, b1, b2, c1, c2, eps);
-    p1.z = adam1(p1.z, g16[6], m1.z, v1.z, ls, b1, b2, c1, c2, eps);
-    p1.w = adam1(p1.w, 0.0f, m1.w, v1.w, 0.0f, b1, b2, c1, c2, eps);
-    q.x = adam1(q.x, g16[8], m2.x, v2.x, lq, b1, b2, c1, c2, eps);
-    q.y = adam1(q.y, g16[9], m2.y, v2.y, lq, b1, b2, c1, c2, eps);
-    q.z = adam1(q.z, g16[10], m2.z, v2.z, lq, b1, b2, c1, c2, eps);
-    q.w = adam1(q.w, g16[11], m2.w, v2.w, lq, b1, b2, c1, c2, eps);
-    p3.x = adam1(p3.x, g16[12], m3.x, v3.x, ld, b1, b2, c1, c2, eps);
-    p3.y = adam1(p3.y, g16[13], m3.y, v3.y, ld, b1, b2, c1, c2, eps);
-    p3.z = adam1(p3.z, g16[14], m3.z, v3.z, ld, b1, b2, c1, c2, eps);
-    p3.w = adam1(p3.w, 0.0f, m3.w, v3.w, 0.0f, b1, b2, c1, c2, eps);
-    a.P[i] = p0;
-    a.P[a.cap + i] = p1;
-    a.P[2u * a.cap + i] = q;
-    a.P[3u * a.cap + i] = p3;
-    a.M[i] = m0;
-    a.M[a.cap + i] = m1;
-    a.M[2u * a.cap + i] = m2;
-    a.M[3u * a.cap + i] = m3;
-    a.V[i] = v0;
-    a.V[a.cap + i] = v1;
-    a.V[2u * a.cap + i] = v2;
-    a.V[3u * a.cap + i] = v3;
+  if (!sparse || (drew & 1u)) adam_params(a, f0, i, p0, p1, q, p3, g16);
+}
+
+// Part 2 (train_step_sh.comp:21-44): one thread per (SH coefficient, slot), consecutive
+// slots on consecutive threads, the views' colour gradients summed. Splitting the SH
+// update off the geometry keeps each thread's chain of dependent loads short, so both
+// kernels keep many loads in flight (the fused form was latency-bound).
+template <int DEG>
+__global__ void __launch_bounds__(256) k_step_sh(StepArgs a, const uint32_t* n_views_ptr) {
+  (void)n_views_ptr;
+  if (*a.d_pairs > a.accept) return;
+  constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t k = idx / a.slots, i = idx - k * a.slots;
+  if (k >= uint32_t(K)) return;
+  if (a.P[a.cap + i].w < 0.5f) return;
+  float g[3] = {0.f, 0.f, 0.f};
+  bool colour = false;
+  for (uint32_t v = 0; v < a.n_views; ++v) {
+    const size_t gi = size_t(v) * a.cap + i;
+    if (a.tiles[gi] == 0u) continue;
+    const float4 c = a.shin[gi * 2u];
+    const float4 d = a.shin[gi * 2u + 1u];
+    float basis[16];
+    sh_basis<DEG>(d.x, d.y, d.z, basis);
+    const float b = basis[k + 1];
+    g[0] += b * c.x;
+    g[1] += b * c.y;
+    g[2] += b * c.z;
+    colour |= c.w != 0.0f;
   }
-  if constexpr (K > 0) {
-    // train_step_sh.comp:34-35: with sparse Adam, a zero colour gradient keeps the SH.
-    if (!sparse || (drew & 2u)) {
-      const float lr = f0.lr1[1];
+  const gs_frame_data& f0 = a.frames[0];
+  if ((f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u && !colour) return;
+  const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1], lr = f0.lr1[1];
 #pragma unroll
-      for (int k = 0; k < 3 * K; ++k) {
-        const size_t o = size_t(k) * a.cap + i;
-        float m = a.MSH[o], v = a.VSH[o];
-        a.SH[o] = adam1(a.SH[o], gsh[k], m, v, lr, b1, b2, c1, c2, eps);
-        a.MSH[o] = m;
-        a.VSH[o] = v;
-      }
-    }
+  for (int c = 0; c < 3; ++c) {
+    const size_t o = size_t(3 * k + c) * a.cap + i;
+    float m = a.MSH[o], v = a.VSH[o];
+    a.SH[o] = adam1(a.SH[o], g[c], m, v, lr, b1, b2, c1, c2, eps);
+    a.MSH[o] = m;
+    a.VSH[o] = v;
   }
 }
 
@@ -491,13 +592,15 @@ void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const 
                  const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
   if (m.slots == 0u) return;
   StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
-             vb.splat, vb.tiles, vb.grad2d, d_pairs, accept};
+             vb.splat, vb.tiles, vb.grad2d, vb.shin, d_pairs, accept};
   const dim3 grid((m.slots + 127u) / 128u), block(128);
+  const int K = sh_rest_coeffs(degree);
+  const dim3 sh_grid(uint32_t((uint64_t(m.slots) * uint64_t(K > 0 ? K : 1) + 255u) / 256u));
   switch (degree) {
-    case 0: k_step<0><<<grid, block, 0, st>>>(a); break;
-    case 1: k_step<1><<<grid, block, 0, st>>>(a); break;
-    case 2: k_step<2><<<grid, block, 0, st>>>(a); break;
-    default: k_step<3><<<grid, block, 0, st>>>(a); break;
+    case 0: k_step_geometry<0><<<grid, block, 0, st>>>(a); break;
+    case 1: k_step_geometry<1><<<grid, block, 0, st>>>(a); k_step_sh<1><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
+    case 2: k_step_geometry<2><<<grid, block, 0, st>>>(a); k_step_sh<2><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
+    default: k_step_geometry<3><<<grid, block, 0, st>>>(a); k_step_sh<3><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
   }
 }
 

@@ -276,6 +276,7 @@ def test_densify_masks_match_oracle(ctx):
     ds = S.make_test_dataset(64, 48, 1, False, 5)
     scene = S.make_test_scene(200, 1, 3)
     scene.params[::7, 3] = -6.0  # some below the prune opacity
+    scene.params[1::3, 4:7] = np.log(0.02)  # some small enough to clone (percent_dense x extent = 0.033)
     opt = F.scaled_options(100)
     opt.sh_degree = 1
     opt.densify_grad_threshold = 2e-5
