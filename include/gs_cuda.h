@@ -120,6 +120,8 @@ typedef struct gs_tuning {
   uint32_t forward_pixels;    /* pixels per thread in the forward pass: 1, 2 or 4 (0: default) */
   uint32_t backward_pixels;   /* pixels per thread in the backward pass: 1, 2 or 4 (0: default) */
   uint32_t retry;             /* 1 (default): grow the pair buffers and run again on overflow */
+  uint32_t graph;             /* 1: capture the step as a CUDA graph and replay it while its launch
+                                 structure (views, slots, buffer sizes, SH degree, mode) holds */
 } gs_tuning;
 
 typedef struct gs_model_info {
@@ -152,8 +154,18 @@ int gs_model_moments(gs_context* ctx, float* m16, float* v16, float* m_sh, float
 
 /* The views of the next step: one FrameData each, with its own resolution, and each
    view's target image (RGBA8, width x height x 4 bytes; NULL: no loss). Replaces
-   Trainer::write_frame's host-visible uploads (trainer.cpp:440-547, 1024-1031). */
+   Trainer::write_frame's host-visible uploads (trainer.cpp:440-547, 1024-1031). The
+   targets are copied asynchronously on the context's stream: their buffers must stay
+   unchanged until the next gs_step returns (pinned memory is copied by DMA). */
 int gs_set_views(gs_context* ctx, uint32_t n_views, const gs_frame_data* frames, const uint8_t* const* rgba_targets);
+
+/* Target images kept in HBM across steps (the dataset's views): n_images RGBA8 images of
+   widths[i] x heights[i]. Replaces the per-step target uploads of Trainer::run_batch
+   (trainer.cpp:1024-1031) for callers that train on a fixed dataset. */
+int gs_dataset_set(gs_context* ctx, uint32_t n_images, const uint32_t* widths, const uint32_t* heights,
+                   const uint8_t* const* rgba);
+/* As gs_set_views, with view v's target the dataset image images[v] (same size). */
+int gs_set_views_dataset(gs_context* ctx, uint32_t n_views, const gs_frame_data* frames, const uint32_t* images);
 
 #define GS_STEP_TRAIN 1u   /* backward pass and Adam (else: forward and loss only) */
 #define GS_STEP_PROFILE 2u /* time each pass with CUDA events (pass_ms) */

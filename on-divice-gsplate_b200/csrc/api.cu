@@ -74,14 +74,24 @@ struct gs_context {
   bool profile = false;
   gsk::Model model;
   gs_tuning tuning{};
-  // views of the step
+  int sm_count = 148;
+  // views of the step: host copies, and the step table uploaded each step
   uint32_t n_views = 0;
   std::vector<gs_frame_data> frames;
-  gs_frame_data* d_frames = nullptr;
-  gs_frame_data* h_frames = nullptr;  // pinned
   gsk::ViewTable vt{};
   uint32_t total_tiles = 0, total_pixels = 0;
   bool has_target = false;
+  gsk::StepTable* d_table = nullptr;
+  gsk::StepTable* h_table = nullptr;  // pinned
+  uint32_t* d_queue = nullptr;        // work-queue counters
+  // targets kept in HBM across steps (gs_dataset_set)
+  uint32_t* d_dataset = nullptr;
+  std::vector<size_t> ds_offset;
+  std::vector<uint32_t> ds_width, ds_height;
+  // the step captured as a CUDA graph
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uint64_t> graph_key;
+  int graph_launches = 0;
   // (view, slot) buffers
   uint32_t vb_views = 0;
   gsk::ViewBuffers vb;
@@ -132,13 +142,16 @@ struct gs_context {
                          &dens.counters})
       dev_free(*p);
     dev_free(ranges);
-    dev_free(d_frames);
+    dev_free(d_table);
+    dev_free(d_queue);
+    dev_free(d_dataset);
     dev_free(d_view_sums);
     dev_free(sort.scan_lookback);
-    if (h_frames) cudaFreeHost(h_frames);
+    drop_graph();
+    if (h_table) cudaFreeHost(h_table);
     if (h_scalars) cudaFreeHost(h_scalars);
     if (h_view_sums) cudaFreeHost(h_view_sums);
-    h_frames = nullptr;
+    h_table = nullptr;
     h_scalars = nullptr;
     h_view_sums = nullptr;
     if (ev0) cudaEventDestroy(ev0);
@@ -152,6 +165,12 @@ struct gs_context {
     stream = nullptr;
   }
 
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    graph_key.clear();
+  }
+
   void check_launch(const char* what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(GS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -160,6 +179,7 @@ struct gs_context {
   // (view, slot) buffers for `views` views of `cap` slots.
   void reserve_views(uint32_t views) {
     if (views <= vb_views) return;
+    drop_graph();
     const size_t n = size_t(views) * model.cap;
     dev_alloc(vb.splat, n * 3);
     dev_alloc(vb.foot, n);
@@ -187,6 +207,7 @@ struct gs_context {
   }
 
   void reserve_pixels(size_t pixels, size_t tiles) {
+    if (pixels > pixel_cap || tiles + 1 > tile_cap) drop_graph();
     if (pixels > pixel_cap) {
       dev_alloc(target, pixels);
       dev_alloc(pixel_grad, pixels);
@@ -211,6 +232,7 @@ struct gs_context {
     if (expected > kMaxPairs) fail(GS_ERR_CAPACITY, "more tile-gaussian pairs than the pair buffers can hold (" +
                                                         std::to_string(expected) + ")");
     const uint64_t n = std::min<uint64_t>(kMaxPairs, std::max<uint64_t>(wanted + wanted / 4, tuning.min_pair_capacity));
+    drop_graph();
     dev_alloc(keys, n);
     dev_alloc(values, n);
     dev_alloc(keys_alt, n);
@@ -225,11 +247,62 @@ struct gs_context {
     pair_cap = n;
   }
 
+  // Milliseconds between two recorded events (0 if they cannot be timed).
+  static float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+      (void)cudaGetLastError();
+      ms = 0.0f;
+    }
+    return ms;
+  }
+
   void mark(int k) {
     if (profile) GS_CUDA_TRY(cudaEventRecord(marks[k], stream));
   }
 
-  void run_step(bool train, gs_step_result* out) {
+  // Everything one step puts on the stream: the step table upload, the queue reset, the
+  // launch sequence and the readback of the pair count and loss sums.
+  void enqueue_step(bool train, uint32_t degree) {
+    GS_CUDA_TRY(cudaMemcpyAsync(d_table, h_table, sizeof(gsk::StepTable), cudaMemcpyHostToDevice, stream));
+    GS_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(uint32_t) * gsk::kQueueCount, stream));
+    record(train, degree);
+    GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * 8 * n_views, cudaMemcpyDeviceToHost,
+                                stream));
+  }
+
+  // The step as a CUDA graph: captured once per launch structure (views, slots, buffer
+  // sizes, SH degree, mode, tuning), replayed while only the step table changes.
+  void launch_graph(bool train, uint32_t degree) {
+    const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
+    const std::vector<uint64_t> key = {n_views, model.slots, model.cap, pair_cap, tile_cap, pixel_cap, degree,
+                                       train ? 1u : 0u, ssim ? 1u : 0u, tuning.deterministic,
+                                       tuning.forward_pixels, tuning.backward_pixels};
+    if (graph_exec == nullptr || key != graph_key) {
+      drop_graph();
+      cudaGraph_t g = nullptr;
+      GS_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      launches = 0;
+      try {
+        enqueue_step(train, degree);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      GS_CUDA_TRY(cudaStreamEndCapture(stream, &g));
+      const cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+      cudaGraphDestroy(g);
+      GS_CUDA_TRY(e);
+      graph_key = key;
+      graph_launches = launches;
+    }
+    launches = graph_launches;
+    GS_CUDA_TRY(cudaGraphLaunch(graph_exec, stream));
+  }
+
+  void run_step(bool train, gs_step_result* out, bool allow_graph = true) {
     if (n_views == 0) fail(GS_ERR_INVALID, "gs_step: no views (gs_set_views first)");
     if (train && !has_target) fail(GS_ERR_INVALID, "gs_step: training needs target images");
     const uint32_t degree = frames[0].model[1];
@@ -239,21 +312,24 @@ struct gs_context {
                              : tuning.initial_pairs ? tuning.initial_pairs
                                                     : uint64_t(model.slots) * 4u * n_views;
       reserve_pairs(guess);
+      h_table->vt = vt;
       for (uint32_t v = 0; v < n_views; ++v) {
-        h_frames[v] = frames[v];
-        h_frames[v].model[0] = model.slots;
-        h_frames[v].model[2] = model.sh_stride;
-        h_frames[v].limits[0] = uint32_t(pair_cap);
-        h_frames[v].limits[3] = uint32_t(pair_cap);
+        gs_frame_data& f = h_table->frames[v];
+        f = frames[v];
+        f.model[0] = model.slots;
+        f.model[2] = model.sh_stride;
+        f.limits[0] = uint32_t(pair_cap);
+        f.limits[3] = uint32_t(pair_cap);
       }
-      GS_CUDA_TRY(cudaMemcpyAsync(d_frames, h_frames, sizeof(gs_frame_data) * n_views, cudaMemcpyHostToDevice, stream));
       GS_CUDA_TRY(cudaEventRecord(ev0, stream));
-      launches = 0;
-      record(train, degree);
+      // A profiled step runs directly: its pass events must be recorded by the stream.
+      if (tuning.graph && allow_graph && !profile) {
+        launch_graph(train, degree);
+      } else {
+        launches = 0;
+        enqueue_step(train, degree);
+      }
       GS_CUDA_TRY(cudaEventRecord(ev1, stream));
-      GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-      GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * 8 * n_views, cudaMemcpyDeviceToHost,
-                                  stream));
       GS_CUDA_TRY(cudaStreamSynchronize(stream));
       check_launch("step");
       uint32_t err = 0;
@@ -277,22 +353,13 @@ struct gs_context {
         out->overflow = overflow ? 1u : 0u;
         out->retries = retries;
         out->tile_mismatch = h_scalars[1];
-        // Pairs per view: the emitted offsets are global; per-view counts come from the
-        // per-view tile sums, summed on the host.
         view_pairs(out->pairs);
         for (uint32_t v = 0; v < n_views; ++v)
           for (int k = 0; k < 8; ++k) out->losses[v][k] = h_view_sums[v * 8 + k];
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev0, ev1);
-        out->gpu_ms = ms;
+        out->gpu_ms = elapsed(ev0, ev1);
         out->kernels = uint32_t(launches);
-        if (profile) {
-          for (int k = 0; k < 6; ++k) {
-            float t = 0.f;
-            if (train || k < 4) cudaEventElapsedTime(&t, marks[k], marks[k + 1]);
-            out->pass_ms[k] = t;
-          }
-        }
+        if (profile)
+          for (int k = 0; k < 6; ++k) out->pass_ms[k] = (train || k < 4) ? elapsed(marks[k], marks[k + 1]) : 0.0f;
       }
       return;
     }
@@ -319,11 +386,12 @@ struct gs_context {
 
   gsk::StepPointers step_pointers() const {
     gsk::StepPointers sp;
-    sp.frames = d_frames;
-    sp.vt = vt;
+    sp.frames = d_table->frames;
+    sp.vt = &d_table->vt;
     sp.n_views = n_views;
-    sp.total_tiles = total_tiles;
-    sp.total_pixels = total_pixels;
+    sp.tile_cap = tile_cap > 0 ? uint32_t(tile_cap - 1) : 0u;
+    sp.queue = d_queue;
+    sp.sm_count = sm_count;
     return sp;
   }
 
@@ -332,7 +400,6 @@ struct gs_context {
     rb.ranges = ranges;
     rb.values = sorted_values;
     rb.pair_gaussian = pair_gaussian;
-    rb.target = has_target ? target : nullptr;
     rb.pixel_grad = pixel_grad;
     rb.pixel_out = pixel_out;
     rb.pixel_count = pixel_count;
@@ -365,12 +432,13 @@ struct gs_context {
     gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, uint32_t(pair_cap), keys, values,
                      pair_gaussian, pair_grads, d_scalars + 1, stream);
     launches += items ? 1 : 0;
-    const int tile_bits = int(bits_for(total_tiles + 1));
+    const uint32_t max_tiles = uint32_t(tile_cap - 1);
+    const int tile_bits = int(bits_for(max_tiles + 1));
     const bool pairs_alt = gsk::radix_sort_pairs(sort, keys, values, keys_alt, values_alt, d_scalars,
                                                  uint32_t(pair_cap), std::max(tile_bits, 1), stream, &launches);
     sorted_keys = pairs_alt ? keys_alt : keys;
     sorted_values = pairs_alt ? values_alt : values;
-    GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (total_tiles + 1), stream));
+    GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (max_tiles + 1), stream));
     gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, stream);
     ++launches;
     mark(2);
@@ -406,49 +474,86 @@ struct gs_context {
     check_launch("launch");
   }
 
-  void set_views(uint32_t n, const gs_frame_data* fr, const uint8_t* const* targets) {
+  // The views of the next step. Targets come from host images (copied into the step's
+  // target buffer) or from images already in HBM (`images`: dataset indices), or neither.
+  void set_views(uint32_t n, const gs_frame_data* fr, const uint8_t* const* targets, const uint32_t* images) {
     if (n == 0 || n > GS_MAX_VIEWS) fail(GS_ERR_INVALID, "gs_set_views: 1 to 16 views");
     if (model.cap == 0) fail(GS_ERR_INVALID, "gs_set_views: no model (gs_model_init first)");
-    frames.assign(fr, fr + n);
+    std::vector<gs_frame_data> next(fr, fr + n);
     gsk::ViewTable t{};
     t.n_views = n;
     uint64_t tiles = 0, pixels = 0;
     for (uint32_t v = 0; v < n; ++v) {
-      gs_frame_data& f = frames[v];
+      gs_frame_data& f = next[v];
       const uint32_t w = f.image[0], h = f.image[1];
       if (w == 0 || h == 0) fail(GS_ERR_INVALID, "gs_set_views: empty image");
       f.image[2] = (w + gsk::kTile - 1) / gsk::kTile;
       f.image[3] = (h + gsk::kTile - 1) / gsk::kTile;
       if (f.model[1] > 3u || gsk::sh_rest_coeffs(f.model[1]) * 3u > model.sh_stride)
         fail(GS_ERR_INVALID, "gs_set_views: active SH degree beyond the model's SH storage");
-      if (v > 0 && f.model[1] != frames[0].model[1])
+      if (v > 0 && f.model[1] != next[0].model[1])
         fail(GS_ERR_INVALID, "gs_set_views: the views of a step share the active SH degree");
+      if (images != nullptr) {
+        if (images[v] >= ds_width.size()) fail(GS_ERR_INVALID, "gs_set_views_dataset: no such image");
+        if (ds_width[images[v]] != w || ds_height[images[v]] != h)
+          fail(GS_ERR_INVALID, "gs_set_views_dataset: image size differs from the view's");
+      }
       t.tile_base[v] = uint32_t(tiles);
       t.pixel_base[v] = uint32_t(pixels);
       tiles += uint64_t(f.image[2]) * f.image[3];
       pixels += uint64_t(w) * h;
     }
-    t.tile_base[n] = uint32_t(tiles);
-    t.pixel_base[n] = uint32_t(pixels);
     if (tiles >= (1ull << 24) || pixels >= (1ull << 31)) fail(GS_ERR_INVALID, "gs_set_views: images too large");
-    for (uint32_t v = n + 1; v <= GS_MAX_VIEWS; ++v) {
-      t.tile_base[v] = t.tile_base[n];
-      t.pixel_base[v] = t.pixel_base[n];
+    for (uint32_t v = n; v <= GS_MAX_VIEWS; ++v) {
+      t.tile_base[v] = uint32_t(tiles);
+      t.pixel_base[v] = uint32_t(pixels);
     }
+    t.total_tiles = uint32_t(tiles);
+    t.total_pixels = uint32_t(pixels);
+    if (targets != nullptr)
+      for (uint32_t v = 0; v < n; ++v)
+        if (targets[v] == nullptr) fail(GS_ERR_INVALID, "gs_set_views: missing target image");
     reserve_views(n);
     reserve_pixels(pixels, tiles);
-    vt = t;
-    n_views = n;
-    total_tiles = uint32_t(tiles);
-    total_pixels = uint32_t(pixels);
-    has_target = targets != nullptr;
-    if (targets) {
-      for (uint32_t v = 0; v < n; ++v) {
-        if (targets[v] == nullptr) fail(GS_ERR_INVALID, "gs_set_views: missing target image");
-        const size_t bytes = size_t(frames[v].image[0]) * frames[v].image[1] * 4;
+    for (uint32_t v = 0; v < n; ++v) {
+      if (targets != nullptr) {
+        t.target[v] = target + t.pixel_base[v];
+        const size_t bytes = size_t(next[v].image[0]) * next[v].image[1] * 4;
         GS_CUDA_TRY(cudaMemcpyAsync(target + t.pixel_base[v], targets[v], bytes, cudaMemcpyHostToDevice, stream));
+      } else if (images != nullptr) {
+        t.target[v] = d_dataset + ds_offset[images[v]];
       }
     }
+    frames = std::move(next);
+    vt = t;
+    n_views = n;
+    total_tiles = t.total_tiles;
+    total_pixels = t.total_pixels;
+    has_target = targets != nullptr || images != nullptr;
+  }
+
+  void set_dataset(uint32_t n, const uint32_t* widths, const uint32_t* heights, const uint8_t* const* rgba) {
+    size_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      if (widths[i] == 0 || heights[i] == 0 || rgba[i] == nullptr) fail(GS_ERR_INVALID, "gs_dataset_set: empty image");
+      total += size_t(widths[i]) * heights[i];
+    }
+    GS_CUDA_TRY(cudaStreamSynchronize(stream));
+    drop_graph();
+    ds_offset.assign(n, 0);
+    ds_width.assign(widths, widths + n);
+    ds_height.assign(heights, heights + n);
+    dev_alloc(d_dataset, total);
+    size_t off = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      ds_offset[i] = off;
+      GS_CUDA_TRY(cudaMemcpyAsync(d_dataset + off, rgba[i], size_t(widths[i]) * heights[i] * 4,
+                                  cudaMemcpyHostToDevice, stream));
+      off += size_t(widths[i]) * heights[i];
+    }
+    GS_CUDA_TRY(cudaStreamSynchronize(stream));
+    // Views that pointed at the old dataset must be set again.
+    if (has_target && n_views > 0) n_views = 0;
   }
 };
 
@@ -553,15 +658,19 @@ int gs_create(int device, gs_context** out) {
     c->tuning.forward_pixels = 2u;
     c->tuning.backward_pixels = 2u;
     c->tuning.retry = 1u;
+    c->tuning.graph = 0u;
     try {
       GS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
       GS_CUDA_TRY(cudaEventCreate(&c->ev0));
       GS_CUDA_TRY(cudaEventCreate(&c->ev1));
       for (cudaEvent_t& e : c->marks) GS_CUDA_TRY(cudaEventCreate(&e));
-      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_frames), sizeof(gs_frame_data) * GS_MAX_VIEWS));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_table), sizeof(gsk::StepTable)));
+      std::memset(c->h_table, 0, sizeof(gsk::StepTable));
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), 4 * sizeof(uint32_t)));
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_view_sums), 8 * sizeof(double) * GS_MAX_VIEWS));
-      dev_alloc(c->d_frames, GS_MAX_VIEWS);
+      dev_alloc(c->d_table, 1);
+      dev_alloc(c->d_queue, gsk::kQueueCount);
+      c->sm_count = prop.multiProcessorCount;
       dev_alloc(c->d_scalars, 4);
       dev_alloc(c->d_view_sums, 8 * GS_MAX_VIEWS);
       dev_alloc(c->sort.hist, 4 * 256);
@@ -591,6 +700,7 @@ int gs_model_init(gs_context* c, uint32_t capacity, uint32_t sh_stride, const fl
     if (count > 0 && sh_stride > 0 && sh == nullptr) fail(GS_ERR_INVALID, "gs_model_init: null sh");
     GS_CUDA_TRY(cudaSetDevice(c->device));
     GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->drop_graph();
     gsk::Model& m = c->model;
     dev_free(m.P);
     dev_free(m.M);
@@ -704,7 +814,25 @@ int gs_set_views(gs_context* c, uint32_t n_views, const gs_frame_data* frames, c
   return guarded([&] {
     if (c == nullptr || frames == nullptr) fail(GS_ERR_INVALID, "gs_set_views: null argument");
     GS_CUDA_TRY(cudaSetDevice(c->device));
-    c->set_views(n_views, frames, rgba_targets);
+    c->set_views(n_views, frames, rgba_targets, nullptr);
+  });
+}
+
+int gs_dataset_set(gs_context* c, uint32_t n_images, const uint32_t* widths, const uint32_t* heights,
+                   const uint8_t* const* rgba) {
+  return guarded([&] {
+    if (c == nullptr || (n_images > 0 && (widths == nullptr || heights == nullptr || rgba == nullptr)))
+      fail(GS_ERR_INVALID, "gs_dataset_set: null argument");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    c->set_dataset(n_images, widths, heights, rgba);
+  });
+}
+
+int gs_set_views_dataset(gs_context* c, uint32_t n_views, const gs_frame_data* frames, const uint32_t* images) {
+  return guarded([&] {
+    if (c == nullptr || frames == nullptr || images == nullptr) fail(GS_ERR_INVALID, "gs_set_views_dataset: null argument");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    c->set_views(n_views, frames, nullptr, images);
   });
 }
 
@@ -724,9 +852,9 @@ int gs_render(gs_context* c, const gs_frame_data* frame, uint8_t* rgba_out) {
     GS_CUDA_TRY(cudaSetDevice(c->device));
     gs_frame_data f = *frame;
     f.model[3] &= ~GS_FLAG_SSIM;
-    c->set_views(1, &f, nullptr);
+    c->set_views(1, &f, nullptr, nullptr);
     c->profile = false;
-    c->run_step(false, nullptr);
+    c->run_step(false, nullptr, false);
     GS_CUDA_TRY(cudaMemcpy(rgba_out, c->image, size_t(f.image[0]) * f.image[1] * 4, cudaMemcpyDeviceToHost));
   });
 }
@@ -738,11 +866,13 @@ int gs_densify(gs_context* c, const gs_frame_data* frame, uint32_t counters_out[
     gs_frame_data f = *frame;
     f.model[0] = c->model.slots;
     f.model[2] = c->model.sh_stride;
-    *c->h_frames = f;
-    GS_CUDA_TRY(cudaMemcpyAsync(c->d_frames, c->h_frames, sizeof(gs_frame_data), cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->h_table->frames[0] = f;
+    GS_CUDA_TRY(cudaMemcpyAsync(c->d_table->frames, c->h_table->frames, sizeof(gs_frame_data), cudaMemcpyHostToDevice,
+                                c->stream));
     int launches = 0;
     c->densify_slots = c->model.slots;
-    gsk::launch_densify(c->d_frames, c->model, c->dens, c->sort, c->stream, &launches);
+    gsk::launch_densify(c->d_table->frames, c->model, c->dens, c->sort, c->stream, &launches);
     uint32_t counters[4] = {0, 0, 0, 0};
     GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
     GS_CUDA_TRY(cudaMemcpy(counters, c->dens.counters, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -750,7 +880,10 @@ int gs_densify(gs_context* c, const gs_frame_data* frame, uint32_t counters_out[
     const uint32_t free_slots = counters[0], spawned = counters[1];
     const uint32_t room = free_slots + (c->model.cap - c->model.slots);
     const uint32_t placed = std::min(spawned, room);
-    if (placed > free_slots) c->model.slots += placed - free_slots;
+    if (placed > free_slots) {
+      c->model.slots += placed - free_slots;
+      c->drop_graph();
+    }
     counters[3] = c->model.slots;
     if (counters_out) std::memcpy(counters_out, counters, sizeof(counters));
   });
@@ -879,6 +1012,7 @@ int gs_set_tuning(gs_context* c, const gs_tuning* t) {
         fail(GS_ERR_INVALID, "gs_set_tuning: pixels per thread must be 1, 2 or 4");
     c->tuning = *t;
     if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
+    c->drop_graph();
   });
 }
 

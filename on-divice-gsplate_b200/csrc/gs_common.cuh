@@ -26,15 +26,28 @@ constexpr float kMinTransmittance = 1e-4f;
 constexpr uint32_t kMaxViews = GS_MAX_VIEWS;
 
 // Views of one step, laid out for the flattened (view, tile) and (view, pixel) spaces.
+// Lives in device memory (uploaded with the views' FrameData each step), so the step's
+// launches do not change when the views do and the step can be replayed as a CUDA graph.
 struct ViewTable {
   uint32_t n_views;
+  uint32_t total_tiles;
+  uint32_t total_pixels;
+  uint32_t pad;
   uint32_t tile_base[kMaxViews + 1];   // global tile index of each view's tile 0
   uint32_t pixel_base[kMaxViews + 1];  // global pixel index of each view's pixel 0
+  const uint32_t* target[kMaxViews];   // each view's RGBA8 target (width x height), or null
 };
 
-__device__ __forceinline__ uint32_t view_of_tile(const ViewTable& vt, uint32_t gtile) {
+// What one step uploads: the view table and each view's FrameData.
+struct StepTable {
+  ViewTable vt;
+  gs_frame_data frames[kMaxViews];
+};
+
+__device__ __forceinline__ uint32_t view_of_tile(const ViewTable* vt, uint32_t gtile) {
+  const uint32_t n = vt->n_views;
   uint32_t v = 0;
-  while (v + 1 < vt.n_views && gtile >= vt.tile_base[v + 1]) ++v;
+  while (v + 1 < n && gtile >= vt->tile_base[v + 1]) ++v;
   return v;
 }
 

@@ -36,9 +36,12 @@ struct ViewBuffers {
 };
 
 struct StepPointers {
-  const gs_frame_data* frames = nullptr;  // device copy, n_views entries
-  ViewTable vt{};
-  uint32_t n_views = 0, total_tiles = 0, total_pixels = 0;
+  const gs_frame_data* frames = nullptr;  // device: the step table's FrameData, n_views entries
+  const ViewTable* vt = nullptr;          // device: the step table's view layout
+  uint32_t n_views = 0;                   // fixed for a captured step
+  uint32_t tile_cap = 0;                  // grids of per-tile kernels (>= any step's tiles)
+  uint32_t* queue = nullptr;              // device work-queue counters, zeroed each step
+  int sm_count = 148;
 };
 
 // ---- project.cu ----
@@ -77,7 +80,6 @@ struct RasterBuffers {
   const uint2* ranges = nullptr;
   const uint32_t* values = nullptr;         // pre-sort pair index per sorted pair
   const uint32_t* pair_gaussian = nullptr;  // g per pre-sort pair
-  const uint32_t* target = nullptr;         // RGBA8 per global pixel (nullptr: no loss)
   float4* pixel_grad = nullptr;             // dL/dC rgb, final T
   float4* pixel_out = nullptr;              // rendered colour rgb (over the background), loss weight
   uint32_t* pixel_count = nullptr;
@@ -118,6 +120,9 @@ struct DensifyScratch {
 void launch_densify(const gs_frame_data* d_frame, const Model& m, const DensifyScratch& ds, const SortScratch& ss,
                     cudaStream_t st, int* launches);
 void launch_reset_opacity(const Model& m, float max_logit, cudaStream_t st);
+
+// Work-queue counters (StepPointers::queue).
+constexpr int kQueueForward = 0, kQueueBackward = 1, kQueueCount = 4;
 
 // ---- layout conversions (api.cu) ----
 void launch_params_to_planes(const float* params16, const float* sh, uint32_t count, const Model& m, cudaStream_t st);

@@ -19,7 +19,7 @@ __constant__ float c_window[11] = {0.001028380f, 0.007598758f, 0.036000772f, 0.1
 
 struct LossArgs {
   const gs_frame_data* frames;
-  ViewTable vt;
+  const ViewTable* vt;
   RasterBuffers rb;
 };
 
@@ -44,7 +44,7 @@ __device__ bool background_only(const LossArgs& a, const gs_frame_data& f, uint3
     for (int dx = -1; dx <= 1; ++dx) {
       const int nx = tx + dx, ny = ty + dy;
       if (nx < 0 || ny < 0 || nx >= int(f.image[2]) || ny >= int(f.image[3])) continue;
-      const uint32_t t = a.vt.tile_base[v] + uint32_t(ny) * f.image[2] + uint32_t(nx);
+      const uint32_t t = a.vt->tile_base[v] + uint32_t(ny) * f.image[2] + uint32_t(nx);
       const uint2 r = a.rb.ranges[t];
       if (r.y > r.x || a.rb.tile_loss[size_t(t) * 16u + 15u] > 0.0f) return false;
     }
@@ -57,10 +57,13 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   __shared__ float s_h[5][kWin * kTile];
   __shared__ float s_sum[8][2];
   const uint32_t gt = blockIdx.x;
+  if (gt >= a.vt->total_tiles) return;
   const uint32_t v = view_of_tile(a.vt, gt);
   const gs_frame_data& f = a.frames[v];
+  const uint32_t* target = a.vt->target[v];
+  if (target == nullptr) return;
   const uint32_t W = f.image[0], H = f.image[1];
-  const uint32_t t = gt - a.vt.tile_base[v];
+  const uint32_t t = gt - a.vt->tile_base[v];
   const int tx = int(t % f.image[2]), ty = int(t / f.image[2]);
   const uint32_t lid = threadIdx.x;
   if (background_only(a, f, v, tx, ty)) {
@@ -72,17 +75,17 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
     }
     return;
   }
-  const size_t pbase = a.vt.pixel_base[v];
+  const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
   for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
     const int gx = ox + int(e % kWin), gy = oy + int(e / kWin);
     const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
     float3 x = make_float3(0.f, 0.f, 0.f), y = x;
     if (in) {
-      const size_t pix = pbase + size_t(gy) * W + size_t(gx);
-      const float4 o = a.rb.pixel_out[pix];
+      const size_t local = size_t(gy) * W + size_t(gx);
+      const float4 o = a.rb.pixel_out[pbase + local];
       x = make_float3(o.x, o.y, o.z);
-      y = target_colour(f, a.rb.target[pix]);
+      y = target_colour(f, target[local]);
     }
     s_x[0][e] = x.x; s_x[1][e] = x.y; s_x[2][e] = x.z;
     s_y[0][e] = y.x; s_y[1][e] = y.y; s_y[2][e] = y.z;
@@ -169,16 +172,19 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   __shared__ float s_m[3][kWin * kWin];
   __shared__ float s_h[3][kWin * kTile];
   const uint32_t gt = blockIdx.x;
+  if (gt >= a.vt->total_tiles) return;
   const uint32_t v = view_of_tile(a.vt, gt);
   const gs_frame_data& f = a.frames[v];
+  const uint32_t* target = a.vt->target[v];
+  if (target == nullptr) return;
   // Without splats in the tile nothing reads its pixels' gradients (masked targets).
   const uint2 own = a.rb.ranges[gt];
   if ((f.model[3] & GS_FLAG_MASKED_TARGET) != 0u && own.y <= own.x) return;
   const uint32_t W = f.image[0], H = f.image[1];
-  const uint32_t t = gt - a.vt.tile_base[v];
+  const uint32_t t = gt - a.vt->tile_base[v];
   const int tx = int(t % f.image[2]), ty = int(t / f.image[2]);
   const uint32_t lid = threadIdx.x;
-  const size_t pbase = a.vt.pixel_base[v];
+  const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
   const uint32_t lx = lid % kTile, ly = lid / kTile;
   const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
@@ -188,7 +194,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   if (inside) {
     const float4 o = a.rb.pixel_out[pix];
     x = make_float3(o.x, o.y, o.z);
-    y = target_colour(f, a.rb.target[pix]);
+    y = target_colour(f, target[size_t(py) * W + px]);
   }
   float ds[3];
   for (int c = 0; c < 3; ++c) {
@@ -240,12 +246,13 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_loss_reduce(ViewTable vt, const float* __restrict__ tile_loss,
+__global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const float* __restrict__ tile_loss,
                                                      double* __restrict__ view_sums) {
   __shared__ double s[8][8];
   const uint32_t v = blockIdx.x;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (uint32_t t = vt.tile_base[v] + threadIdx.x; t < vt.tile_base[v + 1]; t += 256u)
+  const uint32_t t0 = vt->tile_base[v], t1 = vt->tile_base[v + 1];
+  for (uint32_t t = t0 + threadIdx.x; t < t1; t += 256u)
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] += double(tile_loss[size_t(t) * 16u + k]);
 #pragma unroll
@@ -266,13 +273,13 @@ __global__ void __launch_bounds__(256) k_loss_reduce(ViewTable vt, const float* 
 }  // namespace
 
 void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st) {
-  if (sp.total_tiles == 0u) return;
-  k_ssim<<<sp.total_tiles, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
+  if (sp.tile_cap == 0u) return;
+  k_ssim<<<sp.tile_cap, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
 }
 
 void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st) {
-  if (sp.total_tiles == 0u) return;
-  k_ssim_grad<<<sp.total_tiles, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
+  if (sp.tile_cap == 0u) return;
+  k_ssim_grad<<<sp.tile_cap, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
 }
 
 void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, cudaStream_t st) {

@@ -14,8 +14,8 @@ namespace {
 
 struct EmitArgs {
   const gs_frame_data* frames;
-  ViewTable vt;
-  uint32_t cap, n_items, pair_capacity, pad_tile;
+  const ViewTable* vt;
+  uint32_t cap, n_items, pair_capacity;
   const uint32_t* sorted_vals;
   const uint32_t* sorted_offsets;
   const float4* splat;
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   uint32_t p = a.sorted_offsets[k];
   a.offsets[g] = p;
   const uint32_t end = min(p + count, a.pair_capacity);
-  const uint32_t tile_base = a.vt.tile_base[v];
+  const uint32_t tile_base = a.vt->tile_base[v];
   const uint32_t width = f.image[0], height = f.image[1], tiles_x = f.image[2];
   uint32_t wanted = 0u;
   const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
@@ -62,8 +62,9 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   // The count and the walk disagree (never expected: same inputs, same arithmetic).
   // Pad the rest into the unused tile after the last one, with zero gradient.
   atomicAdd(a.mismatch, 1u);
+  const uint32_t pad_tile = a.vt->total_tiles;
   for (; p < end; ++p) {
-    a.keys[p] = a.pad_tile;
+    a.keys[p] = pad_tile;
     a.values[p] = p;
     a.pair_gaussian[p] = g;
     if (a.pair_grads != nullptr) {
@@ -99,7 +100,7 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
                  const uint32_t* sorted_vals, const uint32_t* sorted_offsets, uint32_t pair_capacity, uint32_t* keys,
                  uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads, uint32_t* mismatch, cudaStream_t st) {
   if (n_items == 0u) return;
-  EmitArgs a{sp.frames, sp.vt, cap, n_items, pair_capacity, sp.total_tiles, sorted_vals, sorted_offsets,
+  EmitArgs a{sp.frames, sp.vt, cap, n_items, pair_capacity, sorted_vals, sorted_offsets,
              vb.splat, vb.foot, vb.tiles, vb.offsets, keys, values, pair_gaussian, pair_grads, mismatch};
   k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }

@@ -27,7 +27,8 @@ namespace {
 
 struct RasterArgs {
   const gs_frame_data* frames;
-  ViewTable vt;
+  const ViewTable* vt;
+  uint32_t* queue;  // work-queue counter of this pass
   RasterBuffers rb;
   const float4* splat;
   const float4* foot;
@@ -61,12 +62,12 @@ struct TileLayout {
   static constexpr int kWarps = kThreads / 32;
   uint32_t v, t, W, H, tx, ty;
   float bx, by;  // centre of the warp block's first pixel
-  __device__ TileLayout(const ViewTable& vt, const gs_frame_data* frames, uint32_t gt, uint32_t warp) {
+  __device__ TileLayout(const ViewTable* vt, const gs_frame_data* frames, uint32_t gt, uint32_t warp) {
     v = view_of_tile(vt, gt);
     const gs_frame_data& f = frames[v];
     W = f.image[0];
     H = f.image[1];
-    t = gt - vt.tile_base[v];
+    t = gt - vt->tile_base[v];
     tx = t % f.image[2];
     ty = t / f.image[2];
     bx = float(tx * kTile + (warp & 1u) * 8u) + 0.5f;
@@ -78,8 +79,19 @@ struct TileLayout {
   }
 };
 
+// The next work item of a persistent block: tiles of the flattened (view, tile) space, in
+// order, handed out by an atomic counter; `total` or more ends the loop.
+__device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
+  __shared__ uint32_t s_item;
+  if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+  __syncthreads();
+  const uint32_t item = s_item;
+  __syncthreads();
+  return item;
+}
+
 template <int PX>
-__global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
+__device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
   __shared__ float4 s_a[256];    // centre xy, opacity, conic a
   __shared__ float4 s_b[256];    // conic b, conic c, red, green
@@ -88,7 +100,6 @@ __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   __shared__ float s_red[L::kWarps][16];
   __shared__ uint32_t s_max[L::kWarps];
 
-  const uint32_t gt = blockIdx.x;
   const uint32_t lid = threadIdx.x, lane = lid & 31u, warp = lid >> 5;
   const L lay(a.vt, a.frames, gt, warp);
   const gs_frame_data& f = a.frames[lay.v];
@@ -183,12 +194,14 @@ __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   for (int p = 0; p < PX; ++p) {
     if (!inside[p]) continue;
     const uint2 px = lay.pixel(lane, p);
-    const size_t pix = size_t(a.vt.pixel_base[lay.v]) + size_t(px.y) * lay.W + px.x;
+    const size_t local = size_t(px.y) * lay.W + px.x;
+    const size_t pix = size_t(a.vt->pixel_base[lay.v]) + local;
     const float o0 = C0[p] + T[p] * f.background[0], o1 = C1[p] + T[p] * f.background[1],
                 o2 = C2[p] + T[p] * f.background[2];
     float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, w = 1.0f;
-    if (a.rb.target != nullptr) {
-      const uint32_t u = a.rb.target[pix];
+    const uint32_t* target = a.vt->target[lay.v];
+    if (target != nullptr) {
+      const uint32_t u = target[local];
       const float ta = float(u >> 24) / 255.0f;
       const float tr[3] = {float(u & 255u) / 255.0f, float((u >> 8) & 255u) / 255.0f, float((u >> 16) & 255u) / 255.0f};
       const bool masked = (f.model[3] & GS_FLAG_MASKED_TARGET) != 0u;
@@ -266,11 +279,16 @@ __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   }
 }
 
+template <int PX>
+__global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
+  const uint32_t total = a.vt->total_tiles;
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX>(a, gt);
+}
+
 template <int BATCH, bool DET, int PX>
-__global__ void __launch_bounds__(256 / PX) k_raster_bwd(RasterArgs a) {
+__device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
   static_assert(BATCH <= L::kThreads, "one staged splat per thread");
-  if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
   __shared__ float4 s_a[BATCH];
   __shared__ float4 s_b[BATCH];
   __shared__ float s_c[BATCH];
@@ -279,7 +297,6 @@ __global__ void __launch_bounds__(256 / PX) k_raster_bwd(RasterArgs a) {
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
 
-  const uint32_t gt = blockIdx.x;
   const uint32_t lid = threadIdx.x, lane = lid & 31u, warp = lid >> 5;
   const L lay(a.vt, a.frames, gt, warp);
   const uint2 range = a.rb.ranges[gt];
@@ -308,7 +325,7 @@ __global__ void __launch_bounds__(256 / PX) k_raster_bwd(RasterArgs a) {
     T[p] = 1.0f;
     last[p] = 0u;
     if (px.x < lay.W && px.y < lay.H) {
-      const size_t pix = size_t(a.vt.pixel_base[lay.v]) + size_t(px.y) * lay.W + px.x;
+      const size_t pix = size_t(a.vt->pixel_base[lay.v]) + size_t(px.y) * lay.W + px.x;
       const float4 pg = a.rb.pixel_grad[pix];
       dl0[p] = pg.x;
       dl1[p] = pg.y;
@@ -437,37 +454,67 @@ __global__ void __launch_bounds__(256 / PX) k_raster_bwd(RasterArgs a) {
   }
 }
 
+template <int BATCH, bool DET, int PX>
+__global__ void __launch_bounds__(256 / PX) k_raster_bwd(RasterArgs a) {
+  if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
+  const uint32_t total = a.vt->total_tiles;
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_bwd_tile<BATCH, DET, PX>(a, gt);
+}
+
+// A persistent grid: as many blocks as fit on the GPU at once (at most one per tile).
+template <typename Kernel>
+uint32_t persistent_grid(Kernel kernel, int threads, const StepPointers& sp) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return min(sp.tile_cap, uint32_t(per_sm) * uint32_t(sp.sm_count));
+}
+
 template <bool DET, int PX>
-void launch_bwd(const RasterArgs& a, uint32_t tiles, cudaStream_t st) {
-  k_raster_bwd<32, DET, PX><<<tiles, 256 / PX, 0, st>>>(a);
+void launch_bwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
+  static uint32_t grid = 0, cap = 0;
+  if (grid == 0 || cap != sp.tile_cap) {
+    grid = persistent_grid(k_raster_bwd<32, DET, PX>, 256 / PX, sp);
+    cap = sp.tile_cap;
+  }
+  k_raster_bwd<32, DET, PX><<<grid, 256 / PX, 0, st>>>(a);
+}
+
+template <int PX>
+void launch_fwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
+  static uint32_t grid = 0, cap = 0;
+  if (grid == 0 || cap != sp.tile_cap) {
+    grid = persistent_grid(k_raster_fwd<PX>, 256 / PX, sp);
+    cap = sp.tile_cap;
+  }
+  k_raster_fwd<PX><<<grid, 256 / PX, 0, st>>>(a);
 }
 
 }  // namespace
 
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,
                            cudaStream_t st) {
-  if (sp.total_tiles == 0u) return;
-  RasterArgs a{sp.frames, sp.vt, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u};
-  if (px >= 4) k_raster_fwd<4><<<sp.total_tiles, 64, 0, st>>>(a);
-  else if (px == 2) k_raster_fwd<2><<<sp.total_tiles, 128, 0, st>>>(a);
-  else k_raster_fwd<1><<<sp.total_tiles, 256, 0, st>>>(a);
+  if (sp.tile_cap == 0u) return;
+  RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u};
+  if (px >= 4) launch_fwd<4>(a, sp, st);
+  else if (px == 2) launch_fwd<2>(a, sp, st);
+  else launch_fwd<1>(a, sp, st);
 }
 
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
                             float4* pair_grads, bool deterministic, int px, const uint32_t* d_pairs,
                             uint32_t accept, cudaStream_t st) {
-  if (sp.total_tiles == 0u) return;
-  RasterArgs a{sp.frames, sp.vt, rb, vb.splat, vb.foot, reinterpret_cast<float*>(pair_grads),
-               reinterpret_cast<float*>(vb.grad2d), d_pairs, accept};
-  const uint32_t t = sp.total_tiles;
+  if (sp.tile_cap == 0u) return;
+  RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueBackward, rb, vb.splat, vb.foot,
+               reinterpret_cast<float*>(pair_grads), reinterpret_cast<float*>(vb.grad2d), d_pairs, accept};
   if (deterministic) {
-    if (px >= 4) launch_bwd<true, 4>(a, t, st);
-    else if (px == 2) launch_bwd<true, 2>(a, t, st);
-    else launch_bwd<true, 1>(a, t, st);
+    if (px >= 4) launch_bwd<true, 4>(a, sp, st);
+    else if (px == 2) launch_bwd<true, 2>(a, sp, st);
+    else launch_bwd<true, 1>(a, sp, st);
   } else {
-    if (px >= 4) launch_bwd<false, 4>(a, t, st);
-    else if (px == 2) launch_bwd<false, 2>(a, t, st);
-    else launch_bwd<false, 1>(a, t, st);
+    if (px >= 4) launch_bwd<false, 4>(a, sp, st);
+    else if (px == 2) launch_bwd<false, 2>(a, sp, st);
+    else launch_bwd<false, 1>(a, sp, st);
   }
 }
 

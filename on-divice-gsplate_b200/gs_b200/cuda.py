@@ -33,7 +33,7 @@ SNAP = {
 
 EXPORTED = ["gs_last_error", "gs_create", "gs_destroy", "gs_model_init", "gs_model_info_get", "gs_model_export",
             "gs_model_moments", "gs_set_views", "gs_step", "gs_render", "gs_densify", "gs_reset_opacity",
-            "gs_snapshot", "gs_set_tuning", "gs_get_tuning"]
+            "gs_snapshot", "gs_set_tuning", "gs_get_tuning", "gs_dataset_set", "gs_set_views_dataset"]
 
 
 class StepResult(ctypes.Structure):
@@ -46,7 +46,7 @@ class StepResult(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("min_pair_capacity", ctypes.c_uint32), ("initial_pairs", ctypes.c_uint64),
                 ("deterministic", ctypes.c_uint32), ("forward_pixels", ctypes.c_uint32),
-                ("backward_pixels", ctypes.c_uint32), ("retry", ctypes.c_uint32)]
+                ("backward_pixels", ctypes.c_uint32), ("retry", ctypes.c_uint32), ("graph", ctypes.c_uint32)]
 
 
 class ModelInfo(ctypes.Structure):
@@ -87,6 +87,8 @@ def load(path: str = LIB_PATH):
     L.gs_snapshot.argtypes = [vp, u32, ctypes.c_int, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
     L.gs_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.gs_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.gs_dataset_set.argtypes = [vp, u32, vp, vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.gs_set_views_dataset.argtypes = [vp, u32, vp, vp]
     for name in EXPORTED[1:]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -177,6 +179,20 @@ class Context:
             tptr = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
         self._keep = keep  # the library may read the targets until the next step returns
         _check(self.lib.gs_set_views(self.h, len(frames), _ptr(fr), tptr))
+
+    def set_dataset(self, images: list[np.ndarray]) -> None:
+        """Keeps RGBA8 target images (H x W x 4 uint8) in HBM across steps."""
+        arrs = [np.ascontiguousarray(t, np.uint8) for t in images]
+        w = np.array([a.shape[1] for a in arrs], np.uint32)
+        h = np.array([a.shape[0] for a in arrs], np.uint32)
+        ptrs = (ctypes.c_void_p * max(len(arrs), 1))(*[a.ctypes.data for a in arrs])
+        _check(self.lib.gs_dataset_set(self.h, len(arrs), _ptr(w), _ptr(h), ptrs))
+
+    def set_views_dataset(self, frames: list[np.ndarray], images: list[int]) -> None:
+        fr = np.ascontiguousarray(np.concatenate([np.asarray(f, FRAME_DTYPE).reshape(1) for f in frames]))
+        idx = np.ascontiguousarray(images, np.uint32)
+        self._keep = [fr]
+        _check(self.lib.gs_set_views_dataset(self.h, len(frames), _ptr(fr), _ptr(idx)))
 
     def step(self, train: bool = True, profile: bool = False) -> StepResult:
         out = StepResult()
