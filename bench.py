@@ -43,13 +43,13 @@ WIDTH, HEIGHT, FOCAL = 1080, 1920, 1400.0
 VIEWS_PER_STEP = 8
 
 
-def workload():
+def workload(cameras: int = N_CAMERAS):
     from gs_b200 import frame as F
     from gs_b200 import scenes as S
 
     scene = S.make_scene(N_GAUSSIANS, 0, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
     truth = S.make_scene(N_GAUSSIANS, 1, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
-    cams = S.orbit_cameras(N_CAMERAS, 3.0, 0.5, WIDTH, HEIGHT, FOCAL)
+    cams = S.orbit_cameras(cameras, 3.0, 0.5, WIDTH, HEIGHT, FOCAL)
     opt = F.TrainOptions(iterations=30000, sh_degree=3, sh_degree_interval=0, masked=False,
                          random_background=False, lr_opacity=5e-2, lr_sh_rest=2.5e-3,
                          lambda_dssim=0.2, lambda_dssim_end=-1.0)
@@ -275,6 +275,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="both", choices=["both", "plain", "batched"],
                     help="plain or batched alone (profiling runs); the bench line needs both")
+    ap.add_argument("--cameras", type=int, default=N_CAMERAS, help="orbit cameras (fewer: shorter setup)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -302,7 +303,7 @@ def main() -> None:
     from gs_b200.cuda import PASSES, Context
 
     torch.cuda.set_device(local)
-    scene, truth, cams, opt = workload()
+    scene, truth, cams, opt = workload(args.cameras)
     ctx = Context(local)
     targets = render_targets(ctx, truth, cams, opt)
     ctx.set_tuning(graph=1)
