@@ -198,6 +198,24 @@ int gs_snapshot(gs_context* ctx, uint32_t view, gs_snapshot_kind which, void* ho
 int gs_set_tuning(gs_context* ctx, const gs_tuning* tuning);
 int gs_get_tuning(gs_context* ctx, gs_tuning* tuning);
 
+/* No counterpart in the reference: its RadixSort allocates its own temporary buffers
+   (engine/src/radix_sort.cpp:37-39). For callers that cannot allocate device memory —
+   runtimes whose pool owns all device memory and forbids allocations outside it, plugins
+   that get only the buffers such a runtime passes them, loops that cannot afford an
+   allocation's device synchronisation — this sorts n (key, value) pairs already in device
+   memory, in place, stably by key bits [0, key_bits), with the library's onesweep radix
+   sort, and allocates nothing: its scratch is a static device array sized for
+   GS_SORT_NOALLOC_MAX_ITEMS pairs (about 8.3 MB, held by every GPU that loads the library
+   until exit). Larger n is rejected with GS_ERR_INVALID.
+   - `stream` is a cudaStream_t (NULL: the legacy default stream) on the current device;
+     the call returns after the sort has finished on it.
+   - The first call on a device looks up the scratch's device address (set-up, once per
+     device, with that device current); make that first call before any stream capture.
+   - Every call shares the one array: calls that overlap on the GPU (other streams, other
+     host threads on the same device) race and corrupt each other's results. */
+#define GS_SORT_NOALLOC_MAX_ITEMS (1u << 20)
+int gs_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t key_bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,10 @@ constexpr uint64_t kMaxPairs = (1ull << 30) - 1ull;  // look-back words carry 30
 
 }  // namespace
 
+namespace gsk {
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace gsk
+
 struct gs_context {
   int device = 0;
   cudaStream_t stream = nullptr;

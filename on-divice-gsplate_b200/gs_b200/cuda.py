@@ -33,7 +33,8 @@ SNAP = {
 
 EXPORTED = ["gs_last_error", "gs_create", "gs_destroy", "gs_model_init", "gs_model_info_get", "gs_model_export",
             "gs_model_moments", "gs_set_views", "gs_step", "gs_render", "gs_densify", "gs_reset_opacity",
-            "gs_snapshot", "gs_set_tuning", "gs_get_tuning", "gs_dataset_set", "gs_set_views_dataset"]
+            "gs_snapshot", "gs_set_tuning", "gs_get_tuning", "gs_dataset_set", "gs_set_views_dataset",
+            "gs_sort_pairs_noalloc"]
 
 
 class StepResult(ctypes.Structure):
@@ -89,6 +90,7 @@ def load(path: str = LIB_PATH):
     L.gs_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.gs_dataset_set.argtypes = [vp, u32, vp, vp, ctypes.POINTER(ctypes.c_void_p)]
     L.gs_set_views_dataset.argtypes = [vp, u32, vp, vp]
+    L.gs_sort_pairs_noalloc.argtypes = [vp, vp, u32, u32, vp]
     for name in EXPORTED[1:]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
