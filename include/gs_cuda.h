@@ -122,6 +122,7 @@ typedef struct gs_tuning {
   uint32_t retry;             /* 1 (default): grow the pair buffers and run again on overflow */
   uint32_t graph;             /* 1: capture the step as a CUDA graph and replay it while its launch
                                  structure (views, slots, buffer sizes, SH degree, mode) holds */
+  uint32_t backward_batch;    /* splats staged per round of the backward pass: 32 or 64 (0: default) */
 } gs_tuning;
 
 typedef struct gs_model_info {

@@ -282,7 +282,7 @@ struct gs_context {
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
     const std::vector<uint64_t> key = {n_views, model.slots, model.cap, pair_cap, tile_cap, pixel_cap, degree,
                                        train ? 1u : 0u, ssim ? 1u : 0u, tuning.deterministic,
-                                       tuning.forward_pixels, tuning.backward_pixels};
+                                       tuning.forward_pixels, tuning.backward_pixels, tuning.backward_batch};
     if (graph_exec == nullptr || key != graph_key) {
       drop_graph();
       cudaGraph_t g = nullptr;
@@ -463,8 +463,9 @@ struct gs_context {
     ++launches;
     mark(4);
     if (train) {
-      const int px = tuning.backward_pixels ? int(tuning.backward_pixels) : 2;
-      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, px, d_scalars, uint32_t(pair_cap), stream);
+      const int px = tuning.backward_pixels ? int(tuning.backward_pixels) : 4;
+      const int batch = tuning.backward_batch ? int(tuning.backward_batch) : 64;
+      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, px, batch, d_scalars, uint32_t(pair_cap), stream);
       ++launches;
       mark(5);
       if (det) {
@@ -660,7 +661,8 @@ int gs_create(int device, gs_context** out) {
     c->tuning.min_pair_capacity = 1u << 16;
     c->tuning.deterministic = 1u;
     c->tuning.forward_pixels = 2u;
-    c->tuning.backward_pixels = 2u;
+    c->tuning.backward_pixels = 4u;
+    c->tuning.backward_batch = 64u;
     c->tuning.retry = 1u;
     c->tuning.graph = 0u;
     try {
@@ -1014,6 +1016,8 @@ int gs_set_tuning(gs_context* c, const gs_tuning* t) {
     for (uint32_t px : {t->forward_pixels, t->backward_pixels})
       if (px != 0 && px != 1 && px != 2 && px != 4)
         fail(GS_ERR_INVALID, "gs_set_tuning: pixels per thread must be 1, 2 or 4");
+    if (t->backward_batch != 0 && t->backward_batch != 32 && t->backward_batch != 64)
+      fail(GS_ERR_INVALID, "gs_set_tuning: backward_batch must be 32 or 64");
     c->tuning = *t;
     if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
     c->drop_graph();

@@ -93,9 +93,10 @@ struct RasterBuffers {
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,
                            cudaStream_t st);
 // Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
-// vb.grad2d (fast). Skipped on device when *d_pairs > accept.
+// vb.grad2d (fast), staging `batch` (32 or 64) splats per round. Skipped on device when
+// *d_pairs > accept.
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
-                            float4* pair_grads, bool deterministic, int px, const uint32_t* d_pairs,
+                            float4* pair_grads, bool deterministic, int px, int batch, const uint32_t* d_pairs,
                             uint32_t accept, cudaStream_t st);
 
 // ---- loss.cu ----

@@ -6,6 +6,10 @@
 // columns: the separable 11x11 window, sigma 1.5, zero outside the image) and writes the
 // SSIM gradient maps A, B, C; k_ssim_grad blurs those back and subtracts
 // lambda / (3 pixels) (G*A + 2 x G*B + y G*C) from dL/dC, then refreshes dL/dC . C.
+//
+// Both blurs are register-blocked: a thread produces 4 consecutive outputs of a row (or
+// column) from the 14 inputs it loads once, so shared-memory traffic per output is 3.5
+// loads per plane instead of 11, and sums run over the taps in window order.
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -51,10 +55,33 @@ __device__ bool background_only(const LossArgs& a, const gs_frame_data& f, uint3
   return true;
 }
 
+constexpr int kRun = 4;                 // outputs per thread and blur
+constexpr int kSpan = kRun + 2 * kR;    // inputs a thread loads: 14
+constexpr int kQuads = kTile / kRun;    // 4
+constexpr int kS = kWin + 1;            // row stride of a staged plane (odd: at most 2-way conflicts)
+constexpr int kPlane = kWin * kS;       // 702
+constexpr int kHRow = kWin * kTile;     // one plane after the row blur: 26 x 16
+constexpr int kHPlane = kHRow + 16;     // padded so neighbouring planes fall on other banks
+
+// Row blur of 4 consecutive outputs from `src` (14 inputs) into out[4].
+__device__ __forceinline__ void blur_run(const float* src, int stride, float out[kRun]) {
+  float x[kSpan];
+#pragma unroll
+  for (int k = 0; k < kSpan; ++k) x[k] = src[k * stride];
+#pragma unroll
+  for (int o = 0; o < kRun; ++o) {
+    float sum = 0.0f;
+#pragma unroll
+    for (int k = 0; k <= 2 * kR; ++k) sum += c_window[k] * x[o + k];
+    out[o] = sum;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
-  __shared__ float s_x[3][kWin * kWin];
-  __shared__ float s_y[3][kWin * kWin];
-  __shared__ float s_h[5][kWin * kTile];
+  // s_buf: render rgb and target rgb planes of the window (26 x kS each); after the row
+  // blur it holds A, B, C and SSIM per channel for the tile's 256 pixels.
+  __shared__ float s_buf[6 * kPlane];
+  __shared__ float s_h[3 * 5 * kHPlane];  // [channel][moment] after the row blur
   __shared__ float s_sum[8][2];
   const uint32_t gt = blockIdx.x;
   if (gt >= a.vt->total_tiles) return;
@@ -78,7 +105,8 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
   for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
-    const int gx = ox + int(e % kWin), gy = oy + int(e / kWin);
+    const uint32_t row = e / kWin, col = e % kWin;
+    const int gx = ox + int(col), gy = oy + int(row);
     const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
     float3 x = make_float3(0.f, 0.f, 0.f), y = x;
     if (in) {
@@ -87,66 +115,92 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
       x = make_float3(o.x, o.y, o.z);
       y = target_colour(f, target[local]);
     }
-    s_x[0][e] = x.x; s_x[1][e] = x.y; s_x[2][e] = x.z;
-    s_y[0][e] = y.x; s_y[1][e] = y.y; s_y[2][e] = y.z;
+    const uint32_t at = row * kS + col;
+    s_buf[at] = x.x;
+    s_buf[kPlane + at] = x.y;
+    s_buf[2 * kPlane + at] = x.z;
+    s_buf[3 * kPlane + at] = y.x;
+    s_buf[4 * kPlane + at] = y.y;
+    s_buf[5 * kPlane + at] = y.z;
   }
-  const uint32_t lx = lid % kTile, ly = lid / kTile;
-  const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
-  const bool inside = px < W && py < H;
-  const size_t pix = pbase + size_t(py) * W + px;
-  const float w = inside ? a.rb.pixel_out[pix].w : 0.0f;
-  const float c1 = f.loss[1], c2 = f.loss[2];
-  float A[3], B[3], C[3], ssim_sum = 0.0f, wsum = 0.0f;
   __syncthreads();
-  for (int c = 0; c < 3; ++c) {
-    for (uint32_t e = lid; e < uint32_t(kWin * kTile); e += 256u) {
-      const uint32_t row = e / kTile, col = e % kTile;
+  // Row blur of the five moments: 3 channels x 26 rows x 4 runs.
+  for (uint32_t e = lid; e < 3u * kWin * kQuads; e += 256u) {
+    const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, c = e / (kQuads * kWin);
+    const float* xs = s_buf + c * kPlane + row * kS + q * kRun;
+    const float* ys = s_buf + (3u + c) * kPlane + row * kS + q * kRun;
+    float x[kSpan], y[kSpan];
+#pragma unroll
+    for (int k = 0; k < kSpan; ++k) {
+      x[k] = xs[k];
+      y[k] = ys[k];
+    }
+    float* h = s_h + c * 5u * kHPlane + row * kTile + q * kRun;
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) {
       float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f, m4 = 0.f;
 #pragma unroll
       for (int k = 0; k <= 2 * kR; ++k) {
         const float wk = c_window[k];
-        const float x = s_x[c][row * kWin + col + k], y = s_y[c][row * kWin + col + k];
-        m0 += wk * x;
-        m1 += wk * y;
-        m2 += wk * x * x;
-        m3 += wk * y * y;
-        m4 += wk * x * y;
+        const float xv = x[o + k], yv = y[o + k];
+        m0 += wk * xv;
+        m1 += wk * yv;
+        m2 += wk * xv * xv;
+        m3 += wk * yv * yv;
+        m4 += wk * xv * yv;
       }
-      s_h[0][e] = m0;
-      s_h[1][e] = m1;
-      s_h[2][e] = m2;
-      s_h[3][e] = m3;
-      s_h[4][e] = m4;
+      h[o] = m0;
+      h[kHPlane + o] = m1;
+      h[2 * kHPlane + o] = m2;
+      h[3 * kHPlane + o] = m3;
+      h[4 * kHPlane + o] = m4;
     }
-    __syncthreads();
-    float mx = 0.f, my = 0.f, exx = 0.f, eyy = 0.f, exy = 0.f;
+  }
+  __syncthreads();
+  // Column blur and the SSIM terms: 3 channels x 16 columns x 4 runs of 4 pixels.
+  float* s_abc = s_buf;  // [A, B, C, SSIM][channel][256]
+  const float c1 = f.loss[1], c2 = f.loss[2];
+  if (lid < 3u * kTile * kQuads) {
+    const uint32_t col = lid % kTile, c = (lid / kTile) % 3u, q = lid / (3u * kTile);
+    const float* h = s_h + c * 5u * kHPlane + q * kRun * kTile + col;
+    float mom[5][kRun];
 #pragma unroll
-    for (int k = 0; k <= 2 * kR; ++k) {
-      const float wk = c_window[k];
-      const uint32_t e = (ly + k) * kTile + lx;
-      mx += wk * s_h[0][e];
-      my += wk * s_h[1][e];
-      exx += wk * s_h[2][e];
-      eyy += wk * s_h[3][e];
-      exy += wk * s_h[4][e];
+    for (int j = 0; j < 5; ++j) blur_run(h + j * kHPlane, kTile, mom[j]);
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) {
+      const float mx = mom[0][o], my = mom[1][o], exx = mom[2][o], eyy = mom[3][o], exy = mom[4][o];
+      const float vx = exx - mx * mx, vy = eyy - my * my, cxy = exy - mx * my;
+      const float l = 2.0f * mx * my + c1, cs = 2.0f * cxy + c2;
+      const float m = mx * mx + my * my + c1, vv = vx + vy + c2;
+      const float inv = 1.0f / (m * vv);
+      const float ssim = l * cs * inv;
+      const float d_cxy = 2.0f * l * inv;
+      const float d_vx = -ssim / vv;
+      const uint32_t pixel = (q * kRun + o) * kTile + col;
+      s_abc[c * 256u + pixel] = 2.0f * my * cs * inv - ssim * 2.0f * mx / m - 2.0f * mx * d_vx - my * d_cxy;
+      s_abc[(3u + c) * 256u + pixel] = d_vx;
+      s_abc[(6u + c) * 256u + pixel] = d_cxy;
+      s_abc[(9u + c) * 256u + pixel] = ssim;
     }
-    const float vx = exx - mx * mx, vy = eyy - my * my, cxy = exy - mx * my;
-    const float l = 2.0f * mx * my + c1, cs = 2.0f * cxy + c2;
-    const float m = mx * mx + my * my + c1, vv = vx + vy + c2;
-    const float inv = 1.0f / (m * vv);
-    const float ssim = l * cs * inv;
-    const float d_cxy = 2.0f * l * inv;
-    const float d_vx = -ssim / vv;
-    A[c] = 2.0f * my * cs * inv - ssim * 2.0f * mx / m - 2.0f * mx * d_vx - my * d_cxy;
-    B[c] = d_vx;
-    C[c] = d_cxy;
-    if (inside) {
+  }
+  __syncthreads();
+  const uint32_t lx = lid % kTile, ly = lid / kTile;
+  const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
+  const bool inside = px < W && py < H;
+  const size_t pix = pbase + size_t(py) * W + px;
+  float ssim_sum = 0.0f, wsum = 0.0f;
+  if (inside) {
+    const float w = a.rb.pixel_out[pix].w;
+    float A[3], B[3], C[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      A[c] = s_abc[c * 256 + lid];
+      B[c] = s_abc[(3 + c) * 256 + lid];
+      C[c] = s_abc[(6 + c) * 256 + lid];
+      const float ssim = s_abc[(9 + c) * 256 + lid];
       ssim_sum += ssim;
       wsum += w * ssim;
     }
-    __syncthreads();
-  }
-  if (inside) {
     a.rb.ssim_maps[pix * 3u] = make_float4(w * A[0], w * A[1], w * A[2], 0.0f);
     a.rb.ssim_maps[pix * 3u + 1u] = make_float4(w * B[0], w * B[1], w * B[2], 0.0f);
     a.rb.ssim_maps[pix * 3u + 2u] = make_float4(w * C[0], w * C[1], w * C[2], 0.0f);
@@ -169,8 +223,10 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
 }
 
 __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
-  __shared__ float s_m[3][kWin * kWin];
-  __shared__ float s_h[3][kWin * kTile];
+  // s_m: the 9 planes (A, B, C x rgb) of the window; after the row blur it holds the
+  // 9 blurred planes of the tile's 256 pixels.
+  __shared__ float s_m[9 * kPlane];
+  __shared__ float s_h[9 * kHPlane];
   const uint32_t gt = blockIdx.x;
   if (gt >= a.vt->total_tiles) return;
   const uint32_t v = view_of_tile(a.vt, gt);
@@ -186,64 +242,63 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   const uint32_t lid = threadIdx.x;
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
+  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
+    const uint32_t row = e / kWin, col = e % kWin;
+    const int gx = ox + int(col), gy = oy + int(row);
+    const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
+    float4 m[3] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    if (in) {
+      const size_t q = (pbase + size_t(gy) * W + size_t(gx)) * 3u;
+      m[0] = a.rb.ssim_maps[q];
+      m[1] = a.rb.ssim_maps[q + 1u];
+      m[2] = a.rb.ssim_maps[q + 2u];
+    }
+    const uint32_t at = row * kS + col;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      s_m[(3 * q) * kPlane + at] = m[q].x;
+      s_m[(3 * q + 1) * kPlane + at] = m[q].y;
+      s_m[(3 * q + 2) * kPlane + at] = m[q].z;
+    }
+  }
+  __syncthreads();
+  // Row blur: 9 planes x 26 rows x 4 runs.
+  for (uint32_t e = lid; e < 9u * kWin * kQuads; e += 256u) {
+    const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, p = e / (kQuads * kWin);
+    float out[kRun];
+    blur_run(s_m + p * kPlane + row * kS + q * kRun, 1, out);
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) s_h[p * kHPlane + row * kTile + q * kRun + o] = out[o];
+  }
+  __syncthreads();
+  // Column blur: 9 planes x 16 columns x 4 runs.
+  float* s_g = s_m;  // [plane][256]
+  for (uint32_t e = lid; e < 9u * kTile * kQuads; e += 256u) {
+    const uint32_t col = e % kTile, p = (e / kTile) % 9u, q = e / (9u * kTile);
+    float out[kRun];
+    blur_run(s_h + p * kHPlane + q * kRun * kTile + col, kTile, out);
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) s_g[p * 256u + (q * kRun + o) * kTile + col] = out[o];
+  }
+  __syncthreads();
   const uint32_t lx = lid % kTile, ly = lid / kTile;
   const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
-  const bool inside = px < W && py < H;
+  if (px >= W || py >= H) return;
   const size_t pix = pbase + size_t(py) * W + px;
-  float3 x = make_float3(0.f, 0.f, 0.f), y = x;
-  if (inside) {
-    const float4 o = a.rb.pixel_out[pix];
-    x = make_float3(o.x, o.y, o.z);
-    y = target_colour(f, target[size_t(py) * W + px]);
-  }
+  const float4 o = a.rb.pixel_out[pix];
+  const float3 y = target_colour(f, target[size_t(py) * W + px]);
+  const float xs[3] = {o.x, o.y, o.z}, ys[3] = {y.x, y.y, y.z};
   float ds[3];
-  for (int c = 0; c < 3; ++c) {
-    for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
-      const int gx = ox + int(e % kWin), gy = oy + int(e / kWin);
-      const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
-      float m0 = 0.f, m1 = 0.f, m2 = 0.f;
-      if (in) {
-        const size_t q = (pbase + size_t(gy) * W + size_t(gx)) * 3u;
-        const float* maps = reinterpret_cast<const float*>(a.rb.ssim_maps);
-        m0 = maps[q * 4u + c];
-        m1 = maps[(q + 1u) * 4u + c];
-        m2 = maps[(q + 2u) * 4u + c];
-      }
-      s_m[0][e] = m0;
-      s_m[1][e] = m1;
-      s_m[2][e] = m2;
-    }
-    __syncthreads();
-    for (uint32_t e = lid; e < uint32_t(kWin * kTile); e += 256u) {
-      const uint32_t row = e / kTile, col = e % kTile;
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int k = 0; k <= 2 * kR; ++k) sum += c_window[k] * s_m[q][row * kWin + col + k];
-        s_h[q][e] = sum;
-      }
-    }
-    __syncthreads();
-    float g[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-#pragma unroll
-      for (int k = 0; k <= 2 * kR; ++k) g[q] += c_window[k] * s_h[q][(ly + k) * kTile + lx];
-    const float xc = c == 0 ? x.x : (c == 1 ? x.y : x.z);
-    const float yc = c == 0 ? y.x : (c == 1 ? y.y : y.z);
-    ds[c] = g[0] + 2.0f * xc * g[1] + yc * g[2];
-    __syncthreads();
-  }
-  if (inside) {
-    float4 pg = a.rb.pixel_grad[pix];
-    const float s = f.loss[0] * f.background[3];
-    pg.x -= s * ds[0];
-    pg.y -= s * ds[1];
-    pg.z -= s * ds[2];
-    a.rb.pixel_grad[pix] = pg;
-    a.rb.pixel_dot[pix] = pg.x * x.x + pg.y * x.y + pg.z * x.z;
-  }
+  for (int c = 0; c < 3; ++c)
+    ds[c] = s_g[c * 256 + lid] + 2.0f * xs[c] * s_g[(3 + c) * 256 + lid] + ys[c] * s_g[(6 + c) * 256 + lid];
+  float4 pg = a.rb.pixel_grad[pix];
+  const float s = f.loss[0] * f.background[3];
+  pg.x -= s * ds[0];
+  pg.y -= s * ds[1];
+  pg.z -= s * ds[2];
+  a.rb.pixel_grad[pix] = pg;
+  a.rb.pixel_dot[pix] = pg.x * o.x + pg.y * o.y + pg.z * o.z;
 }
 
 __global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const float* __restrict__ tile_loss,

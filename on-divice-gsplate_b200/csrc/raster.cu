@@ -5,16 +5,16 @@
 // views of uneven resolution is one launch. Each thread owns PX pixels (1, 2 or 4) of the
 // tile, stacked 4 rows apart, so a warp covers an 8 x 4PX block. Splat records are
 // gathered through the sorted pair list into shared memory a batch at a time; each warp
-// then ballots which staged splats' footprint boxes reach its block and walks only those,
-// in order (a culled splat is one every pixel of the block would skip anyway).
+// then ballots which staged splats' footprint ellipses reach its block and walks only
+// those, in order (a culled splat is one every pixel of the block would skip anyway).
 //
 // The adjoint keeps no per-fragment state: each pixel walks its splats front to back
 // again from T = 1 and R = dL/dC . C_final (pixel_dot, background included), up to its
 // last contributor (pixel_count), reproducing the forward's transmittance bit for bit
 // (same multiplications). Per splat it needs
 //   dL/dalpha_k = T_k (dL/dC . c_k) - R_{k+1} / (1 - alpha_k),  R_{k+1} = R_k - (dL/dC . c_k) alpha_k T_k.
-// A thread adds its PX pixels' gradients in registers; each warp then sums a splat's 12
-// values over its lanes with a reduce-scatter butterfly (16 shuffles instead of 60 for a
+// A thread adds its PX pixels' gradients in registers; each warp then sums a splat's 11
+// values over its lanes with a reduce-scatter butterfly (13 shuffles instead of 55 for a
 // tree per value), skipped when no lane touched the splat, and the warps' partials are
 // added in a fixed order, so the per-pair gradient is bit-stable. Deterministic mode
 // stores it at the pair's pre-sort index (pair_grads, summed per gaussian by
@@ -40,19 +40,31 @@ struct RasterArgs {
 
 __device__ __forceinline__ uint32_t pack_unorm(float v) { return uint32_t(clampf(v, 0.0f, 1.0f) * 255.0f + 0.5f); }
 
-// Bounding box (x0, x1, y0, y1) of a splat's footprint: the ellipse
-// d^T cov^-1 d <= threshold (train_common.glsl:163-172) spans sqrt(threshold cov_xx)
-// horizontally and sqrt(threshold cov_yy) vertically. The threshold carries slack over
-// the alpha >= 1/255 boundary, and a further 1/64 px margin covers rounding, so a pixel
-// outside the box always has alpha < 1/255 and would be skipped.
-__device__ __forceinline__ float4 footprint_box(float mx, float my, float4 fp) {
-  const float ex = sqrtf(fp.w * fp.x) + 0.015625f, ey = sqrtf(fp.w * fp.z) + 0.015625f;
-  return make_float4(mx - ex, mx + ex, my - ey, my + ey);
+// Culling terms of a staged splat: (limit, -b/c, -b/a) for the conic (a, b, c). A pixel at
+// offset d from the centre contributes only if alpha = opacity exp(-Q(d)/2) >= 1/255, with
+// Q(d) = a dx^2 + 2b dx dy + c dy^2, i.e. Q(d) <= 2 ln(255 opacity); the stored footprint
+// threshold (train_common.glsl:169-172) already exceeds that, and the limit adds 2^-10
+// relative and absolute on top, far above the rounding of Q and of the fast exponential.
+__device__ __forceinline__ float4 cull_terms(float blue, float4 A, float4 B, float threshold) {
+  return make_float4(blue, threshold * 1.0009765625f + 0.0009765625f, -__fdividef(B.x, B.y), -__fdividef(B.x, A.w));
 }
 
-// Whether a footprint box reaches the pixel centres of an 8 x h block at (x0, y0).
-__device__ __forceinline__ bool box_hits(float4 b, float x0, float y0, float h) {
-  return b.y >= x0 && b.x <= x0 + 7.0f && b.w >= y0 && b.z <= y0 + h - 1.0f;
+// Whether a splat's footprint ellipse reaches a pixel centre of the 8 x h block whose first
+// centre is (x0, y0): the minimum of the convex Q over the block's rectangle is 0 when the
+// centre lies inside, else it lies on an edge facing the centre, where the minimiser along
+// the edge is the unconstrained one clamped to the edge.
+// A = (centre x, centre y, opacity, a), B = (b, c, ...), K = cull_terms.
+__device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 K, float x0, float y0, float h) {
+  const float dx0 = x0 - A.x, dx1 = dx0 + 7.0f, dy0 = y0 - A.y, dy1 = dy0 + (h - 1.0f);
+  const float ex = dx0 > 0.0f ? dx0 : fminf(dx1, 0.0f);  // facing vertical edge (0: none)
+  const float ey = dy0 > 0.0f ? dy0 : fminf(dy1, 0.0f);  // facing horizontal edge (0: none)
+  const float a = A.w, b = B.x, c = B.y;
+  const float ty = fminf(fmaxf(K.z * ex, dy0), dy1);
+  const float tx = fminf(fmaxf(K.w * ey, dx0), dx1);
+  const float qv = ex != 0.0f ? ex * (a * ex + 2.0f * b * ty) + c * ty * ty : 3.0e38f;
+  const float qh = ey != 0.0f ? tx * (a * tx + 2.0f * b * ey) + c * ey * ey : 3.0e38f;
+  const float q = (ex == 0.0f && ey == 0.0f) ? 0.0f : fminf(qv, qh);
+  return q <= K.y;
 }
 
 // The tile and pixel layout of one block.
@@ -93,10 +105,9 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
 template <int PX>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
-  __shared__ float4 s_a[256];    // centre xy, opacity, conic a
-  __shared__ float4 s_b[256];    // conic b, conic c, red, green
-  __shared__ float s_c[256];     // blue
-  __shared__ float4 s_box[256];  // footprint box
+  __shared__ float4 s_a[256];  // centre xy, opacity, conic a
+  __shared__ float4 s_b[256];  // conic b, conic c, red, green
+  __shared__ float4 s_c[256];  // blue, culling terms
   __shared__ float s_red[L::kWarps][16];
   __shared__ uint32_t s_max[L::kWarps];
 
@@ -132,10 +143,10 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t g = a.rb.pair_gaussian[a.rb.values[k]];
         const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u],
                      q2 = a.splat[size_t(g) * 3u + 2u];
-        s_a[slot] = make_float4(q0.x, q0.y, q0.w, q1.x);
-        s_b[slot] = make_float4(q1.y, q1.z, q2.x, q2.y);
-        s_c[slot] = q2.z;
-        s_box[slot] = footprint_box(q0.x, q0.y, a.foot[g]);
+        const float4 A = make_float4(q0.x, q0.y, q0.w, q1.x), B = make_float4(q1.y, q1.z, q2.x, q2.y);
+        s_a[slot] = A;
+        s_b[slot] = B;
+        s_c[slot] = cull_terms(q2.z, A, B, a.foot[g].w);
       }
     }
     __syncthreads();
@@ -145,7 +156,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
 #pragma unroll
     for (int w = 0; w < 8; ++w) {
       const uint32_t j = uint32_t(w) * 32u + lane;
-      masks[w] = __ballot_sync(0xffffffffu, j < n && box_hits(s_box[j], lay.bx, lay.by, block_h));
+      masks[w] = __ballot_sync(0xffffffffu, j < n && block_reached(s_a[j], s_b[j], s_c[j], lay.bx, lay.by, block_h));
     }
     const uint32_t base = start - range.x;  // position in the tile's list of the batch's first splat
 #pragma unroll
@@ -157,7 +168,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t contributor = base + j + 1u;
         const float4 A = s_a[j];
         const float4 B = s_b[j];
-        const float blue = s_c[j];
+        const float blue = s_c[j].x;
         const float dx = A.x - cx;
         all_done = true;
 #pragma unroll
@@ -291,9 +302,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   static_assert(BATCH <= L::kThreads, "one staged splat per thread");
   __shared__ float4 s_a[BATCH];
   __shared__ float4 s_b[BATCH];
-  __shared__ float s_c[BATCH];
+  __shared__ float4 s_c[BATCH];  // blue, culling terms
   __shared__ uint32_t s_dst[BATCH];
-  __shared__ float4 s_box[BATCH];
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
 
@@ -344,11 +354,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
       const uint32_t pre = a.rb.values[range.x + start + lid];
       const uint32_t g = a.rb.pair_gaussian[pre];
       const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
-      s_a[lid] = make_float4(q0.x, q0.y, q0.w, q1.x);
-      s_b[lid] = make_float4(q1.y, q1.z, q2.x, q2.y);
-      s_c[lid] = q2.z;
+      const float4 A = make_float4(q0.x, q0.y, q0.w, q1.x), B = make_float4(q1.y, q1.z, q2.x, q2.y);
+      s_a[lid] = A;
+      s_b[lid] = B;
+      s_c[lid] = cull_terms(q2.z, A, B, a.foot[g].w);
       s_dst[lid] = DET ? pre : g;
-      s_box[lid] = footprint_box(q0.x, q0.y, a.foot[g]);
     }
     __syncthreads();
     const uint32_t nb = min(uint32_t(BATCH), n - start);
@@ -356,7 +366,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
 #pragma unroll
     for (int w = 0; w < BATCH / 32; ++w) {
       const uint32_t jj = uint32_t(w) * 32u + lane;
-      uint32_t m = __ballot_sync(0xffffffffu, jj < jmax && box_hits(s_box[jj], lay.bx, lay.by, block_h));
+      uint32_t m = __ballot_sync(0xffffffffu, jj < jmax && block_reached(s_a[jj], s_b[jj], s_c[jj], lay.bx, lay.by, block_h));
       uint32_t wrote = 0u;
 #pragma unroll 1
       while (m != 0u) {
@@ -365,11 +375,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
         const float4 A = s_a[j];
         const float4 B = s_b[j];
-        const float blue = s_c[j];
+        const float blue = s_c[j].x;
         const float dx = A.x - cx;
-        float c[16];
+        float c[12];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) c[k] = 0.0f;
+        for (int k = 0; k < 12; ++k) c[k] = 0.0f;
         bool has = false;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
@@ -406,25 +416,30 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           R[p] = rest;
         }
         if (__any_sync(0xffffffffu, has)) {
-          // Reduce-scatter: lane l ends with the warp sum of value (l >> 1).
+          // Reduce-scatter of 12 slots (11 values and a zero): after the exchanges over
+          // lane bits 4, 3, 2, 1 (6, 3, 2 and 1 shuffles; the 3 slots left after bit 3 are
+          // padded to 4) and a final add over bit 0, lane l holds the warp sum of value
+          // g + 3 b3 + 6 b4, g = (l >> 1) & 3, when g < 3.
           const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const float send = b4 ? c[i] : c[i + 8];
-            const float keep = b4 ? c[i + 8] : c[i];
+          for (int i = 0; i < 6; ++i) {
+            const float send = b4 ? c[i] : c[i + 6];
+            const float keep = b4 ? c[i + 6] : c[i];
             c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
           }
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float send = b3 ? c[i] : c[i + 4];
-            const float keep = b3 ? c[i + 4] : c[i];
+          for (int i = 0; i < 3; ++i) {
+            const float send = b3 ? c[i] : c[i + 3];
+            const float keep = b3 ? c[i + 3] : c[i];
             c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
           }
-#pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const float send = b2 ? c[i] : c[i + 2];
-            const float keep = b2 ? c[i + 2] : c[i];
-            c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+          {
+            const float send0 = b2 ? c[0] : c[2];
+            const float keep0 = b2 ? c[2] : c[0];
+            const float send1 = b2 ? c[1] : 0.0f;
+            const float keep1 = b2 ? 0.0f : c[1];
+            c[0] = keep0 + __shfl_xor_sync(0xffffffffu, send0, 4);
+            c[1] = keep1 + __shfl_xor_sync(0xffffffffu, send1, 4);
           }
           {
             const float send = b1 ? c[0] : c[1];
@@ -432,7 +447,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
             c[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
           }
           c[0] += __shfl_xor_sync(0xffffffffu, c[0], 1);
-          if ((lane & 1u) == 0u && (lane >> 1) < 12u) s_part[warp][j][lane >> 1] = c[0];
+          const uint32_t group = (lane >> 1) & 3u;
+          if ((lane & 1u) == 0u && group < 3u) s_part[warp][j][group + (b3 ? 3u : 0u) + (b4 ? 6u : 0u)] = c[0];
           wrote |= 1u << (j & 31u);
         }
       }
@@ -470,14 +486,27 @@ uint32_t persistent_grid(Kernel kernel, int threads, const StepPointers& sp) {
   return min(sp.tile_cap, uint32_t(per_sm) * uint32_t(sp.sm_count));
 }
 
-template <bool DET, int PX>
+template <int BATCH, bool DET, int PX>
 void launch_bwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_bwd<32, DET, PX>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_bwd<BATCH, DET, PX>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_bwd<32, DET, PX><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_bwd<BATCH, DET, PX><<<grid, 256 / PX, 0, st>>>(a);
+}
+
+template <int BATCH>
+void launch_bwd_batch(const RasterArgs& a, const StepPointers& sp, bool deterministic, int px, cudaStream_t st) {
+  if (deterministic) {
+    if (px >= 4) launch_bwd<BATCH, true, 4>(a, sp, st);
+    else if (px == 2) launch_bwd<BATCH, true, 2>(a, sp, st);
+    else launch_bwd<BATCH, true, 1>(a, sp, st);
+  } else {
+    if (px >= 4) launch_bwd<BATCH, false, 4>(a, sp, st);
+    else if (px == 2) launch_bwd<BATCH, false, 2>(a, sp, st);
+    else launch_bwd<BATCH, false, 1>(a, sp, st);
+  }
 }
 
 template <int PX>
@@ -502,20 +531,13 @@ void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const 
 }
 
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
-                            float4* pair_grads, bool deterministic, int px, const uint32_t* d_pairs,
+                            float4* pair_grads, bool deterministic, int px, int batch, const uint32_t* d_pairs,
                             uint32_t accept, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueBackward, rb, vb.splat, vb.foot,
                reinterpret_cast<float*>(pair_grads), reinterpret_cast<float*>(vb.grad2d), d_pairs, accept};
-  if (deterministic) {
-    if (px >= 4) launch_bwd<true, 4>(a, sp, st);
-    else if (px == 2) launch_bwd<true, 2>(a, sp, st);
-    else launch_bwd<true, 1>(a, sp, st);
-  } else {
-    if (px >= 4) launch_bwd<false, 4>(a, sp, st);
-    else if (px == 2) launch_bwd<false, 2>(a, sp, st);
-    else launch_bwd<false, 1>(a, sp, st);
-  }
+  if (batch >= 64) launch_bwd_batch<64>(a, sp, deterministic, px, st);
+  else launch_bwd_batch<32>(a, sp, deterministic, px, st);
 }
 
 }  // namespace gsk

@@ -390,20 +390,22 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   if (!sparse || (drew & 1u)) adam_params(a, f0, i, p0, p1, q, p3, g16);
 }
 
-// Part 2 (train_step_sh.comp:21-44): one thread per (SH coefficient, slot), consecutive
-// slots on consecutive threads, the views' colour gradients summed. Splitting the SH
-// update off the geometry keeps each thread's chain of dependent loads short, so both
-// kernels keep many loads in flight (the fused form was latency-bound).
+// Part 2 (train_step_sh.comp:21-44): one thread per slot. For each view the slot was seen
+// in, it evaluates the SH basis at the view direction once and adds basis x colour
+// gradient to all 3K coefficient gradients in registers (in view order), then takes the
+// Adam step on the 3K coefficients, plane by plane (consecutive slots on consecutive
+// threads). Each view's colour gradient and direction are read once; the SH planes and
+// both moment sets once each.
 template <int DEG>
-__global__ void __launch_bounds__(256) k_step_sh(StepArgs a, const uint32_t* n_views_ptr) {
-  (void)n_views_ptr;
+__global__ void __launch_bounds__(128) k_step_sh(StepArgs a) {
   if (*a.d_pairs > a.accept) return;
   constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t k = idx / a.slots, i = idx - k * a.slots;
-  if (k >= uint32_t(K)) return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.slots) return;
   if (a.P[a.cap + i].w < 0.5f) return;
-  float g[3] = {0.f, 0.f, 0.f};
+  float g[K][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k) g[k][0] = g[k][1] = g[k][2] = 0.0f;
   bool colour = false;
   for (uint32_t v = 0; v < a.n_views; ++v) {
     const size_t gi = size_t(v) * a.cap + i;
@@ -412,23 +414,27 @@ __global__ void __launch_bounds__(256) k_step_sh(StepArgs a, const uint32_t* n_v
     const float4 d = a.shin[gi * 2u + 1u];
     float basis[16];
     sh_basis<DEG>(d.x, d.y, d.z, basis);
-    const float b = basis[k + 1];
-    g[0] += b * c.x;
-    g[1] += b * c.y;
-    g[2] += b * c.z;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      g[k][0] += basis[k + 1] * c.x;
+      g[k][1] += basis[k + 1] * c.y;
+      g[k][2] += basis[k + 1] * c.z;
+    }
     colour |= c.w != 0.0f;
   }
   const gs_frame_data& f0 = a.frames[0];
   if ((f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u && !colour) return;
   const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1], lr = f0.lr1[1];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const size_t o = size_t(3 * k + c) * a.cap + i;
-    float m = a.MSH[o], v = a.VSH[o];
-    a.SH[o] = adam1(a.SH[o], g[c], m, v, lr, b1, b2, c1, c2, eps);
-    a.MSH[o] = m;
-    a.VSH[o] = v;
-  }
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t o = size_t(3 * k + c) * a.cap + i;
+      float m = a.MSH[o], v = a.VSH[o];
+      a.SH[o] = adam1(a.SH[o], g[k][c], m, v, lr, b1, b2, c1, c2, eps);
+      a.MSH[o] = m;
+      a.VSH[o] = v;
+    }
 }
 
 // ---- densification ----
@@ -594,13 +600,11 @@ void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const 
   StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
              vb.splat, vb.tiles, vb.grad2d, vb.shin, d_pairs, accept};
   const dim3 grid((m.slots + 127u) / 128u), block(128);
-  const int K = sh_rest_coeffs(degree);
-  const dim3 sh_grid(uint32_t((uint64_t(m.slots) * uint64_t(K > 0 ? K : 1) + 255u) / 256u));
   switch (degree) {
     case 0: k_step_geometry<0><<<grid, block, 0, st>>>(a); break;
-    case 1: k_step_geometry<1><<<grid, block, 0, st>>>(a); k_step_sh<1><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
-    case 2: k_step_geometry<2><<<grid, block, 0, st>>>(a); k_step_sh<2><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
-    default: k_step_geometry<3><<<grid, block, 0, st>>>(a); k_step_sh<3><<<sh_grid, 256, 0, st>>>(a, nullptr); break;
+    case 1: k_step_geometry<1><<<grid, block, 0, st>>>(a); k_step_sh<1><<<grid, block, 0, st>>>(a); break;
+    case 2: k_step_geometry<2><<<grid, block, 0, st>>>(a); k_step_sh<2><<<grid, block, 0, st>>>(a); break;
+    default: k_step_geometry<3><<<grid, block, 0, st>>>(a); k_step_sh<3><<<grid, block, 0, st>>>(a); break;
   }
 }
 
