@@ -135,7 +135,7 @@ struct gs_context {
 
   void release() {
     cudaSetDevice(device);
-    for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.shin, &pixel_grad,
+    for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.dir_grad, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
     for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss}) dev_free(*p);
@@ -190,7 +190,7 @@ struct gs_context {
     dev_alloc(vb.tiles, n);
     dev_alloc(vb.offsets, n);
     dev_alloc(vb.grad2d, n * 3);
-    dev_alloc(vb.shin, n * 2);
+    dev_alloc(vb.dir_grad, model.cap);
     dev_alloc(dkeys, n);
     dev_alloc(dvals, n);
     dev_alloc(dkeys_alt, n);
@@ -469,11 +469,12 @@ struct gs_context {
       ++launches;
       mark(5);
       if (det) {
-        gsk::launch_pair_sum(sp, vb, model.cap, model.slots, pair_grads, d_scalars, uint32_t(pair_cap), stream);
+        gsk::launch_pair_sum(vb, items, depth_sorted_vals, sorted_offsets, pair_grads, d_scalars, uint32_t(pair_cap),
+                             stream);
         ++launches;
       }
       gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), stream);
-      ++launches;
+      launches += degree > 0 ? 2 : 1;
       mark(6);
     }
     check_launch("launch");

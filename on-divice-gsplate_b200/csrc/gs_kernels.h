@@ -32,7 +32,7 @@ struct ViewBuffers {
   uint32_t* tiles = nullptr; // tiles touched
   uint32_t* offsets = nullptr;  // first pair, pre-sort order
   float4* grad2d = nullptr;  // 3 per g: summed pair gradients (train_pair_sum layout)
-  float4* shin = nullptr;    // 2 per g (several views): colour gradient + flag, view direction
+  float4* dir_grad = nullptr; // 1 per slot: position gradient through the SH view direction, summed over views
 };
 
 struct StepPointers {
@@ -105,7 +105,7 @@ void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStrea
 void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, cudaStream_t st);
 
 // ---- step.cu ----
-void launch_pair_sum(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t slots,
+void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* depth_order, const uint32_t* first,
                      const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
 void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
                  const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);

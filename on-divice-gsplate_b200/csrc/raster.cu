@@ -40,31 +40,57 @@ struct RasterArgs {
 
 __device__ __forceinline__ uint32_t pack_unorm(float v) { return uint32_t(clampf(v, 0.0f, 1.0f) * 255.0f + 0.5f); }
 
-// Culling terms of a staged splat: (limit, -b/c, -b/a) for the conic (a, b, c). A pixel at
-// offset d from the centre contributes only if alpha = opacity exp(-Q(d)/2) >= 1/255, with
-// Q(d) = a dx^2 + 2b dx dy + c dy^2, i.e. Q(d) <= 2 ln(255 opacity); the stored footprint
-// threshold (train_common.glsl:169-172) already exceeds that, and the limit adds 2^-10
-// relative and absolute on top, far above the rounding of Q and of the fast exponential.
-__device__ __forceinline__ float4 cull_terms(float blue, float4 A, float4 B, float threshold) {
-  return make_float4(blue, threshold * 1.0009765625f + 0.0009765625f, -__fdividef(B.x, B.y), -__fdividef(B.x, A.w));
+// A staged splat, in three float4s:
+//   A = (centre x, centre y, opacity, ha)   B = (hb, hc, red, green)   C = (blue, limit, kz, kw)
+// with the conic (a, b, c) scaled to the base-2 exponent: for the offset d = centre - pixel,
+//   E(d) = ha dx^2 + hb dx dy + hc dy^2 = log2(e) power(d),   power = -(a dx^2 + c dy^2)/2 - b dx dy,
+// (ha, hb, hc) = -log2(e) (a/2, b, c/2), so alpha = min(0.99, opacity 2^E). Both passes
+// evaluate E, alpha and the transmittance with the same operations in the same order
+// (fmaf and the non-contracting _rn forms), so the backward reproduces the forward's
+// transmittance bit for bit.
+//
+// Culling: a pixel contributes only if alpha >= 1/255, i.e. Q(d) = -2 power(d) <= 2 ln(255
+// opacity); the footprint threshold (train_common.glsl:169-172) already exceeds that, and
+// `limit` adds 2^-10 relative and absolute on top (far above the rounding of Q and of the
+// fast exponential), stored as the matching bound on E: E >= -log2(e)/2 limit. kz = -b/c and
+// kw = -b/a locate the maximum of E along a vertical and a horizontal edge.
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ void stage_splat(float4 q0, float4 q1, float4 q2, float threshold, float4& A, float4& B,
+                                            float4& C) {
+  const float a = q1.x, b = q1.y, c = q1.z;
+  A = make_float4(q0.x, q0.y, q0.w, __fmul_rn(a, -0.5f * kLog2e));
+  B = make_float4(__fmul_rn(b, -kLog2e), __fmul_rn(c, -0.5f * kLog2e), q2.x, q2.y);
+  const float limit = threshold * 1.0009765625f + 0.0009765625f;
+  C = make_float4(q2.z, limit * (-0.5f * kLog2e), -__fdividef(b, c), -__fdividef(b, a));
 }
 
-// Whether a splat's footprint ellipse reaches a pixel centre of the 8 x h block whose first
-// centre is (x0, y0): the minimum of the convex Q over the block's rectangle is 0 when the
-// centre lies inside, else it lies on an edge facing the centre, where the minimiser along
-// the edge is the unconstrained one clamped to the edge.
-// A = (centre x, centre y, opacity, a), B = (b, c, ...), K = cull_terms.
-__device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 K, float x0, float y0, float h) {
+// The base-2 exponent at offset (dx, dy); e0 = ha dx dx and e1 = hb dx are per splat and lane.
+__device__ __forceinline__ float splat_exponent(float e0, float e1, float hc, float dy) {
+  return fmaf(fmaf(hc, dy, e1), dy, e0);
+}
+
+__device__ __forceinline__ float exp2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Whether a staged splat's footprint ellipse reaches a pixel centre of the 8 x h block
+// whose first centre is (x0, y0): the maximum of the concave E over the block's rectangle
+// is 0 when the centre lies inside, else it lies on an edge facing the centre, at the
+// unconstrained maximiser along that edge clamped to the edge.
+__device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 C, float x0, float y0, float h) {
   const float dx0 = x0 - A.x, dx1 = dx0 + 7.0f, dy0 = y0 - A.y, dy1 = dy0 + (h - 1.0f);
   const float ex = dx0 > 0.0f ? dx0 : fminf(dx1, 0.0f);  // facing vertical edge (0: none)
   const float ey = dy0 > 0.0f ? dy0 : fminf(dy1, 0.0f);  // facing horizontal edge (0: none)
-  const float a = A.w, b = B.x, c = B.y;
-  const float ty = fminf(fmaxf(K.z * ex, dy0), dy1);
-  const float tx = fminf(fmaxf(K.w * ey, dx0), dx1);
-  const float qv = ex != 0.0f ? ex * (a * ex + 2.0f * b * ty) + c * ty * ty : 3.0e38f;
-  const float qh = ey != 0.0f ? tx * (a * tx + 2.0f * b * ey) + c * ey * ey : 3.0e38f;
-  const float q = (ex == 0.0f && ey == 0.0f) ? 0.0f : fminf(qv, qh);
-  return q <= K.y;
+  const float ha = A.w, hb = B.x, hc = B.y;
+  const float ty = fminf(fmaxf(C.z * ex, dy0), dy1);
+  const float tx = fminf(fmaxf(C.w * ey, dx0), dx1);
+  const float ev = ex != 0.0f ? ex * (ha * ex + hb * ty) + hc * ty * ty : -3.0e38f;
+  const float eh = ey != 0.0f ? tx * (ha * tx + hb * ey) + hc * ey * ey : -3.0e38f;
+  const float e = (ex == 0.0f && ey == 0.0f) ? 0.0f : fmaxf(ev, eh);
+  return e >= C.y;
 }
 
 // The tile and pixel layout of one block.
@@ -105,9 +131,9 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
 template <int PX>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
-  __shared__ float4 s_a[256];  // centre xy, opacity, conic a
-  __shared__ float4 s_b[256];  // conic b, conic c, red, green
-  __shared__ float4 s_c[256];  // blue, culling terms
+  __shared__ float4 s_a[256];  // staged splats (stage_splat)
+  __shared__ float4 s_b[256];
+  __shared__ float4 s_c[256];
   __shared__ float s_red[L::kWarps][16];
   __shared__ uint32_t s_max[L::kWarps];
 
@@ -143,10 +169,11 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t g = a.rb.pair_gaussian[a.rb.values[k]];
         const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u],
                      q2 = a.splat[size_t(g) * 3u + 2u];
-        const float4 A = make_float4(q0.x, q0.y, q0.w, q1.x), B = make_float4(q1.y, q1.z, q2.x, q2.y);
+        float4 A, B, C;
+        stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
         s_a[slot] = A;
         s_b[slot] = B;
-        s_c[slot] = cull_terms(q2.z, A, B, a.foot[g].w);
+        s_c[slot] = C;
       }
     }
     __syncthreads();
@@ -169,16 +196,16 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         const float4 A = s_a[j];
         const float4 B = s_b[j];
         const float blue = s_c[j].x;
-        const float dx = A.x - cx;
+        const float dx = __fsub_rn(A.x, cx);
+        const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
         all_done = true;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
           if (!done[p]) {
-            const float dy = A.y - cy[p];
-            const float power = -0.5f * (A.w * dx * dx + B.y * dy * dy) - B.x * dx * dy;
-            const float alpha = fminf(kMaxAlpha, A.z * __expf(power));
-            if (power <= 0.0f && alpha >= kMinAlpha) {
-              const float next_T = T[p] * (1.0f - alpha);
+            const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
+            const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
+            if (e <= 0.0f && alpha >= kMinAlpha) {
+              const float next_T = __fmul_rn(T[p], __fsub_rn(1.0f, alpha));
               if (next_T < kMinTransmittance) {
                 done[p] = true;
               } else {
@@ -302,7 +329,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   static_assert(BATCH <= L::kThreads, "one staged splat per thread");
   __shared__ float4 s_a[BATCH];
   __shared__ float4 s_b[BATCH];
-  __shared__ float4 s_c[BATCH];  // blue, culling terms
+  __shared__ float4 s_c[BATCH];  // staged splats (stage_splat): s_a, s_b, s_c
   __shared__ uint32_t s_dst[BATCH];
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
@@ -354,10 +381,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
       const uint32_t pre = a.rb.values[range.x + start + lid];
       const uint32_t g = a.rb.pair_gaussian[pre];
       const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
-      const float4 A = make_float4(q0.x, q0.y, q0.w, q1.x), B = make_float4(q1.y, q1.z, q2.x, q2.y);
+      float4 A, B, C;
+      stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
       s_a[lid] = A;
       s_b[lid] = B;
-      s_c[lid] = cull_terms(q2.z, A, B, a.foot[g].w);
+      s_c[lid] = C;
       s_dst[lid] = DET ? pre : g;
     }
     __syncthreads();
@@ -376,7 +404,13 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         const float4 A = s_a[j];
         const float4 B = s_b[j];
         const float blue = s_c[j].x;
-        const float dx = A.x - cx;
+        const float dx = __fsub_rn(A.x, cx);
+        const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
+        // The conic (a, b, c) back from the scaled exponent terms, for the mean gradient:
+        // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy).
+        const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
+        const float lx = -ca * dx, ly = -cb * dx, mx = -cb, my = -cc;
+        const float hx = -0.5f * dx * dx;
         float c[12];
 #pragma unroll
         for (int k = 0; k < 12; ++k) c[k] = 0.0f;
@@ -384,26 +418,26 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
           if (pos > last[p]) continue;
-          const float dy = A.y - cy[p];
-          const float power = -0.5f * (A.w * dx * dx + B.y * dy * dy) - B.x * dx * dy;
-          const float G = __expf(power);
-          const float raw = A.z * G;
+          const float dy = __fsub_rn(A.y, cy[p]);
+          const float e = splat_exponent(e0, e1, B.y, dy);
+          const float G = exp2_approx(e);
+          const float raw = __fmul_rn(A.z, G);
           const float alpha = fminf(kMaxAlpha, raw);
-          if (power > 0.0f || alpha < kMinAlpha) continue;
+          if (e > 0.0f || alpha < kMinAlpha) continue;
           has = true;
           const float gc = dl0[p] * B.z + dl1[p] * B.w + dl2[p] * blue;
           const float weight = alpha * T[p];
           const float rest = R[p] - gc * weight;
-          const float one_minus = 1.0f - alpha;
+          const float one_minus = __fsub_rn(1.0f, alpha);
           const float dlda = T[p] * gc - __fdividef(rest, one_minus);
           const bool clamped = raw >= kMaxAlpha;
           const float dop = clamped ? 0.0f : G * dlda;
           const float dpow = clamped ? 0.0f : raw * dlda;
-          const float dmx = dpow * -(A.w * dx + B.x * dy);
-          const float dmy = dpow * -(B.y * dy + B.x * dx);
+          const float dmx = dpow * fmaf(mx, dy, lx);
+          const float dmy = dpow * fmaf(my, dy, ly);
           c[0] += dmx;
           c[1] += dmy;
-          c[2] += dpow * (-0.5f * dx * dx);
+          c[2] += dpow * hx;
           c[3] += dpow * (-dx * dy);
           c[4] += dpow * (-0.5f * dy * dy);
           c[5] += dop;
@@ -412,7 +446,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           c[8] += weight * dl2[p];
           c[9] += fabsf(dmx);
           c[10] += fabsf(dmy);
-          T[p] = T[p] * one_minus;
+          T[p] = __fmul_rn(T[p], one_minus);
           R[p] = rest;
         }
         if (__any_sync(0xffffffffu, has)) {

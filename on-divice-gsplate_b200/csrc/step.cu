@@ -4,9 +4,10 @@
 // train_densify_spawn.comp) and the opacity reset (train_reset_opacity.comp).
 //
 // The step back-propagates every view's summed 2D gradient through that view's projection
-// (views of one step add up) and takes one Adam step on the 16 parameters
-// (k_step_geometry) and on the active SH coefficients (k_step_sh). HBM-bound: parameters,
-// SH and both moment sets are read and written once per step (SH read twice).
+// (views of one step add up) and takes one Adam step on the active SH coefficients
+// (k_step_sh, first: it also produces the position gradient through the SH view
+// direction) and on the 16 parameters (k_step_geometry). HBM-bound: parameters, SH and
+// both moment sets are read and written once per step.
 #include <utility>
 
 #include "gs_kernels.h"
@@ -15,28 +16,33 @@ namespace gsk {
 namespace {
 
 struct PairSumArgs {
-  uint32_t n_views, cap, slots;
-  const uint32_t* tiles;
-  const uint32_t* offsets;
+  uint32_t n_items;
+  const uint32_t* order;   // items (view * cap + slot) in depth order
+  const uint32_t* first;   // their first pair, in the same order
   const float4* pair_grads;
   float4* grad2d;
   const uint32_t* d_pairs;
   uint32_t accept;
 };
 
+// Items in depth order, so consecutive threads sum consecutive runs of pairs (the emit
+// order); an item's count is the gap to the next item's first pair. Items that drew no
+// pair are skipped: the step reads grad2d only where tiles > 0.
 __global__ void __launch_bounds__(128) k_pair_sum(PairSumArgs a) {
-  if (*a.d_pairs > a.accept) return;
+  const uint32_t total = *a.d_pairs;
+  if (total > a.accept) return;
   const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.n_views * a.slots) return;
-  const uint32_t v = idx / a.slots, i = idx - v * a.slots;
-  const size_t g = size_t(v) * a.cap + i;
-  const uint32_t count = a.tiles[g];
+  if (idx >= a.n_items) return;
+  const uint32_t first = a.first[idx];
+  const uint32_t count = (idx + 1u < a.n_items ? a.first[idx + 1u] : total) - first;
+  if (count == 0u) return;
+  const size_t g = a.order[idx];
   float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0, s2 = s0;
-  if (count > 0u) {
-    const size_t first = a.offsets[g];
+  {
+#pragma unroll 4
     for (uint32_t k = 0; k < count; ++k) {
-      const float4 x = a.pair_grads[(first + k) * 3u], y = a.pair_grads[(first + k) * 3u + 1u],
-                   z = a.pair_grads[(first + k) * 3u + 2u];
+      const size_t q = (size_t(first) + k) * 3u;
+      const float4 x = a.pair_grads[q], y = a.pair_grads[q + 1u], z = a.pair_grads[q + 2u];
       s0.x += x.x; s0.y += x.y; s0.z += x.z; s0.w += x.w;
       s1.x += y.x; s1.y += y.y; s1.z += y.z; s1.w += y.w;
       s2.x += z.x; s2.y += z.y; s2.z += z.z; s2.w += z.w;
@@ -60,16 +66,30 @@ struct StepArgs {
   const float4* splat;
   const uint32_t* tiles;
   const float4* grad2d;
-  float4* shin;  // several views: per (view, slot) colour gradient + drew flag, view direction
+  float4* dir_grad;  // per slot: position gradient through the SH view direction (k_step_sh -> k_step_geometry)
   const uint32_t* d_pairs;
   uint32_t accept;
 };
 
+// Adam (train_step.glsl:62-67). The square root and the division use the hardware's
+// approximate forms (PTX sqrt.approx.f32, relative error within 2^-23; div.full.f32,
+// within 2 ulp), the precision class of the reference's GLSL sqrt and division; the
+// IEEE-rounded sequences cost several times the instructions and a branch each.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float div_full(float a, float b) {
+  float r;
+  asm("div.full.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
 __device__ __forceinline__ float adam1(float p, float g, float& m, float& v, float lr, float b1, float b2, float c1,
                                        float c2, float eps) {
   m = g * (1.0f - b1) + m * b1;
   v = g * g * (1.0f - b2) + v * b2;
-  return p - lr * (m * c1) / (sqrtf(v * c2) + eps);
+  return p - lr * div_full(m * c1, sqrt_approx(v * c2) + eps);
 }
 
 // Basis function k (1..15) of the real SH basis and its gradient w.r.t. the unit
@@ -142,11 +162,18 @@ __device__ __forceinline__ void slot_geometry(float4 p0, float4 p1, float4 q, Ge
   G.opacity = sigmoidf(p0.w);
 }
 
+// Colour gradient of one view with the clamped channels zeroed (train_step.glsl:135-138).
+__device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t clamped, float dcol[3]) {
+  dcol[0] = (clamped & 1u) ? 0.0f : a1.z;
+  dcol[1] = (clamped & 2u) ? 0.0f : a1.w;
+  dcol[2] = (clamped & 4u) ? 0.0f : a2.x;
+}
+
 // One view's projection backward (train_step.glsl:82-219) of a slot: adds the gradient of
-// the 14 geometry + DC parameters to g16 (without the SH view-direction term, which the
-// caller adds through `dir`/`dir_len`), updates the densification statistics, and returns
-// the clamped colour gradient and the view direction. drew: bit 0 any pair gradient, bit
-// 1 a non-zero colour gradient.
+// the 14 geometry + DC parameters to g16 (without the SH view-direction term, which
+// k_step_sh computes), updates the densification statistics, and returns the clamped
+// colour gradient and the view direction. drew: bit 0 any pair gradient, bit 1 a non-zero
+// colour gradient.
 template <int DEG>
 __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0, const Geometry& G, float4 a0, float4 a1,
                                               float4 a2, uint32_t clamped, float radius, float g16[16], float4& st,
@@ -157,9 +184,7 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   const float dmx = a0.x, dmy = a0.y;
   const float ga = a0.z, gb = a0.w, gc = a1.x;
   const float dop = a1.y;
-  dcol[0] = (clamped & 1u) ? 0.0f : a1.z;
-  dcol[1] = (clamped & 2u) ? 0.0f : a1.w;
-  dcol[2] = (clamped & 4u) ? 0.0f : a2.x;
+  view_colour_grad(a1, a2, clamped, dcol);
   if (dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f) drew |= 2u;
   const float width = float(f.image[0]), height = float(f.image[1]);
   const float nx = 0.5f * width, ny = 0.5f * height;
@@ -333,8 +358,91 @@ __device__ __forceinline__ void copy_frames(const StepArgs& a, gs_frame_data* s_
   __syncthreads();
 }
 
-// Part 1 (train_step.glsl:72-240): every view's projection backward summed, Adam on the
-// 16 parameters; each view's colour gradient and direction go to `shin` for part 2.
+// Part 1 (train_step_sh.comp:21-44 and the SH view-direction term of
+// train_step.glsl:131-155): one thread per slot. The slot's SH coefficients are loaded
+// once; for each view the slot was seen in, the basis and its direction gradient are
+// evaluated once, giving all 3K coefficient gradients (added in view order) and dL/d(dir),
+// which goes through the normalisation into the position gradient (summed over views,
+// stored for part 2). Then Adam on the 3K coefficients, 3 coefficients' moments loaded
+// together so each thread keeps 18 loads in flight (the SH values are already loaded).
+template <int DEG>
+__global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
+  __shared__ gs_frame_data s_frames[kMaxViews];
+  copy_frames(a, s_frames, a.n_views);
+  if (*a.d_pairs > a.accept) return;
+  constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.slots) return;
+  const float4 p0 = a.P[i];
+  if (a.P[a.cap + i].w < 0.5f) return;
+  float sh[K][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sh[k][c] = a.SH[size_t(3 * k + c) * a.cap + i];
+  float g[K][3];
+#pragma unroll
+  for (int k = 0; k < K; ++k) g[k][0] = g[k][1] = g[k][2] = 0.0f;
+  float pd[3] = {0.f, 0.f, 0.f};
+  bool colour = false;
+  for (uint32_t v = 0; v < a.n_views; ++v) {
+    const size_t gv = size_t(v) * a.cap + i;
+    if (a.tiles[gv] == 0u) continue;
+    float dcol[3];
+    view_colour_grad(a.grad2d[gv * 3u + 1u], a.grad2d[gv * 3u + 2u], __float_as_uint(a.splat[gv * 3u + 2u].w), dcol);
+    colour |= dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f;
+    const gs_frame_data& f = s_frames[v];
+    const float dr0 = p0.x - f.cam_pos[0], dr1 = p0.y - f.cam_pos[1], dr2 = p0.z - f.cam_pos[2];
+    const float dir_len = fmaxf(sqrtf(dr0 * dr0 + dr1 * dr1 + dr2 * dr2), 1e-12f);
+    const float dir[3] = {dr0 / dir_len, dr1 / dir_len, dr2 / dir_len};
+    float dd[3] = {0.f, 0.f, 0.f};
+    for_terms(std::make_integer_sequence<int, K>{}, [&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      float gx, gy, gz;
+      const float b = sh_term<k>(dir[0], dir[1], dir[2], gx, gy, gz);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[k - 1][c] += b * dcol[c];
+      const float w = sh[k - 1][0] * dcol[0] + sh[k - 1][1] * dcol[1] + sh[k - 1][2] * dcol[2];
+      dd[0] += w * gx;
+      dd[1] += w * gy;
+      dd[2] += w * gz;
+    });
+    const float proj = dir[0] * dd[0] + dir[1] * dd[1] + dir[2] * dd[2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pd[c] += (dd[c] - dir[c] * proj) / dir_len;
+  }
+  a.dir_grad[i] = make_float4(pd[0], pd[1], pd[2], 0.0f);
+  const gs_frame_data& f0 = s_frames[0];
+  if ((f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u && !colour) return;
+  const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1], lr = f0.lr1[1];
+  constexpr int kChunk = 3;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += kChunk) {
+    float m[kChunk][3], v[kChunk][3];
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (k0 + j < K) {
+          const size_t o = size_t(3 * (k0 + j) + c) * a.cap + i;
+          m[j][c] = a.MSH[o];
+          v[j][c] = a.VSH[o];
+        }
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (k0 + j < K) {
+          const size_t o = size_t(3 * (k0 + j) + c) * a.cap + i;
+          a.SH[o] = adam1(sh[k0 + j][c], g[k0 + j][c], m[j][c], v[j][c], lr, b1, b2, c1, c2, eps);
+          a.MSH[o] = m[j][c];
+          a.VSH[o] = v[j][c];
+        }
+  }
+}
+
+// Part 2 (train_step.glsl:72-240): every view's projection backward summed, plus the SH
+// view-direction term from part 1, then Adam on the 16 parameters.
 template <int DEG>
 __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
@@ -342,7 +450,6 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   if (*a.d_pairs > a.accept) return;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.slots) return;
-  constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
   const float4 p0 = a.P[i], p1 = a.P[a.cap + i], q = a.P[2u * a.cap + i], p3 = a.P[3u * a.cap + i];
   if (p1.w < 0.5f) return;
   float g16[16];
@@ -355,86 +462,23 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   bool seen = false;
   for (uint32_t v = 0; v < a.n_views; ++v) {
     const size_t g = size_t(v) * a.cap + i;
-    if (a.tiles[g] == 0u) {
-      a.shin[g * 2u] = make_float4(0.f, 0.f, 0.f, 0.f);
-      continue;
-    }
+    if (a.tiles[g] == 0u) continue;
     seen = true;
     float dcol[3], dir[3], dir_len;
-    uint32_t vdrew = 0u;
     view_backward<DEG>(s_frames[v], p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u], a.grad2d[g * 3u + 2u],
                        __float_as_uint(a.splat[g * 3u + 2u].w), a.splat[g * 3u + 1u].w, g16, st, dcol, dir, dir_len,
-                       vdrew);
-    drew |= vdrew;
-    if constexpr (K > 0) {
-      float dd[3] = {0.f, 0.f, 0.f};
-      for_terms(std::make_integer_sequence<int, K>{}, [&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        float gx, gy, gz;
-        sh_term<k>(dir[0], dir[1], dir[2], gx, gy, gz);
-        const float w = a.SH[size_t(3 * (k - 1)) * a.cap + i] * dcol[0] +
-                        a.SH[size_t(3 * (k - 1) + 1) * a.cap + i] * dcol[1] +
-                        a.SH[size_t(3 * (k - 1) + 2) * a.cap + i] * dcol[2];
-        dd[0] += w * gx;
-        dd[1] += w * gy;
-        dd[2] += w * gz;
-      });
-      add_direction_term(g16, dir, dir_len, dd);
-    }
-    a.shin[g * 2u] = make_float4(dcol[0], dcol[1], dcol[2], (vdrew & 2u) ? 1.0f : 0.0f);
-    a.shin[g * 2u + 1u] = make_float4(dir[0], dir[1], dir[2], 0.0f);
+                       drew);
+  }
+  if (DEG > 0) {
+    const float4 pd = a.dir_grad[i];
+    g16[0] += pd.x;
+    g16[1] += pd.y;
+    g16[2] += pd.z;
   }
   if (seen) a.stats[i] = st;
   const gs_frame_data& f0 = s_frames[0];
   const bool sparse = (f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u;
   if (!sparse || (drew & 1u)) adam_params(a, f0, i, p0, p1, q, p3, g16);
-}
-
-// Part 2 (train_step_sh.comp:21-44): one thread per slot. For each view the slot was seen
-// in, it evaluates the SH basis at the view direction once and adds basis x colour
-// gradient to all 3K coefficient gradients in registers (in view order), then takes the
-// Adam step on the 3K coefficients, plane by plane (consecutive slots on consecutive
-// threads). Each view's colour gradient and direction are read once; the SH planes and
-// both moment sets once each.
-template <int DEG>
-__global__ void __launch_bounds__(128) k_step_sh(StepArgs a) {
-  if (*a.d_pairs > a.accept) return;
-  constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.slots) return;
-  if (a.P[a.cap + i].w < 0.5f) return;
-  float g[K][3];
-#pragma unroll
-  for (int k = 0; k < K; ++k) g[k][0] = g[k][1] = g[k][2] = 0.0f;
-  bool colour = false;
-  for (uint32_t v = 0; v < a.n_views; ++v) {
-    const size_t gi = size_t(v) * a.cap + i;
-    if (a.tiles[gi] == 0u) continue;
-    const float4 c = a.shin[gi * 2u];
-    const float4 d = a.shin[gi * 2u + 1u];
-    float basis[16];
-    sh_basis<DEG>(d.x, d.y, d.z, basis);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      g[k][0] += basis[k + 1] * c.x;
-      g[k][1] += basis[k + 1] * c.y;
-      g[k][2] += basis[k + 1] * c.z;
-    }
-    colour |= c.w != 0.0f;
-  }
-  const gs_frame_data& f0 = a.frames[0];
-  if ((f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u && !colour) return;
-  const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1], lr = f0.lr1[1];
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const size_t o = size_t(3 * k + c) * a.cap + i;
-      float m = a.MSH[o], v = a.VSH[o];
-      a.SH[o] = adam1(a.SH[o], g[k][c], m, v, lr, b1, b2, c1, c2, eps);
-      a.MSH[o] = m;
-      a.VSH[o] = v;
-    }
 }
 
 // ---- densification ----
@@ -586,25 +630,24 @@ __global__ void __launch_bounds__(256) k_reset_opacity(float4* P, float4* M, flo
 
 }  // namespace
 
-void launch_pair_sum(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t slots,
+void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* depth_order, const uint32_t* first,
                      const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
-  const uint32_t n = sp.n_views * slots;
-  if (n == 0u) return;
-  PairSumArgs a{sp.n_views, cap, slots, vb.tiles, vb.offsets, pair_grads, vb.grad2d, d_pairs, accept};
-  k_pair_sum<<<(n + 127u) / 128u, 128, 0, st>>>(a);
+  if (n_items == 0u) return;
+  PairSumArgs a{n_items, depth_order, first, pair_grads, vb.grad2d, d_pairs, accept};
+  k_pair_sum<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 
 void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
                  const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
   if (m.slots == 0u) return;
   StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
-             vb.splat, vb.tiles, vb.grad2d, vb.shin, d_pairs, accept};
+             vb.splat, vb.tiles, vb.grad2d, vb.dir_grad, d_pairs, accept};
   const dim3 grid((m.slots + 127u) / 128u), block(128);
   switch (degree) {
     case 0: k_step_geometry<0><<<grid, block, 0, st>>>(a); break;
-    case 1: k_step_geometry<1><<<grid, block, 0, st>>>(a); k_step_sh<1><<<grid, block, 0, st>>>(a); break;
-    case 2: k_step_geometry<2><<<grid, block, 0, st>>>(a); k_step_sh<2><<<grid, block, 0, st>>>(a); break;
-    default: k_step_geometry<3><<<grid, block, 0, st>>>(a); k_step_sh<3><<<grid, block, 0, st>>>(a); break;
+    case 1: k_step_sh<1><<<grid, block, 0, st>>>(a); k_step_geometry<1><<<grid, block, 0, st>>>(a); break;
+    case 2: k_step_sh<2><<<grid, block, 0, st>>>(a); k_step_geometry<2><<<grid, block, 0, st>>>(a); break;
+    default: k_step_sh<3><<<grid, block, 0, st>>>(a); k_step_geometry<3><<<grid, block, 0, st>>>(a); break;
   }
 }
 
