@@ -123,6 +123,7 @@ typedef struct gs_tuning {
   uint32_t graph;             /* 1: capture the step as a CUDA graph and replay it while its launch
                                  structure (views, slots, buffer sizes, SH degree, mode) holds */
   uint32_t backward_batch;    /* splats staged per round of the backward pass: 32 or 64 (0: default) */
+  uint32_t sort_digit_bits;   /* radix digit width of the depth and pair sorts: 4..8 (0: default 8) */
 } gs_tuning;
 
 typedef struct gs_model_info {
@@ -198,6 +199,17 @@ int gs_snapshot(gs_context* ctx, uint32_t view, gs_snapshot_kind which, void* ho
 
 int gs_set_tuning(gs_context* ctx, const gs_tuning* tuning);
 int gs_get_tuning(gs_context* ctx, gs_tuning* tuning);
+
+/* Picks the tuning for the views set last (gs_set_views / gs_set_views_dataset, with
+   targets), as Trainer's backward retune does (trainer.h:150-157; trainer.cpp:876-897, 983-987): it
+   times training steps under candidate settings of forward_pixels, (backward_pixels,
+   backward_batch) and sort_digit_bits, one knob after the other keeping the fastest (each
+   candidate: one untimed step, then `steps_per_candidate` steps timed with CUDA events),
+   and makes the fastest the context's tuning (written to `chosen` when not NULL). The
+   candidates compute the same gradients up to summation order. The model, its moments and
+   densification statistics are restored afterwards, so the call leaves training where it
+   was; it needs device memory for one copy of them. */
+int gs_autotune(gs_context* ctx, uint32_t steps_per_candidate, gs_tuning* chosen);
 
 /* No counterpart in the reference: its RadixSort allocates its own temporary buffers
    (engine/src/radix_sort.cpp:37-39). For callers that cannot allocate device memory —

@@ -282,7 +282,8 @@ struct gs_context {
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
     const std::vector<uint64_t> key = {n_views, model.slots, model.cap, pair_cap, tile_cap, pixel_cap, degree,
                                        train ? 1u : 0u, ssim ? 1u : 0u, tuning.deterministic,
-                                       tuning.forward_pixels, tuning.backward_pixels, tuning.backward_batch};
+                                       tuning.forward_pixels, tuning.backward_pixels, tuning.backward_batch,
+                                       tuning.sort_digit_bits};
     if (graph_exec == nullptr || key != graph_key) {
       drop_graph();
       cudaGraph_t g = nullptr;
@@ -369,6 +370,98 @@ struct gs_context {
     }
   }
 
+  // Mean device time of `steps` training steps under tuning `t`, after one untimed step
+  // (graph capture, buffer growth).
+  float time_tuning(const gs_tuning& t, uint32_t steps) {
+    tuning = t;
+    drop_graph();
+    run_step(true, nullptr);
+    float ms = 0.0f;
+    for (uint32_t k = 0; k < steps; ++k) {
+      gs_step_result r;
+      run_step(true, &r);
+      ms += r.gpu_ms;
+    }
+    return ms / float(steps);
+  }
+
+  // gs_autotune: greedy over the knobs, the model restored afterwards (trainer.cpp:876-897
+  // times its backward variants on training steps the same way and keeps the fastest).
+  void autotune(uint32_t steps) {
+    if (n_views == 0 || !has_target) fail(GS_ERR_INVALID, "gs_autotune: needs views with targets (gs_set_views)");
+    const size_t planes4 = sizeof(float4) * model.cap, planes_sh = sizeof(float) * size_t(model.sh_stride) * model.cap;
+    struct Part {
+      void* ptr;
+      size_t bytes;
+    };
+    const Part parts[] = {{model.P, 4 * planes4},     {model.M, 4 * planes4},      {model.V, 4 * planes4},
+                          {model.stats, planes4},     {model.SH, planes_sh},       {model.MSH, planes_sh},
+                          {model.VSH, planes_sh}};
+    size_t total = 0;
+    for (const Part& p : parts) total += p.bytes;
+    uint8_t* backup = nullptr;
+    if (cudaMalloc(&backup, total) != cudaSuccess) {
+      cudaGetLastError();
+      fail(GS_ERR_NO_MEMORY, "gs_autotune: no device memory for a copy of the model");
+    }
+    size_t at = 0;
+    for (const Part& p : parts) {
+      if (p.bytes) cudaMemcpyAsync(backup + at, p.ptr, p.bytes, cudaMemcpyDeviceToDevice, stream);
+      at += p.bytes;
+    }
+    const gs_tuning start = tuning;
+    gs_tuning best = start;
+    std::string failure;
+    int failure_code = GS_OK;
+    try {
+      float best_ms = time_tuning(best, steps);
+      auto consider = [&](gs_tuning t) {
+        const float ms = time_tuning(t, steps);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = t;
+        }
+      };
+      const uint32_t fpx0 = best.forward_pixels;
+      for (uint32_t fpx : {1u, 2u, 4u})
+        if (fpx != fpx0) {
+          gs_tuning t = best;
+          t.forward_pixels = fpx;
+          consider(t);
+        }
+      const uint32_t bpx0 = best.backward_pixels, batch0 = best.backward_batch;
+      for (uint32_t bpx : {2u, 4u})
+        for (uint32_t batch : {32u, 64u})
+          if (bpx != bpx0 || batch != batch0) {
+            gs_tuning t = best;
+            t.backward_pixels = bpx;
+            t.backward_batch = batch;
+            consider(t);
+          }
+      const uint32_t digits0 = best.sort_digit_bits;
+      for (uint32_t digits : {6u, 7u, 8u})
+        if (digits != digits0) {
+          gs_tuning t = best;
+          t.sort_digit_bits = digits;
+          consider(t);
+        }
+    } catch (const Failure& e) {
+      failure_code = e.code;
+      failure = e.message;
+    }
+    at = 0;
+    for (const Part& p : parts) {
+      if (p.bytes) cudaMemcpyAsync(p.ptr, backup + at, p.bytes, cudaMemcpyDeviceToDevice, stream);
+      at += p.bytes;
+    }
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    cudaFree(backup);
+    tuning = failure_code == GS_OK ? best : start;
+    drop_graph();
+    if (failure_code != GS_OK) fail(failure_code, "gs_autotune: " + failure);
+    if (e != cudaSuccess) fail(GS_ERR_CUDA, std::string("gs_autotune: ") + cudaGetErrorString(e));
+  }
+
   // Pairs of each view: pairs are ordered by view, so the first pair of view v+1 bounds v.
   void view_pairs(uint64_t* out) {
     if (n_views == 1) {
@@ -427,8 +520,9 @@ struct gs_context {
     mark(1);
     // Depth sort of every (view, slot): key = view << 16 | depth16.
     const int depth_bits = 16 + int(bits_for(n_views));
+    const int digit_bits = tuning.sort_digit_bits ? int(tuning.sort_digit_bits) : 8;
     const bool in_alt = gsk::radix_sort_pairs(sort, dkeys, dvals, dkeys_alt, dvals_alt, nullptr, items, depth_bits,
-                                              stream, &launches);
+                                              stream, &launches, digit_bits);
     depth_sorted_keys = in_alt ? dkeys_alt : dkeys;
     depth_sorted_vals = in_alt ? dvals_alt : dvals;
     // Offsets of each item's pairs in depth order; the total is the step's pair count.
@@ -439,7 +533,8 @@ struct gs_context {
     const uint32_t max_tiles = uint32_t(tile_cap - 1);
     const int tile_bits = int(bits_for(max_tiles + 1));
     const bool pairs_alt = gsk::radix_sort_pairs(sort, keys, values, keys_alt, values_alt, d_scalars,
-                                                 uint32_t(pair_cap), std::max(tile_bits, 1), stream, &launches);
+                                                 uint32_t(pair_cap), std::max(tile_bits, 1), stream, &launches,
+                                                 digit_bits);
     sorted_keys = pairs_alt ? keys_alt : keys;
     sorted_values = pairs_alt ? values_alt : values;
     GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (max_tiles + 1), stream));
@@ -664,6 +759,7 @@ int gs_create(int device, gs_context** out) {
     c->tuning.forward_pixels = 2u;
     c->tuning.backward_pixels = 4u;
     c->tuning.backward_batch = 64u;
+    c->tuning.sort_digit_bits = 8u;
     c->tuning.retry = 1u;
     c->tuning.graph = 0u;
     try {
@@ -680,7 +776,7 @@ int gs_create(int device, gs_context** out) {
       c->sm_count = prop.multiProcessorCount;
       dev_alloc(c->d_scalars, 4);
       dev_alloc(c->d_view_sums, 8 * GS_MAX_VIEWS);
-      dev_alloc(c->sort.hist, 4 * 256);
+      dev_alloc(c->sort.hist, 8 * 256);
       dev_alloc(c->sort.ticket, 1);
       dev_alloc(c->sort.err, 1);
       GS_CUDA_TRY(cudaMemset(c->d_scalars, 0, 4 * sizeof(uint32_t)));
@@ -1019,6 +1115,8 @@ int gs_set_tuning(gs_context* c, const gs_tuning* t) {
         fail(GS_ERR_INVALID, "gs_set_tuning: pixels per thread must be 1, 2 or 4");
     if (t->backward_batch != 0 && t->backward_batch != 32 && t->backward_batch != 64)
       fail(GS_ERR_INVALID, "gs_set_tuning: backward_batch must be 32 or 64");
+    if (t->sort_digit_bits != 0 && (t->sort_digit_bits < 4 || t->sort_digit_bits > 8))
+      fail(GS_ERR_INVALID, "gs_set_tuning: sort_digit_bits must be 4..8");
     c->tuning = *t;
     if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
     c->drop_graph();
@@ -1029,6 +1127,16 @@ int gs_get_tuning(gs_context* c, gs_tuning* t) {
   return guarded([&] {
     if (c == nullptr || t == nullptr) fail(GS_ERR_INVALID, "gs_get_tuning: null argument");
     *t = c->tuning;
+  });
+}
+
+int gs_autotune(gs_context* c, uint32_t steps_per_candidate, gs_tuning* chosen) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_autotune: null context");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    c->profile = false;
+    c->autotune(std::max(1u, steps_per_candidate));
+    if (chosen != nullptr) *chosen = c->tuning;
   });
 }
 

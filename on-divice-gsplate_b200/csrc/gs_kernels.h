@@ -50,7 +50,7 @@ void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, con
 
 // ---- sort.cu ----
 struct SortScratch {
-  uint32_t* hist = nullptr;           // 4 passes x 256
+  uint32_t* hist = nullptr;           // passes x 256 (up to 8 passes: 32-bit keys at 4-bit digits)
   uint32_t* lookback = nullptr;       // tiles x 256 status words
   uint32_t lookback_tiles = 0;
   unsigned long long* scan_lookback = nullptr;
@@ -60,10 +60,12 @@ struct SortScratch {
 };
 constexpr uint32_t kSortTile = 256 * 15;
 constexpr uint32_t kScanTile = 256 * 8;
-// Sorts (keys, vals) of min(*d_count, n_max) items by key bits [0, bits), stable. Returns
-// true when the result ended in the alternate buffers.
+// Sorts (keys, vals) of min(*d_count, n_max) items by key bits [0, bits), stable, in
+// passes of `digit_bits` (4..8) bits. Returns true when the result ended in the alternate
+// buffers.
 bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
-                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches);
+                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches,
+                      int digit_bits = 8);
 // Exclusive scan of in[gather ? gather[k] : k] for k < n; *d_total (if non-null) = the sum.
 void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* gather, uint32_t* out, uint32_t n,
                     uint32_t* d_total, cudaStream_t st, int* launches);

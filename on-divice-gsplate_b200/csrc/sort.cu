@@ -3,7 +3,8 @@
 // The reference sorts with a 3-kernel LSD radix sort of 4-bit digits (count, single
 // workgroup scan, scatter: engine/src/radix_sort.cpp:57-108, radix_{count,scan,scatter}.comp)
 // and scans with scan_local/blocks/add. Here:
-//  - radix_sort_pairs: onesweep LSD sort, 8-bit digits. One kernel computes every pass's
+//  - radix_sort_pairs: onesweep LSD sort, digits of 4 to 8 bits (8 by default; the width is
+//    a tuning knob). One kernel computes every pass's
 //    digit histogram; each pass is then one kernel in which a block ranks its 3840 keys
 //    (warp match + per-warp counters, stable), publishes its digit counts and looks back
 //    over its predecessors' (decoupled look-back) for its global digit offsets, then
@@ -22,7 +23,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kIpt = 15;  // keys per thread
-constexpr int kRadix = 256;
+constexpr int kRadix = 256;  // digit tables are sized for 8-bit digits; narrower digits use a prefix
+constexpr int kMaxPasses = 8;  // 32-bit keys at 4-bit digits
 constexpr uint32_t kSpinLimit = 1u << 22;
 constexpr uint32_t kAgg = 1u << 30, kPrefix = 2u << 30, kValueMask = (1u << 30) - 1u;
 
@@ -67,15 +69,22 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T& total) {
   return warp_prefix + x - v;
 }
 
+// Digit of pass p: bits [digit_bits p, min(digit_bits (p + 1), bits)) of the key.
+__device__ __forceinline__ uint32_t pass_mask(int bits, int digit_bits, int p) {
+  return (1u << min(digit_bits, bits - digit_bits * p)) - 1u;
+}
+
 __global__ void __launch_bounds__(kThreads) k_histogram(const uint32_t* __restrict__ keys, const uint32_t* d_count,
-                                                        uint32_t n_max, int passes, uint32_t* __restrict__ hist) {
-  __shared__ uint32_t s_hist[4][kRadix];
-  for (int k = threadIdx.x; k < 4 * kRadix; k += kThreads) (&s_hist[0][0])[k] = 0u;
+                                                        uint32_t n_max, int passes, int bits, int digit_bits,
+                                                        uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[kMaxPasses][kRadix];
+  for (int k = threadIdx.x; k < passes * kRadix; k += kThreads) (&s_hist[0][0])[k] = 0u;
   __syncthreads();
   const uint32_t n = count_of(d_count, n_max);
   for (uint32_t idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
     const uint32_t key = keys[idx];
-    for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(key >> (8 * p)) & 255u], 1u);
+    for (int p = 0; p < passes; ++p)
+      atomicAdd(&s_hist[p][(key >> (digit_bits * p)) & pass_mask(bits, digit_bits, p)], 1u);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < passes * kRadix; k += kThreads) {
@@ -272,19 +281,21 @@ __global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ 
 }  // namespace
 
 bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
-                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches) {
+                      const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches,
+                      int digit_bits) {
   if (n_max <= 1u || bits <= 0) return false;
-  const int passes = (bits + 7) / 8;
+  digit_bits = digit_bits < 4 ? 4 : (digit_bits > 8 ? 8 : digit_bits);
+  const int passes = (bits + digit_bits - 1) / digit_bits;
   const uint32_t tiles = (n_max + kSortTile - 1u) / kSortTile;
-  cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 4 * kRadix, st);
+  cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * passes * kRadix, st);
   const uint32_t hist_blocks = min((n_max + kThreads - 1u) / kThreads, 148u * 8u);
-  k_histogram<<<hist_blocks, kThreads, 0, st>>>(keys, d_count, n_max, passes, s.hist);
+  k_histogram<<<hist_blocks, kThreads, 0, st>>>(keys, d_count, n_max, passes, bits, digit_bits, s.hist);
   k_histogram_scan<<<1, kThreads, 0, st>>>(s.hist, passes);
   if (launches) *launches += 2 + passes;
   uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_alt, *dst_v = vals_alt;
   for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    const int width = min(8, bits - shift);
+    const int shift = digit_bits * p;
+    const int width = min(digit_bits, bits - shift);
     cudaMemsetAsync(s.ticket, 0, sizeof(uint32_t), st);
     cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * size_t(tiles) * kRadix, st);
     k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, (1u << width) - 1u,

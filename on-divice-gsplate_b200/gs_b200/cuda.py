@@ -34,7 +34,7 @@ SNAP = {
 EXPORTED = ["gs_last_error", "gs_create", "gs_destroy", "gs_model_init", "gs_model_info_get", "gs_model_export",
             "gs_model_moments", "gs_set_views", "gs_step", "gs_render", "gs_densify", "gs_reset_opacity",
             "gs_snapshot", "gs_set_tuning", "gs_get_tuning", "gs_dataset_set", "gs_set_views_dataset",
-            "gs_sort_pairs_noalloc"]
+            "gs_sort_pairs_noalloc", "gs_autotune"]
 
 
 class StepResult(ctypes.Structure):
@@ -48,7 +48,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("min_pair_capacity", ctypes.c_uint32), ("initial_pairs", ctypes.c_uint64),
                 ("deterministic", ctypes.c_uint32), ("forward_pixels", ctypes.c_uint32),
                 ("backward_pixels", ctypes.c_uint32), ("retry", ctypes.c_uint32), ("graph", ctypes.c_uint32),
-                ("backward_batch", ctypes.c_uint32)]
+                ("backward_batch", ctypes.c_uint32), ("sort_digit_bits", ctypes.c_uint32)]
 
 
 class ModelInfo(ctypes.Structure):
@@ -92,6 +92,7 @@ def load(path: str = LIB_PATH):
     L.gs_dataset_set.argtypes = [vp, u32, vp, vp, ctypes.POINTER(ctypes.c_void_p)]
     L.gs_set_views_dataset.argtypes = [vp, u32, vp, vp]
     L.gs_sort_pairs_noalloc.argtypes = [vp, vp, u32, u32, vp]
+    L.gs_autotune.argtypes = [vp, u32, vp]
     for name in EXPORTED[1:]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -238,3 +239,10 @@ class Context:
         for k, v in kw.items():
             setattr(t, k, v)
         _check(self.lib.gs_set_tuning(self.h, ctypes.byref(t)))
+
+    def autotune(self, steps_per_candidate: int = 2) -> Tuning:
+        """gs_autotune on the views set last: the fastest tuning becomes the context's; the
+        model is left as it was."""
+        t = Tuning()
+        _check(self.lib.gs_autotune(self.h, steps_per_candidate, ctypes.byref(t)))
+        return t
