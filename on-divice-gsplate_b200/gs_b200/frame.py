@@ -111,7 +111,7 @@ class TrainOptions:
     lr_rotation: float = 1e-3
     lr_opacity: float = 2.5e-2
     lr_sh_dc: float = 2.5e-3
-    lr_sh_rest: float = 2.5e-3 / 20.0
+    lr_sh_rest: float = float(np.float32(2.5e-3) / np.float32(20.0))  # 2.5e-3f / 20.0f
     lambda_dssim: float = 0.2
     lambda_dssim_end: float = 1.0
     head_weight: float = 1.0
@@ -193,8 +193,10 @@ def make_frame(camera: Camera, slots: int, sh_stride: int, step: int, options: T
     f["lr0"][0] = (lr_pos * np.float32(camera_extent), options.lr_scale, options.lr_rotation, options.lr_opacity)
     f["lr1"][0, :2] = (options.lr_sh_dc, options.lr_sh_rest)
     f["adam"][0, :3] = (BETA1, BETA2, EPSILON)
+    # In double from the float constants, as trainer.cpp:510-511 computes them.
     n = float(step) + 1.0
-    f["bias"][0, :2] = (1.0 / (1.0 - BETA1 ** n), 1.0 / (1.0 - BETA2 ** n))
+    b1, b2 = float(np.float32(BETA1)), float(np.float32(BETA2))
+    f["bias"][0, :2] = (1.0 / (1.0 - b1 ** n), 1.0 / (1.0 - b2 ** n))
     prune_big = options.opacity_reset_interval > 0 and step > options.opacity_reset_interval
     f["densify0"][0] = (options.densify_grad_threshold, options.percent_dense * camera_extent, options.prune_opacity,
                         0.1 * camera_extent if prune_big else 0.0)

@@ -1,0 +1,68 @@
+// Posed training images: the reference engine's Dataset (engine/include/gs/dataset.h),
+// plus synthetic orbit captures rendered on the GPU from a known scene.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "gs/camera.h"
+#include "gs/splat_scene.h"
+
+namespace gs {
+
+struct DatasetFrame {
+  std::string name;
+  float c2w[16];              // camera-to-world, OpenGL convention, row-major
+  std::vector<uint8_t> rgba;  // training resolution; alpha = subject mask (255 without masks)
+  bool holdout = false;       // reserved for evaluation
+  // A frame of its own resolution (0: the dataset's width, height and intrinsics). The
+  // reference's datasets share one resolution; batched training mixes them.
+  uint32_t width = 0, height = 0;
+  float fx = 0, fy = 0, cx = 0, cy = 0;
+};
+
+struct Dataset {
+  std::string name;
+  uint32_t width = 0;  // training resolution
+  uint32_t height = 0;
+  float fx = 0, fy = 0, cx = 0, cy = 0;  // at training resolution
+  bool has_masks = false;
+  std::vector<DatasetFrame> frames;
+  float camera_center[3] = {0, 0, 0};
+  float camera_extent = 1.0f;  // max camera distance from camera_center, x 1.1 (3DGS "scene extent")
+  float world_up[3] = {0, 1, 0};
+
+  size_t train_count() const;
+  size_t holdout_count() const;
+};
+
+// Sets camera_center (mean camera position) and camera_extent from the frames
+// (dataset.cpp:66-83).
+void compute_camera_bounds(Dataset& dataset);
+
+// Pinhole camera (scene -> camera, OpenCV convention) for a frame, at the frame's own
+// resolution when it has one.
+Camera dataset_camera(const Dataset& dataset, const DatasetFrame& frame);
+
+// A synthetic orbit capture: `cameras` views evenly spaced on a circle of `radius` at
+// `height` around the origin, all looking at it; each view's resolution drawn from
+// `resolutions` with the given probabilities (std::mt19937_64 seeded with `seed`), focal
+// lengths scaled with the short side; every `holdout_every`-th view held out (0: none).
+// Targets are `truth` rendered on `device` over black (alpha 255).
+struct Resolution {
+  uint32_t width, height;
+  float focal;
+  float probability;
+};
+struct OrbitCaptureOptions {
+  uint32_t cameras = 60;
+  float radius = 3.0f, height = 0.5f;
+  std::vector<Resolution> resolutions = {{360, 640, 500.0f, 1.0f}};
+  uint32_t holdout_every = 8;
+  uint64_t seed = 7;
+  int device = 0;
+};
+Dataset make_orbit_capture(const SplatScene& truth, const OrbitCaptureOptions& options);
+
+}  // namespace gs

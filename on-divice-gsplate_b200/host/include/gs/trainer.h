@@ -1,0 +1,222 @@
+// The training loop on the B200 path: the reference engine's gs::Trainer
+// (engine/include/gs/trainer.h:20-330) over libgs_cuda's C ABI.
+//
+// The public API keeps the reference's names, argument meanings and error behaviour
+// (std::runtime_error from the constructor when the device cannot train; overflowing pair
+// buffers are grown and the step re-run, not an error). The GPU work of a step, the
+// buffers and their growth live in libgs_cuda; this class keeps the host side: view order,
+// backgrounds, learning-rate, SH-degree and loss-weight schedules, densification and
+// opacity-reset schedules, statistics, evaluation and export.
+//
+// Extensions: `views_per_step` > 1 renders and differentiates that many views in one
+// launch per pass and takes one Adam step on their summed gradients (batched training;
+// a step still counts one iteration), and the retune steps run gs_autotune, which picks
+// pixels per thread, the backward batch and the sort digit width.
+// Not supported on this path: pose, motion and exposure refinement and head weighting
+// (the constructor throws when they are asked for).
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <random>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "gs/camera.h"
+#include "gs/dataset.h"
+#include "gs/splat_scene.h"
+
+struct gs_context;
+struct gs_frame_data;
+
+namespace gs {
+
+// The role of the reference's VkContext& (device + stream owner): which CUDA device the
+// trainer's libgs_cuda context is created on.
+struct CudaContext {
+  int device = 0;
+};
+
+struct TrainOptions {
+  uint32_t iterations = 3000;
+  uint32_t max_gaussians = 300000;  // slot capacity
+  int sh_degree = 3;
+  uint32_t sh_degree_interval = 500;  // the active SH degree goes up by one every this many steps
+  bool masked = true;                 // composite masked targets over the background (datasets with masks)
+  bool random_background = true;      // otherwise `background`
+  float background[3] = {0.0f, 0.0f, 0.0f};
+  float lr_position = 1.6e-4f;  // times the camera extent, decaying exponentially to lr_position_final
+  float lr_position_final = 1.6e-6f;
+  float lr_scale = 5e-3f;
+  float lr_rotation = 1e-3f;
+  float lr_opacity = 2.5e-2f;
+  float lr_sh_dc = 2.5e-3f;
+  float lr_sh_rest = 2.5e-3f / 20.0f;
+  float lambda_dssim = 0.2f;     // loss (1 - lambda) L1 + lambda (1 - SSIM), lambda ramping
+  float lambda_dssim_end = 1.0f;  // to this by the last step (< 0: no ramp)
+  float head_weight = 1.0f;       // not supported here: must stay 1
+  bool refine_poses = false;      // not supported here
+  bool refine_motion = false;     // not supported here
+  bool refine_exposure = false;   // not supported here
+  bool sparse_adam = false;       // gaussians that drew nothing in a step keep their values and moments
+  uint32_t densify_from = 300;
+  uint32_t densify_until = 2000;
+  uint32_t densify_interval = 100;
+  uint32_t opacity_reset_interval = 0;  // 0 disables
+  float densify_grad_threshold = 2e-4f;
+  float percent_dense = 0.01f;  // clone below, split above this fraction of the extent
+  float prune_opacity = 0.005f;
+  // Retuning: at step retune_first and every retune_interval steps (0: never) gs_autotune
+  // times the candidate tunings on training steps and keeps the fastest.
+  uint32_t retune_first = 20;
+  uint32_t retune_interval = 500;
+  bool autotune = true;
+  bool deterministic = true;  // fixed-order gradient sums (bit-stable); false: atomics
+  uint32_t views_per_step = 1;  // batched training: views rendered and differentiated per Adam step (1..16)
+  uint32_t min_pair_capacity = 1 << 16;
+  uint64_t initial_pair_guess = 0;  // pairs to allocate for before the first count (0: four per gaussian)
+  uint32_t seed = 1;
+};
+
+// The defaults' schedule (densification, opacity reset, SH degree) scaled to `iterations`
+// (trainer.cpp:133-145).
+TrainOptions scaled_options(uint32_t iterations);
+
+// GPU milliseconds of each pass in one profiled step.
+struct PassTimes {
+  double project = 0.0;    // projection + pair count
+  double sort = 0.0;       // depth sort, scan, pair emission, pair sort, tile ranges
+  double rasterize = 0.0;  // forward + L1 loss
+  double ssim = 0.0;       // SSIM and its gradient
+  double backward = 0.0;   // per-pair gradients
+  double optimize = 0.0;   // pair sums, projection backward, Adam
+  bool valid = false;
+};
+
+struct TrainStats {
+  uint32_t step = 0;
+  uint32_t gaussians = 0;  // alive
+  uint32_t slots = 0;      // slots in use (alive + free)
+  uint64_t pairs = 0;      // (tile, gaussian) pairs of the last step (all its views)
+  double l1 = 0.0;         // mean absolute error of the last step's views
+  double psnr = 0.0;       // of the last step's views (their mean)
+  double ssim = 0.0;       // of the last step's views (0 when not computed)
+  double loss = 0.0;       // the training loss of the last step's views
+  double step_ms = 0.0;    // exponential moving average of the wall-clock step time
+  int sh_degree = 0;       // active
+  uint32_t densify_events = 0;
+  uint32_t spawned = 0;
+  uint32_t pruned = 0;
+  uint32_t tile_mismatch = 0;   // gaussians whose emitted tiles differed from the count (0)
+  uint32_t overflow_steps = 0;  // steps whose pairs did not fit (their update was skipped)
+  uint64_t views = 0;           // training views processed
+  struct Timing {
+    double wall_ms = 0.0;  // moving averages per step
+    double gpu_ms = 0.0;
+    double batch = 0.0;    // views per step
+  } timing;
+};
+
+struct RetuneResult {
+  uint32_t step = 0;
+  std::string chosen;  // "fpx=2 bpx=4 batch=64 digits=8"
+};
+
+struct EvalResult {
+  double psnr = 0.0;  // mean over the held-out views
+  bool aligned = false;
+  double psnr_unaligned = 0.0;
+  double ssim = 0.0;
+  double head_psnr = 0.0;
+  uint32_t head_views = 0;
+  double l1 = 0.0;
+  uint32_t views = 0;
+};
+
+class Trainer {
+ public:
+  // Throws std::runtime_error if the device cannot train (or a feature this path does not
+  // have is asked for). Takes the dataset by value: move it in to avoid a copy.
+  Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, const TrainOptions& options);
+  ~Trainer();
+  Trainer(const Trainer&) = delete;
+  Trainer& operator=(const Trainer&) = delete;
+
+  // One optimisation step on the next training view(s), then densification on schedule.
+  // With `profile`, the passes are timed (last_profile()).
+  void step(bool profile = false);
+  // Up to `count` steps (fewer at the end); returns the steps run.
+  uint32_t steps(uint32_t count);
+  const PassTimes& last_profile() const { return profile_; }
+  bool finished() const { return stats_.step >= options_.iterations; }
+  const TrainStats& stats() const { return stats_; }
+  const TrainOptions& options() const { return options_; }
+  const Dataset& dataset() const { return dataset_; }
+
+  // The current model from `camera` over `background`: RGBA8, alpha = coverage.
+  std::vector<uint8_t> render(const Camera& camera, const float background[3]);
+  // Held-out views over a black background.
+  EvalResult evaluate();
+  std::vector<uint8_t> render_view(size_t frame, const float background[3]);
+  Camera camera_for(size_t frame) const;
+  // The alive gaussians, in the dataset's world.
+  SplatScene export_scene();
+
+  // Testing: one step on `frame` over `background`. With all learning rates zero the
+  // parameters stay put and first_step_gradients() returns the first step's gradients.
+  void step_on(size_t frame, const float background[3], bool profile = false);
+  struct Gradients {
+    std::vector<float> params;  // 16 per slot
+    std::vector<float> sh;      // sh_stride() per slot
+  };
+  Gradients first_step_gradients();
+  struct DebugSnapshot {
+    std::vector<uint32_t> pixel_count;
+    std::vector<float> pixel_grad;
+    std::vector<float> projected;
+    std::vector<uint32_t> tiles;
+    std::vector<uint32_t> offsets;
+    std::vector<float> pair_grads;
+    std::vector<uint32_t> pair_tile;
+    std::vector<uint32_t> render_order;
+    std::vector<uint32_t> depth_key;
+  };
+  DebugSnapshot debug_snapshot();
+  uint32_t sh_stride() const { return sh_stride_; }
+  // The tuning in use ("fpx=2 bpx=4 batch=64 digits=8 deterministic"), in place of the
+  // reference's backward-variant name.
+  std::string reduction() const;
+  const std::vector<RetuneResult>& retunes() const { return retunes_; }
+
+ private:
+  void next_view(size_t& frame, float background[3]);
+  void run_step(const std::vector<size_t>& frames, const std::vector<std::array<float, 3>>& backgrounds,
+                bool profile);
+  void write_frame(gs_frame_data& f, const Camera& camera, const float background[3], uint32_t step, bool ssim,
+                   bool masked) const;
+  uint32_t sh_degree_at(uint32_t step) const;
+  double lambda_at(uint32_t step) const;
+  bool uses_ssim() const;
+  void after_step();
+  void densify();
+  void reset_opacity();
+  bool retune_due(uint32_t s) const;
+  void check(int code, const char* what) const;
+
+  CudaContext& ctx_;
+  gs_context* gpu_ = nullptr;
+  Dataset dataset_;
+  TrainOptions options_;
+  uint32_t sh_stride_ = 0;
+  uint32_t capacity_ = 0;
+  std::vector<size_t> train_frames_, order_;
+  size_t order_pos_ = 0;
+  std::mt19937 rng_;
+  TrainStats stats_;
+  PassTimes profile_;
+  std::vector<RetuneResult> retunes_;
+  std::vector<uint8_t> frame_bytes_;  // the last step's first FrameData (densify thresholds)
+};
+
+}  // namespace gs
