@@ -286,6 +286,8 @@ def main() -> None:
     ap.add_argument("--mode", default="both", choices=["both", "plain", "batched"],
                     help="plain or batched alone (profiling runs); the bench line needs both")
     ap.add_argument("--cameras", type=int, default=N_CAMERAS, help="orbit cameras (fewer: shorter setup)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default tuning (profiling runs: timings under ncu would mislead the autotuner)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -325,14 +327,16 @@ def main() -> None:
     plain_ms, step = 0.0, 0
     tunings = {}
     if args.mode != "batched":
-        tunings["plain"] = autotune(ctx, scene, cams, opt, 1, order, 0)
+        if not args.no_autotune:
+            tunings["plain"] = autotune(ctx, scene, cams, opt, 1, order, 0)
         plain_ms, _, _, step = measure(ctx, scene, cams, opt, 1, args.steps, args.warmup, order, 0, dist)
     if args.mode == "plain":
         print(json.dumps({"mode": "plain", "plain_views_per_s": 1000.0 * args.steps / plain_ms}), flush=True)
         ctx.close()
         return
     # Batched: 8 views per step (the headline), clocks sampled meanwhile.
-    tunings["batched"] = autotune(ctx, scene, cams, opt, VIEWS_PER_STEP, order, step)
+    if not args.no_autotune:
+        tunings["batched"] = autotune(ctx, scene, cams, opt, VIEWS_PER_STEP, order, step)
     clocks = ClockSampler(local)
     gpu_ms, launches, pairs, step = measure(ctx, scene, cams, opt, VIEWS_PER_STEP, args.steps, args.warmup, order,
                                             step, dist, clocks)
