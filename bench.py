@@ -197,6 +197,17 @@ def measure(ctx, scene, cams, opt, views_per_step, steps, warmup, order, step0, 
     return gpu_ms, launches, pairs / steps, step
 
 
+def max_over_ranks(values, dist, device="cuda"):
+    """Each timing's maximum over the ranks (one all-reduce; a no-op on one process)."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def autotune(ctx, scene, cams, opt, views_per_step, order, step):
     """gs_autotune on a step of `views_per_step` dataset views (the model is left as it was)."""
     idx = order.next(views_per_step)
@@ -367,10 +378,7 @@ def main() -> None:
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
 
-    if dist is not None:
-        t = torch.tensor([gpu_ms, plain_ms, e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        gpu_ms, plain_ms, e2e_s = float(t[0]), float(t[1]), float(t[2])
+    gpu_ms, plain_ms, e2e_s = max_over_ranks([gpu_ms, plain_ms, e2e_s], dist)
     ms_per_step = gpu_ms / args.steps
     value = world * VIEWS_PER_STEP * 1000.0 / ms_per_step
     plain = world * 1000.0 / (plain_ms / args.steps)
