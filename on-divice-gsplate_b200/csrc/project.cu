@@ -1,10 +1,12 @@
 // Projection: EWA 2D covariance, SH colour, opacity-aware tile count and the 16-bit
 // depth key of every slot, for every view of the step (train_project.comp:26-112).
 //
-// One thread per slot reads its parameters once (four coalesced float4 planes and the
-// SH planes) and projects them into each view, so a batch of views costs one pass over
-// the model. HBM-bound: per slot and view it writes 48 B of splat record, 16 B of
-// footprint, a tile count and a depth key/value pair.
+// One thread per slot reads its parameters once (four coalesced float4 planes; the SH
+// planes when the slot is visible, again from L1 for later views) and projects them into
+// each view, so a batch of views costs one pass over the model. HBM-bound: per slot and
+// view it writes 48 B of splat record, 16 B of footprint, a tile count and a depth
+// key/value pair. 128-thread blocks capped at 128 registers keep 4 blocks per SM resident
+// (one 256-thread block of 151 registers fit alone: 8 warps per SM).
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -24,7 +26,7 @@ struct ProjectArgs {
 };
 
 template <int DEG>
-__global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
+__global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   {
     const uint32_t words = a.n_views * uint32_t(sizeof(gs_frame_data) / 4);
@@ -57,9 +59,6 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) Sig[r][c] = M[r][0] * M[c][0] + M[r][1] * M[c][1] + M[r][2] * M[c][2];
   }
-  float shc[kCoeffs > 0 ? kCoeffs * 3 : 1];
-  bool sh_loaded = false;
-
   for (uint32_t v = 0; v < a.n_views; ++v) {
     const gs_frame_data& f = s_frames[v];
     const size_t g = size_t(v) * a.cap + i;
@@ -111,16 +110,11 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
           sh_basis<DEG>(dx, dy, dz, basis);
           float col[3] = {basis[0] * p3.x, basis[0] * p3.y, basis[0] * p3.z};
           if constexpr (kCoeffs > 0) {
-            if (!sh_loaded) {
-#pragma unroll
-              for (int k = 0; k < kCoeffs * 3; ++k) shc[k] = a.SH[size_t(k) * a.cap + i];
-              sh_loaded = true;
-            }
 #pragma unroll
             for (int k = 0; k < kCoeffs; ++k) {
-              col[0] += basis[k + 1] * shc[k * 3];
-              col[1] += basis[k + 1] * shc[k * 3 + 1];
-              col[2] += basis[k + 1] * shc[k * 3 + 2];
+              col[0] += basis[k + 1] * a.SH[size_t(3 * k) * a.cap + i];
+              col[1] += basis[k + 1] * a.SH[size_t(3 * k + 1) * a.cap + i];
+              col[2] += basis[k + 1] * a.SH[size_t(3 * k + 2) * a.cap + i];
             }
           }
           uint32_t clamped = 0u;
@@ -163,7 +157,7 @@ void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, con
   if (m.slots == 0) return;
   ProjectArgs a{sp.frames, sp.n_views, m.slots, m.cap, m.P, m.SH, vb.splat, vb.foot, vb.tiles,
                 depth_keys, depth_vals, zero_grad2d ? vb.grad2d : nullptr};
-  const dim3 grid((m.slots + 255u) / 256u), block(256);
+  const dim3 grid((m.slots + 127u) / 128u), block(128);
   switch (degree) {
     case 0: k_project<0><<<grid, block, 0, st>>>(a); break;
     case 1: k_project<1><<<grid, block, 0, st>>>(a); break;

@@ -308,13 +308,6 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   for (int k = 0; k < 4; ++k) g16[8 + k] += (dq[k] - G.qn[k] * qd) / G.qlen;
 }
 
-// dL/d(position) through the SH view direction: (dL/ddir - dir (dir . dL/ddir)) / |p - c|.
-__device__ __forceinline__ void add_direction_term(float g16[16], const float dir[3], float dir_len, const float dd[3]) {
-  const float proj = dir[0] * dd[0] + dir[1] * dd[1] + dir[2] * dd[2];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) g16[c] += (dd[c] - dir[c] * proj) / dir_len;
-}
-
 __device__ __forceinline__ void adam_params(const StepArgs& a, const gs_frame_data& f0, uint32_t i, float4 p0,
                                             float4 p1, float4 q, float4 p3, const float g16[16]) {
   const float b1 = f0.adam[0], b2 = f0.adam[1], eps = f0.adam[2], c1 = f0.bias[0], c2 = f0.bias[1];
