@@ -410,7 +410,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy).
         const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
         const float lx = -ca * dx, ly = -cb * dx, mx = -cb, my = -cc;
-        const float hx = -0.5f * dx * dx;
+        const float hx = -0.5f * dx * dx, ndx = -dx;
         float c[12];
 #pragma unroll
         for (int k = 0; k < 12; ++k) c[k] = 0.0f;
@@ -430,17 +430,18 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           const float rest = R[p] - gc * weight;
           const float one_minus = __fsub_rn(1.0f, alpha);
           const float dlda = T[p] * gc - __fdividef(rest, one_minus);
-          const bool clamped = raw >= kMaxAlpha;
-          const float dop = clamped ? 0.0f : G * dlda;
-          const float dpow = clamped ? 0.0f : raw * dlda;
-          const float dmx = dpow * fmaf(mx, dy, lx);
-          const float dmy = dpow * fmaf(my, dy, ly);
+          // Opacity and exponent gradients vanish where alpha is clamped at 0.99.
+          const float dl = raw >= kMaxAlpha ? 0.0f : dlda;
+          const float dpow = raw * dl;
+          const float t = dpow * dy;
+          const float dmx = fmaf(t, mx, dpow * lx);  // dpow (lx + mx dy)
+          const float dmy = fmaf(t, my, dpow * ly);
           c[0] += dmx;
           c[1] += dmy;
-          c[2] += dpow * hx;
-          c[3] += dpow * (-dx * dy);
-          c[4] += dpow * (-0.5f * dy * dy);
-          c[5] += dop;
+          c[2] = fmaf(dpow, hx, c[2]);
+          c[3] = fmaf(t, ndx, c[3]);
+          c[4] = fmaf(t, -0.5f * dy, c[4]);
+          c[5] = fmaf(G, dl, c[5]);
           c[6] += weight * dl0[p];
           c[7] += weight * dl1[p];
           c[8] += weight * dl2[p];
