@@ -29,8 +29,9 @@ struct LossArgs {
 
 // The target colour the loss compares against (train_forward.comp:124-126).
 __device__ __forceinline__ float3 target_colour(const gs_frame_data& f, uint32_t u) {
-  const float ta = float(u >> 24) / 255.0f;
-  const float tr[3] = {float(u & 255u) / 255.0f, float((u >> 8) & 255u) / 255.0f, float((u >> 16) & 255u) / 255.0f};
+  constexpr float k = 1.0f / 255.0f;
+  const float ta = float(u >> 24) * k;
+  const float tr[3] = {float(u & 255u) * k, float((u >> 8) & 255u) * k, float((u >> 16) & 255u) * k};
   const bool masked = (f.model[3] & GS_FLAG_MASKED_TARGET) != 0u;
   float tc[3];
 #pragma unroll
@@ -129,11 +130,15 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
     const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, c = e / (kQuads * kWin);
     const float* xs = s_buf + c * kPlane + row * kS + q * kRun;
     const float* ys = s_buf + (3u + c) * kPlane + row * kS + q * kRun;
-    float x[kSpan], y[kSpan];
+    // The inputs and their products, once per loaded pixel.
+    float x[kSpan], y[kSpan], xx[kSpan], yy[kSpan], xy[kSpan];
 #pragma unroll
     for (int k = 0; k < kSpan; ++k) {
       x[k] = xs[k];
       y[k] = ys[k];
+      xx[k] = x[k] * x[k];
+      yy[k] = y[k] * y[k];
+      xy[k] = x[k] * y[k];
     }
     float* h = s_h + c * 5u * kHPlane + row * kTile + q * kRun;
 #pragma unroll
@@ -142,12 +147,11 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
 #pragma unroll
       for (int k = 0; k <= 2 * kR; ++k) {
         const float wk = c_window[k];
-        const float xv = x[o + k], yv = y[o + k];
-        m0 += wk * xv;
-        m1 += wk * yv;
-        m2 += wk * xv * xv;
-        m3 += wk * yv * yv;
-        m4 += wk * xv * yv;
+        m0 = fmaf(wk, x[o + k], m0);
+        m1 = fmaf(wk, y[o + k], m1);
+        m2 = fmaf(wk, xx[o + k], m2);
+        m3 = fmaf(wk, yy[o + k], m3);
+        m4 = fmaf(wk, xy[o + k], m4);
       }
       h[o] = m0;
       h[kHPlane + o] = m1;
@@ -172,12 +176,14 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
       const float vx = exx - mx * mx, vy = eyy - my * my, cxy = exy - mx * my;
       const float l = 2.0f * mx * my + c1, cs = 2.0f * cxy + c2;
       const float m = mx * mx + my * my + c1, vv = vx + vy + c2;
-      const float inv = 1.0f / (m * vv);
+      // One reciprocal: 1/(m vv), 1/vv = m/(m vv), 1/m = vv/(m vv).
+      const float inv = __fdividef(1.0f, m * vv);
       const float ssim = l * cs * inv;
       const float d_cxy = 2.0f * l * inv;
-      const float d_vx = -ssim / vv;
+      const float d_vx = -ssim * (m * inv);
       const uint32_t pixel = (q * kRun + o) * kTile + col;
-      s_abc[c * 256u + pixel] = 2.0f * my * cs * inv - ssim * 2.0f * mx / m - 2.0f * mx * d_vx - my * d_cxy;
+      s_abc[c * 256u + pixel] =
+          2.0f * my * cs * inv - ssim * 2.0f * mx * (vv * inv) - 2.0f * mx * d_vx - my * d_cxy;
       s_abc[(3u + c) * 256u + pixel] = d_vx;
       s_abc[(6u + c) * 256u + pixel] = d_cxy;
       s_abc[(9u + c) * 256u + pixel] = ssim;
