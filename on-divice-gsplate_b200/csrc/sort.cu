@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kThreads) k_histogram_scan(uint32_t* hist, int
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out, const uint32_t* d_count,
