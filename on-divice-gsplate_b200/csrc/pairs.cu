@@ -76,22 +76,23 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   }
 }
 
+// Grid-stride over the stored pairs (the grid is sized for the SMs, not the capacity).
 __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count,
                                                 uint32_t capacity, uint2* __restrict__ ranges) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t count = min(*d_count, capacity);
-  if (s >= count) return;
-  const uint32_t tile = keys[s];
-  if (s == 0u) {
-    ranges[tile].x = 0u;
-  } else {
-    const uint32_t prev = keys[s - 1u];
-    if (prev != tile) {
-      ranges[prev].y = s;
-      ranges[tile].x = s;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
+    const uint32_t tile = keys[s];
+    if (s == 0u) {
+      ranges[tile].x = 0u;
+    } else {
+      const uint32_t prev = keys[s - 1u];
+      if (prev != tile) {
+        ranges[prev].y = s;
+        ranges[tile].x = s;
+      }
     }
+    if (s == count - 1u) ranges[tile].y = count;
   }
-  if (s == count - 1u) ranges[tile].y = count;
 }
 
 }  // namespace
@@ -108,7 +109,8 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
                    cudaStream_t st) {
   if (pair_capacity == 0u) return;
-  k_ranges<<<(pair_capacity + 255u) / 256u, 256, 0, st>>>(sorted_keys, d_count, pair_capacity, ranges);
+  k_ranges<<<min((pair_capacity + 255u) / 256u, 148u * 16u), 256, 0, st>>>(sorted_keys, d_count, pair_capacity,
+                                                                          ranges);
 }
 
 }  // namespace gsk
