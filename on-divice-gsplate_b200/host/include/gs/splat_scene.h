@@ -66,8 +66,14 @@ class PlyVertices {
 };
 
 SplatScene load_ply(const uint8_t* data, size_t size);
-SplatScene load_splat_file(const uint8_t* data, size_t size);  // PLY (detected by its magic)
+// SPZ v2/v3 (a gzip stream; RUB axes; quantized attributes), as the reference reads it
+// (splat_scene.cpp:367-433).
+SplatScene load_spz(const uint8_t* data, size_t size);
+SplatScene load_splat_file(const uint8_t* data, size_t size);  // PLY or SPZ, detected by magic
 std::vector<uint8_t> save_ply(const SplatScene& scene);
+// SPZ v3 with `fractional_bits` of position precision (the scene is written in its own
+// axes: convert to RUB first for files other SPZ readers open). Not in the reference.
+std::vector<uint8_t> save_spz(const SplatScene& scene, int fractional_bits = 12);
 
 // Rewrites the scene in `target` axes (RDF <-> RUB is a half turn about x): positions,
 // rotations and the sign of each SH coefficient by its parity in y and z.

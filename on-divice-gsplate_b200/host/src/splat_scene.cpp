@@ -13,6 +13,8 @@
 #include <sstream>
 #include <stdexcept>
 
+#include <zlib.h>
+
 namespace gs {
 
 namespace {
@@ -208,9 +210,181 @@ SplatScene load_ply(const uint8_t* data, size_t size) {
   return scene;
 }
 
+// ---- SPZ ----
+// Layout (v2/v3): a gzip stream holding a 16-byte header -- magic "NGSP" (0x5053474e LE),
+// version, point count (u32 each), SH degree, fractional bits, flags (bit 0: antialiased),
+// reserved (u8 each) -- then per-attribute blocks over all points: positions (3 x 24-bit
+// signed fixed point), alpha (u8, sigmoid(opacity) x 255), colour (3 x u8, DC x 0.15 + 0.5
+// in [0, 1]), log-scales (3 x u8, (s + 10) x 16), rotations (v2: 3 x u8 of x, y, z in
+// [-1, 1] with w >= 0; v3: u32 "smallest three": the largest component's index in the top
+// 2 bits, the other three as 9-bit magnitudes / sqrt(2) with a sign bit, last component
+// lowest) and SH beyond DC (coefficients x rgb, u8 around 128, / 128).
+namespace {
+
+constexpr uint32_t kSpzMagic = 0x5053474eu;
+constexpr float kSpzColourScale = 0.15f;
+
+std::vector<uint8_t> gunzip(const uint8_t* data, size_t size) {
+  z_stream zs{};
+  if (inflateInit2(&zs, 16 + MAX_WBITS) != Z_OK) throw std::runtime_error("SPZ: zlib init failed");
+  std::vector<uint8_t> out;
+  zs.next_in = const_cast<Bytef*>(data);
+  zs.avail_in = uInt(size);
+  int rc = Z_OK;
+  do {
+    const size_t at = out.size();
+    out.resize(at + std::max<size_t>(size * 4, 1 << 16));
+    zs.next_out = out.data() + at;
+    zs.avail_out = uInt(out.size() - at);
+    rc = inflate(&zs, Z_NO_FLUSH);
+    out.resize(out.size() - zs.avail_out);
+    if (rc != Z_OK && rc != Z_STREAM_END) {
+      inflateEnd(&zs);
+      throw std::runtime_error("SPZ: not a valid gzip stream");
+    }
+  } while (rc != Z_STREAM_END && (zs.avail_in > 0 || zs.avail_out == 0));
+  inflateEnd(&zs);
+  if (rc != Z_STREAM_END) throw std::runtime_error("SPZ: gzip stream is truncated");
+  return out;
+}
+
+std::vector<uint8_t> gzip(const std::vector<uint8_t>& raw) {
+  z_stream zs{};
+  if (deflateInit2(&zs, Z_BEST_SPEED, Z_DEFLATED, 16 + MAX_WBITS, 8, Z_DEFAULT_STRATEGY) != Z_OK)
+    throw std::runtime_error("SPZ: zlib init failed");
+  std::vector<uint8_t> out(deflateBound(&zs, uLong(raw.size())) + 64);
+  zs.next_in = const_cast<Bytef*>(raw.data());
+  zs.avail_in = uInt(raw.size());
+  zs.next_out = out.data();
+  zs.avail_out = uInt(out.size());
+  const int rc = deflate(&zs, Z_FINISH);
+  out.resize(out.size() - zs.avail_out);
+  deflateEnd(&zs);
+  if (rc != Z_STREAM_END) throw std::runtime_error("SPZ: compression failed");
+  return out;
+}
+
+uint8_t quantize(float v) { return uint8_t(std::lround(std::min(std::max(v, 0.0f), 255.0f))); }
+
+}  // namespace
+
+SplatScene load_spz(const uint8_t* data, size_t size) {
+  if (size >= 4 && load_le<uint32_t>(data) == kSpzMagic)
+    throw std::runtime_error("SPZ: uncompressed (v4) files are not supported (v2/v3 only)");
+  if (size < 2 || data[0] != 0x1f || data[1] != 0x8b) throw std::runtime_error("not an SPZ file");
+  const std::vector<uint8_t> raw = gunzip(data, size);
+  if (raw.size() < 16 || load_le<uint32_t>(raw.data()) != kSpzMagic) throw std::runtime_error("SPZ: bad header");
+  const uint32_t version = load_le<uint32_t>(raw.data() + 4), n = load_le<uint32_t>(raw.data() + 8);
+  const int file_degree = raw[12], fractional_bits = raw[13];
+  if (version < 2 || version > 3) throw std::runtime_error("SPZ: version " + std::to_string(version) + " (v2/v3 only)");
+  if (file_degree > 4) throw std::runtime_error("SPZ: bad SH degree");
+  const int file_coeffs = file_degree == 4 ? 24 : sh_rest_coeffs(file_degree);
+  const int degree = std::min(file_degree, 3), coeffs = sh_rest_coeffs(degree);
+  const size_t rot_bytes = version >= 3 ? 4 : 3;
+  const size_t positions = 16, alphas = positions + size_t(n) * 9, colours = alphas + n, scales = colours + size_t(n) * 3,
+               rotations = scales + size_t(n) * 3, sh = rotations + size_t(n) * rot_bytes,
+               end = sh + size_t(n) * file_coeffs * 3;
+  if (n == 0 || raw.size() < end) throw std::runtime_error("SPZ: data is truncated");
+  SplatScene s;
+  s.convention = AxisConvention::RUB;
+  s.antialiased = (raw[14] & 1u) != 0;
+  s.resize(n, degree);
+  const float unit = 1.0f / float(1u << fractional_bits);
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      const uint8_t* p = &raw[positions + (size_t(i) * 3 + k) * 3];
+      int32_t v = int32_t(uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16);
+      if (v & 0x800000) v -= 0x1000000;  // sign of the 24-bit value
+      s.positions[size_t(i) * 3 + k] = float(v) * unit;
+      s.sh_dc[size_t(i) * 3 + k] = (float(raw[colours + size_t(i) * 3 + k]) / 255.0f - 0.5f) / kSpzColourScale;
+      s.log_scales[size_t(i) * 3 + k] = float(raw[scales + size_t(i) * 3 + k]) / 16.0f - 10.0f;
+    }
+    const float a = std::min(std::max(float(raw[alphas + i]) / 255.0f, 1e-6f), 1.0f - 1e-6f);
+    s.opacity_logits[i] = std::log(a / (1.0f - a));
+    float xyzw[4];
+    const uint8_t* r = &raw[rotations + size_t(i) * rot_bytes];
+    if (version >= 3) {
+      uint32_t bits = load_le<uint32_t>(r);
+      const int largest = int(bits >> 30);
+      float sum = 0.0f;
+      for (int c = 3; c >= 0; --c) {
+        if (c == largest) continue;
+        const float mag = float(bits & 511u) / 511.0f * 0.70710678118654752f;
+        xyzw[c] = (bits >> 9) & 1u ? -mag : mag;
+        sum += xyzw[c] * xyzw[c];
+        bits >>= 10;
+      }
+      xyzw[largest] = std::sqrt(std::max(0.0f, 1.0f - sum));
+    } else {
+      for (int k = 0; k < 3; ++k) xyzw[k] = float(r[k]) / 127.5f - 1.0f;
+      xyzw[3] = std::sqrt(std::max(0.0f, 1.0f - (xyzw[0] * xyzw[0] + xyzw[1] * xyzw[1] + xyzw[2] * xyzw[2])));
+    }
+    s.rotations[size_t(i) * 4 + 0] = xyzw[3];  // (w, x, y, z)
+    for (int k = 0; k < 3; ++k) s.rotations[size_t(i) * 4 + 1 + k] = xyzw[k];
+    for (int j = 0; j < coeffs; ++j)
+      for (int c = 0; c < 3; ++c)
+        s.sh_rest[(size_t(i) * coeffs + j) * 3 + c] =
+            (float(raw[sh + (size_t(i) * file_coeffs + j) * 3 + c]) - 128.0f) / 128.0f;
+  }
+  return s;
+}
+
+std::vector<uint8_t> save_spz(const SplatScene& s, int fractional_bits) {
+  if (fractional_bits < 0 || fractional_bits > 23) throw std::runtime_error("save_spz: fractional_bits 0..23");
+  const uint32_t n = s.count;
+  const int coeffs = sh_rest_coeffs(s.sh_degree);
+  std::vector<uint8_t> raw(16 + size_t(n) * (9 + 1 + 3 + 3 + 4 + size_t(coeffs) * 3));
+  const uint32_t head[3] = {kSpzMagic, 3u, n};
+  std::memcpy(raw.data(), head, 12);
+  raw[12] = uint8_t(s.sh_degree);
+  raw[13] = uint8_t(fractional_bits);
+  raw[14] = s.antialiased ? 1u : 0u;
+  const size_t positions = 16, alphas = positions + size_t(n) * 9, colours = alphas + n, scales = colours + size_t(n) * 3,
+               rotations = scales + size_t(n) * 3, sh = rotations + size_t(n) * 4;
+  const float unit = float(1u << fractional_bits);
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      const long v = std::min(std::max(std::lround(s.positions[size_t(i) * 3 + k] * unit), -0x800000l), 0x7fffffl);
+      const uint32_t u = uint32_t(v) & 0xffffffu;
+      uint8_t* p = &raw[positions + (size_t(i) * 3 + k) * 3];
+      p[0] = uint8_t(u);
+      p[1] = uint8_t(u >> 8);
+      p[2] = uint8_t(u >> 16);
+      raw[colours + size_t(i) * 3 + k] = quantize((s.sh_dc[size_t(i) * 3 + k] * kSpzColourScale + 0.5f) * 255.0f);
+      raw[scales + size_t(i) * 3 + k] = quantize((s.log_scales[size_t(i) * 3 + k] + 10.0f) * 16.0f);
+    }
+    raw[alphas + i] = quantize(255.0f / (1.0f + std::exp(-s.opacity_logits[i])));
+    // (x, y, z, w), normalised, the largest component made positive.
+    const float* q = &s.rotations[size_t(i) * 4];
+    float xyzw[4] = {q[1], q[2], q[3], q[0]};
+    const float len = std::sqrt(xyzw[0] * xyzw[0] + xyzw[1] * xyzw[1] + xyzw[2] * xyzw[2] + xyzw[3] * xyzw[3]);
+    int largest = 0;
+    for (int c = 0; c < 4; ++c) {
+      xyzw[c] = len > 0.0f ? xyzw[c] / len : (c == 3 ? 1.0f : 0.0f);
+      if (std::fabs(xyzw[c]) > std::fabs(xyzw[largest])) largest = c;
+    }
+    const float flip = xyzw[largest] < 0.0f ? -1.0f : 1.0f;
+    uint32_t bits = uint32_t(largest) << 30;
+    int shift = 20;
+    for (int c = 0; c < 4; ++c) {
+      if (c == largest) continue;
+      const float v = xyzw[c] * flip;
+      const uint32_t mag = uint32_t(std::min(511l, std::lround(std::fabs(v) * 1.41421356237309505f * 511.0f)));
+      bits |= ((v < 0.0f ? 1u : 0u) << 9 | mag) << shift;
+      shift -= 10;
+    }
+    std::memcpy(&raw[rotations + size_t(i) * 4], &bits, 4);
+    for (int j = 0; j < coeffs * 3; ++j)
+      raw[sh + size_t(i) * coeffs * 3 + j] = quantize(s.sh_rest[size_t(i) * coeffs * 3 + j] * 128.0f + 128.0f);
+  }
+  return gzip(raw);
+}
+
 SplatScene load_splat_file(const uint8_t* data, size_t size) {
   if (size >= 3 && std::memcmp(data, "ply", 3) == 0) return load_ply(data, size);
-  throw std::runtime_error("not a PLY splat file");
+  if (size >= 4 && ((data[0] == 0x1f && data[1] == 0x8b) || load_le<uint32_t>(data) == kSpzMagic))
+    return load_spz(data, size);
+  throw std::runtime_error("not a PLY or SPZ splat file");
 }
 
 std::vector<uint8_t> save_ply(const SplatScene& scene) {

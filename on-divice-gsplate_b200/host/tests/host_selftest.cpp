@@ -1,5 +1,6 @@
 // CPU checks of the host layer, driven by tests/test_host.py:
-//   gs_host_selftest scene <dir>   PLY round trip (bit-exact), RDF <-> RUB twice = identity
+//   gs_host_selftest scene <dir>   PLY round trip (bit-exact), RDF <-> RUB twice = identity,
+//                                  SPZ v3 and v2 round trips within their quantization
 //   gs_host_selftest frame         one FrameData as 72 hex words (compared with gs_b200.frame)
 //   gs_host_selftest camera        look-at camera as 12 floats (rotation rows, translation)
 #include <cmath>
@@ -7,6 +8,9 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
+
+#include <zlib.h>
 
 #include "../src/frame.h"
 #include "gs/camera.h"
@@ -19,6 +23,78 @@ bool same(const gs::SplatScene& a, const gs::SplatScene& b) {
   return a.count == b.count && a.sh_degree == b.sh_degree && a.positions == b.positions &&
          a.log_scales == b.log_scales && a.rotations == b.rotations && a.opacity_logits == b.opacity_logits &&
          a.sh_dc == b.sh_dc && a.sh_rest == b.sh_rest;
+}
+
+void expect(bool ok, const std::string& what) {
+  if (!ok) throw std::runtime_error(what);
+}
+
+// The SPZ quantization steps: 2^-12 in position (12 fractional bits), 1/255 of colour
+// (DC / 0.15), 1/16 of log scale, 1/255 of alpha, 1/128 of SH; the rotation to 9 bits.
+void check_spz(const gs::SplatScene& s, const gs::SplatScene& back, const char* what) {
+  expect(back.count == s.count && back.sh_degree == s.sh_degree, std::string(what) + ": count/degree");
+  for (uint32_t i = 0; i < s.count; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      const size_t a = size_t(i) * 3 + k;
+      expect(std::fabs(back.positions[a] - s.positions[a]) <= 0.5f / 4096.0f + 1e-6f, std::string(what) + ": position");
+      expect(std::fabs(back.log_scales[a] - s.log_scales[a]) <= 1.0f / 32.0f + 1e-5f, std::string(what) + ": scale");
+      expect(std::fabs(back.sh_dc[a] - s.sh_dc[a]) <= 0.5f / 255.0f / 0.15f + 1e-5f, std::string(what) + ": colour");
+    }
+    const float o0 = 1.0f / (1.0f + std::exp(-s.opacity_logits[i])), o1 = 1.0f / (1.0f + std::exp(-back.opacity_logits[i]));
+    expect(std::fabs(o0 - o1) <= 0.5f / 255.0f + 1e-5f, std::string(what) + ": opacity");
+    const float* q0 = &s.rotations[size_t(i) * 4];
+    const float* q1 = &back.rotations[size_t(i) * 4];
+    const float n0 = std::sqrt(q0[0] * q0[0] + q0[1] * q0[1] + q0[2] * q0[2] + q0[3] * q0[3]);
+    const float dot = (q0[0] * q1[0] + q0[1] * q1[1] + q0[2] * q1[2] + q0[3] * q1[3]) / n0;
+    expect(std::fabs(dot) >= 0.9999f, std::string(what) + ": rotation");  // the same rotation (q or -q)
+    const int c = gs::sh_rest_coeffs(s.sh_degree);
+    for (int j = 0; j < c * 3; ++j) {
+      const size_t a = size_t(i) * c * 3 + j;
+      const float v = std::min(std::max(s.sh_rest[a], -1.0f), 127.0f / 128.0f);
+      expect(std::fabs(back.sh_rest[a] - v) <= 0.5f / 128.0f + 1e-6f, std::string(what) + ": sh");
+    }
+  }
+}
+
+// A v2 file (3-byte rotations) written byte by byte from the published layout.
+std::vector<uint8_t> spz_v2(const gs::SplatScene& s) {
+  const uint32_t n = s.count;
+  const int coeffs = gs::sh_rest_coeffs(s.sh_degree);
+  std::vector<uint8_t> raw(16);
+  const uint32_t head[3] = {0x5053474eu, 2u, n};
+  std::memcpy(raw.data(), head, 12);
+  raw[12] = uint8_t(s.sh_degree);
+  raw[13] = 12;
+  auto q8 = [](float v) { return uint8_t(std::lround(std::min(std::max(v, 0.0f), 255.0f))); };
+  for (uint32_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t u = uint32_t(std::lround(s.positions[size_t(i) * 3 + k] * 4096.0f)) & 0xffffffu;
+      raw.insert(raw.end(), {uint8_t(u), uint8_t(u >> 8), uint8_t(u >> 16)});
+    }
+  for (uint32_t i = 0; i < n; ++i) raw.push_back(q8(255.0f / (1.0f + std::exp(-s.opacity_logits[i]))));
+  for (uint32_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) raw.push_back(q8((s.sh_dc[size_t(i) * 3 + k] * 0.15f + 0.5f) * 255.0f));
+  for (uint32_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) raw.push_back(q8((s.log_scales[size_t(i) * 3 + k] + 10.0f) * 16.0f));
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* q = &s.rotations[size_t(i) * 4];
+    const float len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const float sign = q[0] < 0.0f ? -1.0f : 1.0f;  // w >= 0
+    for (int k = 1; k <= 3; ++k) raw.push_back(q8((sign * q[k] / len + 1.0f) * 127.5f));
+  }
+  for (uint32_t i = 0; i < n; ++i)
+    for (int j = 0; j < coeffs * 3; ++j) raw.push_back(q8(s.sh_rest[size_t(i) * coeffs * 3 + j] * 128.0f + 128.0f));
+  std::vector<uint8_t> out(compressBound(uLong(raw.size())) + 64);
+  z_stream zs{};
+  deflateInit2(&zs, Z_BEST_SPEED, Z_DEFLATED, 16 + MAX_WBITS, 8, Z_DEFAULT_STRATEGY);
+  zs.next_in = raw.data();
+  zs.avail_in = uInt(raw.size());
+  zs.next_out = out.data();
+  zs.avail_out = uInt(out.size());
+  deflate(&zs, Z_FINISH);
+  out.resize(out.size() - zs.avail_out);
+  deflateEnd(&zs);
+  return out;
 }
 
 int scene_checks(const std::string& dir) {
@@ -42,6 +118,19 @@ int scene_checks(const std::string& dir) {
     for (float& v : q.rotations) v = -v;
     if (q.positions != s.positions || q.sh_rest != s.sh_rest || q.rotations != s.rotations)
       throw std::runtime_error("convention round trip is not the identity at degree " + std::to_string(degree));
+    const std::vector<uint8_t> spz = gs::save_spz(s, 12);
+    check_spz(s, gs::load_splat_file(spz.data(), spz.size()), "spz v3");
+    const std::vector<uint8_t> v2 = spz_v2(s);
+    gs::SplatScene b2 = gs::load_splat_file(v2.data(), v2.size());
+    // v2 rotations keep 8 bits per component: compare to a looser bound.
+    for (uint32_t i = 0; i < s.count; ++i) {
+      const float* q0 = &s.rotations[size_t(i) * 4];
+      const float* q1 = &b2.rotations[size_t(i) * 4];
+      const float n0 = std::sqrt(q0[0] * q0[0] + q0[1] * q0[1] + q0[2] * q0[2] + q0[3] * q0[3]);
+      expect(std::fabs(q0[0] * q1[0] + q0[1] * q1[1] + q0[2] * q1[2] + q0[3] * q1[3]) / n0 >= 0.995f, "spz v2: rotation");
+      for (int k = 0; k < 4; ++k) b2.rotations[size_t(i) * 4 + k] = q0[k];
+    }
+    check_spz(s, b2, "spz v2");
   }
   std::printf("ok\n");
   return 0;

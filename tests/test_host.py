@@ -1,6 +1,8 @@
 """The C++ host layer (libgs_host: gs::Trainer, scenes, datasets) on CPU.
 
-Runs the in-tree bin/gs_host_selftest: PLY round trips and axis conversion, and the
+Runs the in-tree bin/gs_host_selftest: PLY round trips (bit-exact), SPZ v3/v2 round trips
+(within the format's quantization; the layout is the published one, no SPZ files from
+other writers are available here), axis conversion, and the
 FrameData the C++ trainer writes compared word for word with the Python mirror
 (gs_b200.frame.make_frame, itself pinned to the oracle by the GPU parity tests).
 """
