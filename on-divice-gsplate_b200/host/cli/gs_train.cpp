@@ -5,8 +5,11 @@
 //   gs_train <dataset> <out.ply> [--iters 3000] [--views-per-step 1] [--max-gaussians N] [--sh 3]
 //            [--eval-every 1000] [--dssim 0.2] [--dssim-end L] [--grad-threshold 2e-4] [--opacity-reset N]
 //            [--sparse-adam] [--atomic] [--no-autotune] [--seed 1] [--json <metrics.json>]
-//            [--gt-gaussians N] [--init-gaussians N] [--cameras N]
-// <dataset> is a synthetic orbit capture (no capture folders are read by this build):
+//            [--gt-gaussians N] [--init-gaussians N] [--cameras N] [--width 360] [--no-masks]
+// <dataset> is a capture folder (transforms.json; PNG/PPM images, resized so the short side
+// is --width; initial gaussians from its point cloud or random, up to --init-gaussians,
+// 150000 by default; the reference's default options with the schedule scaled to --iters)
+// or a synthetic orbit capture:
 //   synthetic:orbit        ground truth of 100k gaussians (radius-1 ball, log-scales N(-4, 0.5),
 //                          SH 3 ~ N(0, 0.2)), 60 cameras on a circle of radius 3 at height 0.5,
 //                          360x640 f=500, every 8th held out; 20k initial gaussians at ground-truth
@@ -95,19 +98,22 @@ int main(int argc, char** argv) {
   }
   try {
     const std::string source = argv[1], out_path = argv[2];
-    if (source.rfind("synthetic:", 0) != 0)
-      throw std::runtime_error("this build reads synthetic:<name> datasets only (no image decoder for captures)");
-    Synthetic syn = preset(source.substr(10));
+    const bool synthetic = source.rfind("synthetic:", 0) == 0;
+    Synthetic syn;
     gs::TrainOptions options;
-    options.lr_opacity = 5e-2f;  // the orbit workload's rates: means 1.6e-4, scales 5e-3, rot 1e-3,
-    options.lr_sh_rest = 2.5e-3f;  // opacity 5e-2, SH 2.5e-3
-    options.masked = false;
-    options.random_background = false;
-    options.lambda_dssim_end = -1.0f;
-    options.densify_from = 500;
-    options.densify_until = 2500;
-    options.densify_interval = 100;
-    options.max_gaussians = syn.max_gaussians;
+    uint32_t width = 360, init_max = 150000;
+    if (synthetic) {
+      syn = preset(source.substr(10));
+      options.lr_opacity = 5e-2f;  // the orbit workload's rates: means 1.6e-4, scales 5e-3, rot 1e-3,
+      options.lr_sh_rest = 2.5e-3f;  // opacity 5e-2, SH 2.5e-3
+      options.masked = false;
+      options.random_background = false;
+      options.lambda_dssim_end = -1.0f;
+      options.densify_from = 500;
+      options.densify_until = 2500;
+      options.densify_interval = 100;
+      options.max_gaussians = syn.max_gaussians;
+    }
     uint32_t iterations = 3000, eval_every = 1000;
     std::string json_path;
     for (int i = 3; i < argc; ++i) {
@@ -131,8 +137,10 @@ int main(int argc, char** argv) {
       else if (arg == "--seed") options.seed = uint32_t(std::atoi(next()));
       else if (arg == "--json") json_path = next();
       else if (arg == "--gt-gaussians") syn.truth.count = uint32_t(std::atoi(next()));
-      else if (arg == "--init-gaussians") syn.init = uint32_t(std::atoi(next()));
+      else if (arg == "--init-gaussians") syn.init = init_max = uint32_t(std::atoi(next()));
       else if (arg == "--cameras") syn.capture.cameras = uint32_t(std::atoi(next()));
+      else if (arg == "--width") width = uint32_t(std::atoi(next()));
+      else if (arg == "--no-masks") options.masked = false;
       else throw std::runtime_error("unknown option " + arg);
     }
     // The schedule (densify window, SH degree interval) scales with the iterations, as
@@ -141,14 +149,28 @@ int main(int argc, char** argv) {
     options.iterations = iterations;
     options.densify_from = uint32_t(options.densify_from * scale);
     options.densify_until = uint32_t(options.densify_until * scale);
-    options.densify_interval = std::max(1u, uint32_t(options.densify_interval * scale));
+    if (synthetic) options.densify_interval = std::max(1u, uint32_t(options.densify_interval * scale));
+    options.opacity_reset_interval = uint32_t(options.opacity_reset_interval * scale);
     options.sh_degree_interval = std::max(1u, uint32_t(options.sh_degree_interval * scale));
     options.retune_first = std::min(options.retune_first, iterations / 2);
 
     const auto t0 = std::chrono::steady_clock::now();
-    const gs::SplatScene truth = gs::make_random_scene(syn.truth);
-    gs::Dataset dataset = gs::make_orbit_capture(truth, syn.capture);
-    const gs::SplatScene init = initial_scene(truth, syn.truth, syn.init, options.seed);
+    gs::Dataset dataset;
+    gs::SplatScene init;
+    if (synthetic) {
+      const gs::SplatScene truth = gs::make_random_scene(syn.truth);
+      dataset = gs::make_orbit_capture(truth, syn.capture);
+      init = initial_scene(truth, syn.truth, syn.init, options.seed);
+    } else {
+      dataset = gs::load_dataset(source, width);
+      for (const std::string& s : dataset.skipped) std::printf("skipped %s\n", s.c_str());
+      gs::InitOptions io;
+      io.max_gaussians = init_max;
+      io.seed = options.seed;
+      gs::InitStats st;
+      init = gs::initialize_gaussians(dataset, io, &st);
+      std::printf("initial gaussians from %s: %zu points -> %u\n", st.source.c_str(), st.raw_points, init.count);
+    }
     std::printf("dataset %s: %zu views (%zu held out), camera extent %.3f; %u initial gaussians (%.1f s)\n",
                 source.c_str(), dataset.frames.size(), dataset.holdout_count(), dataset.camera_extent, init.count,
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());

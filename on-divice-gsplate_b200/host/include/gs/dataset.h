@@ -29,9 +29,12 @@ struct Dataset {
   float fx = 0, fy = 0, cx = 0, cy = 0;  // at training resolution
   bool has_masks = false;
   std::vector<DatasetFrame> frames;
+  std::vector<float> points;          // optional sparse point cloud, xyz
+  std::vector<uint8_t> point_colors;  // rgb per point
   float camera_center[3] = {0, 0, 0};
   float camera_extent = 1.0f;  // max camera distance from camera_center, x 1.1 (3DGS "scene extent")
   float world_up[3] = {0, 1, 0};
+  std::vector<std::string> skipped;  // frames left out because their files could not be read
 
   size_t train_count() const;
   size_t holdout_count() const;
@@ -40,6 +43,36 @@ struct Dataset {
 // Sets camera_center (mean camera position) and camera_extent from the frames
 // (dataset.cpp:66-83).
 void compute_camera_bounds(Dataset& dataset);
+
+// Loads `directory`/transforms.json (nerfstudio layout: w, h, fl_x[, fl_y, cx, cy],
+// frames with file_path, transform_matrix (OpenGL camera-to-world) and optional
+// mask_path; optional ply_file_path point cloud and gsplat_lab.world_up), as the
+// reference's load_dataset does (dataset.cpp:85-223): images resized by area so their
+// short side is `target_width` (never enlarged), masks into alpha (255 without masks),
+// every 8th frame held out, unreadable frames skipped and listed (throws when fewer than
+// 2 or half remain). Images are PNG (8/16-bit) or binary PPM/PGM; JPEG frames and depth
+// maps are not decoded by this build (JPEG frames are skipped like unreadable ones).
+Dataset load_dataset(const std::string& directory, uint32_t target_width);
+
+struct InitOptions {
+  uint32_t max_gaussians = 150000;
+  float initial_opacity = 0.2f;
+  uint32_t seed = 1;
+};
+
+struct InitStats {
+  std::string source;  // "points" or "random"
+  size_t raw_points = 0;
+  float voxel_size = 0;
+};
+
+// Initial gaussians (SH degree 0) from the dataset's sparse points, or random points
+// around the cameras' centre (initialize_gaussians, dataset.cpp:291-523 without its depth
+// source): over budget the points are merged per voxel (cell size bisected in log space to
+// land under max_gaussians; the bracket widens until it does), ordered along a Morton curve, given isotropic scales from the
+// mean distance to their 3 nearest neighbours (clamped to [1e-4, 0.02] x the points'
+// robust extent), identity rotations and `initial_opacity`.
+SplatScene initialize_gaussians(const Dataset& dataset, const InitOptions& options, InitStats* stats = nullptr);
 
 // Pinhole camera (scene -> camera, OpenCV convention) for a frame, at the frame's own
 // resolution when it has one.

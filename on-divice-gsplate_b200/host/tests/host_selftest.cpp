@@ -3,6 +3,9 @@
 //                                  SPZ v3 and v2 round trips within their quantization
 //   gs_host_selftest frame         one FrameData as 72 hex words (compared with gs_b200.frame)
 //   gs_host_selftest camera        look-at camera as 12 floats (rotation rows, translation)
+//   gs_host_selftest dataset <dir> <width> <max_init>
+//                                  load_dataset + initialize_gaussians: a JSON summary on
+//                                  stdout, frame 0's RGBA in <dir>/frame0.rgba
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +17,7 @@
 
 #include "../src/frame.h"
 #include "gs/camera.h"
+#include "gs/dataset.h"
 #include "gs/splat_scene.h"
 #include "gs/trainer.h"
 
@@ -167,6 +171,32 @@ int camera_floats() {
   return 0;
 }
 
+int dataset_summary(const std::string& dir, uint32_t width, uint32_t max_init) {
+  const gs::Dataset ds = gs::load_dataset(dir, width);
+  gs::InitOptions io;
+  io.max_gaussians = max_init;
+  gs::InitStats st;
+  const gs::SplatScene init = gs::initialize_gaussians(ds, io, &st);
+  gs::write_file(dir + "/frame0.rgba", ds.frames.at(0).rgba);
+  float smin = INFINITY, smax = -INFINITY;
+  for (float v : init.log_scales) {
+    smin = std::min(smin, v);
+    smax = std::max(smax, v);
+  }
+  std::printf("{\"name\": \"%s\", \"width\": %u, \"height\": %u, \"fx\": %.6g, \"fy\": %.6g, \"cx\": %.6g, "
+              "\"cy\": %.6g, \"frames\": %zu, \"holdout\": %zu, \"skipped\": %zu, \"has_masks\": %s, \"points\": %zu, "
+              "\"extent\": %.6g, \"names\": [",
+              ds.name.c_str(), ds.width, ds.height, ds.fx, ds.fy, ds.cx, ds.cy, ds.frames.size(), ds.holdout_count(),
+              ds.skipped.size(), ds.has_masks ? "true" : "false", ds.points.size() / 3, ds.camera_extent);
+  for (size_t i = 0; i < ds.frames.size(); ++i)
+    std::printf("%s\"%s\"", i ? ", " : "", ds.frames[i].name.c_str());
+  std::printf("], \"init_source\": \"%s\", \"init_raw\": %zu, \"init_count\": %u, \"init_voxel\": %.6g, "
+              "\"log_scale_min\": %.6g, \"log_scale_max\": %.6g, \"init_opacity_logit\": %.6g}\n",
+              st.source.c_str(), st.raw_points, init.count, st.voxel_size, smin, smax,
+              init.count ? init.opacity_logits[0] : 0.0f);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -175,6 +205,7 @@ int main(int argc, char** argv) {
     if (mode == "scene" && argc > 2) return scene_checks(argv[2]);
     if (mode == "frame") return frame_words();
     if (mode == "camera") return camera_floats();
+    if (mode == "dataset" && argc > 4) return dataset_summary(argv[2], uint32_t(std::atoi(argv[3])), uint32_t(std::atoi(argv[4])));
     std::fprintf(stderr, "usage: %s scene <dir> | frame | camera\n", argv[0]);
     return 2;
   } catch (const std::exception& e) {
