@@ -419,7 +419,7 @@ def main() -> None:
                          "unit": "GB/s", "frac": per_pass[dom]["frac"], "traffic": traffic,
                          "peak_source": pk["source"], "per_pass": per_pass},
             "e2e": {"value": round(e2e, 3), "unit": "views/s", "h2d_bytes_per_step": VIEWS_PER_STEP * WIDTH * HEIGHT * 4,
-                    "d2h_bytes_per_step": 16 + 64 * VIEWS_PER_STEP},
+                    "d2h_bytes_per_step": 4 * (4 + 2 * 16) + 64 * VIEWS_PER_STEP},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

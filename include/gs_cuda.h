@@ -157,8 +157,9 @@ int gs_model_moments(gs_context* ctx, float* m16, float* v16, float* m_sh, float
 /* The views of the next step: one FrameData each, with its own resolution, and each
    view's target image (RGBA8, width x height x 4 bytes; NULL: no loss). Replaces
    Trainer::write_frame's host-visible uploads (trainer.cpp:440-547, 1024-1031). The
-   targets are copied asynchronously on the context's stream: their buffers must stay
-   unchanged until the next gs_step returns (pinned memory is copied by DMA). */
+   targets are copied asynchronously on a second stream of the context, overlapping the
+   next step's projection and sort: their buffers must stay unchanged until the next
+   gs_step returns (pinned memory is copied by DMA). */
 int gs_set_views(gs_context* ctx, uint32_t n_views, const gs_frame_data* frames, const uint8_t* const* rgba_targets);
 
 /* Target images kept in HBM across steps (the dataset's views): n_images RGBA8 images of

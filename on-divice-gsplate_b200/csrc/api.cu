@@ -73,6 +73,11 @@ void set_last_error(const std::string& message) { g_last_error = message; }
 struct gs_context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Host targets are uploaded on copy_stream while the step's projection and sort run;
+  // the step waits for targets_ready just before the forward raster, the first pass that
+  // reads them.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t targets_ready = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t marks[7] = {};  // pass boundaries when profiling
   bool profile = false;
@@ -119,6 +124,9 @@ struct gs_context {
   const uint32_t* sorted_keys = nullptr;
   const uint32_t* sorted_values = nullptr;
   // scalars: [0] pairs (the scan's total), [1] emit mismatches (whole run)
+  // Step scalars: [0] pairs, [1] emit mismatches (accumulate), [2] the sort's error word,
+  // [3] unused, [4 + v] first pair of view v, [4 + kMaxViews + v] its end.
+  static constexpr uint32_t kScalars = 4 + 2 * GS_MAX_VIEWS;
   uint32_t* d_scalars = nullptr;
   uint32_t* h_scalars = nullptr;  // pinned
   double* d_view_sums = nullptr;
@@ -164,6 +172,10 @@ struct gs_context {
       if (e) cudaEventDestroy(e);
       e = nullptr;
     }
+    if (targets_ready) cudaEventDestroy(targets_ready);
+    targets_ready = nullptr;
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
     if (stream) cudaStreamDestroy(stream);
     ev0 = ev1 = nullptr;
     stream = nullptr;
@@ -271,7 +283,8 @@ struct gs_context {
     GS_CUDA_TRY(cudaMemcpyAsync(d_table, h_table, sizeof(gsk::StepTable), cudaMemcpyHostToDevice, stream));
     GS_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(uint32_t) * gsk::kQueueCount, stream));
     record(train, degree);
-    GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    GS_CUDA_TRY(cudaMemcpyAsync(d_scalars + 2, sort.err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
+    GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, kScalars * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * 8 * n_views, cudaMemcpyDeviceToHost,
                                 stream));
   }
@@ -337,8 +350,7 @@ struct gs_context {
       GS_CUDA_TRY(cudaEventRecord(ev1, stream));
       GS_CUDA_TRY(cudaStreamSynchronize(stream));
       check_launch("step");
-      uint32_t err = 0;
-      GS_CUDA_TRY(cudaMemcpy(&err, sort.err, sizeof(err), cudaMemcpyDeviceToHost));
+      const uint32_t err = h_scalars[2];  // copied with the step's scalars
       if (err != 0u) {
         GS_CUDA_TRY(cudaMemset(sort.err, 0, sizeof(uint32_t)));
         fail(GS_ERR_TIMEOUT, "a bounded device-side wait (sort/scan look-back) gave up; results discarded");
@@ -468,15 +480,9 @@ struct gs_context {
       out[0] = last_pairs;
       return;
     }
-    std::vector<uint2> r(total_tiles + 1);
-    cudaMemcpy(r.data(), ranges, sizeof(uint2) * r.size(), cudaMemcpyDeviceToHost);
+    // The views' spans in the sorted pairs, found by k_ranges (stored pairs only).
     for (uint32_t v = 0; v < n_views; ++v) {
-      uint64_t lo = UINT64_MAX, hi = 0;
-      for (uint32_t t = vt.tile_base[v]; t < vt.tile_base[v + 1]; ++t)
-        if (r[t].y > r[t].x) {
-          lo = std::min<uint64_t>(lo, r[t].x);
-          hi = std::max<uint64_t>(hi, r[t].y);
-        }
+      const uint32_t lo = h_scalars[4 + v], hi = h_scalars[4 + GS_MAX_VIEWS + v];
       out[v] = hi > lo ? hi - lo : 0;
     }
   }
@@ -538,10 +544,17 @@ struct gs_context {
     sorted_keys = pairs_alt ? keys_alt : keys;
     sorted_values = pairs_alt ? values_alt : values;
     GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (max_tiles + 1), stream));
-    gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, stream);
+    GS_CUDA_TRY(cudaMemsetAsync(d_scalars + 4, 0, 2 * GS_MAX_VIEWS * sizeof(uint32_t), stream));
+    gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, sp.vt, d_scalars + 4, stream);
     ++launches;
     mark(2);
     const gsk::RasterBuffers rb = raster_buffers();
+    {
+      cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+      GS_CUDA_TRY(cudaStreamIsCapturing(stream, &capture));
+      GS_CUDA_TRY(cudaStreamWaitEvent(stream, targets_ready,
+                                      capture == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0u));
+    }
     gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2, stream);
     ++launches;
     mark(3);
@@ -620,7 +633,7 @@ struct gs_context {
       if (targets != nullptr) {
         t.target[v] = target + t.pixel_base[v];
         const size_t bytes = size_t(next[v].image[0]) * next[v].image[1] * 4;
-        GS_CUDA_TRY(cudaMemcpyAsync(target + t.pixel_base[v], targets[v], bytes, cudaMemcpyHostToDevice, stream));
+        GS_CUDA_TRY(cudaMemcpyAsync(target + t.pixel_base[v], targets[v], bytes, cudaMemcpyHostToDevice, copy_stream));
       } else if (images != nullptr) {
         t.target[v] = d_dataset + ds_offset[images[v]];
       }
@@ -630,6 +643,9 @@ struct gs_context {
     n_views = n;
     total_tiles = t.total_tiles;
     total_pixels = t.total_pixels;
+    // Recorded for every view set (no copies: already complete), so the step's wait on it
+    // keeps one launch structure.
+    GS_CUDA_TRY(cudaEventRecord(targets_ready, copy_stream));
     has_target = targets != nullptr || images != nullptr;
   }
 
@@ -764,22 +780,24 @@ int gs_create(int device, gs_context** out) {
     c->tuning.graph = 0u;
     try {
       GS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      GS_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      GS_CUDA_TRY(cudaEventCreateWithFlags(&c->targets_ready, cudaEventDisableTiming));
       GS_CUDA_TRY(cudaEventCreate(&c->ev0));
       GS_CUDA_TRY(cudaEventCreate(&c->ev1));
       for (cudaEvent_t& e : c->marks) GS_CUDA_TRY(cudaEventCreate(&e));
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_table), sizeof(gsk::StepTable)));
       std::memset(c->h_table, 0, sizeof(gsk::StepTable));
-      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), 4 * sizeof(uint32_t)));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), gs_context::kScalars * sizeof(uint32_t)));
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_view_sums), 8 * sizeof(double) * GS_MAX_VIEWS));
       dev_alloc(c->d_table, 1);
       dev_alloc(c->d_queue, gsk::kQueueCount);
       c->sm_count = prop.multiProcessorCount;
-      dev_alloc(c->d_scalars, 4);
+      dev_alloc(c->d_scalars, gs_context::kScalars);
       dev_alloc(c->d_view_sums, 8 * GS_MAX_VIEWS);
       dev_alloc(c->sort.hist, 8 * 256);
       dev_alloc(c->sort.ticket, 1);
       dev_alloc(c->sort.err, 1);
-      GS_CUDA_TRY(cudaMemset(c->d_scalars, 0, 4 * sizeof(uint32_t)));
+      GS_CUDA_TRY(cudaMemset(c->d_scalars, 0, gs_context::kScalars * sizeof(uint32_t)));
       GS_CUDA_TRY(cudaMemset(c->sort.err, 0, sizeof(uint32_t)));
     } catch (...) {
       delete c;

@@ -76,22 +76,33 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   }
 }
 
-// Grid-stride over the stored pairs (the grid is sized for the SMs, not the capacity).
+// Grid-stride over the stored pairs (the grid is sized for the SMs, not the capacity). At
+// each tile boundary that is also a view boundary the view spans are written too.
 __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count,
-                                                uint32_t capacity, uint2* __restrict__ ranges) {
+                                                uint32_t capacity, uint2* __restrict__ ranges, const ViewTable* vt,
+                                                uint32_t* __restrict__ view_span) {
   const uint32_t count = min(*d_count, capacity);
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
     const uint32_t tile = keys[s];
     if (s == 0u) {
       ranges[tile].x = 0u;
+      view_span[view_of_tile(vt, tile)] = 0u;
     } else {
       const uint32_t prev = keys[s - 1u];
       if (prev != tile) {
         ranges[prev].y = s;
         ranges[tile].x = s;
+        const uint32_t v = view_of_tile(vt, tile), vp = view_of_tile(vt, prev);
+        if (v != vp) {
+          view_span[v] = s;
+          view_span[kMaxViews + vp] = s;
+        }
       }
     }
-    if (s == count - 1u) ranges[tile].y = count;
+    if (s == count - 1u) {
+      ranges[tile].y = count;
+      view_span[kMaxViews + view_of_tile(vt, tile)] = count;
+    }
   }
 }
 
@@ -107,10 +118,10 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
 }
 
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
-                   cudaStream_t st) {
+                   const ViewTable* vt, uint32_t* view_span, cudaStream_t st) {
   if (pair_capacity == 0u) return;
   k_ranges<<<min((pair_capacity + 255u) / 256u, 148u * 16u), 256, 0, st>>>(sorted_keys, d_count, pair_capacity,
-                                                                          ranges);
+                                                                          ranges, vt, view_span);
 }
 
 }  // namespace gsk

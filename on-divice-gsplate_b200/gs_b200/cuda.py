@@ -104,6 +104,14 @@ def _check(code: int) -> None:
         raise GsError(code, load().gs_last_error().decode())
 
 
+def _frames(frames) -> np.ndarray:
+    """The views' FrameData as one contiguous array (no copies beyond the concatenation when
+    they already are FRAME_DTYPE records)."""
+    if all(isinstance(f, np.ndarray) and f.dtype == FRAME_DTYPE for f in frames):
+        return np.concatenate([f.reshape(1) for f in frames])
+    return np.ascontiguousarray(np.concatenate([np.asarray(f, FRAME_DTYPE).reshape(1) for f in frames]))
+
+
 def _ptr(a):
     return None if a is None else ctypes.c_void_p(a.ctypes.data)
 
@@ -174,7 +182,7 @@ class Context:
 
     # ---- step ----
     def set_views(self, frames: list[np.ndarray], targets: list[np.ndarray] | None) -> None:
-        fr = np.ascontiguousarray(np.concatenate([np.asarray(f, FRAME_DTYPE).reshape(1) for f in frames]))
+        fr = _frames(frames)
         tptr = None
         keep = [fr]
         if targets is not None:
@@ -193,7 +201,7 @@ class Context:
         _check(self.lib.gs_dataset_set(self.h, len(arrs), _ptr(w), _ptr(h), ptrs))
 
     def set_views_dataset(self, frames: list[np.ndarray], images: list[int]) -> None:
-        fr = np.ascontiguousarray(np.concatenate([np.asarray(f, FRAME_DTYPE).reshape(1) for f in frames]))
+        fr = _frames(frames)
         idx = np.ascontiguousarray(images, np.uint32)
         self._keep = [fr]
         _check(self.lib.gs_set_views_dataset(self.h, len(frames), _ptr(fr), _ptr(idx)))
