@@ -78,6 +78,15 @@ struct gs_context {
   // reads them.
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t targets_ready = nullptr;
+  // Host targets of the views set last, uploaded by the next step (after its step table,
+  // so the table does not queue behind them on the copy engine), once per gs_set_views.
+  struct PendingTarget {
+    uint32_t offset;
+    const uint8_t* host;
+    size_t bytes;
+  };
+  std::vector<PendingTarget> pending_targets;
+  bool targets_uploaded = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t marks[7] = {};  // pass boundaries when profiling
   bool profile = false;
@@ -279,8 +288,8 @@ struct gs_context {
 
   // Everything one step puts on the stream: the step table upload, the queue reset, the
   // launch sequence and the readback of the pair count and loss sums.
+  // The step table is uploaded by run_step before this (outside any graph).
   void enqueue_step(bool train, uint32_t degree) {
-    GS_CUDA_TRY(cudaMemcpyAsync(d_table, h_table, sizeof(gsk::StepTable), cudaMemcpyHostToDevice, stream));
     GS_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(uint32_t) * gsk::kQueueCount, stream));
     record(train, degree);
     GS_CUDA_TRY(cudaMemcpyAsync(d_scalars + 2, sort.err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
@@ -338,6 +347,16 @@ struct gs_context {
         f.model[2] = model.sh_stride;
         f.limits[0] = uint32_t(pair_cap);
         f.limits[3] = uint32_t(pair_cap);
+      }
+      // The table first, then the targets of a new view set on the copy stream (the step
+      // waits for them before the forward raster; views without host targets record an
+      // event that is already complete).
+      GS_CUDA_TRY(cudaMemcpyAsync(d_table, h_table, sizeof(gsk::StepTable), cudaMemcpyHostToDevice, stream));
+      if (!targets_uploaded) {
+        for (const PendingTarget& p : pending_targets)
+          GS_CUDA_TRY(cudaMemcpyAsync(target + p.offset, p.host, p.bytes, cudaMemcpyHostToDevice, copy_stream));
+        GS_CUDA_TRY(cudaEventRecord(targets_ready, copy_stream));
+        targets_uploaded = true;
       }
       GS_CUDA_TRY(cudaEventRecord(ev0, stream));
       // A profiled step runs directly: its pass events must be recorded by the stream.
@@ -627,13 +646,14 @@ struct gs_context {
     if (targets != nullptr)
       for (uint32_t v = 0; v < n; ++v)
         if (targets[v] == nullptr) fail(GS_ERR_INVALID, "gs_set_views: missing target image");
+    std::vector<PendingTarget> pending;
     reserve_views(n);
     reserve_pixels(pixels, tiles);
     for (uint32_t v = 0; v < n; ++v) {
       if (targets != nullptr) {
         t.target[v] = target + t.pixel_base[v];
         const size_t bytes = size_t(next[v].image[0]) * next[v].image[1] * 4;
-        GS_CUDA_TRY(cudaMemcpyAsync(target + t.pixel_base[v], targets[v], bytes, cudaMemcpyHostToDevice, copy_stream));
+        pending.push_back({t.pixel_base[v], targets[v], bytes});
       } else if (images != nullptr) {
         t.target[v] = d_dataset + ds_offset[images[v]];
       }
@@ -643,9 +663,8 @@ struct gs_context {
     n_views = n;
     total_tiles = t.total_tiles;
     total_pixels = t.total_pixels;
-    // Recorded for every view set (no copies: already complete), so the step's wait on it
-    // keeps one launch structure.
-    GS_CUDA_TRY(cudaEventRecord(targets_ready, copy_stream));
+    pending_targets = std::move(pending);
+    targets_uploaded = false;
     has_target = targets != nullptr || images != nullptr;
   }
 
