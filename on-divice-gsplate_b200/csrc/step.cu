@@ -162,6 +162,15 @@ __device__ __forceinline__ void slot_geometry(float4 p0, float4 p1, float4 q, Ge
   G.opacity = sigmoidf(p0.w);
 }
 
+// The views slot i was seen in, as a bit mask: every view's tile count is loaded at once.
+__device__ __forceinline__ uint32_t seen_views(const uint32_t* tiles, uint32_t n_views, uint32_t cap, uint32_t i) {
+  uint32_t mask = 0u;
+#pragma unroll
+  for (uint32_t v = 0; v < kMaxViews; ++v)
+    if (v < n_views && tiles[size_t(v) * cap + i] != 0u) mask |= 1u << v;
+  return mask;
+}
+
 // Colour gradient of one view with the clamped channels zeroed (train_step.glsl:135-138).
 __device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t clamped, float dcol[3]) {
   dcol[0] = (clamped & 1u) ? 0.0f : a1.z;
@@ -378,11 +387,31 @@ __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
   for (int k = 0; k < K; ++k) g[k][0] = g[k][1] = g[k][2] = 0.0f;
   float pd[3] = {0.f, 0.f, 0.f};
   bool colour = false;
-  for (uint32_t v = 0; v < a.n_views; ++v) {
-    const size_t gv = size_t(v) * a.cap + i;
-    if (a.tiles[gv] == 0u) continue;
+  // Views in order; the next view's loads are issued before this view's arithmetic.
+  uint32_t mask = seen_views(a.tiles, a.n_views, a.cap, i);
+  uint32_t nv = mask ? uint32_t(__ffs(mask) - 1) : 0u;
+  float4 n1 = make_float4(0.f, 0.f, 0.f, 0.f), n2 = n1;
+  float nw = 0.0f;
+  if (mask) {
+    const size_t gv = size_t(nv) * a.cap + i;
+    n1 = a.grad2d[gv * 3u + 1u];
+    n2 = a.grad2d[gv * 3u + 2u];
+    nw = a.splat[gv * 3u + 2u].w;
+  }
+  while (mask) {
+    const uint32_t v = nv;
+    const float4 a1 = n1, a2 = n2;
+    const float cw = nw;
+    mask &= mask - 1u;
+    if (mask) {
+      nv = uint32_t(__ffs(mask) - 1);
+      const size_t gv = size_t(nv) * a.cap + i;
+      n1 = a.grad2d[gv * 3u + 1u];
+      n2 = a.grad2d[gv * 3u + 2u];
+      nw = a.splat[gv * 3u + 2u].w;
+    }
     float dcol[3];
-    view_colour_grad(a.grad2d[gv * 3u + 1u], a.grad2d[gv * 3u + 2u], __float_as_uint(a.splat[gv * 3u + 2u].w), dcol);
+    view_colour_grad(a1, a2, __float_as_uint(cw), dcol);
     colour |= dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f;
     const gs_frame_data& f = s_frames[v];
     const float dr0 = p0.x - f.cam_pos[0], dr1 = p0.y - f.cam_pos[1], dr2 = p0.z - f.cam_pos[2];
@@ -452,15 +481,36 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   Geometry G;
   slot_geometry(p0, p1, q, G);
   float4 st = a.stats[i];
-  bool seen = false;
-  for (uint32_t v = 0; v < a.n_views; ++v) {
-    const size_t g = size_t(v) * a.cap + i;
-    if (a.tiles[g] == 0u) continue;
-    seen = true;
+  // Views in order; the next view's loads are issued before this view's arithmetic.
+  uint32_t mask = seen_views(a.tiles, a.n_views, a.cap, i);
+  const bool seen = mask != 0u;
+  uint32_t nv = mask ? uint32_t(__ffs(mask) - 1) : 0u;
+  float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0, n2 = n0;
+  float nw = 0.0f, nr = 0.0f;
+  if (mask) {
+    const size_t g = size_t(nv) * a.cap + i;
+    n0 = a.grad2d[g * 3u];
+    n1 = a.grad2d[g * 3u + 1u];
+    n2 = a.grad2d[g * 3u + 2u];
+    nw = a.splat[g * 3u + 2u].w;
+    nr = a.splat[g * 3u + 1u].w;
+  }
+  while (mask) {
+    const uint32_t v = nv;
+    const float4 a0 = n0, a1 = n1, a2 = n2;
+    const float cw = nw, radius = nr;
+    mask &= mask - 1u;
+    if (mask) {
+      nv = uint32_t(__ffs(mask) - 1);
+      const size_t g = size_t(nv) * a.cap + i;
+      n0 = a.grad2d[g * 3u];
+      n1 = a.grad2d[g * 3u + 1u];
+      n2 = a.grad2d[g * 3u + 2u];
+      nw = a.splat[g * 3u + 2u].w;
+      nr = a.splat[g * 3u + 1u].w;
+    }
     float dcol[3], dir[3], dir_len;
-    view_backward<DEG>(s_frames[v], p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u], a.grad2d[g * 3u + 2u],
-                       __float_as_uint(a.splat[g * 3u + 2u].w), a.splat[g * 3u + 1u].w, g16, st, dcol, dir, dir_len,
-                       drew);
+    view_backward<DEG>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, st, dcol, dir, dir_len, drew);
   }
   if (DEG > 0) {
     const float4 pd = a.dir_grad[i];
