@@ -46,6 +46,12 @@ extern "C" {
 /* Flags in gs_frame_data.model[3] (train_common.glsl:50-57). */
 #define GS_FLAG_MASKED_TARGET 1u /* composite the target over the background by its alpha */
 #define GS_FLAG_SSIM 4u          /* measure SSIM (and its gradient when training) */
+/* Sum the gradient of the loss with respect to a small change of this view's camera pose
+   (gs_step_result.pose_grad; train_step.glsl:7-10, trainer.cpp:74). */
+#define GS_FLAG_POSE_GRAD 8u
+/* On the first view: the step computes gradients (pose_grad) but changes neither the
+   model nor its densification statistics (train_step.glsl:92-100, 222). */
+#define GS_FLAG_POSE_ONLY 16u
 #define GS_FLAG_SPARSE_ADAM 128u /* gaussians that drew nothing keep their values and moments */
 
 /* Per-view step constants: FrameData of train_common.glsl:15-37, filled as
@@ -89,6 +95,15 @@ typedef struct gs_step_result {
      ranges), [2] rasterize, [3] loss (SSIM and its gradient), [4] backward,
      [5] optimize (pair sum + projection backward + Adam). */
   float pass_ms[6];
+  /* Per view, the rest of the tile sums (train_forward.comp:142-151; Trainer::read_slot's
+     fit_): [0..2] sum R^2 rgb, [3] pixels, [4..6] sum R P rgb, with R the model's colour
+     and P the photo's over the pixels where both are opaque (target alpha > 0.95,
+     transmittance < 0.05); [7] pixels whose target alpha is above 0. */
+  double fit[GS_MAX_VIEWS][8];
+  /* Per view with GS_FLAG_POSE_GRAD (else 0): dL/dd xyz then dL/dw xyz in camera axes,
+     for world -> camera [W | t] becoming [(I + [w]x) W | (I + [w]x) t + d]
+     (train_step.glsl:196-203; Trainer::pose_gradient, trainer.cpp:1336-1348). */
+  double pose_grad[GS_MAX_VIEWS][6];
 } gs_step_result;
 
 /* Which intermediate buffer gs_snapshot copies (Trainer::DebugSnapshot, trainer.h:302-313). */

@@ -138,8 +138,12 @@ struct gs_context {
   static constexpr uint32_t kScalars = 4 + 2 * GS_MAX_VIEWS;
   uint32_t* d_scalars = nullptr;
   uint32_t* h_scalars = nullptr;  // pinned
+  // Per view: [0..15] the tile sums (losses, then the exposure fit), [16..21] the pose
+  // gradient, [22..23] unused.
+  static constexpr uint32_t kViewSums = 24;
   double* d_view_sums = nullptr;
   double* h_view_sums = nullptr;  // pinned
+  float* pose_partial = nullptr;  // per view and 128 slots: the pose gradient's partial sums
   gsk::SortScratch sort;
   gsk::DensifyScratch dens;
   uint64_t max_pairs_seen = 0;
@@ -155,7 +159,7 @@ struct gs_context {
     for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.dir_grad, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
-    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss}) dev_free(*p);
+    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial}) dev_free(*p);
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
                          &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
                          &d_scalars, &sort.hist, &sort.lookback, &sort.ticket, &sort.err, &dens.spawn,
@@ -217,6 +221,7 @@ struct gs_context {
     dev_alloc(dkeys_alt, n);
     dev_alloc(dvals_alt, n);
     dev_alloc(sorted_offsets, n);
+    dev_alloc(pose_partial, size_t(views) * gsk::pose_blocks(model.cap) * 8u);
     GS_CUDA_TRY(cudaMemsetAsync(vb.tiles, 0, n * sizeof(uint32_t), stream));
     const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
     if (sort_tiles > sort.lookback_tiles) {
@@ -294,8 +299,8 @@ struct gs_context {
     record(train, degree);
     GS_CUDA_TRY(cudaMemcpyAsync(d_scalars + 2, sort.err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
     GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, kScalars * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * 8 * n_views, cudaMemcpyDeviceToHost,
-                                stream));
+    GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * kViewSums * n_views,
+                                cudaMemcpyDeviceToHost, stream));
   }
 
   // The step as a CUDA graph: captured once per launch structure (views, slots, buffer
@@ -305,7 +310,7 @@ struct gs_context {
     const std::vector<uint64_t> key = {n_views, model.slots, model.cap, pair_cap, tile_cap, pixel_cap, degree,
                                        train ? 1u : 0u, ssim ? 1u : 0u, tuning.deterministic,
                                        tuning.forward_pixels, tuning.backward_pixels, tuning.backward_batch,
-                                       tuning.sort_digit_bits};
+                                       tuning.sort_digit_bits, pose_mode()};
     if (graph_exec == nullptr || key != graph_key) {
       drop_graph();
       cudaGraph_t g = nullptr;
@@ -390,8 +395,13 @@ struct gs_context {
         out->retries = retries;
         out->tile_mismatch = h_scalars[1];
         view_pairs(out->pairs);
-        for (uint32_t v = 0; v < n_views; ++v)
-          for (int k = 0; k < 8; ++k) out->losses[v][k] = h_view_sums[v * 8 + k];
+        for (uint32_t v = 0; v < n_views; ++v) {
+          const double* s = h_view_sums + size_t(v) * kViewSums;
+          for (int k = 0; k < 8; ++k) out->losses[v][k] = s[k];
+          for (int k = 0; k < 8; ++k) out->fit[v][k] = s[8 + k];
+          if (train && (pose_mode() & 1u))
+            for (int k = 0; k < 6; ++k) out->pose_grad[v][k] = s[16 + k];
+        }
         out->gpu_ms = elapsed(ev0, ev1);
         out->kernels = uint32_t(launches);
         if (profile)
@@ -533,6 +543,16 @@ struct gs_context {
     return rb;
   }
 
+  // Bit 0: some view asks for its pose gradient; bit 1: the step changes nothing (the
+  // first view's GS_FLAG_POSE_ONLY).
+  uint32_t pose_mode() const {
+    uint32_t m = 0u;
+    for (uint32_t v = 0; v < n_views; ++v)
+      if (frames[v].model[3] & GS_FLAG_POSE_GRAD) m |= 1u;
+    if (n_views > 0 && (frames[0].model[3] & GS_FLAG_POSE_ONLY)) m |= 2u;
+    return m;
+  }
+
   // The launch sequence of one step (trainer.cpp:825-831), all on `stream`.
   void record(bool train, uint32_t degree) {
     const gsk::StepPointers sp = step_pointers();
@@ -586,7 +606,7 @@ struct gs_context {
         ++launches;
       }
     }
-    gsk::launch_loss_reduce(sp, tile_loss, d_view_sums, stream);
+    gsk::launch_loss_reduce(sp, tile_loss, d_view_sums, kViewSums, stream);
     ++launches;
     mark(4);
     if (train) {
@@ -600,8 +620,16 @@ struct gs_context {
                              stream);
         ++launches;
       }
-      gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), stream);
-      launches += degree > 0 ? 2 : 1;
+      const uint32_t pose = pose_mode();
+      if (pose & 1u) {
+        gsk::launch_pose_grad(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), pose_partial,
+                              d_view_sums + 16, kViewSums, stream);
+        launches += model.slots ? 2 : 1;
+      }
+      if ((pose & 2u) == 0u) {
+        gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), stream);
+        launches += model.slots ? (degree > 0 ? 2 : 1) : 0;
+      }
       mark(6);
     }
     check_launch("launch");
@@ -807,12 +835,13 @@ int gs_create(int device, gs_context** out) {
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_table), sizeof(gsk::StepTable)));
       std::memset(c->h_table, 0, sizeof(gsk::StepTable));
       GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), gs_context::kScalars * sizeof(uint32_t)));
-      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_view_sums), 8 * sizeof(double) * GS_MAX_VIEWS));
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_view_sums),
+                                 gs_context::kViewSums * sizeof(double) * GS_MAX_VIEWS));
       dev_alloc(c->d_table, 1);
       dev_alloc(c->d_queue, gsk::kQueueCount);
       c->sm_count = prop.multiProcessorCount;
       dev_alloc(c->d_scalars, gs_context::kScalars);
-      dev_alloc(c->d_view_sums, 8 * GS_MAX_VIEWS);
+      dev_alloc(c->d_view_sums, gs_context::kViewSums * GS_MAX_VIEWS);
       dev_alloc(c->sort.hist, 8 * 256);
       dev_alloc(c->sort.ticket, 1);
       dev_alloc(c->sort.err, 1);

@@ -106,13 +106,21 @@ void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const
 // ---- loss.cu ----
 void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
 void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
-void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, cudaStream_t st);
+// view_sums[v * stride + 0..15]: the view's 16 tile sums.
+void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, uint32_t stride,
+                        cudaStream_t st);
 
 // ---- step.cu ----
 void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* depth_order, const uint32_t* first,
                      const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
 void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
                  const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
+// Camera pose gradients of the views with GS_FLAG_POSE_GRAD (before launch_step, which
+// updates the parameters): out[v * stride + 0..5]. partial: n_views * pose_blocks(slots) * 8.
+uint32_t pose_blocks(uint32_t slots);
+void launch_pose_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                      const uint32_t* d_pairs, uint32_t accept, float* partial, double* out, uint32_t stride,
+                      cudaStream_t st);
 struct DensifyScratch {
   uint32_t* spawn = nullptr;     // action per slot
   uint32_t* release = nullptr;   // 1 per freed slot

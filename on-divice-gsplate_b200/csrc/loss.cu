@@ -307,27 +307,39 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   a.rb.pixel_dot[pix] = pg.x * o.x + pg.y * o.y + pg.z * o.z;
 }
 
+// The 16 tile sums of each view (Trainer::read_slot, trainer.cpp:778-795), in double and
+// a fixed order, into view_sums[v * stride + 0..15].
 __global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const float* __restrict__ tile_loss,
-                                                     double* __restrict__ view_sums) {
-  __shared__ double s[8][8];
+                                                     double* __restrict__ view_sums, uint32_t stride) {
+  __shared__ double s[8][16];
   const uint32_t v = blockIdx.x;
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
   const uint32_t t0 = vt->tile_base[v], t1 = vt->tile_base[v + 1];
-  for (uint32_t t = t0 + threadIdx.x; t < t1; t += 256u)
+  for (uint32_t t = t0 + threadIdx.x; t < t1; t += 256u) {
+    const float4* row = reinterpret_cast<const float4*>(tile_loss + size_t(t) * 16u);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] += double(tile_loss[size_t(t) * 16u + k]);
+    for (int q = 0; q < 4; ++q) {
+      const float4 x = row[q];
+      acc[4 * q] += double(x.x);
+      acc[4 * q + 1] += double(x.y);
+      acc[4 * q + 2] += double(x.z);
+      acc[4 * q + 3] += double(x.w);
+    }
+  }
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < 16; ++k)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
   if ((threadIdx.x & 31u) == 0u)
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s[threadIdx.x >> 5][k] = acc[k];
+    for (int k = 0; k < 16; ++k) s[threadIdx.x >> 5][k] = acc[k];
   __syncthreads();
-  if (threadIdx.x < 8u) {
+  if (threadIdx.x < 16u) {
     double sum = 0.0;
     for (int w = 0; w < 8; ++w) sum += s[w][threadIdx.x];
-    view_sums[v * 8u + threadIdx.x] = sum;
+    view_sums[size_t(v) * stride + threadIdx.x] = sum;
   }
 }
 
@@ -343,9 +355,10 @@ void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStrea
   k_ssim_grad<<<sp.tile_cap, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
 }
 
-void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, cudaStream_t st) {
+void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, uint32_t stride,
+                        cudaStream_t st) {
   if (sp.n_views == 0u) return;
-  k_loss_reduce<<<sp.n_views, 256, 0, st>>>(sp.vt, tile_loss, view_sums);
+  k_loss_reduce<<<sp.n_views, 256, 0, st>>>(sp.vt, tile_loss, view_sums, stride);
 }
 
 }  // namespace gsk

@@ -182,11 +182,13 @@ __device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t 
 // the 14 geometry + DC parameters to g16 (without the SH view-direction term, which
 // k_step_sh computes), updates the densification statistics, and returns the clamped
 // colour gradient and the view direction. drew: bit 0 any pair gradient, bit 1 a non-zero
-// colour gradient.
-template <int DEG>
+// colour gradient. With POSE it also adds the slot's share of the camera pose gradient to
+// pose (dL/dd, dL/dw; train_step.glsl:196-202).
+template <int DEG, bool POSE = false>
 __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0, const Geometry& G, float4 a0, float4 a1,
                                               float4 a2, uint32_t clamped, float radius, float g16[16], float4& st,
-                                              float dcol[3], float dir[3], float& dir_len, uint32_t& drew) {
+                                              float dcol[3], float dir[3], float& dir_len, uint32_t& drew,
+                                              float* pose = nullptr) {
   if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f || a0.w != 0.f || a1.x != 0.f || a1.y != 0.f || a1.z != 0.f ||
       a1.w != 0.f || a2.x != 0.f || a2.y != 0.f || a2.z != 0.f || a2.w != 0.f)
     drew |= 1u;
@@ -284,6 +286,18 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   dt[2] += -(dmx * fx * t[0] + dmy * fy * t[1]) * inv_z2;
 #pragma unroll
   for (int c = 0; c < 3; ++c) g16[c] += f.rot[0][c] * dt[0] + f.rot[1][c] * dt[1] + f.rot[2][c] * dt[2];
+  if (POSE) {
+    // A shift d moves t by d; a turn w moves t by w x t and W by [w]x W, so with
+    // X = dL/dW W^T = J^T dJ: dL/dw = t x dL/dt + (X21 - X12, X02 - X20, X10 - X01).
+    const float x01 = j00 * dJ[0][1], x02 = j00 * dJ[0][2], x10 = j11 * dJ[1][0], x12 = j11 * dJ[1][2];
+    const float x20 = j02 * dJ[0][0] + j12 * dJ[1][0], x21 = j02 * dJ[0][1] + j12 * dJ[1][1];
+    pose[0] += dt[0];
+    pose[1] += dt[1];
+    pose[2] += dt[2];
+    pose[3] += t[1] * dt[2] - t[2] * dt[1] + (x21 - x12);
+    pose[4] += t[2] * dt[0] - t[0] * dt[2] + (x02 - x20);
+    pose[5] += t[0] * dt[1] - t[1] * dt[0] + (x10 - x01);
+  }
 
   // 3D covariance -> log scale and rotation; dSigma = T^T G2 T folded into dM = 2 dSigma M.
   float dM[3][3];
@@ -524,6 +538,80 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   if (!sparse || (drew & 1u)) adam_params(a, f0, i, p0, p1, q, p3, g16);
 }
 
+// Camera pose gradient (train_step.glsl:196-202, 254-268): block (x, v) sums the shares of
+// its 128 slots in view v, if that view asks for it, in a fixed order (a butterfly per
+// warp, then the warps) into partial[(v * gridDim.x + x) * 8 + 0..5]. Parameters are read
+// before the step's update, as in the reference's single pass; the SH view-direction term
+// is left out there too.
+template <int DEG>
+__global__ void __launch_bounds__(128) k_pose_grad(StepArgs a, float* __restrict__ partial) {
+  __shared__ gs_frame_data s_frame;
+  __shared__ float s_red[4][6];
+  const uint32_t v = blockIdx.y;
+  if (threadIdx.x < uint32_t(sizeof(gs_frame_data) / 4))
+    reinterpret_cast<uint32_t*>(&s_frame)[threadIdx.x] = reinterpret_cast<const uint32_t*>(a.frames + v)[threadIdx.x];
+  __syncthreads();
+  if ((s_frame.model[3] & GS_FLAG_POSE_GRAD) == 0u) return;  // the whole block
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float pose[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (i < a.slots && *a.d_pairs <= a.accept) {
+    const size_t g = size_t(v) * a.cap + i;
+    const float4 p1 = a.P[a.cap + i];
+    if (p1.w >= 0.5f && a.tiles[g] != 0u) {
+      const float4 p0 = a.P[i], q = a.P[2u * a.cap + i];
+      Geometry G;
+      slot_geometry(p0, p1, q, G);
+      float g16[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) g16[k] = 0.0f;
+      float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+      float dcol[3], dir[3], dir_len;
+      uint32_t drew = 0u;
+      view_backward<DEG, true>(s_frame, p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u], a.grad2d[g * 3u + 2u],
+                               __float_as_uint(a.splat[g * 3u + 2u].w), 0.0f, g16, st, dcol, dir, dir_len, drew,
+                               pose);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pose[k] += __shfl_xor_sync(0xffffffffu, pose[k], o);
+  if ((threadIdx.x & 31u) == 0u)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s_red[threadIdx.x >> 5][k] = pose[k];
+  __syncthreads();
+  if (threadIdx.x < 6u)
+    partial[(size_t(v) * gridDim.x + blockIdx.x) * 8u + threadIdx.x] =
+        ((s_red[0][threadIdx.x] + s_red[1][threadIdx.x]) + s_red[2][threadIdx.x]) + s_red[3][threadIdx.x];
+}
+
+// The blocks' pose sums per view, in double and a fixed order (Trainer::pose_gradient,
+// trainer.cpp:1336-1348), into out[v * stride + 0..5]; 0 for views without the flag.
+__global__ void __launch_bounds__(256) k_pose_reduce(const gs_frame_data* frames, const float* __restrict__ partial,
+                                                     uint32_t blocks, double* __restrict__ out, uint32_t stride) {
+  __shared__ double s[8][6];
+  const uint32_t v = blockIdx.x;
+  const bool wanted = (frames[v].model[3] & GS_FLAG_POSE_GRAD) != 0u;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (wanted)
+    for (uint32_t b = threadIdx.x; b < blocks; b += 256u)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) acc[k] += double(partial[(size_t(v) * blocks + b) * 8u + k]);
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if ((threadIdx.x & 31u) == 0u)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s[threadIdx.x >> 5][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6u) {
+    double sum = 0.0;
+    for (int w = 0; w < 8; ++w) sum += s[w][threadIdx.x];
+    out[size_t(v) * stride + threadIdx.x] = sum;
+  }
+}
+
 // ---- densification ----
 
 struct DensifyArgs {
@@ -692,6 +780,26 @@ void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const 
     case 2: k_step_sh<2><<<grid, block, 0, st>>>(a); k_step_geometry<2><<<grid, block, 0, st>>>(a); break;
     default: k_step_sh<3><<<grid, block, 0, st>>>(a); k_step_geometry<3><<<grid, block, 0, st>>>(a); break;
   }
+}
+
+uint32_t pose_blocks(uint32_t slots) { return (slots + 127u) / 128u; }
+
+void launch_pose_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                      const uint32_t* d_pairs, uint32_t accept, float* partial, double* out, uint32_t stride,
+                      cudaStream_t st) {
+  const uint32_t blocks = pose_blocks(m.slots);
+  if (blocks > 0u) {
+    StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
+               vb.splat, vb.tiles, vb.grad2d, vb.dir_grad, d_pairs, accept};
+    const dim3 grid(blocks, sp.n_views), block(128);
+    switch (degree) {
+      case 0: k_pose_grad<0><<<grid, block, 0, st>>>(a, partial); break;
+      case 1: k_pose_grad<1><<<grid, block, 0, st>>>(a, partial); break;
+      case 2: k_pose_grad<2><<<grid, block, 0, st>>>(a, partial); break;
+      default: k_pose_grad<3><<<grid, block, 0, st>>>(a, partial); break;
+    }
+  }
+  k_pose_reduce<<<sp.n_views, 256, 0, st>>>(sp.frames, partial, blocks, out, stride);
 }
 
 void launch_densify(const gs_frame_data* d_frame, const Model& m, const DensifyScratch& ds, const SortScratch& ss,

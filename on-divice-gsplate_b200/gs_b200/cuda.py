@@ -41,7 +41,8 @@ class StepResult(ctypes.Structure):
     _fields_ = [("n_views", ctypes.c_uint32), ("overflow", ctypes.c_uint32), ("retries", ctypes.c_uint32),
                 ("tile_mismatch", ctypes.c_uint32), ("pairs", ctypes.c_uint64 * GS_MAX_VIEWS),
                 ("losses", (ctypes.c_double * 8) * GS_MAX_VIEWS), ("gpu_ms", ctypes.c_float),
-                ("kernels", ctypes.c_uint32), ("pass_ms", ctypes.c_float * 6)]
+                ("kernels", ctypes.c_uint32), ("pass_ms", ctypes.c_float * 6),
+                ("fit", (ctypes.c_double * 8) * GS_MAX_VIEWS), ("pose_grad", (ctypes.c_double * 6) * GS_MAX_VIEWS)]
 
 
 class Tuning(ctypes.Structure):

@@ -37,6 +37,8 @@ _SEED_WORD = FRAME_DTYPE.fields["densify1"][1] // 4 + 1
 TILE = 16
 FLAG_MASKED_TARGET = 1
 FLAG_SSIM = 4
+FLAG_POSE_GRAD = 8  # sum the view's camera pose gradient (StepResult.pose_grad)
+FLAG_POSE_ONLY = 16  # on the first view: gradients only, the model and its statistics stay
 FLAG_SPARSE_ADAM = 128
 BETA1, BETA2, EPSILON = 0.9, 0.999, 1e-15  # trainer.cpp:68-70
 

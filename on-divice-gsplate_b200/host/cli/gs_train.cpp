@@ -6,6 +6,8 @@
 //            [--eval-every 1000] [--dssim 0.2] [--dssim-end L] [--grad-threshold 2e-4] [--opacity-reset N]
 //            [--sparse-adam] [--atomic] [--no-autotune] [--seed 1] [--json <metrics.json>]
 //            [--gt-gaussians N] [--init-gaussians N] [--cameras N] [--width 360] [--no-masks]
+//            [--head-weight W] [--refine-poses] [--pose-lr shift,turn] [--pose-lr-final F] [--pose-from N]
+//            [--eval-pose-steps N] [--pose-out poses.json] [--refine-exposure]
 // <dataset> is a capture folder (transforms.json; PNG/PPM images, resized so the short side
 // is --width; initial gaussians from its point cloud or random, up to --init-gaussians,
 // 150000 by default; the reference's default options with the schedule scaled to --iters)
@@ -115,7 +117,7 @@ int main(int argc, char** argv) {
       options.max_gaussians = syn.max_gaussians;
     }
     uint32_t iterations = 3000, eval_every = 1000;
-    std::string json_path;
+    std::string json_path, pose_out;
     for (int i = 3; i < argc; ++i) {
       const std::string arg = argv[i];
       auto next = [&]() -> const char* {
@@ -141,6 +143,16 @@ int main(int argc, char** argv) {
       else if (arg == "--cameras") syn.capture.cameras = uint32_t(std::atoi(next()));
       else if (arg == "--width") width = uint32_t(std::atoi(next()));
       else if (arg == "--no-masks") options.masked = false;
+      else if (arg == "--head-weight") options.head_weight = float(std::atof(next()));
+      else if (arg == "--refine-poses") options.refine_poses = true;
+      else if (arg == "--pose-lr") {
+        if (std::sscanf(next(), "%f,%f", &options.lr_pose_shift, &options.lr_pose_turn) != 2)
+          throw std::runtime_error("--pose-lr needs shift,turn");
+      } else if (arg == "--pose-lr-final") options.lr_pose_final = float(std::atof(next()));
+      else if (arg == "--pose-from") options.pose_from = uint32_t(std::atoi(next()));
+      else if (arg == "--eval-pose-steps") options.eval_pose_steps = uint32_t(std::atoi(next()));
+      else if (arg == "--pose-out") pose_out = next();
+      else if (arg == "--refine-exposure") options.refine_exposure = true;
       else throw std::runtime_error("unknown option " + arg);
     }
     // The schedule (densify window, SH degree interval) scales with the iterations, as
@@ -170,6 +182,12 @@ int main(int argc, char** argv) {
       gs::InitStats st;
       init = gs::initialize_gaussians(dataset, io, &st);
       std::printf("initial gaussians from %s: %zu points -> %u\n", st.source.c_str(), st.raw_points, init.count);
+      // The head region from the subject's points (masked captures with a point cloud).
+      if (options.masked && dataset.has_masks && st.source != "random") options.head = gs::estimate_head(dataset, init);
+      if (options.head.found)
+        std::printf("head region: centre %.2f %.2f %.2f, radius %.2f (subject %.2f tall), weight %.1f\n",
+                    options.head.center[0], options.head.center[1], options.head.center[2], options.head.radius,
+                    options.head.subject_height, options.head_weight);
     }
     std::printf("dataset %s: %zu views (%zu held out), camera extent %.3f; %u initial gaussians (%.1f s)\n",
                 source.c_str(), dataset.frames.size(), dataset.holdout_count(), dataset.camera_extent, init.count,
@@ -187,14 +205,41 @@ int main(int argc, char** argv) {
       const gs::TrainStats& s = trainer.stats();
       std::printf("step %5u  l1 %.4f  psnr %5.2f  gaussians %7u (+%u -%u)  pairs %9llu  sh %d  %.2f ms/step\n", s.step,
                   s.l1, s.psnr, s.gaussians, s.spawned, s.pruned, (unsigned long long)s.pairs, s.sh_degree, s.step_ms);
+      if (options.refine_poses)
+        std::printf("  poses: shift %.4f (max %.4f), turn %.3f deg (max %.3f) over %u updates\n", s.pose_shift_mean,
+                    s.pose_shift_max, s.pose_turn_mean, s.pose_turn_max, s.pose_updates);
+      if (options.refine_exposure)
+        std::printf("  exposure: luminance gain %.3f..%.3f, tint spread %.4f over %u updates\n", s.exposure_low,
+                    s.exposure_high, s.exposure_tint, s.exposure_updates);
       const gs::EvalResult e = trainer.evaluate();
-      std::printf("  eval: held-out PSNR %.2f dB, SSIM %.4f over %u views\n", e.psnr, e.ssim, e.views);
+      std::printf("  eval: held-out PSNR %.2f dB, SSIM %.4f over %u views", e.psnr, e.ssim, e.views);
+      if (e.aligned) std::printf(" (%.2f dB at the poses as given)", e.psnr_unaligned);
+      if (e.head_views) std::printf("; head %.2f dB over %u views", e.head_psnr, e.head_views);
+      std::printf("\n");
       evals.push_back({s.step, e.psnr});
     }
     const gs::TrainStats& s = trainer.stats();
     const double views_per_s = double(s.views) / train_s;
     std::printf("trained %u steps, %llu views in %.1f s: %.1f views/s; tuning %s\n", s.step,
                 (unsigned long long)s.views, train_s, views_per_s, trainer.reduction().c_str());
+    if (!pose_out.empty()) {
+      // Every frame's camera-to-world (OpenGL axes, row-major) after refinement.
+      std::ofstream poses(pose_out);
+      poses.precision(9);
+      poses << "{\"frames\": [";
+      const gs::Dataset& d = trainer.dataset();
+      for (size_t f = 0; f < d.frames.size(); ++f) {
+        const gs::Camera c = trainer.camera_for(f);
+        poses << (f ? "," : "") << "\n{\"file_path\": \"" << d.frames[f].name
+              << "\", \"holdout\": " << (d.frames[f].holdout ? "true" : "false") << ", \"transform_matrix\": [";
+        // Columns R^T e0, -R^T e1, -R^T e2 (OpenCV to OpenGL axes) and the centre.
+        for (int r = 0; r < 3; ++r)
+          poses << (r ? "," : "") << "[" << c.rotation[r] << "," << -c.rotation[3 + r] << ","
+                << -c.rotation[6 + r] << "," << c.position[r] << "]";
+        poses << ",[0,0,0,1]]}";
+      }
+      poses << "\n]}\n";
+    }
     gs::SplatScene out = trainer.export_scene();
     gs::convert_convention(out, gs::AxisConvention::RDF);  // what .ply readers expect
     gs::write_file(out_path, gs::save_ply(out));

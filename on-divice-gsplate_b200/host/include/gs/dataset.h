@@ -74,6 +74,19 @@ struct InitStats {
 // robust extent), identity rotations and `initial_opacity`.
 SplatScene initialize_gaussians(const Dataset& dataset, const InitOptions& options, InitStats* stats = nullptr);
 
+// Where a standing person's head is, from points on them (estimate_head,
+// dataset.cpp:252-289): the top 13% of their extent along world up, a sphere of a tenth of
+// that extent around the slab's median, 8.5% of the extent below the top. Not found for
+// fewer than 200 points, subjects under 1 unit tall or fewer than 20 points in the slab.
+struct HeadRegion {
+  bool found = false;
+  float center[3] = {0, 0, 0};
+  float radius = 0;
+  float subject_height = 0;  // extent of the points along world up
+};
+HeadRegion estimate_head(const Dataset& dataset, const SplatScene& subject);
+HeadRegion estimate_head(const SplatScene& subject, const float up[3]);
+
 // Pinhole camera (scene -> camera, OpenCV convention) for a frame, at the frame's own
 // resolution when it has one.
 Camera dataset_camera(const Dataset& dataset, const DatasetFrame& frame);

@@ -8,12 +8,19 @@
 // backgrounds, learning-rate, SH-degree and loss-weight schedules, densification and
 // opacity-reset schedules, statistics, evaluation and export.
 //
+// Camera pose refinement, exposure refinement and head weighting follow the reference
+// (trainer.cpp:1164-1394, 1691-1771; trainer.h:60-131): pose corrections per training
+// view by Adam on the pose gradient the step sums on the GPU, held-out views aligned
+// before evaluation, per-view colour gains fitted from the forward pass's sums, and the
+// head region's pixels weighted in the loss.
+//
 // Extensions: `views_per_step` > 1 renders and differentiates that many views in one
 // launch per pass and takes one Adam step on their summed gradients (batched training;
-// a step still counts one iteration), and the retune steps run gs_autotune, which picks
-// pixels per thread, the backward batch and the sort digit width.
-// Not supported on this path: pose, motion and exposure refinement and head weighting
-// (the constructor throws when they are asked for).
+// a step still counts one iteration; each view still gets its own pose gradient and gain
+// fit), and the retune steps run gs_autotune, which picks pixels per thread, the backward
+// batch and the sort digit width.
+// Not supported on this path: subject-motion refinement (the constructor throws when it
+// is asked for).
 #pragma once
 
 #include <array>
@@ -29,6 +36,7 @@
 
 struct gs_context;
 struct gs_frame_data;
+struct gs_step_result;
 
 namespace gs {
 
@@ -55,10 +63,27 @@ struct TrainOptions {
   float lr_sh_rest = 2.5e-3f / 20.0f;
   float lambda_dssim = 0.2f;     // loss (1 - lambda) L1 + lambda (1 - SSIM), lambda ramping
   float lambda_dssim_end = 1.0f;  // to this by the last step (< 0: no ramp)
-  float head_weight = 1.0f;       // not supported here: must stay 1
-  bool refine_poses = false;      // not supported here
+  // Pixels in the head region (estimate_head) weigh this much in the loss; views where the
+  // head covers much of the frame (radius >= a quarter of the height) are left at 1.
+  HeadRegion head;
+  float head_weight = 1.0f;
+  // Camera pose refinement (trainer.h:69-81): from step pose_from each training view's
+  // pose correction takes an Adam step on its pose gradient; held-out views are aligned
+  // with eval_pose_steps steps that move only their camera before evaluation.
+  bool refine_poses = false;
+  uint32_t pose_from = 300;
+  float lr_pose_shift = 1e-3f;    // per update, times the camera extent
+  float lr_pose_turn = 1e-3f;     // radians per update
+  float lr_pose_final = 1.0f;     // the rates decay exponentially to this fraction by the last step
+  uint32_t eval_pose_steps = 8;
+  float eval_pose_step = 0.005f;  // the alignment's first step, times the camera extent
   bool refine_motion = false;     // not supported here
-  bool refine_exposure = false;   // not supported here
+  // Exposure refinement (trainer.h:121-131): per-view colour gains fitted from the
+  // forward pass's sums, blended in at exposure_rate from step exposure_from, used
+  // divided by their geometric mean over the trained views.
+  bool refine_exposure = false;
+  uint32_t exposure_from = 300;
+  float exposure_rate = 0.3f;
   bool sparse_adam = false;       // gaussians that drew nothing in a step keep their values and moments
   uint32_t densify_from = 300;
   uint32_t densify_until = 2000;
@@ -111,6 +136,11 @@ struct TrainStats {
   uint32_t tile_mismatch = 0;   // gaussians whose emitted tiles differed from the count (0)
   uint32_t overflow_steps = 0;  // steps whose pairs did not fit (their update was skipped)
   uint64_t views = 0;           // training views processed
+  double pose_shift_mean = 0.0, pose_shift_max = 0.0;  // dataset units
+  double pose_turn_mean = 0.0, pose_turn_max = 0.0;    // degrees
+  uint32_t pose_updates = 0;
+  double exposure_low = 1.0, exposure_high = 1.0, exposure_tint = 0.0;  // 5th/95th percentile luminance gain
+  uint32_t exposure_updates = 0;
   struct Timing {
     double wall_ms = 0.0;  // moving averages per step
     double gpu_ms = 0.0;
@@ -124,9 +154,9 @@ struct RetuneResult {
 };
 
 struct EvalResult {
-  double psnr = 0.0;  // mean over the held-out views
+  double psnr = 0.0;  // mean over the held-out views (aligned first when refining poses)
   bool aligned = false;
-  double psnr_unaligned = 0.0;
+  double psnr_unaligned = 0.0;  // at the poses as given, when aligned
   double ssim = 0.0;
   double head_psnr = 0.0;
   uint32_t head_views = 0;
@@ -159,7 +189,11 @@ class Trainer {
   // Held-out views over a black background.
   EvalResult evaluate();
   std::vector<uint8_t> render_view(size_t frame, const float background[3]);
+  // A view's camera with its pose correction (the dataset's pose without refinement).
   Camera camera_for(size_t frame) const;
+  // A view's exposure gains (the photo is divided by them): centred, interpolated for views
+  // not trained on, 1 without refine_exposure.
+  void view_gain(size_t frame, float gain[3]) const;
   // The alive gaussians, in the dataset's world.
   SplatScene export_scene();
 
@@ -171,6 +205,8 @@ class Trainer {
     std::vector<float> sh;      // sh_stride() per slot
   };
   Gradients first_step_gradients();
+  // The pose gradient of the latest pose update: dL/dd xyz, dL/dw xyz.
+  const double* last_pose_gradient() const { return last_pose_grad_; }
   struct DebugSnapshot {
     std::vector<uint32_t> pixel_count;
     std::vector<float> pixel_grad;
@@ -190,11 +226,34 @@ class Trainer {
   const std::vector<RetuneResult>& retunes() const { return retunes_; }
 
  private:
+  struct PoseFix {
+    float rotation[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // applied after the dataset's rotation (camera axes)
+    float shift[3] = {0, 0, 0};
+    double m[6] = {}, v[6] = {};  // Adam moments: shift xyz, turn xyz
+    uint32_t updates = 0;
+  };
+
   void next_view(size_t& frame, float background[3]);
   void run_step(const std::vector<size_t>& frames, const std::vector<std::array<float, 3>>& backgrounds,
                 bool profile);
   void write_frame(gs_frame_data& f, const Camera& camera, const float background[3], uint32_t step, bool ssim,
-                   bool masked) const;
+                   bool masked, uint32_t flags = 0u, const float* gain = nullptr) const;
+  // One held-out measurement (forward only) or alignment probe of `camera` against frame
+  // `frame`'s image over black.
+  void run_eval_view(const Camera& camera, size_t frame, const float gain[3], uint32_t flags, gs_step_result& r);
+  bool refines_pose_at(uint32_t step) const { return options_.refine_poses && step >= options_.pose_from; }
+  bool refines_exposure_at(uint32_t step) const {
+    return options_.refine_exposure && step >= options_.exposure_from;
+  }
+  void update_pose(const double grad[6], size_t frame);
+  static void apply_pose_step(PoseFix& fix, const double step[6]);
+  static Camera with_fix(Camera camera, const PoseFix& fix);  // [R | t] -> [E R | E t + d]
+  PoseFix align_camera(const Camera& camera, size_t frame, const float gain[3], const PoseFix* start);
+  PoseFix neighbour_fix(size_t frame) const;
+  void update_pose_stats();
+  void update_exposure(const double fit[8], size_t frame);
+  std::array<float, 3> exposure_gain(size_t frame) const;
+  void update_exposure_stats();
   uint32_t sh_degree_at(uint32_t step) const;
   double lambda_at(uint32_t step) const;
   bool uses_ssim() const;
@@ -217,6 +276,12 @@ class Trainer {
   PassTimes profile_;
   std::vector<RetuneResult> retunes_;
   std::vector<uint8_t> frame_bytes_;  // the last step's first FrameData (densify thresholds)
+  static constexpr size_t kNone = ~size_t(0);
+  std::vector<size_t> train_before_, train_after_;  // each frame's nearest training frames in capture order
+  std::vector<PoseFix> pose_fix_;                    // per dataset frame
+  double last_pose_grad_[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<std::array<double, 3>> gain_log_;  // per frame: log gain per channel, as measured (blended)
+  std::vector<uint32_t> gain_updates_;
 };
 
 }  // namespace gs

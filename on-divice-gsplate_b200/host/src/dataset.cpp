@@ -39,6 +39,47 @@ void compute_camera_bounds(Dataset& ds) {
   ds.camera_extent = std::max(1.1f * max_dist, 1e-3f);
 }
 
+HeadRegion estimate_head(const Dataset& dataset, const SplatScene& subject) {
+  return estimate_head(subject, dataset.world_up);
+}
+
+HeadRegion estimate_head(const SplatScene& subject, const float up[3]) {
+  HeadRegion head;
+  const size_t n = subject.count;
+  if (n < 200) return head;
+  // Heights along world up; the extent ignores the lowest 1% and the highest 0.5%.
+  std::vector<float> h(n);
+  for (size_t i = 0; i < n; ++i) {
+    const float* p = &subject.positions[i * 3];
+    h[i] = up[0] * p[0] + up[1] * p[1] + up[2] * p[2];
+  }
+  std::vector<float> order(h);
+  std::sort(order.begin(), order.end());
+  const float bottom = order[n / 100], top = order[n - 1 - n / 200];
+  const float extent = top - bottom;
+  if (!(extent >= 1.0f)) return head;  // not a standing person (or not in metres)
+  // The head slab: the top 13% of the extent. Its points projected off the up axis.
+  const float slab = top - 0.13f * extent;
+  std::vector<float> across[3];
+  for (size_t i = 0; i < n; ++i) {
+    if (h[i] < slab || h[i] > top) continue;
+    for (int k = 0; k < 3; ++k) across[k].push_back(subject.positions[i * 3 + k] - h[i] * up[k]);
+  }
+  if (across[0].size() < 20) return head;
+  // Per axis the median across the slab, at 8.5% of the extent below the top (below the
+  // slab's middle: hair raises the top).
+  const float level = top - 0.085f * extent;
+  for (int k = 0; k < 3; ++k) {
+    std::vector<float>& a = across[k];
+    std::nth_element(a.begin(), a.begin() + a.size() / 2, a.end());
+    head.center[k] = a[a.size() / 2] + level * up[k];
+  }
+  head.radius = 0.1f * extent;
+  head.subject_height = extent;
+  head.found = true;
+  return head;
+}
+
 Camera dataset_camera(const Dataset& ds, const DatasetFrame& f) {
   if (f.width != 0) return camera_from_c2w_gl(f.c2w, f.fx, f.fy, f.cx, f.cy, f.width, f.height);
   return camera_from_c2w_gl(f.c2w, ds.fx, ds.fy, ds.cx, ds.cy, ds.width, ds.height);

@@ -77,6 +77,24 @@ void frame_geometry(gs_frame_data& f, const Camera& camera, uint32_t slots, uint
   f.exposure[0] = f.exposure[1] = f.exposure[2] = 1.0f;
 }
 
+void frame_refinement(gs_frame_data& f, const Camera& camera, const HeadRegion& head, float head_weight,
+                      const float* gain) {
+  for (int c = 0; c < 3; ++c) f.exposure[c] = gain != nullptr && gain[c] > 0.0f ? 1.0f / gain[c] : 1.0f;
+  f.head[0] = f.head[1] = f.head[2] = 0.0f;
+  f.head[3] = 1.0f;
+  if (!head.found) return;
+  float t[3];
+  for (int r = 0; r < 3; ++r)
+    t[r] = camera.rotation[r * 3] * head.center[0] + camera.rotation[r * 3 + 1] * head.center[1] +
+           camera.rotation[r * 3 + 2] * head.center[2] + camera.translation[r];
+  if (!(t[2] > 0.05f)) return;  // behind (or at) the camera
+  f.head[0] = camera.fx * t[0] / t[2] + camera.cx;
+  f.head[1] = camera.fy * t[1] / t[2] + camera.cy;
+  f.head[2] = camera.fx * head.radius / t[2];
+  // Close-ups (the head's radius a quarter of the height or more) keep weight 1.
+  f.head[3] = f.head[2] < 0.25f * float(camera.height) ? head_weight : 1.0f;
+}
+
 void frame_schedule(gs_frame_data& f, const TrainOptions& o, uint32_t step, float camera_extent, float lambda) {
   constexpr float kBeta1 = 0.9f, kBeta2 = 0.999f, kEpsilon = 1e-15f;  // trainer.cpp:68-70
   const float t = o.iterations > 0 ? std::min(1.0f, float(step) / float(o.iterations)) : 1.0f;

@@ -21,6 +21,12 @@ void frame_geometry(gs_frame_data& f, const Camera& camera, uint32_t slots, uint
 // bias corrections, densification thresholds and seed, loss weight and SSIM constants.
 void frame_schedule(gs_frame_data& f, const TrainOptions& options, uint32_t step, float camera_extent, float lambda);
 
+// The exposure and head words of FrameData (write_frame, trainer.cpp:444, 531-544): the
+// photo is divided by `gain` (null: 1); a head region in front of the camera gives its
+// projected centre and radius, weighted head_weight unless it fills much of the view.
+void frame_refinement(gs_frame_data& f, const Camera& camera, const HeadRegion& head, float head_weight,
+                      const float* gain);
+
 // The scene in libgs_cuda's layout (the Trainer constructor's upload, trainer.cpp:388-417):
 // 16 floats per slot (position + opacity logit, log scale + alive flag, quaternion, DC)
 // and sh_stride floats of SH beyond DC, the scene's coefficients up to `degree`.

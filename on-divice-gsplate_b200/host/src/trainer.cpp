@@ -2,7 +2,8 @@
 // (next_view, :911-924), FrameData (write_frame, :440-547), statistics (read_slot /
 // set_view_stats, :778-805), the densify and opacity-reset schedule (after_step,
 // :932-945; densify, :1083-1119; reset_opacity, :1121-1128), evaluation (evaluate_views,
-// :1244-1292) and export (export_scene, :1773-1800).
+// :1244-1292) and export (export_scene, :1773-1800). Pose and exposure refinement are in
+// refine.cpp.
 #include "gs/trainer.h"
 
 #include <algorithm>
@@ -54,9 +55,8 @@ void Trainer::check(int code, const char* what) const { detail::check_status(cod
 Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, const TrainOptions& options)
     : ctx_(ctx), dataset_(std::move(dataset)), options_(options), rng_(options.seed) {
   if (dataset_.frames.empty() || dataset_.width == 0) throw std::runtime_error("Trainer: empty dataset");
-  if (options_.refine_poses || options_.refine_motion || options_.refine_exposure || options_.head_weight != 1.0f)
-    throw std::runtime_error("Trainer: pose, motion and exposure refinement and head weighting are not available "
-                             "on the CUDA path");
+  if (options_.refine_motion)
+    throw std::runtime_error("Trainer: subject-motion refinement is not available on the CUDA path");
   if (options_.views_per_step < 1 || options_.views_per_step > GS_MAX_VIEWS)
     throw std::runtime_error("Trainer: views_per_step must be 1.." + std::to_string(GS_MAX_VIEWS));
   if (options_.sh_degree < 0 || options_.sh_degree > 3) throw std::runtime_error("Trainer: sh_degree must be 0..3");
@@ -68,6 +68,21 @@ Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, c
     if (!f.holdout) train_frames_.push_back(i);
   }
   if (train_frames_.empty()) throw std::runtime_error("Trainer: no training frames");
+  // Each frame's nearest training frames in capture order (trainer.cpp:314-329).
+  const size_t nf = dataset_.frames.size();
+  train_before_.assign(nf, kNone);
+  train_after_.assign(nf, kNone);
+  for (size_t f = 0, last = kNone; f < nf; ++f) {
+    train_before_[f] = last;
+    if (!dataset_.frames[f].holdout) last = f;
+  }
+  for (size_t f = nf, last = kNone; f-- > 0;) {
+    train_after_[f] = last;
+    if (!dataset_.frames[f].holdout) last = f;
+  }
+  pose_fix_.assign(nf, PoseFix{});
+  gain_log_.assign(nf, {0.0, 0.0, 0.0});
+  gain_updates_.assign(nf, 0u);
   sh_stride_ = uint32_t(sh_rest_coeffs(options_.sh_degree) * 3);
   capacity_ = std::max(std::max(options_.max_gaussians, initial.count), 1u);
 
@@ -123,11 +138,12 @@ double Trainer::lambda_at(uint32_t step) const {
 bool Trainer::uses_ssim() const { return options_.lambda_dssim > 0.0f || options_.lambda_dssim_end > 0.0f; }
 
 void Trainer::write_frame(gs_frame_data& f, const Camera& camera, const float background[3], uint32_t step,
-                          bool ssim, bool masked) const {
-  const uint32_t flags = (masked ? GS_FLAG_MASKED_TARGET : 0u) | (ssim ? GS_FLAG_SSIM : 0u) |
-                         (options_.sparse_adam ? GS_FLAG_SPARSE_ADAM : 0u);
+                          bool ssim, bool masked, uint32_t flags, const float* gain) const {
+  flags |= (masked ? GS_FLAG_MASKED_TARGET : 0u) | (ssim ? GS_FLAG_SSIM : 0u) |
+           (options_.sparse_adam ? GS_FLAG_SPARSE_ADAM : 0u);
   detail::frame_geometry(f, camera, stats_.slots, sh_stride_, int(sh_degree_at(step)), flags, background);
   detail::frame_schedule(f, options_, step, dataset_.camera_extent, float(lambda_at(step)));
+  detail::frame_refinement(f, camera, options_.head, options_.head_weight, gain);
 }
 
 void Trainer::next_view(size_t& frame, float background[3]) {
@@ -167,9 +183,12 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   std::vector<gs_frame_data> fd(k);
   std::vector<uint32_t> images(k);
   std::vector<Camera> cams(k);
+  const bool pose = refines_pose_at(step), exposure = refines_exposure_at(step);
   for (uint32_t v = 0; v < k; ++v) {
     cams[v] = camera_for(frames[v]);
-    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked);
+    const std::array<float, 3> gain = exposure_gain(frames[v]);
+    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked, pose ? GS_FLAG_POSE_GRAD : 0u,
+                gain.data());
     images[v] = uint32_t(frames[v]);
   }
   check(gs_set_views_dataset(gpu_, k, fd.data(), images.data()), "Trainer::step: gs_set_views_dataset");
@@ -180,6 +199,15 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   }
   gs_step_result r;
   check(gs_step(gpu_, GS_STEP_TRAIN | (profile ? GS_STEP_PROFILE : 0u), &r), "Trainer::step: gs_step");
+  // A step whose pairs did not fit left the model alone: no pose or gain update either.
+  if (!r.overflow) {
+    for (uint32_t v = 0; v < k; ++v) {
+      if (pose) update_pose(r.pose_grad[v], frames[v]);
+      if (exposure) update_exposure(r.fit[v], frames[v]);
+    }
+    if (pose) update_pose_stats();
+    if (exposure) update_exposure_stats();
+  }
   // Statistics: the views' sums (read_slot / set_view_stats), averaged over the views.
   const double lambda = lambda_at(step);
   ViewLosses mean;
@@ -273,7 +301,6 @@ void Trainer::reset_opacity() {
   check(gs_reset_opacity(gpu_, max_logit), "Trainer::reset_opacity");
 }
 
-Camera Trainer::camera_for(size_t frame) const { return dataset_camera(dataset_, dataset_.frames.at(frame)); }
 
 std::vector<uint8_t> Trainer::render(const Camera& camera, const float background[3]) {
   gs_frame_data f;
@@ -287,31 +314,64 @@ std::vector<uint8_t> Trainer::render_view(size_t frame, const float background[3
   return render(camera_for(frame), background);
 }
 
-EvalResult Trainer::evaluate() {
-  EvalResult result;
+void Trainer::run_eval_view(const Camera& camera, size_t frame, const float gain[3], uint32_t flags,
+                            gs_step_result& r) {
+  // A measurement renders forward only with SSIM; an alignment probe trains with only the
+  // camera moving (pose gradient, the model untouched) on L1 (trainer.cpp:1180-1183, 1250).
   const float black[3] = {0.0f, 0.0f, 0.0f};
-  const bool ssim = uses_ssim();
-  double sums[3] = {0, 0, 0};
-  for (size_t i = 0; i < dataset_.frames.size(); ++i) {
-    if (!dataset_.frames[i].holdout) continue;
-    const Camera cam = camera_for(i);
-    gs_frame_data f;
-    write_frame(f, cam, black, stats_.step, ssim, options_.masked);
-    const uint32_t image = uint32_t(i);
-    check(gs_set_views_dataset(gpu_, 1, &f, &image), "Trainer::evaluate: gs_set_views_dataset");
+  const bool align = (flags & GS_FLAG_POSE_ONLY) != 0u;
+  gs_frame_data f;
+  write_frame(f, camera, black, stats_.step, !align, options_.masked, flags, gain);
+  const uint32_t image = uint32_t(frame);
+  check(gs_set_views_dataset(gpu_, 1, &f, &image), "Trainer::evaluate: gs_set_views_dataset");
+  check(gs_step(gpu_, align ? GS_STEP_TRAIN : 0u, &r), "Trainer::evaluate: gs_step");
+}
+
+EvalResult Trainer::evaluate() {
+  // evaluate_views (trainer.cpp:1244-1292) on this trainer's own dataset.
+  EvalResult result;
+  const bool align = options_.refine_poses && options_.eval_pose_steps > 0;
+  double sums[5] = {0, 0, 0, 0, 0}, unaligned = 0.0;
+  auto measure = [&](const Camera& cam, size_t i, const float gain[3], double* psnr_out) {
     gs_step_result r;
-    check(gs_step(gpu_, 0u, &r), "Trainer::evaluate: gs_step");
-    const ViewLosses l = view_losses(r.losses[0], cam.width, cam.height, lambda_at(stats_.step), ssim);
+    run_eval_view(cam, i, gain, 0u, r);
+    const ViewLosses l = view_losses(r.losses[0], cam.width, cam.height, lambda_at(stats_.step), true);
+    if (psnr_out) {
+      *psnr_out += l.psnr;
+      return;
+    }
     sums[0] += l.psnr;
     sums[1] += l.l1;
     sums[2] += l.ssim;
+    if (r.losses[0][7] > 0.0) {  // the head region's pixels
+      sums[3] += -10.0 * std::log10(std::max(r.losses[0][6] / (3.0 * r.losses[0][7]), 1e-12));
+      sums[4] += 1.0;
+    }
+  };
+  for (size_t i = 0; i < dataset_.frames.size(); ++i) {
+    if (!dataset_.frames[i].holdout) continue;
+    float gain[3];
+    view_gain(i, gain);
+    const Camera given = dataset_camera(dataset_, dataset_.frames[i]);
+    PoseFix fix{};
+    if (align) {
+      measure(given, i, gain, &unaligned);
+      // A view aligned before starts where it got to; otherwise between its neighbours.
+      const PoseFix start = pose_fix_[i].updates > 0 ? pose_fix_[i] : neighbour_fix(i);
+      fix = align_camera(given, i, gain, &start);
+      pose_fix_[i] = fix;
+    }
+    measure(with_fix(given, fix), i, gain, nullptr);
     ++result.views;
   }
   if (result.views > 0) {
     result.psnr = sums[0] / result.views;
     result.l1 = sums[1] / result.views;
     result.ssim = sums[2] / result.views;
-    result.psnr_unaligned = result.psnr;
+    result.head_views = uint32_t(sums[4]);
+    result.head_psnr = sums[4] > 0.0 ? sums[3] / sums[4] : 0.0;
+    result.aligned = align;
+    result.psnr_unaligned = align ? unaligned / result.views : result.psnr;
   }
   return result;
 }

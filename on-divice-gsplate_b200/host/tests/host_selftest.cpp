@@ -6,6 +6,10 @@
 //   gs_host_selftest dataset <dir> <width> <max_init>
 //                                  load_dataset + initialize_gaussians: a JSON summary on
 //                                  stdout, frame 0's RGBA in <dir>/frame0.rgba
+//   gs_host_selftest head <xyz> <ux> <uy> <uz> <weight>
+//                                  estimate_head over the float32 xyz triples in <xyz> with
+//                                  world up (ux, uy, uz), then the head and exposure words of
+//                                  a FrameData for the test camera with gains (0.8, 1, 1.25)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -197,6 +201,24 @@ int dataset_summary(const std::string& dir, uint32_t width, uint32_t max_init) {
   return 0;
 }
 
+int head_summary(const std::string& path, const float up[3], float weight) {
+  const std::vector<uint8_t> bytes = gs::read_file(path);
+  gs::SplatScene s;
+  s.resize(uint32_t(bytes.size() / 12), 0);
+  std::memcpy(s.positions.data(), bytes.data(), size_t(s.count) * 12);
+  const gs::HeadRegion h = gs::estimate_head(s, up);
+  gs_frame_data f;
+  const float bg[3] = {0.0f, 0.0f, 0.0f}, gain[3] = {0.8f, 1.0f, 1.25f};
+  const gs::Camera cam = test_camera();
+  gs::detail::frame_geometry(f, cam, s.count, 0, 0, 0u, bg);
+  gs::detail::frame_refinement(f, cam, h, weight, gain);
+  std::printf("{\"found\": %s, \"center\": [%.9g, %.9g, %.9g], \"radius\": %.9g, \"height\": %.9g, "
+              "\"frame_head\": [%.9g, %.9g, %.9g, %.9g], \"frame_exposure\": [%.9g, %.9g, %.9g]}\n",
+              h.found ? "true" : "false", h.center[0], h.center[1], h.center[2], h.radius, h.subject_height,
+              f.head[0], f.head[1], f.head[2], f.head[3], f.exposure[0], f.exposure[1], f.exposure[2]);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -206,6 +228,10 @@ int main(int argc, char** argv) {
     if (mode == "frame") return frame_words();
     if (mode == "camera") return camera_floats();
     if (mode == "dataset" && argc > 4) return dataset_summary(argv[2], uint32_t(std::atoi(argv[3])), uint32_t(std::atoi(argv[4])));
+    if (mode == "head" && argc > 6) {
+      const float up[3] = {float(std::atof(argv[3])), float(std::atof(argv[4])), float(std::atof(argv[5]))};
+      return head_summary(argv[2], up, float(std::atof(argv[6])));
+    }
     std::fprintf(stderr, "usage: %s scene <dir> | frame | camera\n", argv[0]);
     return 2;
   } catch (const std::exception& e) {

@@ -1,0 +1,318 @@
+// GPU checks of gs::Trainer's pose and exposure refinement, driven by tests/test_gpu_host.py.
+// They follow the reference's own tests of these features (engine/tests/test_trainer.cpp:
+// test_pose_gradient :404-460, test_pose_recovery :505-547, test_exposure_recovery
+// :700-742), plus the held-out alignment of evaluate (trainer.cpp:1164-1212, 1244-1292):
+//   gs_refine_selftest pose-gradient <lambda>
+//   gs_refine_selftest pose-recovery
+//   gs_refine_selftest exposure-recovery
+//   gs_refine_selftest align
+// Each prints one JSON line with what it measured and exits 1 when its check fails.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gs/camera.h"
+#include "gs/dataset.h"
+#include "gs/splat_scene.h"
+#include "gs/trainer.h"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// The distributions of the reference's make_test_scene (train_selftest.cpp:314-332):
+// positions 0.7 U(-1, 1)^3, scales exp(log(0.08 + 0.06 U)), rotations U^4 with w + 1.5,
+// opacity logits 0.6 U - 0.2, DC 0.8 U, SH beyond DC 0.25 U.
+gs::SplatScene test_scene(uint32_t n, int degree, uint32_t seed) {
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+  gs::SplatScene s;
+  s.resize(n, degree);
+  const int rest = gs::sh_rest_coeffs(degree) * 3;
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) s.positions[i * 3 + k] = 0.7f * U(rng);
+    for (int k = 0; k < 3; ++k) s.log_scales[i * 3 + k] = std::log(0.08f + 0.06f * U(rng));
+    for (int k = 0; k < 4; ++k) s.rotations[i * 4 + k] = U(rng) + (k == 0 ? 1.5f : 0.0f);
+    s.opacity_logits[i] = 0.6f * U(rng) - 0.2f;
+    for (int k = 0; k < 3; ++k) s.sh_dc[i * 3 + k] = 0.8f * U(rng);
+    for (int k = 0; k < rest; ++k) s.sh_rest[size_t(i) * rest + k] = 0.25f * U(rng);
+  }
+  s.convention = gs::AxisConvention::RUB;
+  return s;
+}
+
+// The reference's make_test_dataset (train_selftest.cpp:285-312): `frames` cameras on an
+// orbit of radius 3 (height 0.6 + 0.3 sin 3a) looking at the origin, f = 0.9 width, noise
+// targets (alpha 255 without masks), every 8th frame held out, camera extent 3.3.
+gs::Dataset test_dataset(uint32_t w, uint32_t h, uint32_t frames, bool masks, uint32_t seed) {
+  gs::Dataset ds;
+  ds.name = "test";
+  ds.width = w;
+  ds.height = h;
+  ds.fx = ds.fy = 0.9f * float(w);
+  ds.cx = 0.5f * float(w);
+  ds.cy = 0.5f * float(h);
+  ds.has_masks = masks;
+  std::mt19937 rng(seed);
+  std::uniform_int_distribution<int> byte(0, 255);
+  for (uint32_t i = 0; i < frames; ++i) {
+    gs::DatasetFrame f;
+    f.name = "frame" + std::to_string(i);
+    const float a = 6.2831853f * float(i) / float(std::max(frames, 1u));
+    const float eye[3] = {3.0f * std::sin(a), 0.6f + 0.3f * std::sin(3.0f * a), 3.0f * std::cos(a)};
+    const float target[3] = {0.0f, 0.0f, 0.0f};
+    gs::look_at_c2w_gl(eye, target, f.c2w);
+    f.rgba.resize(size_t(w) * h * 4);
+    for (size_t p = 0; p < size_t(w) * h; ++p)
+      for (int c = 0; c < 4; ++c) f.rgba[p * 4 + c] = uint8_t(c == 3 && !masks ? 255 : byte(rng));
+    f.holdout = frames > 1 && i % 8 == 0;
+    ds.frames.push_back(std::move(f));
+  }
+  gs::compute_camera_bounds(ds);
+  ds.camera_extent = 3.3f;
+  return ds;
+}
+
+// All learning rates zero, no densification, no retuning (frozen_train_options,
+// train_selftest.cpp:334-346).
+gs::TrainOptions frozen_options(int degree, bool masked) {
+  gs::TrainOptions o;
+  o.iterations = 1;
+  o.max_gaussians = 0;
+  o.sh_degree = degree;
+  o.sh_degree_interval = 0;
+  o.masked = masked;
+  o.random_background = false;
+  o.lr_position = o.lr_position_final = o.lr_scale = o.lr_rotation = 0.0f;
+  o.lr_opacity = o.lr_sh_dc = o.lr_sh_rest = 0.0f;
+  o.densify_from = o.densify_until = 1000000;
+  o.opacity_reset_interval = 0;
+  o.autotune = false;
+  return o;
+}
+
+// Targets rendered from `scene` at the true cameras over black, alpha 255.
+void render_targets(gs::Dataset& ds, const gs::SplatScene& scene, const gs::TrainOptions& o) {
+  gs::CudaContext ctx;
+  gs::Trainer renderer(ctx, ds, scene, o);
+  const float black[3] = {0.0f, 0.0f, 0.0f};
+  for (gs::DatasetFrame& f : ds.frames) {
+    f.rgba = renderer.render(gs::dataset_camera(ds, f), black);
+    for (size_t p = 0; p < f.rgba.size() / 4; ++p) f.rgba[p * 4 + 3] = 255;
+  }
+}
+
+// Moves frame f's camera as a pose correction does: world -> camera [W | t] becomes
+// [E W | E t + d], E the rotation by the turn vector w (Rodrigues).
+void nudge_camera(gs::Dataset& ds, size_t f, const double d[3], const double w[3]) {
+  const gs::Camera cam = gs::dataset_camera(ds, ds.frames[f]);
+  const double t = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+  const double k[3] = {w[0] / t, w[1] / t, w[2] / t};
+  const double K[9] = {0, -k[2], k[1], k[2], 0, -k[0], -k[1], k[0], 0};
+  double E[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double k2 = 0.0;
+      for (int i = 0; i < 3; ++i) k2 += K[r * 3 + i] * K[i * 3 + c];
+      E[r * 3 + c] = (r == c ? 1.0 : 0.0) + std::sin(t) * K[r * 3 + c] + (1.0 - std::cos(t)) * k2;
+    }
+  double W[9], tr[3];
+  for (int r = 0; r < 3; ++r) {
+    tr[r] = d[r];
+    for (int c = 0; c < 3; ++c) {
+      W[r * 3 + c] = 0.0;
+      for (int i = 0; i < 3; ++i) W[r * 3 + c] += E[r * 3 + i] * cam.rotation[i * 3 + c];
+      tr[r] += E[r * 3 + c] * cam.translation[c];
+    }
+  }
+  // Back to an OpenGL camera-to-world: columns W^T e0, -W^T e1, -W^T e2 and the centre -W^T t.
+  float* m = ds.frames[f].c2w;
+  for (int r = 0; r < 3; ++r) {
+    m[r * 4 + 0] = float(W[0 * 3 + r]);
+    m[r * 4 + 1] = float(-W[1 * 3 + r]);
+    m[r * 4 + 2] = float(-W[2 * 3 + r]);
+    m[r * 4 + 3] = float(-(W[0 * 3 + r] * tr[0] + W[1 * 3 + r] * tr[1] + W[2 * 3 + r] * tr[2]));
+  }
+}
+
+// Distance between camera centres and the angle between their rotations (degrees).
+void camera_error(const gs::Camera& a, const gs::Camera& b, double* shift, double* turn) {
+  double d2 = 0.0, trace = 0.0;
+  for (int k = 0; k < 3; ++k) d2 += (double(a.position[k]) - b.position[k]) * (double(a.position[k]) - b.position[k]);
+  for (int i = 0; i < 9; ++i) trace += double(a.rotation[i]) * b.rotation[i];
+  *shift = std::sqrt(d2);
+  *turn = std::acos(std::clamp((trace - 1.0) / 2.0, -1.0, 1.0)) * 180.0 / kPi;
+}
+
+int pose_gradient(double lambda) {
+  gs::Dataset ds = test_dataset(64, 48, 2, true, 3);
+  const gs::SplatScene scene = test_scene(120, 0, 9);
+  const float bg[3] = {0.2f, 0.3f, 0.4f};
+  gs::TrainOptions o = frozen_options(0, true);
+  o.lambda_dssim = o.lambda_dssim_end = float(lambda);
+  o.refine_poses = true;
+  o.pose_from = 0;
+  o.lr_pose_shift = o.lr_pose_turn = 0.0f;  // measure only
+  gs::CudaContext ctx;
+  const gs::Camera cam = gs::dataset_camera(ds, ds.frames[0]);
+  gs::Trainer t(ctx, ds, scene, o);
+  t.step_on(0, bg);
+  const double* g = t.last_pose_gradient();
+  const gs::Trainer::Gradients grads = t.first_step_gradients();
+  double sum_d[3] = {0, 0, 0}, sum_w[3] = {0, 0, 0};
+  for (uint32_t i = 0; i < scene.count; ++i) {
+    const float* gp = &grads.params[size_t(i) * 16];
+    double rel[3];
+    for (int k = 0; k < 3; ++k) {
+      sum_d[k] += gp[k];
+      rel[k] = double(scene.positions[i * 3 + k]) - cam.position[k];
+    }
+    sum_w[0] += rel[1] * gp[2] - rel[2] * gp[1];
+    sum_w[1] += rel[2] * gp[0] - rel[0] * gp[2];
+    sum_w[2] += rel[0] * gp[1] - rel[1] * gp[0];
+    // The orientation turning by phi: q -> (1, phi / 2) q, so with q = (w, u) normalised and
+    // g the quaternion gradient's tangent part times |q|: dL/dphi = (-g_w u + w g_u + u x g_u) / 2.
+    const float* q = &scene.rotations[i * 4];
+    const double len = std::sqrt(double(q[0]) * q[0] + double(q[1]) * q[1] + double(q[2]) * q[2] + double(q[3]) * q[3]);
+    const double w = q[0] / len, u[3] = {q[1] / len, q[2] / len, q[3] / len};
+    const double gw = gp[8] * len, gu[3] = {gp[9] * len, gp[10] * len, gp[11] * len};
+    const double ug[3] = {u[1] * gu[2] - u[2] * gu[1], u[2] * gu[0] - u[0] * gu[2], u[0] * gu[1] - u[1] * gu[0]};
+    for (int k = 0; k < 3; ++k) sum_w[k] += 0.5 * (-gw * u[k] + w * gu[k] + ug[k]);
+  }
+  double expected[6], worst = 0.0, largest = 0.0;
+  for (int r = 0; r < 3; ++r) {
+    expected[r] = expected[3 + r] = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      expected[r] += cam.rotation[r * 3 + c] * sum_d[c];
+      expected[3 + r] += cam.rotation[r * 3 + c] * sum_w[c];
+    }
+  }
+  std::printf("{\"lambda\": %.2f, \"pose_gradient\": [", lambda);
+  for (int k = 0; k < 6; ++k) {
+    std::printf("%s%.6g", k ? ", " : "", g[k]);
+    worst = std::max(worst, std::fabs(g[k] - expected[k]));
+    largest = std::max(largest, std::fabs(expected[k]));
+  }
+  std::printf("], \"expected\": [");
+  for (int k = 0; k < 6; ++k) std::printf("%s%.6g", k ? ", " : "", expected[k]);
+  std::printf("], \"worst\": %.4g, \"largest\": %.4g}\n", worst, largest);
+  return largest > 0.0 && worst <= 1e-3 * largest ? 0 : 1;
+}
+
+int pose_recovery() {
+  // Targets rendered at the true cameras; frame 1's camera then moved 10 cm and 1.5 degrees
+  // (3 m away: about 2 px each at 128 px). With the gaussians frozen, refining that view's
+  // pose must bring it back.
+  constexpr uint32_t w = 128, h = 96;
+  gs::Dataset ds = test_dataset(w, h, 2, false, 3);
+  const gs::SplatScene scene = test_scene(300, 0, 9);
+  gs::TrainOptions o = frozen_options(0, false);
+  render_targets(ds, scene, o);
+  const gs::Camera truth = gs::dataset_camera(ds, ds.frames[1]);
+  gs::Dataset moved = ds;
+  const double d[3] = {0.07, -0.05, 0.05}, rot[3] = {0.012, 0.02, -0.01};
+  nudge_camera(moved, 1, d, rot);
+  const gs::Camera given = gs::dataset_camera(moved, moved.frames[1]);
+  o.iterations = 200;
+  o.refine_poses = true;
+  o.pose_from = 0;
+  o.lr_pose_shift = 2e-3f;
+  o.lr_pose_turn = 2e-3f;
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, moved, scene, o);
+  const float black[3] = {0.0f, 0.0f, 0.0f};
+  for (int s = 0; s < 150; ++s) t.step_on(1, black);
+  double shift0, turn0, shift1, turn1;
+  camera_error(given, truth, &shift0, &turn0);
+  camera_error(t.camera_for(1), truth, &shift1, &turn1);
+  const gs::TrainStats& st = t.stats();
+  std::printf("{\"shift_before\": %.5f, \"turn_before\": %.4f, \"shift_after\": %.5f, \"turn_after\": %.4f, "
+              "\"pose_updates\": %u, \"pose_shift_mean\": %.5f, \"pose_turn_mean\": %.4f}\n",
+              shift0, turn0, shift1, turn1, st.pose_updates, st.pose_shift_mean, st.pose_turn_mean);
+  return shift1 < 0.25 * shift0 && turn1 < 0.25 * turn0 && st.pose_updates == 150 ? 0 : 1;
+}
+
+int exposure_recovery() {
+  // Views rendered from a scene, frame 1 darkened and tinted as a camera's exposure and
+  // white balance would; with the gaussians frozen, the trained views' gains must come
+  // out in that ratio, their geometric mean kept at 1.
+  constexpr uint32_t w = 128, h = 96;
+  gs::Dataset ds = test_dataset(w, h, 3, false, 3);  // frame 0 held out
+  const gs::SplatScene scene = test_scene(300, 0, 9);
+  const float dim[3] = {0.8f, 0.85f, 0.9f};
+  gs::TrainOptions o = frozen_options(0, false);
+  render_targets(ds, scene, o);
+  for (size_t p = 0; p < size_t(w) * h; ++p)
+    for (int c = 0; c < 3; ++c) {
+      uint8_t& v = ds.frames[1].rgba[p * 4 + c];
+      v = uint8_t(std::lround(v * dim[c]));
+    }
+  o.iterations = 100;
+  o.refine_exposure = true;
+  o.exposure_from = 0;
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  const float black[3] = {0.0f, 0.0f, 0.0f};
+  for (int s = 0; s < 30; ++s) t.step_on(1 + s % 2, black);
+  float g0[3], g1[3], g2[3];
+  t.view_gain(0, g0);  // held out, before every trained view: view 1's
+  t.view_gain(1, g1);
+  t.view_gain(2, g2);
+  double worst = 0.0;
+  for (int c = 0; c < 3; ++c) worst = std::max(worst, std::fabs(double(g1[c]) / g2[c] / dim[c] - 1.0));
+  const double centred = std::fabs(std::log(double(g1[1])) + std::log(double(g2[1])));
+  const gs::TrainStats& st = t.stats();
+  std::printf("{\"gain1\": [%.4f, %.4f, %.4f], \"gain2\": [%.4f, %.4f, %.4f], \"held_out\": [%.4f, %.4f, %.4f], "
+              "\"ratio_error\": %.5f, \"centred\": %.3g, \"updates\": %u, \"low\": %.4f, \"high\": %.4f}\n",
+              g1[0], g1[1], g1[2], g2[0], g2[1], g2[2], g0[0], g0[1], g0[2], worst, centred, st.exposure_updates,
+              st.exposure_low, st.exposure_high);
+  bool ok = worst < 0.02 && centred < 1e-4 && st.exposure_updates == 30;
+  for (int c = 0; c < 3; ++c) ok = ok && g0[c] == g1[c];
+  return ok ? 0 : 1;
+}
+
+int align() {
+  // A held-out view whose given pose is off by about 2 px: evaluate aligns it before
+  // measuring, so its PSNR must be above the unaligned one, and a second evaluation starts
+  // from where the first ended.
+  constexpr uint32_t w = 128, h = 96;
+  gs::Dataset ds = test_dataset(w, h, 9, false, 3);  // frames 0 and 8 held out
+  const gs::SplatScene scene = test_scene(300, 0, 9);
+  gs::TrainOptions o = frozen_options(0, false);
+  render_targets(ds, scene, o);
+  const double d[3] = {0.05, 0.03, -0.04}, rot[3] = {-0.01, 0.015, 0.008};
+  nudge_camera(ds, 0, d, rot);
+  o.iterations = 10;
+  o.refine_poses = true;
+  o.pose_from = 1000;  // no training view moves: only the evaluation's alignment
+  o.eval_pose_steps = 8;
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  const gs::EvalResult a = t.evaluate();
+  const gs::EvalResult b = t.evaluate();
+  std::printf("{\"views\": %u, \"aligned\": %d, \"psnr_unaligned\": %.3f, \"psnr\": %.3f, \"second_psnr\": %.3f}\n",
+              a.views, int(a.aligned), a.psnr_unaligned, a.psnr, b.psnr);
+  return a.views == 2 && a.aligned && a.psnr > a.psnr_unaligned + 0.5 && b.psnr > a.psnr_unaligned + 0.5 ? 0 : 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    const std::string mode = argc > 1 ? argv[1] : "";
+    if (mode == "pose-gradient" && argc > 2) return pose_gradient(std::atof(argv[2]));
+    if (mode == "pose-recovery") return pose_recovery();
+    if (mode == "exposure-recovery") return exposure_recovery();
+    if (mode == "align") return align();
+    std::fprintf(stderr, "usage: gs_refine_selftest pose-gradient <lambda> | pose-recovery | exposure-recovery | align\n");
+    return 2;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+}

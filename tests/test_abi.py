@@ -35,7 +35,28 @@ def test_struct_layouts_match_header():
     # gs_frame_data is FrameData (train_common.glsl:15-37): 18 vec4 = 288 bytes.
     assert FRAME_DTYPE.itemsize == 288
     assert ctypes.sizeof(cuda.Tuning) == 48
-    assert ctypes.sizeof(cuda.StepResult) == 16 + 8 * 16 + 8 * 8 * 16 + 4 + 4 + 24
+    assert ctypes.sizeof(cuda.StepResult) == 16 + 8 * 16 + 8 * 8 * 16 + 4 + 4 + 24 + 8 * 8 * 16 + 6 * 8 * 16
+
+
+def test_ctypes_offsets_match_the_c_compiler(tmp_path):
+    """Every field of the ctypes mirrors sits where gcc puts it in the header's structs."""
+    structs = {"gs_step_result": cuda.StepResult, "gs_tuning": cuda.Tuning, "gs_model_info": cuda.ModelInfo}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gs_cuda.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{cname}.{field} %zu\\n", offsetof({cname}, {field}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, cls in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert int(got[f"{cname}.{field}"]) == getattr(cls, field).offset, (cname, field)
 
 
 def test_no_device_call_errors_cleanly():

@@ -122,3 +122,52 @@ def test_gs_train_capture_folder(tmp_path):
     evals = [e["psnr"] for e in m["eval"]]
     assert evals[-1] > evals[0] + 1.0, r.stdout
     assert ply_vertices(out_ply) == m["gaussians"]
+
+
+def refine_selftest(*args):
+    r = subprocess.run([os.path.join(BIN, "gs_refine_selftest"), *args], capture_output=True, text=True, timeout=600)
+    return r.returncode, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("lam", ["0.0", "0.2"])
+def test_trainer_pose_gradient(lam):
+    """test_pose_gradient (test_trainer.cpp:404-460) through gs::Trainer: the pose gradient
+    of a step equals what its per-gaussian gradients imply, within 1e-3 of the largest."""
+    rc, out = refine_selftest("pose-gradient", lam)
+    assert rc == 0, out
+
+
+def test_trainer_pose_recovery():
+    """test_pose_recovery (test_trainer.cpp:505-547): a camera moved 10 cm and 1.5 degrees
+    comes back to within a quarter of that by refining its pose with frozen gaussians."""
+    rc, out = refine_selftest("pose-recovery")
+    assert rc == 0, out
+
+
+def test_trainer_exposure_recovery():
+    """test_exposure_recovery (test_trainer.cpp:700-742): gains of a darkened, tinted view
+    come out in the ratio it was dimmed by (2%), centred on the trained views."""
+    rc, out = refine_selftest("exposure-recovery")
+    assert rc == 0, out
+
+
+def test_trainer_aligns_held_out_views():
+    """evaluate with refine_poses: a held-out view given 2 px off is aligned before it is
+    measured (align_camera, trainer.cpp:1164-1212)."""
+    rc, out = refine_selftest("align")
+    assert rc == 0, out
+
+
+def test_gs_train_with_refinement(tmp_path):
+    """gs_train with pose and exposure refinement and a pose export runs and still learns."""
+    poses = tmp_path / "poses.json"
+    _, m, out = train(tmp_path, "refine", "--iters", "300", "--eval-every", "150", "--views-per-step", "4",
+                      "--refine-poses", "--pose-from", "50", "--refine-exposure", "--eval-pose-steps", "4",
+                      "--pose-out", str(poses))
+    assert "poses: shift" in out and "exposure: luminance gain" in out and "at the poses as given" in out
+    assert m["eval"][-1]["psnr"] > m["eval"][0]["psnr"]
+    frames = json.loads(poses.read_text())["frames"]
+    assert len(frames) == 24 and sum(f["holdout"] for f in frames) == 3
+    for f in frames:
+        M = np.array(f["transform_matrix"])
+        assert M.shape == (4, 4) and np.allclose(M[:3, :3] @ M[:3, :3].T, np.eye(3), atol=1e-4)

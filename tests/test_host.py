@@ -63,3 +63,77 @@ def test_frame_matches_python_mirror():
     integer[F._SEED_WORD] = True
     np.testing.assert_array_equal(words[integer], ref[integer])
     np.testing.assert_allclose(got[~integer], want[~integer], rtol=2e-6, atol=0)
+
+
+def head_region_numpy(p, up):
+    """estimate_head (dataset.cpp:252-289) restated in float32 numpy: the top 13% of the
+    extent along up (lowest 1% and highest 0.5% ignored), centre at the slab's per-axis
+    median off the up axis, 8.5% of the extent below the top; radius a tenth of the extent."""
+    n = len(p)
+    up = np.asarray(up, np.float32)
+    h = (p[:, 0] * up[0] + p[:, 1] * up[1]) + p[:, 2] * up[2]
+    s = np.sort(h)
+    lo, hi = s[n // 100], s[n - 1 - n // 200]
+    extent = np.float32(hi - lo)
+    if not extent >= 1.0:
+        return None
+    slab = np.float32(hi - np.float32(0.13) * extent)
+    sel = (h >= slab) & (h <= hi)
+    across = p[sel] - h[sel, None] * up[None, :]
+    level = np.float32(hi - np.float32(0.085) * extent)
+    center = np.array([np.sort(across[:, k])[sel.sum() // 2] + level * up[k] for k in range(3)], np.float32)
+    return center, np.float32(0.1) * extent, extent
+
+
+def standing_person(rng, n=6000):
+    """Points on a 1.75-tall figure: a body cylinder, a head sphere and a few strays."""
+    body = n * 4 // 5
+    a = rng.uniform(0, 2 * np.pi, body)
+    y = rng.uniform(0.0, 1.5, body)
+    pts = [np.stack([0.2 * np.cos(a) + 0.1, y, 0.2 * np.sin(a) - 0.05], 1)]
+    d = rng.normal(size=(n - body - 20, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pts.append(np.array([0.1, 1.62, -0.05]) + 0.12 * d)
+    pts.append(rng.uniform(-3, 3, (20, 3)))
+    return np.concatenate(pts).astype(np.float32)
+
+
+@pytest.mark.parametrize("axis", [1, 2])
+def test_head_region_matches_numpy_restatement(tmp_path, axis):
+    rng = np.random.default_rng(7)
+    p = standing_person(rng)
+    up = np.zeros(3, np.float32)
+    up[axis] = 1.0
+    if axis == 2:  # the same figure standing along z
+        p = p[:, [0, 2, 1]].copy()
+        p[:, 1] *= -1.0
+    f = tmp_path / "xyz.f32"
+    f.write_bytes(p.tobytes())
+    out = run("head", str(f), *[str(float(u)) for u in up], "3.0")
+    import json
+    got = json.loads(out)
+    want = head_region_numpy(p, up)
+    assert got["found"] and want is not None
+    np.testing.assert_allclose(got["center"], want[0], rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose([got["radius"], got["height"]], [want[1], want[2]], rtol=1e-6)
+    # The head lands on the figure's head sphere.
+    assert abs(got["center"][axis] - (1.62 - np.float32(0.0))) < 0.1
+    # FrameData words for the test camera (write_frame, trainer.cpp:531-544): the projected
+    # centre and radius, the weight (the head is small in a 640-tall view), 1 / gain.
+    cam = S.front_camera(360, 640, 500.0)
+    t = cam.rotation.reshape(3, 3).astype(np.float64) @ np.asarray(got["center"]) + cam.translation
+    want_head = [cam.fx * t[0] / t[2] + cam.cx, cam.fy * t[1] / t[2] + cam.cy, cam.fx * got["radius"] / t[2], 3.0]
+    np.testing.assert_allclose(got["frame_head"], want_head, rtol=1e-5)
+    np.testing.assert_allclose(got["frame_exposure"], [1 / 0.8, 1.0, 1 / 1.25], rtol=1e-7)
+
+
+def test_no_head_region_for_small_or_sparse_subjects(tmp_path):
+    rng = np.random.default_rng(8)
+    small = standing_person(rng) * np.float32(0.5)  # under 1 unit tall: a close-up
+    f = tmp_path / "xyz.f32"
+    f.write_bytes(small.tobytes())
+    import json
+    got = json.loads(run("head", str(f), "0", "1", "0", "3.0"))
+    assert not got["found"] and got["frame_head"] == [0, 0, 0, 1]
+    f.write_bytes(standing_person(rng)[:150].tobytes())  # under 200 points
+    assert not json.loads(run("head", str(f), "0", "1", "0", "3.0"))["found"]
