@@ -52,6 +52,14 @@ extern "C" {
 /* On the first view: the step computes gradients (pose_grad) but changes neither the
    model nor its densification statistics (train_step.glsl:92-100, 222). */
 #define GS_FLAG_POSE_ONLY 16u
+/* The gaussians follow the subject's motion in this view (the node motions set with
+   gs_set_view_motion; train_motion.glsl, train_common.glsl:55). */
+#define GS_FLAG_MOTION 32u
+/* Sum the loss gradient with respect to each node's motion in this view
+   (gs_motion_gradient; train_step.glsl:11-17, train_common.glsl:56). */
+#define GS_FLAG_MOTION_GRAD 64u
+/* Most subject-motion control nodes (the reference's kMaxMotionNodes). */
+#define GS_MAX_MOTION_NODES 128u
 #define GS_FLAG_SPARSE_ADAM 128u /* gaussians that drew nothing keep their values and moments */
 
 /* Per-view step constants: FrameData of train_common.glsl:15-37, filled as
@@ -124,7 +132,8 @@ typedef enum gs_snapshot_kind {
   GS_SNAP_STATS = 13,       /* 4 floats per slot: densification statistics */
   GS_SNAP_PAIR_GAUSSIAN = 14, /* uint32 per pair, pre-sort order: the slot */
   GS_SNAP_PIXEL_OUT = 15,     /* 4 floats per pixel: rendered rgb over the background, loss weight */
-  GS_SNAP_SPAWN = 16          /* uint32 per slot after gs_densify: 0 none, 1 clone, 2 split */
+  GS_SNAP_SPAWN = 16,         /* uint32 per slot after gs_densify: 0 none, 1 clone, 2 split */
+  GS_SNAP_MOTION_BIND = 17    /* 8 uint32 per slot: 4 motion nodes, their 4 weights (float bits) */
 } gs_snapshot_kind;
 
 /* Tuning knobs (Trainer options that shape buffers and kernels; trainer.h:150-165). */
@@ -226,6 +235,26 @@ int gs_get_tuning(gs_context* ctx, gs_tuning* tuning);
    densification statistics are restored afterwards, so the call leaves training where it
    was; it needs device memory for one copy of them. */
 int gs_autotune(gs_context* ctx, uint32_t steps_per_candidate, gs_tuning* chosen);
+
+/* Subject motion (SC-GS; train_motion.glsl, train_motion_bind.comp, Trainer's motion state,
+   trainer.cpp:1398-1690). The model stays the subject at rest; in a view with
+   GS_FLAG_MOTION each control node k moves rigidly (x -> R_k x + b_k) and every slot
+   follows its 4 nearest nodes, blended by weight.
+   gs_motion_nodes: the nodes at rest, count <= GS_MAX_MOTION_NODES, 4 floats each
+   (position xyz, 1 / (2 r^2) with r the node's radius); binds every slot in use to its 4
+   nearest nodes with weights exp(-d^2 / (2 r^2)) normalised (the nearest alone when all
+   underflow). count 0 removes them. gs_model_init removes them too; gs_densify re-binds. */
+int gs_motion_nodes(gs_context* ctx, uint32_t count, const float* nodes4);
+/* Binds the slots in use again (train_motion_bind.comp), for gaussians that moved. */
+int gs_motion_bind(gs_context* ctx);
+/* Node motions for view `view` (< GS_MAX_VIEWS) of the next steps, 20 floats per node:
+   the 3 rows of [R | b] (b = c - R n), the turn vector (xyz, 0) and the moved position c
+   (xyz, 0). gs_render uses view 0's. Kept until set again. */
+int gs_set_view_motion(gs_context* ctx, uint32_t view, const float* nodes20);
+/* After a training step whose view `view` had GS_FLAG_MOTION_GRAD: per node (count of
+   them) dL/dshift xyz then dL/dturn xyz in world axes, summed over the slots
+   (train_step.glsl:270-337, train_motion_sum.comp). */
+int gs_motion_gradient(gs_context* ctx, uint32_t view, double* out, uint32_t count);
 
 /* No counterpart in the reference: its RadixSort allocates its own temporary buffers
    (engine/src/radix_sort.cpp:37-39). For callers that cannot allocate device memory —

@@ -144,6 +144,20 @@ struct gs_context {
   double* d_view_sums = nullptr;
   double* h_view_sums = nullptr;  // pinned
   float* pose_partial = nullptr;  // per view and 128 slots: the pose gradient's partial sums
+  // Subject motion: the nodes at rest, each slot's binding, the node motions per view (a
+  // pinned host copy the setters fill, uploaded with the step), the gradient's per-block
+  // partial sums and its totals per view and node.
+  uint32_t motion_nodes = 0;
+  float4* motion_rest = nullptr;  // kMaxMotionNodes
+  uint4* motion_bind = nullptr;   // 2 per slot
+  uint32_t motion_bind_cap = 0;
+  gsk::MotionNode* d_motion_views = nullptr;  // GS_MAX_VIEWS x kMaxMotionNodes
+  gsk::MotionNode* h_motion_views = nullptr;  // pinned
+  float* motion_partial = nullptr;
+  size_t motion_partial_floats = 0;
+  double* d_motion_grad = nullptr;  // GS_MAX_VIEWS x kMaxMotionNodes x 8
+  double* h_motion_grad = nullptr;  // pinned
+  bool motion_grad_ready = false;
   gsk::SortScratch sort;
   gsk::DensifyScratch dens;
   uint64_t max_pairs_seen = 0;
@@ -159,7 +173,16 @@ struct gs_context {
     for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.dir_grad, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
-    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial}) dev_free(*p);
+    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial, &motion_partial})
+      dev_free(*p);
+    dev_free(motion_rest);
+    dev_free(motion_bind);
+    dev_free(d_motion_views);
+    dev_free(d_motion_grad);
+    if (h_motion_views) cudaFreeHost(h_motion_views);
+    if (h_motion_grad) cudaFreeHost(h_motion_grad);
+    h_motion_views = nullptr;
+    h_motion_grad = nullptr;
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
                          &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
                          &d_scalars, &sort.hist, &sort.lookback, &sort.ticket, &sort.err, &dens.spawn,
@@ -301,6 +324,9 @@ struct gs_context {
     GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, kScalars * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * kViewSums * n_views,
                                 cudaMemcpyDeviceToHost, stream));
+    if (train && (motion_mode() & 2u))
+      GS_CUDA_TRY(cudaMemcpyAsync(h_motion_grad, d_motion_grad, sizeof(double) * 8 * gsk::kMaxMotionNodes * n_views,
+                                  cudaMemcpyDeviceToHost, stream));
   }
 
   // The step as a CUDA graph: captured once per launch structure (views, slots, buffer
@@ -310,7 +336,7 @@ struct gs_context {
     const std::vector<uint64_t> key = {n_views, model.slots, model.cap, pair_cap, tile_cap, pixel_cap, degree,
                                        train ? 1u : 0u, ssim ? 1u : 0u, tuning.deterministic,
                                        tuning.forward_pixels, tuning.backward_pixels, tuning.backward_batch,
-                                       tuning.sort_digit_bits, pose_mode()};
+                                       tuning.sort_digit_bits, pose_mode(), motion_mode(), motion_nodes};
     if (graph_exec == nullptr || key != graph_key) {
       drop_graph();
       cudaGraph_t g = nullptr;
@@ -357,6 +383,13 @@ struct gs_context {
       // waits for them before the forward raster; views without host targets record an
       // event that is already complete).
       GS_CUDA_TRY(cudaMemcpyAsync(d_table, h_table, sizeof(gsk::StepTable), cudaMemcpyHostToDevice, stream));
+      const uint32_t motion = motion_mode();
+      if (motion != 0u) {
+        GS_CUDA_TRY(cudaMemcpyAsync(d_motion_views, h_motion_views,
+                                    sizeof(gsk::MotionNode) * gsk::kMaxMotionNodes * n_views, cudaMemcpyHostToDevice,
+                                    stream));
+        if (train && (motion & 2u)) reserve_motion_partial();
+      }
       if (!targets_uploaded) {
         for (const PendingTarget& p : pending_targets)
           GS_CUDA_TRY(cudaMemcpyAsync(target + p.offset, p.host, p.bytes, cudaMemcpyHostToDevice, copy_stream));
@@ -403,6 +436,7 @@ struct gs_context {
             for (int k = 0; k < 6; ++k) out->pose_grad[v][k] = s[16 + k];
         }
         out->gpu_ms = elapsed(ev0, ev1);
+        motion_grad_ready = train && (motion_mode() & 2u) != 0u;
         out->kernels = uint32_t(launches);
         if (profile)
           for (int k = 0; k < 6; ++k) out->pass_ms[k] = (train || k < 4) ? elapsed(marks[k], marks[k + 1]) : 0.0f;
@@ -543,6 +577,42 @@ struct gs_context {
     return rb;
   }
 
+  // Bit 0: some view moves with the subject; bit 1: some view asks for its motion gradient.
+  uint32_t motion_mode() const {
+    if (motion_nodes == 0u) return 0u;
+    uint32_t m = 0u;
+    for (uint32_t v = 0; v < n_views; ++v) {
+      if (frames[v].model[3] & GS_FLAG_MOTION) m |= 1u;
+      if (frames[v].model[3] & GS_FLAG_MOTION_GRAD) m |= 2u;
+    }
+    return m;
+  }
+
+  gsk::Motion motion_state() const {
+    gsk::Motion m;
+    m.nodes = motion_nodes;
+    m.rest = motion_rest;
+    m.bind = motion_bind;
+    m.views = d_motion_views;
+    return m;
+  }
+
+  void reserve_motion_partial() {
+    const size_t wanted =
+        size_t(n_views) * gsk::motion_blocks(model.slots, sm_count) * gsk::kMaxMotionNodes * 8u;
+    if (wanted <= motion_partial_floats) return;
+    drop_graph();
+    dev_alloc(motion_partial, wanted);
+    motion_partial_floats = wanted;
+  }
+
+  void bind_motion() {
+    if (motion_nodes == 0u || model.slots == 0u) return;
+    gsk::launch_motion_bind(model, motion_state(), stream);
+    GS_CUDA_TRY(cudaStreamSynchronize(stream));
+    check_launch("motion bind");
+  }
+
   // Bit 0: some view asks for its pose gradient; bit 1: the step changes nothing (the
   // first view's GS_FLAG_POSE_ONLY).
   uint32_t pose_mode() const {
@@ -559,8 +629,11 @@ struct gs_context {
     const uint32_t items = n_views * model.slots;
     const bool det = tuning.deterministic != 0u;
     GS_CUDA_TRY(cudaMemsetAsync(d_scalars, 0, sizeof(uint32_t), stream));  // [0] pairs; [1] mismatches accumulate
+    const uint32_t motion = motion_mode();
+    const gsk::Motion mo = motion_state();
+    const gsk::Motion* moving = (motion & 1u) ? &mo : nullptr;
     mark(0);
-    gsk::launch_project(sp, model, degree, vb, dkeys, dvals, train && !det, stream);
+    gsk::launch_project(sp, model, degree, vb, dkeys, dvals, train && !det, moving, stream);
     launches += model.slots ? 1 : 0;
     mark(1);
     // Depth sort of every (view, slot): key = view << 16 | depth16.
@@ -622,12 +695,17 @@ struct gs_context {
       }
       const uint32_t pose = pose_mode();
       if (pose & 1u) {
-        gsk::launch_pose_grad(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), pose_partial,
+        gsk::launch_pose_grad(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), moving, pose_partial,
                               d_view_sums + 16, kViewSums, stream);
         launches += model.slots ? 2 : 1;
       }
+      if (motion & 2u) {
+        gsk::launch_motion_grad(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), mo, motion_partial,
+                                d_motion_grad, stream);
+        launches += model.slots ? 2 : 1;
+      }
       if ((pose & 2u) == 0u) {
-        gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), stream);
+        gsk::launch_step(sp, model, degree, vb, d_scalars, uint32_t(pair_cap), moving, stream);
         launches += model.slots ? (degree > 0 ? 2 : 1) : 0;
       }
       mark(6);
@@ -921,6 +999,8 @@ int gs_model_init(gs_context* c, uint32_t capacity, uint32_t sh_stride, const fl
     }
     c->max_pairs_seen = 0;
     c->stepped = false;
+    c->motion_nodes = 0;  // the binding was for the old slots
+    c->motion_grad_ready = false;
     c->check_launch("gs_model_init");
     GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
   });
@@ -1054,6 +1134,7 @@ int gs_densify(gs_context* c, const gs_frame_data* frame, uint32_t counters_out[
       c->drop_graph();
     }
     counters[3] = c->model.slots;
+    c->bind_motion();  // new gaussians need nodes (Trainer::after_step, trainer.cpp:944)
     if (counters_out) std::memcpy(counters_out, counters, sizeof(counters));
   });
 }
@@ -1071,7 +1152,8 @@ int gs_reset_opacity(gs_context* c, float max_logit) {
 int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host, size_t bytes, size_t* needed) {
   return guarded([&] {
     if (c == nullptr) fail(GS_ERR_INVALID, "gs_snapshot: null context");
-    if (which != GS_SNAP_SPAWN && which != GS_SNAP_STATS && (!c->stepped || view >= c->n_views))
+    if (which != GS_SNAP_SPAWN && which != GS_SNAP_STATS && which != GS_SNAP_MOTION_BIND &&
+        (!c->stepped || view >= c->n_views))
       fail(GS_ERR_INVALID, "gs_snapshot: no such view in the latest step");
     GS_CUDA_TRY(cudaSetDevice(c->device));
     GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1089,6 +1171,10 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_PROJECTED: size = size_t(slots) * 64; break;
       case GS_SNAP_TILES: case GS_SNAP_OFFSETS: case GS_SNAP_DEPTH_KEY: size = size_t(slots) * 4; break;
       case GS_SNAP_STATS: size = size_t(slots) * 16; break;
+      case GS_SNAP_MOTION_BIND:
+        if (c->motion_nodes == 0u) fail(GS_ERR_INVALID, "gs_snapshot: no motion nodes");
+        size = size_t(slots) * 32;
+        break;
       case GS_SNAP_PAIR_GRADS: size = size_t(pairs) * 48; break;
       case GS_SNAP_PAIR_TILE: case GS_SNAP_RENDER_ORDER: case GS_SNAP_PAIR_GAUSSIAN: size = size_t(pairs) * 4; break;
       case GS_SNAP_RANGES: size = tiles * 8; break;
@@ -1111,6 +1197,7 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_TILES: d2h(host, c->vb.tiles + size_t(view) * cap, size); break;
       case GS_SNAP_OFFSETS: d2h(host, c->vb.offsets + size_t(view) * cap, size); break;
       case GS_SNAP_STATS: d2h(host, c->model.stats, size); break;
+      case GS_SNAP_MOTION_BIND: d2h(host, c->motion_bind, size); break;
       case GS_SNAP_TILE_LOSS: d2h(host, c->tile_loss + tb * 16, size); break;
       case GS_SNAP_PAIR_GRADS: d2h(host, c->pair_grads, size); break;
       case GS_SNAP_PAIR_GAUSSIAN: {
@@ -1170,6 +1257,70 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       }
       default: break;
     }
+  });
+}
+
+int gs_motion_nodes(gs_context* c, uint32_t count, const float* nodes4) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_motion_nodes: null context");
+    if (count > GS_MAX_MOTION_NODES) fail(GS_ERR_INVALID, "gs_motion_nodes: at most 128 nodes");
+    if (count > 0 && nodes4 == nullptr) fail(GS_ERR_INVALID, "gs_motion_nodes: null nodes");
+    if (c->model.cap == 0) fail(GS_ERR_INVALID, "gs_motion_nodes: no model (gs_model_init first)");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->drop_graph();
+    c->motion_grad_ready = false;
+    c->motion_nodes = 0;
+    if (count == 0) return;
+    if (c->motion_rest == nullptr) {
+      dev_alloc(c->motion_rest, gsk::kMaxMotionNodes);
+      dev_alloc(c->d_motion_views, size_t(GS_MAX_VIEWS) * gsk::kMaxMotionNodes);
+      dev_alloc(c->d_motion_grad, size_t(GS_MAX_VIEWS) * gsk::kMaxMotionNodes * 8);
+      const size_t table = sizeof(gsk::MotionNode) * GS_MAX_VIEWS * gsk::kMaxMotionNodes;
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_motion_views), table));
+      std::memset(c->h_motion_views, 0, table);
+      const size_t grads = sizeof(double) * GS_MAX_VIEWS * gsk::kMaxMotionNodes * 8;
+      GS_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&c->h_motion_grad), grads));
+      std::memset(c->h_motion_grad, 0, grads);
+    }
+    if (c->motion_bind_cap < c->model.cap) {
+      dev_alloc(c->motion_bind, size_t(c->model.cap) * 2);
+      c->motion_bind_cap = c->model.cap;
+    }
+    GS_CUDA_TRY(cudaMemcpy(c->motion_rest, nodes4, sizeof(float4) * count, cudaMemcpyHostToDevice));
+    c->motion_nodes = count;
+    c->bind_motion();
+  });
+}
+
+int gs_motion_bind(gs_context* c) {
+  return guarded([&] {
+    if (c == nullptr) fail(GS_ERR_INVALID, "gs_motion_bind: null context");
+    if (c->motion_nodes == 0u) fail(GS_ERR_INVALID, "gs_motion_bind: no motion nodes (gs_motion_nodes first)");
+    GS_CUDA_TRY(cudaSetDevice(c->device));
+    GS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->bind_motion();
+  });
+}
+
+int gs_set_view_motion(gs_context* c, uint32_t view, const float* nodes20) {
+  return guarded([&] {
+    if (c == nullptr || nodes20 == nullptr) fail(GS_ERR_INVALID, "gs_set_view_motion: null argument");
+    if (view >= GS_MAX_VIEWS) fail(GS_ERR_INVALID, "gs_set_view_motion: view out of range");
+    if (c->motion_nodes == 0u) fail(GS_ERR_INVALID, "gs_set_view_motion: no motion nodes (gs_motion_nodes first)");
+    std::memcpy(c->h_motion_views + size_t(view) * gsk::kMaxMotionNodes, nodes20,
+                sizeof(gsk::MotionNode) * c->motion_nodes);
+  });
+}
+
+int gs_motion_gradient(gs_context* c, uint32_t view, double* out, uint32_t count) {
+  return guarded([&] {
+    if (c == nullptr || out == nullptr) fail(GS_ERR_INVALID, "gs_motion_gradient: null argument");
+    if (!c->motion_grad_ready || view >= c->n_views)
+      fail(GS_ERR_INVALID, "gs_motion_gradient: the latest step computed no motion gradient for this view");
+    if (count > c->motion_nodes) fail(GS_ERR_INVALID, "gs_motion_gradient: more nodes than there are");
+    for (uint32_t k = 0; k < count; ++k)
+      for (int j = 0; j < 6; ++j) out[k * 6 + j] = c->h_motion_grad[(size_t(view) * gsk::kMaxMotionNodes + k) * 8 + j];
   });
 }
 

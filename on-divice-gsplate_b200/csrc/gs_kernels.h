@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "gs_common.cuh"
+#include "motion.cuh"
 
 namespace gsk {
 
@@ -45,8 +46,10 @@ struct StepPointers {
 };
 
 // ---- project.cu ----
+// motion: non-null when some view of the step has GS_FLAG_MOTION.
 void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                    uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, cudaStream_t st);
+                    uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, const Motion* motion,
+                    cudaStream_t st);
 
 // ---- sort.cu ----
 struct SortScratch {
@@ -113,14 +116,24 @@ void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* 
 // ---- step.cu ----
 void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* depth_order, const uint32_t* first,
                      const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
+// motion: non-null when some view of the step has GS_FLAG_MOTION.
 void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                 const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
+                 const uint32_t* d_pairs, uint32_t accept, const Motion* motion, cudaStream_t st);
 // Camera pose gradients of the views with GS_FLAG_POSE_GRAD (before launch_step, which
 // updates the parameters): out[v * stride + 0..5]. partial: n_views * pose_blocks(slots) * 8.
 uint32_t pose_blocks(uint32_t slots);
 void launch_pose_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                      const uint32_t* d_pairs, uint32_t accept, float* partial, double* out, uint32_t stride,
-                      cudaStream_t st);
+                      const uint32_t* d_pairs, uint32_t accept, const Motion* motion, float* partial, double* out,
+                      uint32_t stride, cudaStream_t st);
+// Subject motion: the per-node gradient of the views with GS_FLAG_MOTION_GRAD (before
+// launch_step), out[(v * kMaxMotionNodes + node) * 8 + 0..5]; partial holds
+// n_views * motion_blocks(slots, sm_count) * kMaxMotionNodes * 8 floats.
+uint32_t motion_blocks(uint32_t slots, int sm_count);
+void launch_motion_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                        const uint32_t* d_pairs, uint32_t accept, const Motion& motion, float* partial, double* out,
+                        cudaStream_t st);
+// Binds the slots in use to their 4 nearest nodes (train_motion_bind.comp).
+void launch_motion_bind(const Model& m, const Motion& motion, cudaStream_t st);
 struct DensifyScratch {
   uint32_t* spawn = nullptr;     // action per slot
   uint32_t* release = nullptr;   // 1 per freed slot

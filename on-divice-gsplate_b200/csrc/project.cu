@@ -7,7 +7,13 @@
 // view it writes 48 B of splat record, 16 B of footprint, a tile count and a depth
 // key/value pair. 128-thread blocks capped at 128 registers keep 4 blocks per SM resident
 // (one 256-thread block of 151 registers fit alone: 8 warps per SM).
+//
+// With MOTION (any view of the step has GS_FLAG_MOTION) a slot is first moved with the
+// subject in the views that have the flag (train_project.comp:36-41): its position by the
+// node blend, its covariance by the blended turn U (world -> camera becomes V U for it),
+// and the SH colour is looked up in its own rest frame (direction U^T (x - camera)).
 #include "gs_kernels.h"
+#include "motion.cuh"
 
 namespace gsk {
 namespace {
@@ -23,9 +29,10 @@ struct ProjectArgs {
   uint32_t* dkeys;
   uint32_t* dvals;
   float4* grad2d;  // zeroed when non-null (atomic backward)
+  Motion motion;
 };
 
-template <int DEG>
+template <int DEG, bool MOTION>
 __global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   {
@@ -64,10 +71,33 @@ __global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
     const size_t g = size_t(v) * a.cap + i;
     float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0, o2 = o0, o3 = o0;
     uint32_t tiles = 0u;
-    const float tz = f.rot[2][0] * p0.x + f.rot[2][1] * p0.y + f.rot[2][2] * p0.z + f.rot[2][3];
+    float x0 = p0.x, x1 = p0.y, x2 = p0.z;
+    float W[3][3];  // rest frame -> camera, for the covariance
+    float U[3][3];  // the orientation's turn (MOTION only)
+    bool moved = false;
+    if constexpr (MOTION) {
+      if ((f.model[3] & GS_FLAG_MOTION) != 0u && p1.w > 0.5f) {
+        Deformed d;
+        deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, d);
+        x0 = d.x[0];
+        x1 = d.x[1];
+        x2 = d.x[2];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) U[r][c] = d.U[r][c];
+        moved = true;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        W[r][c] = moved ? f.rot[r][0] * U[0][c] + f.rot[r][1] * U[1][c] + f.rot[r][2] * U[2][c] : f.rot[r][c];
+    const float tz = f.rot[2][0] * x0 + f.rot[2][1] * x1 + f.rot[2][2] * x2 + f.rot[2][3];
     if (alive && tz > kNear) {
-      const float tx3 = f.rot[0][0] * p0.x + f.rot[0][1] * p0.y + f.rot[0][2] * p0.z + f.rot[0][3];
-      const float ty3 = f.rot[1][0] * p0.x + f.rot[1][1] * p0.y + f.rot[1][2] * p0.z + f.rot[1][3];
+      const float tx3 = f.rot[0][0] * x0 + f.rot[0][1] * x1 + f.rot[0][2] * x2 + f.rot[0][3];
+      const float ty3 = f.rot[1][0] * x0 + f.rot[1][1] * x1 + f.rot[1][2] * x2 + f.rot[1][3];
       const float fx = f.intrinsics[0], fy = f.intrinsics[1], cx = f.intrinsics[2], cy = f.intrinsics[3];
       const float width = float(f.image[0]), height = float(f.image[1]);
       const float inv_z = 1.0f / tz;
@@ -80,8 +110,8 @@ __global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
       float T0[3], T1[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T0[c] = j00 * f.rot[0][c] + j02 * f.rot[2][c];
-        T1[c] = j11 * f.rot[1][c] + j12 * f.rot[2][c];
+        T0[c] = j00 * W[0][c] + j02 * W[2][c];
+        T1[c] = j11 * W[1][c] + j12 * W[2][c];
       }
       float u0[3], u1[3];
 #pragma unroll
@@ -101,7 +131,15 @@ __global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
         tiles = footprint_count(mx, my, ca, cb, cc, thr, f.image[0], f.image[1]);
         if (tiles > 0u) {
           o3 = make_float4(ca, cb, cc, thr);
-          float dx = p0.x - f.cam_pos[0], dy = p0.y - f.cam_pos[1], dz = p0.z - f.cam_pos[2];
+          float dx = x0 - f.cam_pos[0], dy = x1 - f.cam_pos[1], dz = x2 - f.cam_pos[2];
+          if (moved) {  // into the rest frame: U^T (x - camera)
+            const float rx = U[0][0] * dx + U[1][0] * dy + U[2][0] * dz;
+            const float ry = U[0][1] * dx + U[1][1] * dy + U[2][1] * dz;
+            const float rz = U[0][2] * dx + U[1][2] * dy + U[2][2] * dz;
+            dx = rx;
+            dy = ry;
+            dz = rz;
+          }
           const float dl = sqrtf(dx * dx + dy * dy + dz * dz);
           dx /= dl;
           dy /= dl;
@@ -152,18 +190,25 @@ __global__ void __launch_bounds__(128, 4) k_project(ProjectArgs a) {
 
 }  // namespace
 
+template <bool MOTION>
+void project_degree(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const ProjectArgs& a) {
+  switch (degree) {
+    case 0: k_project<0, MOTION><<<grid, block, 0, st>>>(a); break;
+    case 1: k_project<1, MOTION><<<grid, block, 0, st>>>(a); break;
+    case 2: k_project<2, MOTION><<<grid, block, 0, st>>>(a); break;
+    default: k_project<3, MOTION><<<grid, block, 0, st>>>(a); break;
+  }
+}
+
 void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                    uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, cudaStream_t st) {
+                    uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, const Motion* motion,
+                    cudaStream_t st) {
   if (m.slots == 0) return;
   ProjectArgs a{sp.frames, sp.n_views, m.slots, m.cap, m.P, m.SH, vb.splat, vb.foot, vb.tiles,
-                depth_keys, depth_vals, zero_grad2d ? vb.grad2d : nullptr};
+                depth_keys, depth_vals, zero_grad2d ? vb.grad2d : nullptr, motion ? *motion : Motion{}};
   const dim3 grid((m.slots + 127u) / 128u), block(128);
-  switch (degree) {
-    case 0: k_project<0><<<grid, block, 0, st>>>(a); break;
-    case 1: k_project<1><<<grid, block, 0, st>>>(a); break;
-    case 2: k_project<2><<<grid, block, 0, st>>>(a); break;
-    default: k_project<3><<<grid, block, 0, st>>>(a); break;
-  }
+  if (motion != nullptr) project_degree<true>(degree, grid, block, st, a);
+  else project_degree<false>(degree, grid, block, st, a);
 }
 
 }  // namespace gsk

@@ -8,6 +8,7 @@
 // (k_step_sh, first: it also produces the position gradient through the SH view
 // direction) and on the 16 parameters (k_step_geometry). HBM-bound: parameters, SH and
 // both moment sets are read and written once per step.
+#include <algorithm>
 #include <utility>
 
 #include "gs_kernels.h"
@@ -69,6 +70,7 @@ struct StepArgs {
   float4* dir_grad;  // per slot: position gradient through the SH view direction (k_step_sh -> k_step_geometry)
   const uint32_t* d_pairs;
   uint32_t accept;
+  Motion motion;  // nodes == 0: no view moves
 };
 
 // Adam (train_step.glsl:62-67). The square root and the division use the hardware's
@@ -184,11 +186,17 @@ __device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t 
 // colour gradient and the view direction. drew: bit 0 any pair gradient, bit 1 a non-zero
 // colour gradient. With POSE it also adds the slot's share of the camera pose gradient to
 // pose (dL/dd, dL/dw; train_step.glsl:196-202).
-template <int DEG, bool POSE = false>
+// With MOTION and dm non-null the slot is moved with the subject in this view
+// (train_step.glsl:105-107, 192-194): at dm->x, its covariance turned by dm->U, and the
+// position gradient goes back to the rest position through A^T. share (when non-null)
+// receives the slot's motion share: dL/dx = V^T dL/dt (world; the SH view-direction term
+// is added by the caller) and the turn of its orientation dL/dturn (world axes).
+template <int DEG, bool POSE = false, bool MOTION = false>
 __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0, const Geometry& G, float4 a0, float4 a1,
                                               float4 a2, uint32_t clamped, float radius, float g16[16], float4& st,
                                               float dcol[3], float dir[3], float& dir_len, uint32_t& drew,
-                                              float* pose = nullptr) {
+                                              float* pose = nullptr, const Deformed* dm = nullptr,
+                                              float* share = nullptr) {
   if (a0.x != 0.f || a0.y != 0.f || a0.z != 0.f || a0.w != 0.f || a1.x != 0.f || a1.y != 0.f || a1.z != 0.f ||
       a1.w != 0.f || a2.x != 0.f || a2.y != 0.f || a2.z != 0.f || a2.w != 0.f)
     drew |= 1u;
@@ -205,9 +213,29 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   st.z = fmaxf(st.z, radius);
   st.w += sqrtf((a2.y * nx) * (a2.y * nx) + (a2.z * ny) * (a2.z * ny));
 
+  const bool moved = MOTION && dm != nullptr;
+  float xm[3] = {p0.x, p0.y, p0.z};  // where the slot is in this view
+  // Rest frame -> camera: V, or V U when moved (read from the frame directly without motion).
+  float WU[3][3];
+  if constexpr (MOTION) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        WU[r][c] = moved ? f.rot[r][0] * dm->U[0][c] + f.rot[r][1] * dm->U[1][c] + f.rot[r][2] * dm->U[2][c]
+                         : f.rot[r][c];
+    if (moved) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) xm[r] = dm->x[r];
+    }
+  }
+  auto W = [&](int r, int c) -> float {
+    if constexpr (MOTION) return WU[r][c];
+    else return f.rot[r][c];
+  };
   float t[3];
 #pragma unroll
-  for (int r = 0; r < 3; ++r) t[r] = f.rot[r][0] * p0.x + f.rot[r][1] * p0.y + f.rot[r][2] * p0.z + f.rot[r][3];
+  for (int r = 0; r < 3; ++r) t[r] = f.rot[r][0] * xm[0] + f.rot[r][1] * xm[1] + f.rot[r][2] * xm[2] + f.rot[r][3];
   const float fx = f.intrinsics[0], fy = f.intrinsics[1], cx = f.intrinsics[2], cy = f.intrinsics[3];
   const float inv_z = 1.0f / t[2];
   const float lim_x = 1.3f * fmaxf(cx, width - cx) / fx;
@@ -220,8 +248,8 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   float T[2][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    T[0][c] = j00 * f.rot[0][c] + j02 * f.rot[2][c];
-    T[1][c] = j11 * f.rot[1][c] + j12 * f.rot[2][c];
+    T[0][c] = j00 * W(0, c) + j02 * W(2, c);
+    T[1][c] = j11 * W(1, c) + j12 * W(2, c);
   }
   float TS[2][3];
 #pragma unroll
@@ -233,11 +261,18 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   const float C = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + kDilation;
   const float D = A * C - B * B;
 
-  const float dr0 = p0.x - f.cam_pos[0], dr1 = p0.y - f.cam_pos[1], dr2 = p0.z - f.cam_pos[2];
-  dir_len = fmaxf(sqrtf(dr0 * dr0 + dr1 * dr1 + dr2 * dr2), 1e-12f);
-  dir[0] = dr0 / dir_len;
-  dir[1] = dr1 / dir_len;
-  dir[2] = dr2 / dir_len;
+  float dr[3] = {xm[0] - f.cam_pos[0], xm[1] - f.cam_pos[1], xm[2] - f.cam_pos[2]};
+  if constexpr (MOTION) {
+    if (moved) {  // the rest frame's direction, U^T (x - camera)
+      const float e[3] = {dr[0], dr[1], dr[2]};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dr[c] = dm->U[0][c] * e[0] + dm->U[1][c] * e[1] + dm->U[2][c] * e[2];
+    }
+  }
+  dir_len = fmaxf(sqrtf(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), 1e-12f);
+  dir[0] = dr[0] / dir_len;
+  dir[1] = dr[1] / dir_len;
+  dir[2] = dr[2] / dir_len;
   g16[12] += 0.28209479177387814f * dcol[0];
   g16[13] += 0.28209479177387814f * dcol[1];
   g16[14] += 0.28209479177387814f * dcol[2];
@@ -265,7 +300,7 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
 #pragma unroll
   for (int r = 0; r < 2; ++r)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) dJ[r][c] = dT[r][0] * f.rot[c][0] + dT[r][1] * f.rot[c][1] + dT[r][2] * f.rot[c][2];
+    for (int c = 0; c < 3; ++c) dJ[r][c] = dT[r][0] * W(c, 0) + dT[r][1] * W(c, 1) + dT[r][2] * W(c, 2);
   float dt[3] = {0.f, 0.f, 0.f};
   const float inv_z2 = inv_z * inv_z;
   dt[2] += -fx * inv_z2 * dJ[0][0] - fy * inv_z2 * dJ[1][1];
@@ -284,8 +319,33 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
   dt[0] += dmx * fx * inv_z;
   dt[1] += dmy * fy * inv_z;
   dt[2] += -(dmx * fx * t[0] + dmy * fy * t[1]) * inv_z2;
+  float dx[3];  // dL/dx, world: V^T dL/dt
 #pragma unroll
-  for (int c = 0; c < 3; ++c) g16[c] += f.rot[0][c] * dt[0] + f.rot[1][c] * dt[1] + f.rot[2][c] * dt[2];
+  for (int c = 0; c < 3; ++c) dx[c] = f.rot[0][c] * dt[0] + f.rot[1][c] * dt[1] + f.rot[2][c] * dt[2];
+  if constexpr (MOTION) {
+    if (moved) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g16[c] += dm->A[0][c] * dx[0] + dm->A[1][c] * dx[1] + dm->A[2][c] * dx[2];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g16[c] += dx[c];
+    }
+    if (share != nullptr) {
+      // The orientation's turn in camera axes, (X21 - X12, X02 - X20, X10 - X01) with
+      // X = J^T dJ, then in world axes (V^T).
+      const float x01 = j00 * dJ[0][1], x02 = j00 * dJ[0][2], x10 = j11 * dJ[1][0], x12 = j11 * dJ[1][2];
+      const float x20 = j02 * dJ[0][0] + j12 * dJ[1][0], x21 = j02 * dJ[0][1] + j12 * dJ[1][1];
+      const float tc[3] = {x21 - x12, x02 - x20, x10 - x01};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        share[c] = dx[c];
+        share[3 + c] = f.rot[0][c] * tc[0] + f.rot[1][c] * tc[1] + f.rot[2][c] * tc[2];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g16[c] += dx[c];
+  }
   if (POSE) {
     // A shift d moves t by d; a turn w moves t by w x t and W by [w]x W, so with
     // X = dL/dW W^T = J^T dJ: dL/dw = t x dL/dt + (X21 - X12, X02 - X20, X10 - X01).
@@ -381,7 +441,7 @@ __device__ __forceinline__ void copy_frames(const StepArgs& a, gs_frame_data* s_
 // which goes through the normalisation into the position gradient (summed over views,
 // stored for part 2). Then Adam on the 3K coefficients, 3 coefficients' moments loaded
 // together so each thread keeps 18 loads in flight (the SH values are already loaded).
-template <int DEG>
+template <int DEG, bool MOTION>
 __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
@@ -428,9 +488,20 @@ __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
     view_colour_grad(a1, a2, __float_as_uint(cw), dcol);
     colour |= dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f;
     const gs_frame_data& f = s_frames[v];
-    const float dr0 = p0.x - f.cam_pos[0], dr1 = p0.y - f.cam_pos[1], dr2 = p0.z - f.cam_pos[2];
-    const float dir_len = fmaxf(sqrtf(dr0 * dr0 + dr1 * dr1 + dr2 * dr2), 1e-12f);
-    const float dir[3] = {dr0 / dir_len, dr1 / dir_len, dr2 / dir_len};
+    float dr[3] = {p0.x - f.cam_pos[0], p0.y - f.cam_pos[1], p0.z - f.cam_pos[2]};
+    Deformed dm;
+    bool moved = false;
+    if constexpr (MOTION) {
+      if ((f.model[3] & GS_FLAG_MOTION) != 0u) {  // the rest frame's direction, U^T (x - camera)
+        deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, dm);
+        const float e[3] = {dm.x[0] - f.cam_pos[0], dm.x[1] - f.cam_pos[1], dm.x[2] - f.cam_pos[2]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dr[c] = dm.U[0][c] * e[0] + dm.U[1][c] * e[1] + dm.U[2][c] * e[2];
+        moved = true;
+      }
+    }
+    const float dir_len = fmaxf(sqrtf(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), 1e-12f);
+    const float dir[3] = {dr[0] / dir_len, dr[1] / dir_len, dr[2] / dir_len};
     float dd[3] = {0.f, 0.f, 0.f};
     for_terms(std::make_integer_sequence<int, K>{}, [&](auto kk) {
       constexpr int k = decltype(kk)::value;
@@ -444,6 +515,18 @@ __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
       dd[2] += w * gz;
     });
     const float proj = dir[0] * dd[0] + dir[1] * dd[1] + dir[2] * dd[2];
+    if constexpr (MOTION) {
+      if (moved) {  // back through U to x, then through A^T to the rest position
+        float gd[3], gx[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) gd[c] = (dd[c] - dir[c] * proj) / dir_len;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) gx[r] = dm.U[r][0] * gd[0] + dm.U[r][1] * gd[1] + dm.U[r][2] * gd[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pd[c] += dm.A[0][c] * gx[0] + dm.A[1][c] * gx[1] + dm.A[2][c] * gx[2];
+        continue;
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) pd[c] += (dd[c] - dir[c] * proj) / dir_len;
   }
@@ -479,7 +562,7 @@ __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
 
 // Part 2 (train_step.glsl:72-240): every view's projection backward summed, plus the SH
 // view-direction term from part 1, then Adam on the 16 parameters.
-template <int DEG>
+template <int DEG, bool MOTION>
 __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
@@ -524,6 +607,15 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
       nr = a.splat[g * 3u + 1u].w;
     }
     float dcol[3], dir[3], dir_len;
+    if constexpr (MOTION) {
+      if ((s_frames[v].model[3] & GS_FLAG_MOTION) != 0u) {
+        Deformed dm;
+        deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, dm);
+        view_backward<DEG, false, true>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, st, dcol,
+                                        dir, dir_len, drew, nullptr, &dm);
+        continue;
+      }
+    }
     view_backward<DEG>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, st, dcol, dir, dir_len, drew);
   }
   if (DEG > 0) {
@@ -543,7 +635,7 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
 // warp, then the warps) into partial[(v * gridDim.x + x) * 8 + 0..5]. Parameters are read
 // before the step's update, as in the reference's single pass; the SH view-direction term
 // is left out there too.
-template <int DEG>
+template <int DEG, bool MOTION>
 __global__ void __launch_bounds__(128) k_pose_grad(StepArgs a, float* __restrict__ partial) {
   __shared__ gs_frame_data s_frame;
   __shared__ float s_red[4][6];
@@ -567,9 +659,20 @@ __global__ void __launch_bounds__(128) k_pose_grad(StepArgs a, float* __restrict
       float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
       float dcol[3], dir[3], dir_len;
       uint32_t drew = 0u;
-      view_backward<DEG, true>(s_frame, p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u], a.grad2d[g * 3u + 2u],
-                               __float_as_uint(a.splat[g * 3u + 2u].w), 0.0f, g16, st, dcol, dir, dir_len, drew,
-                               pose);
+      const float4 a0 = a.grad2d[g * 3u], a1 = a.grad2d[g * 3u + 1u], a2 = a.grad2d[g * 3u + 2u];
+      const uint32_t clamped = __float_as_uint(a.splat[g * 3u + 2u].w);
+      bool done = false;
+      if constexpr (MOTION) {
+        if ((s_frame.model[3] & GS_FLAG_MOTION) != 0u) {
+          Deformed dm;
+          deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, dm);
+          view_backward<DEG, true, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, st, dcol, dir, dir_len, drew,
+                                         pose, &dm);
+          done = true;
+        }
+      }
+      if (!done)
+        view_backward<DEG, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, st, dcol, dir, dir_len, drew, pose);
     }
   }
 #pragma unroll
@@ -610,6 +713,240 @@ __global__ void __launch_bounds__(256) k_pose_reduce(const gs_frame_data* frames
     for (int w = 0; w < 8; ++w) sum += s[w][threadIdx.x];
     out[size_t(v) * stride + threadIdx.x] = sum;
   }
+}
+
+// ---- subject motion ----
+
+// The motion gradient (train_step.glsl:270-337 with train_motion_sum.comp) of view
+// blockIdx.y, if it has GS_FLAG_MOTION_GRAD: per node k, over the slots that follow it,
+//   dL/dshift_k = sum w_k dL/dx,   dL/dturn_k = sum w_k (tau + (R_k (p - n_k)) x dL/dx),
+// with dL/dx the slot's moved-position gradient (world, including the SH view-direction
+// term) and tau the turn of its orientation. Blocks walk chunks of 128 slots; a chunk's
+// nodes are listed, the threads split between them (a power of two per node, up to 16),
+// each part sums a slice of the chunk in slot order, and each node adds its parts in order
+// to the block's total: a fixed summation order for a fixed grid. The block writes its
+// totals to partial[((v * gridDim.x + block) * kMaxMotionNodes + node) * 8 + 0..5].
+template <int DEG>
+__global__ void __launch_bounds__(128) k_motion_grad(StepArgs a, float* __restrict__ partial) {
+  constexpr int K = DEG == 0 ? 0 : (DEG + 1) * (DEG + 1) - 1;
+  __shared__ gs_frame_data s_frame;
+  __shared__ float s_rest[3][128];
+  __shared__ float s_share[6][128];
+  __shared__ uint4 s_nodes[128];
+  __shared__ float4 s_w[128];
+  __shared__ uint32_t s_mask[4];
+  __shared__ uint32_t s_list[128];
+  __shared__ float s_part[6][128];
+  __shared__ float s_acc[6][kMaxMotionNodes];
+  const uint32_t v = blockIdx.y, l = threadIdx.x;
+  if (l < uint32_t(sizeof(gs_frame_data) / 4))
+    reinterpret_cast<uint32_t*>(&s_frame)[l] = reinterpret_cast<const uint32_t*>(a.frames + v)[l];
+  for (uint32_t k = l; k < 6u * kMaxMotionNodes; k += 128u) (&s_acc[0][0])[k] = 0.0f;
+  __syncthreads();
+  if ((s_frame.model[3] & GS_FLAG_MOTION_GRAD) == 0u) return;  // the whole block
+  const uint32_t n_nodes = min(a.motion.nodes, kMaxMotionNodes);
+  const MotionNode* table = a.motion.views + size_t(v) * kMaxMotionNodes;
+  const bool moving = (s_frame.model[3] & GS_FLAG_MOTION) != 0u;
+  const bool valid = *a.d_pairs <= a.accept;
+  for (uint32_t base = blockIdx.x * 128u; base < a.slots; base += gridDim.x * 128u) {
+    const uint32_t i = base + l;
+    float share[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint4 nodes = make_uint4(0u, 0u, 0u, 0u), wbits = nodes;
+    bool any = false;
+    if (valid && i < a.slots) {
+      const size_t g = size_t(v) * a.cap + i;
+      const float4 p1 = a.P[a.cap + i];
+      if (p1.w >= 0.5f && a.tiles[g] != 0u) {
+        p0 = a.P[i];
+        Geometry G;
+        slot_geometry(p0, p1, a.P[2u * a.cap + i], G);
+        Deformed dm;
+        if (moving) deform(a.motion, table, i, p0.x, p0.y, p0.z, dm);
+        else at_rest(p0.x, p0.y, p0.z, dm);
+        float g16[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) g16[k] = 0.0f;
+        float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
+        float dcol[3], dir[3], dir_len;
+        uint32_t drew = 0u;
+        view_backward<DEG, false, true>(s_frame, p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u],
+                                        a.grad2d[g * 3u + 2u], __float_as_uint(a.splat[g * 3u + 2u].w), 0.0f, g16,
+                                        st, dcol, dir, dir_len, drew, nullptr, &dm, share);
+        if constexpr (K > 0) {
+          // The SH view-direction term of dL/dx: U (dd - dir (dir . dd)) / |x - c|.
+          float dd[3] = {0.f, 0.f, 0.f};
+          for_terms(std::make_integer_sequence<int, K>{}, [&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            float gx, gy, gz;
+            sh_term<k>(dir[0], dir[1], dir[2], gx, gy, gz);
+            const float w = a.SH[size_t(3 * (k - 1)) * a.cap + i] * dcol[0] +
+                            a.SH[size_t(3 * (k - 1) + 1) * a.cap + i] * dcol[1] +
+                            a.SH[size_t(3 * (k - 1) + 2) * a.cap + i] * dcol[2];
+            dd[0] += w * gx;
+            dd[1] += w * gy;
+            dd[2] += w * gz;
+          });
+          const float proj = dir[0] * dd[0] + dir[1] * dd[1] + dir[2] * dd[2];
+          float gd[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) gd[c] = (dd[c] - dir[c] * proj) / dir_len;
+#pragma unroll
+          for (int r = 0; r < 3; ++r) share[r] += dm.U[r][0] * gd[0] + dm.U[r][1] * gd[1] + dm.U[r][2] * gd[2];
+        }
+        nodes = a.motion.bind[2u * i];
+        wbits = a.motion.bind[2u * i + 1u];
+        any = true;
+      }
+    }
+    s_rest[0][l] = p0.x;
+    s_rest[1][l] = p0.y;
+    s_rest[2][l] = p0.z;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s_share[k][l] = share[k];
+    s_nodes[l] = nodes;
+    s_w[l] = any ? make_float4(__uint_as_float(wbits.x), __uint_as_float(wbits.y), __uint_as_float(wbits.z),
+                               __uint_as_float(wbits.w))
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l < 4u) s_mask[l] = 0u;
+    __syncthreads();
+    if (any) {
+      const uint32_t nk[4] = {nodes.x, nodes.y, nodes.z, nodes.w};
+      const float wk[4] = {__uint_as_float(wbits.x), __uint_as_float(wbits.y), __uint_as_float(wbits.z),
+                           __uint_as_float(wbits.w)};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (wk[j] != 0.0f && nk[j] < n_nodes) atomicOr(&s_mask[nk[j] >> 5], 1u << (nk[j] & 31u));
+    }
+    __syncthreads();
+    const uint32_t word = l >> 5, bit = 1u << (l & 31u);
+    const bool mine = l < n_nodes && (s_mask[word] & bit) != 0u;
+    uint32_t place = __popc(s_mask[word] & (bit - 1u)), count = 0u;
+#pragma unroll
+    for (uint32_t w4 = 0; w4 < 4u; ++w4) {
+      const uint32_t c = __popc(s_mask[w4]);
+      count += c;
+      if (w4 < word) place += c;
+    }
+    if (mine) s_list[place] = l;
+    const uint32_t parts = count <= 1u ? 16u : min(16u, 128u >> (32u - __clz(count - 1u)));
+    const uint32_t per = 128u / parts;
+    __syncthreads();
+    float part[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (l < count * parts) {
+      const uint32_t node = s_list[l / parts], first = (l % parts) * per;
+      const MotionNode& n = table[node];
+      for (uint32_t j = first; j < first + per; ++j) {
+        const uint4 nj = s_nodes[j];
+        const float4 wj = s_w[j];
+        const float wl = nj.x == node ? wj.x : nj.y == node ? wj.y : nj.z == node ? wj.z : nj.w == node ? wj.w : 0.0f;
+        if (wl == 0.0f) continue;
+        const float px = s_rest[0][j], py = s_rest[1][j], pz = s_rest[2][j];
+        // The arm R_k (p - n_k) = R_k p + b_k - c_k.
+        const float arm[3] = {n.row[0].x * px + n.row[0].y * py + n.row[0].z * pz + n.row[0].w - n.moved.x,
+                              n.row[1].x * px + n.row[1].y * py + n.row[1].z * pz + n.row[1].w - n.moved.y,
+                              n.row[2].x * px + n.row[2].y * py + n.row[2].z * pz + n.row[2].w - n.moved.z};
+        const float d[3] = {s_share[0][j], s_share[1][j], s_share[2][j]};
+        part[0] += wl * d[0];
+        part[1] += wl * d[1];
+        part[2] += wl * d[2];
+        part[3] += wl * (s_share[3][j] + (arm[1] * d[2] - arm[2] * d[1]));
+        part[4] += wl * (s_share[4][j] + (arm[2] * d[0] - arm[0] * d[2]));
+        part[5] += wl * (s_share[5][j] + (arm[0] * d[1] - arm[1] * d[0]));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s_part[k][l] = part[k];
+    __syncthreads();
+    if (mine) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        float sum = 0.0f;
+        for (uint32_t q = place * parts; q < (place + 1u) * parts; ++q) sum += s_part[k][q];
+        s_acc[k][l] += sum;
+      }
+    }
+    __syncthreads();
+  }
+  if (l < n_nodes) {
+    float* out = partial + ((size_t(v) * gridDim.x + blockIdx.x) * kMaxMotionNodes + l) * 8u;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out[k] = s_acc[k][l];
+  }
+}
+
+// Per view and node: the blocks' motion sums in double, in block order, into
+// out[(v * kMaxMotionNodes + node) * 8 + 0..5]; 0 for views without GS_FLAG_MOTION_GRAD.
+__global__ void __launch_bounds__(64) k_motion_reduce(const gs_frame_data* frames, const float* __restrict__ partial,
+                                                      uint32_t blocks, double* __restrict__ out) {
+  __shared__ double s[2][6];
+  const uint32_t node = blockIdx.x, v = blockIdx.y;
+  const bool wanted = (frames[v].model[3] & GS_FLAG_MOTION_GRAD) != 0u;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (wanted)
+    for (uint32_t b = threadIdx.x; b < blocks; b += 64u) {
+      const float* p = partial + ((size_t(v) * blocks + b) * kMaxMotionNodes + node) * 8u;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) acc[k] += double(p[k]);
+    }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if ((threadIdx.x & 31u) == 0u)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s[threadIdx.x >> 5][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < 6u) out[(size_t(v) * kMaxMotionNodes + node) * 8u + threadIdx.x] = s[0][threadIdx.x] + s[1][threadIdx.x];
+}
+
+// train_motion_bind.comp: each slot in use to its 4 nearest nodes at its rest position
+// (ties keep the lower node), weights exp(-d^2 / (2 r^2)) normalised, the nearest alone
+// when they all underflow; free slots get no nodes.
+__global__ void __launch_bounds__(128) k_motion_bind(const float4* __restrict__ P, uint32_t cap, uint32_t slots,
+                                                     const float4* __restrict__ rest, uint32_t n_nodes,
+                                                     uint4* __restrict__ bind) {
+  __shared__ float4 s_rest[kMaxMotionNodes];
+  for (uint32_t k = threadIdx.x; k < n_nodes; k += blockDim.x) s_rest[k] = rest[k];
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slots) return;
+  uint32_t best[4] = {0u, 0u, 0u, 0u};
+  float dist[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+  if (P[cap + i].w > 0.5f) {
+    const float4 p = P[i];
+    for (uint32_t k = 0; k < n_nodes; ++k) {
+      const float dx = p.x - s_rest[k].x, dy = p.y - s_rest[k].y, dz = p.z - s_rest[k].z;
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      if (!(d2 < dist[3])) continue;
+      // Insert into the sorted four (strictly nearer moves ahead).
+      int j = 3;
+      while (j > 0 && d2 < dist[j - 1]) {
+        dist[j] = dist[j - 1];
+        best[j] = best[j - 1];
+        --j;
+      }
+      dist[j] = d2;
+      best[j] = k;
+    }
+  }
+  float w[4] = {0.f, 0.f, 0.f, 0.f}, sum = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (dist[j] >= 1e30f) continue;
+    w[j] = expf(-dist[j] * s_rest[best[j]].w);
+    sum += w[j];
+  }
+  if (sum > 1e-20f) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[j] /= sum;
+  } else if (dist[0] < 1e30f) {
+    w[0] = 1.0f;  // far from every node: the nearest alone
+    w[1] = w[2] = w[3] = 0.0f;
+  }
+  bind[2u * i] = make_uint4(best[0], best[1], best[2], best[3]);
+  bind[2u * i + 1u] = make_uint4(__float_as_uint(w[0]), __float_as_uint(w[1]), __float_as_uint(w[2]),
+                                 __float_as_uint(w[3]));
 }
 
 // ---- densification ----
@@ -768,38 +1105,90 @@ void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* de
   k_pair_sum<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 
-void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                 const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
-  if (m.slots == 0u) return;
-  StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
-             vb.splat, vb.tiles, vb.grad2d, vb.dir_grad, d_pairs, accept};
-  const dim3 grid((m.slots + 127u) / 128u), block(128);
+template <bool MOTION>
+void step_degree(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const StepArgs& a) {
   switch (degree) {
-    case 0: k_step_geometry<0><<<grid, block, 0, st>>>(a); break;
-    case 1: k_step_sh<1><<<grid, block, 0, st>>>(a); k_step_geometry<1><<<grid, block, 0, st>>>(a); break;
-    case 2: k_step_sh<2><<<grid, block, 0, st>>>(a); k_step_geometry<2><<<grid, block, 0, st>>>(a); break;
-    default: k_step_sh<3><<<grid, block, 0, st>>>(a); k_step_geometry<3><<<grid, block, 0, st>>>(a); break;
+    case 0: k_step_geometry<0, MOTION><<<grid, block, 0, st>>>(a); break;
+    case 1:
+      k_step_sh<1, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_geometry<1, MOTION><<<grid, block, 0, st>>>(a);
+      break;
+    case 2:
+      k_step_sh<2, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_geometry<2, MOTION><<<grid, block, 0, st>>>(a);
+      break;
+    default:
+      k_step_sh<3, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_geometry<3, MOTION><<<grid, block, 0, st>>>(a);
+      break;
   }
+}
+
+StepArgs step_args(const StepPointers& sp, const Model& m, const ViewBuffers& vb, const uint32_t* d_pairs,
+                   uint32_t accept, const Motion* motion) {
+  return StepArgs{sp.frames, sp.n_views, m.cap,    m.slots,     m.P,     m.M,    m.V,
+                  m.SH,      m.MSH,      m.VSH,    m.stats,     vb.splat, vb.tiles, vb.grad2d,
+                  vb.dir_grad, d_pairs,  accept,   motion ? *motion : Motion{}};
+}
+
+void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                 const uint32_t* d_pairs, uint32_t accept, const Motion* motion, cudaStream_t st) {
+  if (m.slots == 0u) return;
+  const StepArgs a = step_args(sp, m, vb, d_pairs, accept, motion);
+  const dim3 grid((m.slots + 127u) / 128u), block(128);
+  if (motion != nullptr) step_degree<true>(degree, grid, block, st, a);
+  else step_degree<false>(degree, grid, block, st, a);
 }
 
 uint32_t pose_blocks(uint32_t slots) { return (slots + 127u) / 128u; }
 
+template <bool MOTION>
+void pose_degree(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const StepArgs& a, float* partial) {
+  switch (degree) {
+    case 0: k_pose_grad<0, MOTION><<<grid, block, 0, st>>>(a, partial); break;
+    case 1: k_pose_grad<1, MOTION><<<grid, block, 0, st>>>(a, partial); break;
+    case 2: k_pose_grad<2, MOTION><<<grid, block, 0, st>>>(a, partial); break;
+    default: k_pose_grad<3, MOTION><<<grid, block, 0, st>>>(a, partial); break;
+  }
+}
+
 void launch_pose_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
-                      const uint32_t* d_pairs, uint32_t accept, float* partial, double* out, uint32_t stride,
-                      cudaStream_t st) {
+                      const uint32_t* d_pairs, uint32_t accept, const Motion* motion, float* partial, double* out,
+                      uint32_t stride, cudaStream_t st) {
   const uint32_t blocks = pose_blocks(m.slots);
   if (blocks > 0u) {
-    StepArgs a{sp.frames, sp.n_views, m.cap, m.slots, m.P, m.M, m.V, m.SH, m.MSH, m.VSH, m.stats,
-               vb.splat, vb.tiles, vb.grad2d, vb.dir_grad, d_pairs, accept};
+    const StepArgs a = step_args(sp, m, vb, d_pairs, accept, motion);
     const dim3 grid(blocks, sp.n_views), block(128);
-    switch (degree) {
-      case 0: k_pose_grad<0><<<grid, block, 0, st>>>(a, partial); break;
-      case 1: k_pose_grad<1><<<grid, block, 0, st>>>(a, partial); break;
-      case 2: k_pose_grad<2><<<grid, block, 0, st>>>(a, partial); break;
-      default: k_pose_grad<3><<<grid, block, 0, st>>>(a, partial); break;
-    }
+    if (motion != nullptr) pose_degree<true>(degree, grid, block, st, a, partial);
+    else pose_degree<false>(degree, grid, block, st, a, partial);
   }
   k_pose_reduce<<<sp.n_views, 256, 0, st>>>(sp.frames, partial, blocks, out, stride);
+}
+
+uint32_t motion_blocks(uint32_t slots, int sm_count) {
+  return std::min((slots + 127u) / 128u, uint32_t(std::max(sm_count, 1)) * 4u);
+}
+
+void launch_motion_grad(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
+                        const uint32_t* d_pairs, uint32_t accept, const Motion& motion, float* partial, double* out,
+                        cudaStream_t st) {
+  const uint32_t blocks = motion_blocks(m.slots, sp.sm_count);
+  if (blocks > 0u) {
+    const StepArgs a = step_args(sp, m, vb, d_pairs, accept, &motion);
+    const dim3 grid(blocks, sp.n_views), block(128);
+    switch (degree) {
+      case 0: k_motion_grad<0><<<grid, block, 0, st>>>(a, partial); break;
+      case 1: k_motion_grad<1><<<grid, block, 0, st>>>(a, partial); break;
+      case 2: k_motion_grad<2><<<grid, block, 0, st>>>(a, partial); break;
+      default: k_motion_grad<3><<<grid, block, 0, st>>>(a, partial); break;
+    }
+  }
+  k_motion_reduce<<<dim3(std::max(motion.nodes, 1u), sp.n_views), 64, 0, st>>>(sp.frames, partial, blocks, out);
+}
+
+void launch_motion_bind(const Model& m, const Motion& motion, cudaStream_t st) {
+  if (m.slots == 0u || motion.nodes == 0u) return;
+  k_motion_bind<<<(m.slots + 127u) / 128u, 128, 0, st>>>(m.P, m.cap, m.slots, motion.rest, motion.nodes, motion.bind);
 }
 
 void launch_densify(const gs_frame_data* d_frame, const Model& m, const DensifyScratch& ds, const SortScratch& ss,

@@ -28,13 +28,14 @@ SNAP = {
     "pair_tile": (6, np.uint32, 1), "render_order": (7, np.uint32, 1), "depth_key": (8, np.uint32, 1),
     "image": (9, np.uint32, 1), "ranges": (10, np.uint32, 2), "tile_loss": (11, np.float32, 16),
     "pixel_dot": (12, np.float32, 1), "stats": (13, np.float32, 4), "pair_gaussian": (14, np.uint32, 1),
-    "pixel_out": (15, np.float32, 4), "spawn": (16, np.uint32, 1),
+    "pixel_out": (15, np.float32, 4), "spawn": (16, np.uint32, 1), "motion_bind": (17, np.uint32, 8),
 }
 
 EXPORTED = ["gs_last_error", "gs_create", "gs_destroy", "gs_model_init", "gs_model_info_get", "gs_model_export",
             "gs_model_moments", "gs_set_views", "gs_step", "gs_render", "gs_densify", "gs_reset_opacity",
             "gs_snapshot", "gs_set_tuning", "gs_get_tuning", "gs_dataset_set", "gs_set_views_dataset",
-            "gs_sort_pairs_noalloc", "gs_autotune"]
+            "gs_sort_pairs_noalloc", "gs_autotune", "gs_motion_nodes", "gs_motion_bind", "gs_set_view_motion",
+            "gs_motion_gradient"]
 
 
 class StepResult(ctypes.Structure):
@@ -94,6 +95,10 @@ def load(path: str = LIB_PATH):
     L.gs_set_views_dataset.argtypes = [vp, u32, vp, vp]
     L.gs_sort_pairs_noalloc.argtypes = [vp, vp, u32, u32, vp]
     L.gs_autotune.argtypes = [vp, u32, vp]
+    L.gs_motion_nodes.argtypes = [vp, u32, vp]
+    L.gs_motion_bind.argtypes = [vp]
+    L.gs_set_view_motion.argtypes = [vp, u32, vp]
+    L.gs_motion_gradient.argtypes = [vp, u32, vp, u32]
     for name in EXPORTED[1:]:
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -248,6 +253,25 @@ class Context:
         for k, v in kw.items():
             setattr(t, k, v)
         _check(self.lib.gs_set_tuning(self.h, ctypes.byref(t)))
+
+    def motion_nodes(self, nodes4: np.ndarray) -> None:
+        """Control nodes at rest, (K, 4) float32: position, 1 / (2 r^2); binds the slots."""
+        n = np.ascontiguousarray(nodes4, np.float32).reshape(-1, 4)
+        _check(self.lib.gs_motion_nodes(self.h, n.shape[0], _ptr(n) if n.size else None))
+
+    def motion_bind(self) -> None:
+        _check(self.lib.gs_motion_bind(self.h))
+
+    def set_view_motion(self, view: int, nodes20: np.ndarray) -> None:
+        """View `view`'s node motions, (K, 20) float32: rows of [R | b], turn, moved centre."""
+        n = np.ascontiguousarray(nodes20, np.float32).reshape(-1, 20)
+        _check(self.lib.gs_set_view_motion(self.h, view, _ptr(n)))
+
+    def motion_gradient(self, view: int, count: int) -> np.ndarray:
+        """(count, 6): dL/dshift, dL/dturn per node (world axes) of the latest step."""
+        out = np.zeros((count, 6), np.float64)
+        _check(self.lib.gs_motion_gradient(self.h, view, _ptr(out), count))
+        return out
 
     def autotune(self, steps_per_candidate: int = 2) -> Tuning:
         """gs_autotune on the views set last: the fastest tuning becomes the context's; the

@@ -39,6 +39,8 @@ FLAG_MASKED_TARGET = 1
 FLAG_SSIM = 4
 FLAG_POSE_GRAD = 8  # sum the view's camera pose gradient (StepResult.pose_grad)
 FLAG_POSE_ONLY = 16  # on the first view: gradients only, the model and its statistics stay
+FLAG_MOTION = 32  # the gaussians follow the view's node motions (Context.set_view_motion)
+FLAG_MOTION_GRAD = 64  # sum the gradient per motion node (Context.motion_gradient)
 FLAG_SPARSE_ADAM = 128
 BETA1, BETA2, EPSILON = 0.9, 0.999, 1e-15  # trainer.cpp:68-70
 
