@@ -8,6 +8,10 @@
 //            [--gt-gaussians N] [--init-gaussians N] [--cameras N] [--width 360] [--no-masks]
 //            [--head-weight W] [--refine-poses] [--pose-lr shift,turn] [--pose-lr-final F] [--pose-from N]
 //            [--eval-pose-steps N] [--pose-out poses.json] [--refine-exposure]
+//            [--refine-motion] [--motion-nodes 64] [--motion-lr shift,turn] [--motion-lr-final F] [--motion-from N]
+//            [--motion-reg decay,rigidity,smoothness,center] [--motion-out motion.json]
+//            [--eval-rest <capture_dir>] (held-out views of a twin capture with the subject standing still:
+//            the model at rest against it)
 // <dataset> is a capture folder (transforms.json; PNG/PPM images, resized so the short side
 // is --width; initial gaussians from its point cloud or random, up to --init-gaussians,
 // 150000 by default; the reference's default options with the schedule scaled to --iters)
@@ -117,7 +121,7 @@ int main(int argc, char** argv) {
       options.max_gaussians = syn.max_gaussians;
     }
     uint32_t iterations = 3000, eval_every = 1000;
-    std::string json_path, pose_out;
+    std::string json_path, pose_out, motion_out, eval_rest;
     for (int i = 3; i < argc; ++i) {
       const std::string arg = argv[i];
       auto next = [&]() -> const char* {
@@ -153,6 +157,19 @@ int main(int argc, char** argv) {
       else if (arg == "--eval-pose-steps") options.eval_pose_steps = uint32_t(std::atoi(next()));
       else if (arg == "--pose-out") pose_out = next();
       else if (arg == "--refine-exposure") options.refine_exposure = true;
+      else if (arg == "--refine-motion") options.refine_motion = true;
+      else if (arg == "--motion-nodes") options.motion_nodes = uint32_t(std::atoi(next()));
+      else if (arg == "--motion-lr") {
+        if (std::sscanf(next(), "%f,%f", &options.lr_motion_shift, &options.lr_motion_turn) != 2)
+          throw std::runtime_error("--motion-lr needs shift,turn");
+      } else if (arg == "--motion-lr-final") options.lr_motion_final = float(std::atof(next()));
+      else if (arg == "--motion-from") options.motion_from = uint32_t(std::atoi(next()));
+      else if (arg == "--motion-reg") {
+        if (std::sscanf(next(), "%f,%f,%f,%f", &options.motion_decay, &options.motion_rigidity,
+                        &options.motion_smoothness, &options.motion_center) != 4)
+          throw std::runtime_error("--motion-reg needs decay,rigidity,smoothness,center");
+      } else if (arg == "--motion-out") motion_out = next();
+      else if (arg == "--eval-rest") eval_rest = next();
       else throw std::runtime_error("unknown option " + arg);
     }
     // The schedule (densify window, SH degree interval) scales with the iterations, as
@@ -193,8 +210,12 @@ int main(int argc, char** argv) {
                 source.c_str(), dataset.frames.size(), dataset.holdout_count(), dataset.camera_extent, init.count,
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
 
+    gs::Dataset rest;
+    if (!eval_rest.empty()) rest = gs::load_dataset(eval_rest, width);
     gs::CudaContext ctx;
     gs::Trainer trainer(ctx, std::move(dataset), init, options);
+    if (options.refine_motion)
+      std::printf("motion: %zu nodes from step %u\n", trainer.motion_nodes().size(), options.motion_from);
     std::vector<std::pair<uint32_t, double>> evals;
     double train_s = 0.0;
     while (!trainer.finished()) {
@@ -211,11 +232,18 @@ int main(int argc, char** argv) {
       if (options.refine_exposure)
         std::printf("  exposure: luminance gain %.3f..%.3f, tint spread %.4f over %u updates\n", s.exposure_low,
                     s.exposure_high, s.exposure_tint, s.exposure_updates);
+      if (options.refine_motion)
+        std::printf("  motion: shift %.4f (max %.4f), turn %.3f deg (max %.3f) over %u view updates\n",
+                    s.motion_shift_mean, s.motion_shift_max, s.motion_turn_mean, s.motion_turn_max, s.motion_updates);
       const gs::EvalResult e = trainer.evaluate();
       std::printf("  eval: held-out PSNR %.2f dB, SSIM %.4f over %u views", e.psnr, e.ssim, e.views);
       if (e.aligned) std::printf(" (%.2f dB at the poses as given)", e.psnr_unaligned);
       if (e.head_views) std::printf("; head %.2f dB over %u views", e.head_psnr, e.head_views);
       std::printf("\n");
+      if (!rest.frames.empty()) {
+        const gs::EvalResult r = trainer.evaluate_at_rest(rest);
+        std::printf("  at rest: held-out PSNR %.2f dB, SSIM %.4f over %u views\n", r.psnr, r.ssim, r.views);
+      }
       evals.push_back({s.step, e.psnr});
     }
     const gs::TrainStats& s = trainer.stats();
@@ -239,6 +267,32 @@ int main(int argc, char** argv) {
         poses << ",[0,0,0,1]]}";
       }
       poses << "\n]}\n";
+    }
+    if (!motion_out.empty()) {
+      // The nodes at rest (x, y, z, radius) and every view's motion of each: turn (axis-angle) and shift.
+      std::ofstream m(motion_out);
+      m.precision(7);
+      m << "{\"nodes\": [";
+      const auto& nodes = trainer.motion_nodes();
+      for (size_t k = 0; k < nodes.size(); ++k)
+        m << (k ? "," : "") << "[" << nodes[k].position[0] << "," << nodes[k].position[1] << ","
+          << nodes[k].position[2] << "," << nodes[k].radius << "]";
+      m << "],\n\"frames\": [";
+      for (size_t f = 0; f < trainer.dataset().frames.size(); ++f) {
+        std::string turns, shifts;
+        for (size_t k = 0; k < nodes.size(); ++k) {
+          float turn[3], shift[3];
+          trainer.node_motion(f, uint32_t(k), turn, shift);
+          char buf[128];
+          std::snprintf(buf, sizeof(buf), "%s[%.7g,%.7g,%.7g]", k ? "," : "", turn[0], turn[1], turn[2]);
+          turns += buf;
+          std::snprintf(buf, sizeof(buf), "%s[%.7g,%.7g,%.7g]", k ? "," : "", shift[0], shift[1], shift[2]);
+          shifts += buf;
+        }
+        m << (f ? "," : "") << "\n{\"holdout\": " << (trainer.dataset().frames[f].holdout ? "true" : "false")
+          << ", \"turn\": [" << turns << "], \"shift\": [" << shifts << "]}";
+      }
+      m << "\n]}\n";
     }
     gs::SplatScene out = trainer.export_scene();
     gs::convert_convention(out, gs::AxisConvention::RDF);  // what .ply readers expect

@@ -8,19 +8,18 @@
 // backgrounds, learning-rate, SH-degree and loss-weight schedules, densification and
 // opacity-reset schedules, statistics, evaluation and export.
 //
-// Camera pose refinement, exposure refinement and head weighting follow the reference
-// (trainer.cpp:1164-1394, 1691-1771; trainer.h:60-131): pose corrections per training
+// Camera pose refinement, exposure refinement, subject motion and head weighting follow
+// the reference (trainer.cpp:1164-1771; trainer.h:60-131): pose corrections per training
 // view by Adam on the pose gradient the step sums on the GPU, held-out views aligned
-// before evaluation, per-view colour gains fitted from the forward pass's sums, and the
-// head region's pixels weighted in the loss.
+// before evaluation, per-view colour gains fitted from the forward pass's sums, per-view
+// rigid motions of control nodes the gaussians follow (SC-GS), and the head region's
+// pixels weighted in the loss.
 //
 // Extensions: `views_per_step` > 1 renders and differentiates that many views in one
 // launch per pass and takes one Adam step on their summed gradients (batched training;
 // a step still counts one iteration; each view still gets its own pose gradient and gain
 // fit), and the retune steps run gs_autotune, which picks pixels per thread, the backward
 // batch and the sort digit width.
-// Not supported on this path: subject-motion refinement (the constructor throws when it
-// is asked for).
 #pragma once
 
 #include <array>
@@ -77,7 +76,24 @@ struct TrainOptions {
   float lr_pose_final = 1.0f;     // the rates decay exponentially to this fraction by the last step
   uint32_t eval_pose_steps = 8;
   float eval_pose_step = 0.005f;  // the alignment's first step, times the camera extent
-  bool refine_motion = false;     // not supported here
+  // Subject motion (trainer.h:83-117): `motion_nodes` control nodes spread over the
+  // initial gaussians (k-means); in each training view every node moves rigidly (a turn
+  // about itself and a shift) and each gaussian follows its 4 nearest nodes. The motions
+  // are trained by Adam from step motion_from, kept small (motion_decay), alike between
+  // neighbouring nodes (motion_rigidity) and neighbouring views (motion_smoothness), and
+  // centred on the rest pose over the views (motion_center); penalties in units of the
+  // node spacing. The model stays the subject at rest; held-out views take the motion of
+  // the training views next to them.
+  bool refine_motion = false;
+  uint32_t motion_nodes = 64;     // at most 128
+  uint32_t motion_from = 300;
+  float lr_motion_shift = 2e-3f;  // per update, times the camera extent
+  float lr_motion_turn = 3e-3f;   // radians per update
+  float lr_motion_final = 0.1f;   // the rates decay exponentially to this fraction by the last step
+  float motion_decay = 1e-4f;
+  float motion_rigidity = 1e-3f;
+  float motion_smoothness = 1e-2f;
+  float motion_center = 1e-2f;
   // Exposure refinement (trainer.h:121-131): per-view colour gains fitted from the
   // forward pass's sums, blended in at exposure_rate from step exposure_from, used
   // divided by their geometric mean over the trained views.
@@ -141,6 +157,10 @@ struct TrainStats {
   uint32_t pose_updates = 0;
   double exposure_low = 1.0, exposure_high = 1.0, exposure_tint = 0.0;  // 5th/95th percentile luminance gain
   uint32_t exposure_updates = 0;
+  uint32_t motion_nodes = 0;
+  double motion_shift_mean = 0.0, motion_shift_max = 0.0;  // dataset units
+  double motion_turn_mean = 0.0, motion_turn_max = 0.0;    // degrees
+  uint32_t motion_updates = 0;                             // view updates
   struct Timing {
     double wall_ms = 0.0;  // moving averages per step
     double gpu_ms = 0.0;
@@ -184,11 +204,17 @@ class Trainer {
   const TrainOptions& options() const { return options_; }
   const Dataset& dataset() const { return dataset_; }
 
-  // The current model from `camera` over `background`: RGBA8, alpha = coverage.
+  // The current model (at rest) from `camera` over `background`: RGBA8, alpha = coverage.
   std::vector<uint8_t> render(const Camera& camera, const float background[3]);
-  // Held-out views over a black background.
+  // Held-out views over a black background (with the subject's motion interpolated from
+  // the views next to them, when refining motion).
   EvalResult evaluate();
+  // View `frame` as its camera saw it: with its pose correction and, when refining
+  // motion, the subject's motion then.
   std::vector<uint8_t> render_view(size_t frame, const float background[3]);
+  // The held-out views of another dataset of the same subject standing still (a twin
+  // capture): the model at rest against it, gains 1, no motion (trainer.h:283).
+  EvalResult evaluate_at_rest(const Dataset& other);
   // A view's camera with its pose correction (the dataset's pose without refinement).
   Camera camera_for(size_t frame) const;
   // A view's exposure gains (the photo is divided by them): centred, interpolated for views
@@ -207,6 +233,26 @@ class Trainer {
   Gradients first_step_gradients();
   // The pose gradient of the latest pose update: dL/dd xyz, dL/dw xyz.
   const double* last_pose_gradient() const { return last_pose_grad_; }
+
+  // Subject motion: the control nodes at rest (empty without refine_motion).
+  struct MotionNode {
+    float position[3];
+    float radius;  // gaussians weigh it by exp(-d^2 / (2 radius^2))
+  };
+  const std::vector<MotionNode>& motion_nodes() const { return nodes_; }
+  // A node's motion in view `frame`: turn (axis-angle, radians) and shift.
+  void node_motion(size_t frame, uint32_t node, float turn[3], float shift[3]) const;
+  // Testing: sets it (the view then counts as trained).
+  void set_node_motion(size_t frame, uint32_t node, const float turn[3], const float shift[3]);
+  // Testing: the motion gradient of the latest motion update (image loss only), 6 per
+  // node: dL/dshift xyz, dL/dturn xyz (world axes).
+  const std::vector<double>& last_motion_gradient() const { return last_motion_grad_; }
+  // Testing: each slot's 4 nodes and weights.
+  struct MotionBinding {
+    std::vector<uint32_t> nodes;
+    std::vector<float> weights;
+  };
+  MotionBinding motion_binding();
   struct DebugSnapshot {
     std::vector<uint32_t> pixel_count;
     std::vector<float> pixel_grad;
@@ -232,15 +278,36 @@ class Trainer {
     double m[6] = {}, v[6] = {};  // Adam moments: shift xyz, turn xyz
     uint32_t updates = 0;
   };
+  struct NodeMotion {
+    float turn[3] = {0, 0, 0};  // axis-angle, radians
+    float shift[3] = {0, 0, 0};
+    double m[6] = {};           // Adam: shift xyz, turn xyz
+    double v[2] = {};           // one second moment per vector: shift, turn
+  };
+  using ViewMotion = std::vector<NodeMotion>;
 
   void next_view(size_t& frame, float background[3]);
   void run_step(const std::vector<size_t>& frames, const std::vector<std::array<float, 3>>& backgrounds,
                 bool profile);
   void write_frame(gs_frame_data& f, const Camera& camera, const float background[3], uint32_t step, bool ssim,
                    bool masked, uint32_t flags = 0u, const float* gain = nullptr) const;
-  // One held-out measurement (forward only) or alignment probe of `camera` against frame
-  // `frame`'s image over black.
-  void run_eval_view(const Camera& camera, size_t frame, const float gain[3], uint32_t flags, gs_step_result& r);
+  // One held-out measurement (forward only) or alignment probe of `camera` against the
+  // dataset's image `frame` (or `rgba`, another dataset's, when not null) over black, the
+  // subject moved by `motion` when not null.
+  void run_eval_view(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3], uint32_t flags,
+                     const ViewMotion* motion, gs_step_result& r);
+  EvalResult evaluate_views(const Dataset& ds, bool own);
+  std::vector<uint8_t> render_with(const Camera& camera, const float background[3], const ViewMotion* motion);
+  // Subject motion.
+  void place_nodes(const SplatScene& initial);  // k-means over the initial gaussians, then gs_motion_nodes
+  void bind_motion();                           // gs_motion_bind
+  bool refines_motion_at(uint32_t step) const { return !nodes_.empty() && step >= options_.motion_from; }
+  bool uses_motion() const;                     // some view's motion has been trained
+  ViewMotion view_motion(size_t frame) const;   // its own once trained, else between its neighbours'
+  void start_motion(size_t frame);              // before a training view's first motion update
+  void set_motion_table(uint32_t view, const ViewMotion& motion);  // gs_set_view_motion
+  void update_motion(const double* grad, size_t frame);            // Adam step from the image gradient + penalties
+  void update_motion_stats();
   bool refines_pose_at(uint32_t step) const { return options_.refine_poses && step >= options_.pose_from; }
   bool refines_exposure_at(uint32_t step) const {
     return options_.refine_exposure && step >= options_.exposure_from;
@@ -248,7 +315,8 @@ class Trainer {
   void update_pose(const double grad[6], size_t frame);
   static void apply_pose_step(PoseFix& fix, const double step[6]);
   static Camera with_fix(Camera camera, const PoseFix& fix);  // [R | t] -> [E R | E t + d]
-  PoseFix align_camera(const Camera& camera, size_t frame, const float gain[3], const PoseFix* start);
+  PoseFix align_camera(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3],
+                       const ViewMotion* motion, const PoseFix* start);
   PoseFix neighbour_fix(size_t frame) const;
   void update_pose_stats();
   void update_exposure(const double fit[8], size_t frame);
@@ -282,6 +350,13 @@ class Trainer {
   double last_pose_grad_[6] = {0, 0, 0, 0, 0, 0};
   std::vector<std::array<double, 3>> gain_log_;  // per frame: log gain per channel, as measured (blended)
   std::vector<uint32_t> gain_updates_;
+  std::vector<MotionNode> nodes_;
+  std::vector<std::vector<uint32_t>> node_neighbors_;  // up to 6 nearest, per node
+  float node_spacing_ = 1.0f;                          // median node radius
+  std::vector<ViewMotion> motion_;                     // per dataset frame (empty without nodes)
+  std::vector<uint32_t> motion_updates_;               // per dataset frame
+  std::vector<double> last_motion_grad_;
+  uint32_t bound_at_ = 0;  // step of the latest binding
 };
 
 }  // namespace gs

@@ -115,7 +115,8 @@ void Trainer::update_pose(const double grad[6], size_t frame) {
   apply_pose_step(p, step);
 }
 
-Trainer::PoseFix Trainer::align_camera(const Camera& camera, size_t frame, const float gain[3], const PoseFix* start) {
+Trainer::PoseFix Trainer::align_camera(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3],
+                                       const ViewMotion* motion, const PoseFix* start) {
   // align_camera (trainer.cpp:1164-1212): from the better of the given pose and `start`,
   // normalised gradient steps on the L1 loss that grow by 1.5 after a step that lowered it
   // and halve (from the best pose) after one that did not; turns count as the shift they
@@ -125,7 +126,7 @@ Trainer::PoseFix Trainer::align_camera(const Camera& camera, size_t frame, const
   double best_loss = std::numeric_limits<double>::infinity(), best_grad[6] = {0, 0, 0, 0, 0, 0};
   auto try_fix = [&](const PoseFix& fix) {
     gs_step_result r;
-    run_eval_view(with_fix(camera, fix), frame, gain, GS_FLAG_POSE_GRAD | GS_FLAG_POSE_ONLY, r);
+    run_eval_view(with_fix(camera, fix), frame, rgba, gain, GS_FLAG_POSE_GRAD | GS_FLAG_POSE_ONLY, motion, r);
     const double loss = r.losses[0][3];
     if (!(loss < best_loss)) return false;
     best = fix;

@@ -3,7 +3,7 @@
 // set_view_stats, :778-805), the densify and opacity-reset schedule (after_step,
 // :932-945; densify, :1083-1119; reset_opacity, :1121-1128), evaluation (evaluate_views,
 // :1244-1292) and export (export_scene, :1773-1800). Pose and exposure refinement are in
-// refine.cpp.
+// refine.cpp, subject motion in motion.cpp.
 #include "gs/trainer.h"
 
 #include <algorithm>
@@ -55,8 +55,6 @@ void Trainer::check(int code, const char* what) const { detail::check_status(cod
 Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, const TrainOptions& options)
     : ctx_(ctx), dataset_(std::move(dataset)), options_(options), rng_(options.seed) {
   if (dataset_.frames.empty() || dataset_.width == 0) throw std::runtime_error("Trainer: empty dataset");
-  if (options_.refine_motion)
-    throw std::runtime_error("Trainer: subject-motion refinement is not available on the CUDA path");
   if (options_.views_per_step < 1 || options_.views_per_step > GS_MAX_VIEWS)
     throw std::runtime_error("Trainer: views_per_step must be 1.." + std::to_string(GS_MAX_VIEWS));
   if (options_.sh_degree < 0 || options_.sh_degree > 3) throw std::runtime_error("Trainer: sh_degree must be 0..3");
@@ -110,6 +108,7 @@ Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, c
       ptr.push_back(f.rgba.data());
     }
     check(gs_dataset_set(gpu_, uint32_t(ptr.size()), w.data(), h.data(), ptr.data()), "Trainer: gs_dataset_set");
+    if (options_.refine_motion) place_nodes(initial);
   } catch (...) {
     gs_destroy(gpu_);
     gpu_ = nullptr;
@@ -183,15 +182,19 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   std::vector<gs_frame_data> fd(k);
   std::vector<uint32_t> images(k);
   std::vector<Camera> cams(k);
-  const bool pose = refines_pose_at(step), exposure = refines_exposure_at(step);
+  const bool pose = refines_pose_at(step), exposure = refines_exposure_at(step), motion = refines_motion_at(step);
   for (uint32_t v = 0; v < k; ++v) {
     cams[v] = camera_for(frames[v]);
     const std::array<float, 3> gain = exposure_gain(frames[v]);
-    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked, pose ? GS_FLAG_POSE_GRAD : 0u,
-                gain.data());
+    if (motion) start_motion(frames[v]);
+    const uint32_t flags =
+        (pose ? GS_FLAG_POSE_GRAD : 0u) | (motion ? GS_FLAG_MOTION | GS_FLAG_MOTION_GRAD : 0u);
+    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked, flags, gain.data());
     images[v] = uint32_t(frames[v]);
   }
   check(gs_set_views_dataset(gpu_, k, fd.data(), images.data()), "Trainer::step: gs_set_views_dataset");
+  if (motion)
+    for (uint32_t v = 0; v < k; ++v) set_motion_table(v, motion_[frames[v]]);
   if (retune_due(step)) {
     gs_tuning chosen;
     check(gs_autotune(gpu_, 2, &chosen), "Trainer::step: gs_autotune");
@@ -201,12 +204,19 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   check(gs_step(gpu_, GS_STEP_TRAIN | (profile ? GS_STEP_PROFILE : 0u), &r), "Trainer::step: gs_step");
   // A step whose pairs did not fit left the model alone: no pose or gain update either.
   if (!r.overflow) {
+    std::vector<double> motion_grad(nodes_.size() * 6);
     for (uint32_t v = 0; v < k; ++v) {
       if (pose) update_pose(r.pose_grad[v], frames[v]);
       if (exposure) update_exposure(r.fit[v], frames[v]);
+      if (motion) {
+        check(gs_motion_gradient(gpu_, v, motion_grad.data(), uint32_t(nodes_.size())),
+              "Trainer::step: gs_motion_gradient");
+        update_motion(motion_grad.data(), frames[v]);
+      }
     }
     if (pose) update_pose_stats();
     if (exposure) update_exposure_stats();
+    if (motion) update_motion_stats();
   }
   // Statistics: the views' sums (read_slot / set_view_stats), averaged over the views.
   const double lambda = lambda_at(step);
@@ -271,9 +281,18 @@ uint32_t Trainer::steps(uint32_t count) {
 
 void Trainer::after_step() {
   const uint32_t t = stats_.step;
-  if (t >= options_.densify_until) return;
-  if (t > options_.densify_from && options_.densify_interval > 0 && t % options_.densify_interval == 0) densify();
-  if (options_.opacity_reset_interval > 0 && t % options_.opacity_reset_interval == 0) reset_opacity();
+  bool densified = false;
+  if (t < options_.densify_until) {
+    if (t > options_.densify_from && options_.densify_interval > 0 && t % options_.densify_interval == 0) {
+      densify();  // gs_densify binds the new gaussians to their nodes
+      densified = true;
+      bound_at_ = t;
+    }
+    if (options_.opacity_reset_interval > 0 && t % options_.opacity_reset_interval == 0) reset_opacity();
+  }
+  // The gaussians drift away from their nodes: bind them again every 100 steps
+  // (trainer.cpp:949-950).
+  if (!nodes_.empty() && !densified && t >= bound_at_ + 100) bind_motion();
 }
 
 void Trainer::densify() {
@@ -303,38 +322,66 @@ void Trainer::reset_opacity() {
 
 
 std::vector<uint8_t> Trainer::render(const Camera& camera, const float background[3]) {
+  return render_with(camera, background, nullptr);
+}
+
+std::vector<uint8_t> Trainer::render_with(const Camera& camera, const float background[3], const ViewMotion* motion) {
   gs_frame_data f;
-  detail::frame_geometry(f, camera, stats_.slots, sh_stride_, int(sh_degree_at(stats_.step)), 0u, background);
+  const bool moved = motion != nullptr && !nodes_.empty();
+  detail::frame_geometry(f, camera, stats_.slots, sh_stride_, int(sh_degree_at(stats_.step)),
+                         moved ? GS_FLAG_MOTION : 0u, background);
+  if (moved) set_motion_table(0, *motion);  // gs_render moves the subject by view 0's motion
   std::vector<uint8_t> out(size_t(camera.width) * camera.height * 4);
   check(gs_render(gpu_, &f, out.data()), "Trainer::render");
   return out;
 }
 
 std::vector<uint8_t> Trainer::render_view(size_t frame, const float background[3]) {
-  return render(camera_for(frame), background);
+  if (!uses_motion()) return render_with(camera_for(frame), background, nullptr);
+  const ViewMotion motion = view_motion(frame);
+  return render_with(camera_for(frame), background, &motion);
 }
 
-void Trainer::run_eval_view(const Camera& camera, size_t frame, const float gain[3], uint32_t flags,
-                            gs_step_result& r) {
+void Trainer::run_eval_view(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3],
+                            uint32_t flags, const ViewMotion* motion, gs_step_result& r) {
   // A measurement renders forward only with SSIM; an alignment probe trains with only the
   // camera moving (pose gradient, the model untouched) on L1 (trainer.cpp:1180-1183, 1250).
   const float black[3] = {0.0f, 0.0f, 0.0f};
   const bool align = (flags & GS_FLAG_POSE_ONLY) != 0u;
+  const bool moved = motion != nullptr && !nodes_.empty();
   gs_frame_data f;
-  write_frame(f, camera, black, stats_.step, !align, options_.masked, flags, gain);
-  const uint32_t image = uint32_t(frame);
-  check(gs_set_views_dataset(gpu_, 1, &f, &image), "Trainer::evaluate: gs_set_views_dataset");
+  write_frame(f, camera, black, stats_.step, !align, options_.masked, flags | (moved ? GS_FLAG_MOTION : 0u), gain);
+  if (rgba != nullptr) {  // another dataset's image, uploaded with the step
+    check(gs_set_views(gpu_, 1, &f, &rgba), "Trainer::evaluate: gs_set_views");
+  } else {
+    const uint32_t image = uint32_t(frame);
+    check(gs_set_views_dataset(gpu_, 1, &f, &image), "Trainer::evaluate: gs_set_views_dataset");
+  }
+  if (moved) set_motion_table(0, *motion);
   check(gs_step(gpu_, align ? GS_STEP_TRAIN : 0u, &r), "Trainer::evaluate: gs_step");
 }
 
-EvalResult Trainer::evaluate() {
-  // evaluate_views (trainer.cpp:1244-1292) on this trainer's own dataset.
+EvalResult Trainer::evaluate() { return evaluate_views(dataset_, true); }
+
+EvalResult Trainer::evaluate_at_rest(const Dataset& other) {
+  for (const DatasetFrame& f : other.frames) {
+    const Camera c = dataset_camera(other, f);
+    if (f.holdout && f.rgba.size() != size_t(c.width) * c.height * 4)
+      throw std::runtime_error("Trainer::evaluate_at_rest: frame " + f.name + " has the wrong image size");
+  }
+  return evaluate_views(other, false);
+}
+
+EvalResult Trainer::evaluate_views(const Dataset& ds, bool own) {
+  // evaluate_views (trainer.cpp:1244-1292): the held-out views of this trainer's own
+  // dataset (poses, gains and motions as trained) or of another (the subject at rest).
   EvalResult result;
   const bool align = options_.refine_poses && options_.eval_pose_steps > 0;
   double sums[5] = {0, 0, 0, 0, 0}, unaligned = 0.0;
-  auto measure = [&](const Camera& cam, size_t i, const float gain[3], double* psnr_out) {
+  const bool moving = own && uses_motion();
+  auto measure = [&](const Camera& cam, size_t i, const float gain[3], const ViewMotion* motion, double* psnr_out) {
     gs_step_result r;
-    run_eval_view(cam, i, gain, 0u, r);
+    run_eval_view(cam, i, own ? nullptr : ds.frames[i].rgba.data(), gain, 0u, motion, r);
     const ViewLosses l = view_losses(r.losses[0], cam.width, cam.height, lambda_at(stats_.step), true);
     if (psnr_out) {
       *psnr_out += l.psnr;
@@ -348,20 +395,23 @@ EvalResult Trainer::evaluate() {
       sums[4] += 1.0;
     }
   };
-  for (size_t i = 0; i < dataset_.frames.size(); ++i) {
-    if (!dataset_.frames[i].holdout) continue;
-    float gain[3];
-    view_gain(i, gain);
-    const Camera given = dataset_camera(dataset_, dataset_.frames[i]);
+  for (size_t i = 0; i < ds.frames.size(); ++i) {
+    if (!ds.frames[i].holdout) continue;
+    float gain[3] = {1.0f, 1.0f, 1.0f};
+    if (own) view_gain(i, gain);
+    ViewMotion motion;
+    if (moving) motion = view_motion(i);
+    const ViewMotion* m = moving ? &motion : nullptr;
+    const Camera given = dataset_camera(ds, ds.frames[i]);
     PoseFix fix{};
     if (align) {
-      measure(given, i, gain, &unaligned);
+      measure(given, i, gain, m, &unaligned);
       // A view aligned before starts where it got to; otherwise between its neighbours.
-      const PoseFix start = pose_fix_[i].updates > 0 ? pose_fix_[i] : neighbour_fix(i);
-      fix = align_camera(given, i, gain, &start);
-      pose_fix_[i] = fix;
+      const PoseFix start = !own ? PoseFix{} : pose_fix_[i].updates > 0 ? pose_fix_[i] : neighbour_fix(i);
+      fix = align_camera(given, i, own ? nullptr : ds.frames[i].rgba.data(), gain, m, &start);
+      if (own) pose_fix_[i] = fix;
     }
-    measure(with_fix(given, fix), i, gain, nullptr);
+    measure(with_fix(given, fix), i, gain, m, nullptr);
     ++result.views;
   }
   if (result.views > 0) {

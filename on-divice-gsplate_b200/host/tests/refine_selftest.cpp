@@ -1,13 +1,19 @@
-// GPU checks of gs::Trainer's pose and exposure refinement, driven by tests/test_gpu_host.py.
-// They follow the reference's own tests of these features (engine/tests/test_trainer.cpp:
-// test_pose_gradient :404-460, test_pose_recovery :505-547, test_exposure_recovery
-// :700-742), plus the held-out alignment of evaluate (trainer.cpp:1164-1212, 1244-1292):
+// GPU checks of gs::Trainer's pose, exposure and subject-motion refinement, driven by
+// tests/test_gpu_host.py. They follow the reference's own tests of these features
+// (engine/tests/test_trainer.cpp: test_pose_gradient :404-460, test_pose_recovery
+// :505-547, test_motion_gradient :549-606, test_motion_recovery :660-690,
+// test_exposure_recovery :700-742, test_motion_batched :744-782), plus the held-out
+// alignment of evaluate (trainer.cpp:1164-1212, 1244-1292):
 //   gs_refine_selftest pose-gradient <lambda>
 //   gs_refine_selftest pose-recovery
 //   gs_refine_selftest exposure-recovery
 //   gs_refine_selftest align
+//   gs_refine_selftest motion-gradient <nodes>
+//   gs_refine_selftest motion-recovery
+//   gs_refine_selftest motion-batched
 // Each prints one JSON line with what it measured and exits 1 when its check fails.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -300,6 +306,194 @@ int align() {
   return a.views == 2 && a.aligned && a.psnr > a.psnr_unaligned + 0.5 && b.psnr > a.psnr_unaligned + 0.5 ? 0 : 1;
 }
 
+int motion_gradient(uint32_t wanted) {
+  // With every node at rest a shift s of node k moves its gaussians by w s and a turn u
+  // about it moves them by w u x (p - n_k) and turns their orientation by w u, so the
+  // motion gradient is what the per-gaussian gradients imply. SH degree 0.
+  gs::Dataset ds = test_dataset(64, 48, 2, true, 3);
+  const gs::SplatScene scene = test_scene(wanted > 64 ? 400 : 120, 0, 9);
+  const float bg[3] = {0.2f, 0.3f, 0.4f};
+  gs::TrainOptions o = frozen_options(0, true);
+  o.refine_motion = true;
+  o.motion_from = 0;
+  o.motion_nodes = wanted;
+  o.lr_motion_shift = o.lr_motion_turn = 0.0f;  // measure only
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  const size_t nodes = t.motion_nodes().size();
+  t.step_on(1, bg);
+  const std::vector<double>& g = t.last_motion_gradient();
+  const gs::Trainer::Gradients grads = t.first_step_gradients();
+  const gs::Trainer::MotionBinding bind = t.motion_binding();
+  std::vector<double> expected(nodes * 6, 0.0);
+  double weight_error = 0.0;
+  for (uint32_t i = 0; i < scene.count; ++i) {
+    const float* gp = &grads.params[size_t(i) * 16];
+    const float* q = &scene.rotations[i * 4];
+    const double len = std::sqrt(double(q[0]) * q[0] + double(q[1]) * q[1] + double(q[2]) * q[2] + double(q[3]) * q[3]);
+    const double w = q[0] / len, u[3] = {q[1] / len, q[2] / len, q[3] / len};
+    const double gw = gp[8] * len, gu[3] = {gp[9] * len, gp[10] * len, gp[11] * len};
+    const double ug[3] = {u[1] * gu[2] - u[2] * gu[1], u[2] * gu[0] - u[0] * gu[2], u[0] * gu[1] - u[1] * gu[0]};
+    double tau[3], total = 0.0;
+    for (int k = 0; k < 3; ++k) tau[k] = 0.5 * (-gw * u[k] + w * gu[k] + ug[k]);
+    for (int j = 0; j < 4; ++j) {
+      const double wk = bind.weights[i * 4 + j];
+      total += wk;
+      if (wk == 0.0) continue;
+      const uint32_t k = bind.nodes[i * 4 + j];
+      double r[3];
+      for (int c = 0; c < 3; ++c) r[c] = double(scene.positions[i * 3 + c]) - t.motion_nodes()[k].position[c];
+      const double rg[3] = {r[1] * gp[2] - r[2] * gp[1], r[2] * gp[0] - r[0] * gp[2], r[0] * gp[1] - r[1] * gp[0]};
+      for (int c = 0; c < 3; ++c) {
+        expected[k * 6 + c] += wk * gp[c];
+        expected[k * 6 + 3 + c] += wk * (rg[c] + tau[c]);
+      }
+    }
+    weight_error = std::max(weight_error, std::fabs(total - 1.0));
+  }
+  double worst = 0.0, largest = 0.0;
+  for (size_t k = 0; k < nodes * 6 && k < g.size(); ++k) {
+    worst = std::max(worst, std::fabs(g[k] - expected[k]));
+    largest = std::max(largest, std::fabs(expected[k]));
+  }
+  std::printf("{\"nodes\": %zu, \"worst\": %.4g, \"largest\": %.4g, \"weight_error\": %.3g}\n", nodes, worst,
+              largest, weight_error);
+  return nodes == wanted && g.size() == nodes * 6 && weight_error < 1e-5 && largest > 0.0 &&
+                 worst <= 1e-3 * largest
+             ? 0
+             : 1;
+}
+
+// Where the gaussians are in view `frame`: sum_k w_k (R_k (p - n_k) + n_k + s_k).
+std::vector<double> moved_positions(const gs::Trainer& t, const gs::Trainer::MotionBinding& bind,
+                                    const gs::SplatScene& scene, size_t frame) {
+  std::vector<double> out(size_t(scene.count) * 3, 0.0);
+  for (uint32_t i = 0; i < scene.count; ++i)
+    for (int j = 0; j < 4; ++j) {
+      const double wk = bind.weights[i * 4 + j];
+      if (wk == 0.0) continue;
+      const uint32_t k = bind.nodes[i * 4 + j];
+      float turn[3], shift[3];
+      t.node_motion(frame, k, turn, shift);
+      const double th = std::sqrt(double(turn[0]) * turn[0] + double(turn[1]) * turn[1] + double(turn[2]) * turn[2]);
+      double a[3] = {0, 0, 0};
+      if (th > 0)
+        for (int c = 0; c < 3; ++c) a[c] = turn[c] / th;
+      const float* n = t.motion_nodes()[k].position;
+      double r[3];
+      for (int c = 0; c < 3; ++c) r[c] = double(scene.positions[i * 3 + c]) - n[c];
+      const double ar[3] = {a[1] * r[2] - a[2] * r[1], a[2] * r[0] - a[0] * r[2], a[0] * r[1] - a[1] * r[0]};
+      const double dot = a[0] * r[0] + a[1] * r[1] + a[2] * r[2];
+      for (int c = 0; c < 3; ++c)
+        out[i * 3 + c] +=
+            wk * (r[c] * std::cos(th) + ar[c] * std::sin(th) + a[c] * dot * (1 - std::cos(th)) + n[c] + shift[c]);
+    }
+  return out;
+}
+
+// Mean on-screen distance (px) between two sets of positions seen by `cam`.
+double screen_distance(const gs::Camera& cam, const std::vector<double>& a, const std::vector<double>& b) {
+  auto project = [&](const double* p, double out[2]) {
+    double t[3];
+    for (int r = 0; r < 3; ++r) {
+      t[r] = cam.translation[r];
+      for (int c = 0; c < 3; ++c) t[r] += cam.rotation[r * 3 + c] * p[c];
+    }
+    out[0] = cam.fx * t[0] / t[2] + cam.cx;
+    out[1] = cam.fy * t[1] / t[2] + cam.cy;
+  };
+  double sum = 0.0;
+  const size_t n = a.size() / 3;
+  for (size_t i = 0; i < n; ++i) {
+    double pa[2], pb[2];
+    project(&a[i * 3], pa);
+    project(&b[i * 3], pb);
+    sum += std::hypot(pa[0] - pb[0], pa[1] - pb[1]);
+  }
+  return n ? sum / double(n) : 0.0;
+}
+
+int motion_recovery() {
+  // A view's target rendered with one node moved (8.9 cm and 11 degrees; at 3 m and 128 px
+  // its gaussians move a few pixels); with the gaussians frozen, refining that view's
+  // motion must bring them back where the target shows them, on screen.
+  constexpr uint32_t w = 128, h = 96;
+  gs::Dataset ds = test_dataset(w, h, 2, false, 3);
+  const gs::SplatScene scene = test_scene(300, 0, 9);
+  const float black[3] = {0.0f, 0.0f, 0.0f};
+  gs::TrainOptions o = frozen_options(0, false);
+  o.refine_motion = true;
+  o.motion_from = 0;
+  o.motion_nodes = 8;
+  o.motion_decay = o.motion_smoothness = 0.0f;
+  std::vector<double> truth;
+  {
+    gs::CudaContext ctx;
+    gs::Trainer renderer(ctx, ds, scene, o);
+    const float turn[3] = {0.0f, 0.2f, 0.0f}, shift[3] = {0.08f, -0.04f, 0.0f};
+    renderer.set_node_motion(1, 0, turn, shift);
+    ds.frames[1].rgba = renderer.render_view(1, black);
+    for (size_t p = 0; p < size_t(w) * h; ++p) ds.frames[1].rgba[p * 4 + 3] = 255;
+    truth = moved_positions(renderer, renderer.motion_binding(), scene, 1);
+  }
+  o.iterations = 200;
+  o.lr_motion_shift = 2e-3f;
+  o.lr_motion_turn = 3e-3f;
+  o.lr_motion_final = 1.0f;
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  const gs::Trainer::MotionBinding bind = t.motion_binding();
+  const gs::Camera cam = gs::dataset_camera(ds, ds.frames[1]);
+  const double before = screen_distance(cam, moved_positions(t, bind, scene, 1), truth);
+  for (int s = 0; s < 150; ++s) t.step_on(1, black);
+  const double after = screen_distance(cam, moved_positions(t, bind, scene, 1), truth);
+  std::printf("{\"before_px\": %.3f, \"after_px\": %.3f, \"updates\": %u}\n", before, after, t.stats().motion_updates);
+  return before > 0.5 && after < 0.25 * before ? 0 : 1;
+}
+
+int motion_batched() {
+  // Batched steps with motion (3 views per step): each view gets its own motion, gradient
+  // and update, through densification, and the held-out views' motion is interpolated.
+  gs::Dataset ds = test_dataset(64, 48, 6, true, 31);
+  const gs::SplatScene scene = test_scene(150, 1, 37);
+  gs::TrainOptions o = gs::scaled_options(45);
+  o.sh_degree = 1;
+  o.max_gaussians = 400;
+  o.densify_from = 5;
+  o.densify_until = 40;
+  o.densify_interval = 10;
+  o.refine_motion = true;
+  o.motion_nodes = 8;
+  o.motion_from = 5;
+  o.views_per_step = 3;
+  o.autotune = false;
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  while (!t.finished()) t.steps(17);
+  bool finite = true;
+  for (float v : t.export_scene().positions) finite = finite && std::isfinite(v);
+  double largest = 0.0;
+  for (size_t f = 0; f < ds.frames.size(); ++f)
+    for (uint32_t k = 0; k < t.motion_nodes().size(); ++k) {
+      float turn[3], shift[3];
+      t.node_motion(f, k, turn, shift);
+      for (int c = 0; c < 3; ++c) {
+        finite = finite && std::isfinite(turn[c]) && std::isfinite(shift[c]);
+        largest = std::max(largest, double(std::fabs(shift[c])));
+      }
+    }
+  const gs::TrainStats& s = t.stats();
+  const gs::EvalResult e = t.evaluate();
+  const std::vector<uint8_t> img = t.render_view(0, std::array<float, 3>{0, 0, 0}.data());
+  std::printf("{\"motion_updates\": %u, \"densify_events\": %u, \"shift_mean\": %.4g, \"largest\": %.4g, "
+              "\"finite\": %d, \"eval_psnr\": %.3f, \"eval_views\": %u}\n",
+              s.motion_updates, s.densify_events, s.motion_shift_mean, largest, int(finite), e.psnr, e.views);
+  return s.motion_updates == 40 * 3 && s.densify_events > 0 && finite && largest > 0.0 && std::isfinite(e.psnr) &&
+                 e.views > 0 && img.size() == 64 * 48 * 4
+             ? 0
+             : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -309,6 +503,9 @@ int main(int argc, char** argv) {
     if (mode == "pose-recovery") return pose_recovery();
     if (mode == "exposure-recovery") return exposure_recovery();
     if (mode == "align") return align();
+    if (mode == "motion-gradient" && argc > 2) return motion_gradient(uint32_t(std::atoi(argv[2])));
+    if (mode == "motion-recovery") return motion_recovery();
+    if (mode == "motion-batched") return motion_batched();
     std::fprintf(stderr, "usage: gs_refine_selftest pose-gradient <lambda> | pose-recovery | exposure-recovery | align\n");
     return 2;
   } catch (const std::exception& e) {

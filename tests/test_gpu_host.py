@@ -171,3 +171,39 @@ def test_gs_train_with_refinement(tmp_path):
     for f in frames:
         M = np.array(f["transform_matrix"])
         assert M.shape == (4, 4) and np.allclose(M[:3, :3] @ M[:3, :3].T, np.eye(3), atol=1e-4)
+
+
+@pytest.mark.parametrize("nodes", ["8", "100"])
+def test_trainer_motion_gradient(nodes):
+    """test_motion_gradient (test_trainer.cpp:549-606) through gs::Trainer: with the nodes
+    at rest the motion gradient equals what the per-gaussian gradients imply."""
+    rc, out = refine_selftest("motion-gradient", nodes)
+    assert rc == 0, out
+
+
+def test_trainer_motion_recovery():
+    """test_motion_recovery (test_trainer.cpp:660-690): one node moved 9 cm and 11 degrees in
+    a view's target; refining that view's motion with frozen gaussians brings them back
+    to within a quarter of the on-screen distance."""
+    rc, out = refine_selftest("motion-recovery")
+    assert rc == 0, out
+
+
+def test_trainer_motion_batched():
+    """test_motion_batched (test_trainer.cpp:744-782) with 3 views per step: every view of
+    every step from motion_from updates its motion, through densification."""
+    rc, out = refine_selftest("motion-batched")
+    assert rc == 0, out
+
+
+def test_gs_train_with_motion(tmp_path):
+    """gs_train --refine-motion writes the nodes and every view's motion and still learns."""
+    motion = tmp_path / "nodes.json"
+    _, m, out = train(tmp_path, "motion", "--iters", "300", "--eval-every", "150", "--views-per-step", "2",
+                      "--refine-motion", "--motion-nodes", "16", "--motion-from", "50", "--motion-out", str(motion))
+    assert "motion: 16 nodes" in out and "view updates" in out
+    assert m["eval"][-1]["psnr"] > m["eval"][0]["psnr"]
+    data = json.loads(motion.read_text())
+    assert len(data["nodes"]) == 16 and len(data["frames"]) == 24
+    assert all(len(f["turn"]) == 16 and len(f["shift"]) == 16 for f in data["frames"])
+    assert np.isfinite(np.array([f["shift"] for f in data["frames"]])).all()
