@@ -645,8 +645,8 @@ struct gs_context {
     depth_sorted_vals = in_alt ? dvals_alt : dvals;
     // Offsets of each item's pairs in depth order; the total is the step's pair count.
     gsk::exclusive_scan(sort, vb.tiles, depth_sorted_vals, sorted_offsets, items, d_scalars, stream, &launches);
-    gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, uint32_t(pair_cap), keys, values,
-                     pair_gaussian, pair_grads, d_scalars + 1, stream);
+    gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, d_scalars, uint32_t(pair_cap), keys,
+                     values, pair_gaussian, pair_grads, d_scalars + 1, stream);
     launches += items ? 1 : 0;
     const uint32_t max_tiles = uint32_t(tile_cap - 1);
     const int tile_bits = int(bits_for(max_tiles + 1));

@@ -74,9 +74,11 @@ void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* ga
                     uint32_t* d_total, cudaStream_t st, int* launches);
 
 // ---- pairs.cu ----
+// total: the scan's total (the end of the last item's pairs).
 void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
-                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, uint32_t pair_capacity, uint32_t* keys,
-                 uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads, uint32_t* mismatch, cudaStream_t st);
+                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, const uint32_t* total,
+                 uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
+                 uint32_t* mismatch, cudaStream_t st);
 // Tile ranges of the sorted pairs, and each view's span [view_span[v], view_span[kMaxViews + v])
 // of them (zeroed by the caller; views without pairs keep 0, 0).
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,

@@ -9,7 +9,10 @@
 //
 // Both blurs are register-blocked: a thread produces 4 consecutive outputs of a row (or
 // column) from the 14 inputs it loads once, so shared-memory traffic per output is 3.5
-// loads per plane instead of 11, and sums run over the taps in window order.
+// loads per plane instead of 11, and sums run over the taps in window order. The row
+// blur's results are kept column-major (26 rows of a column contiguous): a warp's stores
+// (8 rows x 4 runs) then fall on 32 different banks, and the column blur reads its 14
+// rows as 7 aligned 8-byte loads.
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -61,14 +64,12 @@ constexpr int kSpan = kRun + 2 * kR;    // inputs a thread loads: 14
 constexpr int kQuads = kTile / kRun;    // 4
 constexpr int kS = kWin + 1;            // row stride of a staged plane (odd: at most 2-way conflicts)
 constexpr int kPlane = kWin * kS;       // 702
-constexpr int kHRow = kWin * kTile;     // one plane after the row blur: 26 x 16
-constexpr int kHPlane = kHRow + 16;     // padded so neighbouring planes fall on other banks
+constexpr int kHRow = kWin * kTile;     // one plane after the row blur: 16 columns x 26 rows, column-major
+constexpr int kHPlane = kHRow + 16;     // padded so neighbouring planes fall on other banks (even: 8-byte aligned)
+constexpr int kAbc = kTilePixels + 16;  // stride of the per-pixel planes after the column blur
 
-// Row blur of 4 consecutive outputs from `src` (14 inputs) into out[4].
-__device__ __forceinline__ void blur_run(const float* src, int stride, float out[kRun]) {
-  float x[kSpan];
-#pragma unroll
-  for (int k = 0; k < kSpan; ++k) x[k] = src[k * stride];
+// Blur of 4 consecutive outputs from `src` (14 inputs, `stride` apart) into out[4].
+__device__ __forceinline__ void blur4(const float x[kSpan], float out[kRun]) {
 #pragma unroll
   for (int o = 0; o < kRun; ++o) {
     float sum = 0.0f;
@@ -78,11 +79,31 @@ __device__ __forceinline__ void blur_run(const float* src, int stride, float out
   }
 }
 
+__device__ __forceinline__ void blur_run(const float* src, int stride, float out[kRun]) {
+  float x[kSpan];
+#pragma unroll
+  for (int k = 0; k < kSpan; ++k) x[k] = src[k * stride];
+  blur4(x, out);
+}
+
+// Column blur: 14 contiguous inputs at an 8-byte-aligned address.
+__device__ __forceinline__ void blur_column(const float* src, float out[kRun]) {
+  float x[kSpan];
+  const float2* s2 = reinterpret_cast<const float2*>(src);
+#pragma unroll
+  for (int k = 0; k < kSpan / 2; ++k) {
+    const float2 v = s2[k];
+    x[2 * k] = v.x;
+    x[2 * k + 1] = v.y;
+  }
+  blur4(x, out);
+}
+
 __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   // s_buf: render rgb and target rgb planes of the window (26 x kS each); after the row
   // blur it holds A, B, C and SSIM per channel for the tile's 256 pixels.
   __shared__ float s_buf[6 * kPlane];
-  __shared__ float s_h[3 * 5 * kHPlane];  // [channel][moment] after the row blur
+  __shared__ __align__(16) float s_h[3 * 5 * kHPlane];  // [channel][moment] after the row blur
   __shared__ float s_sum[8][2];
   const uint32_t gt = blockIdx.x;
   if (gt >= a.vt->total_tiles) return;
@@ -140,7 +161,7 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
       yy[k] = y[k] * y[k];
       xy[k] = x[k] * y[k];
     }
-    float* h = s_h + c * 5u * kHPlane + row * kTile + q * kRun;
+    float* h = s_h + c * 5u * kHPlane + (q * kRun) * kWin + row;  // column q * 4 + o, row `row`
 #pragma unroll
     for (int o = 0; o < kRun; ++o) {
       float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f, m4 = 0.f;
@@ -153,23 +174,23 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
         m3 = fmaf(wk, yy[o + k], m3);
         m4 = fmaf(wk, xy[o + k], m4);
       }
-      h[o] = m0;
-      h[kHPlane + o] = m1;
-      h[2 * kHPlane + o] = m2;
-      h[3 * kHPlane + o] = m3;
-      h[4 * kHPlane + o] = m4;
+      h[o * kWin] = m0;
+      h[kHPlane + o * kWin] = m1;
+      h[2 * kHPlane + o * kWin] = m2;
+      h[3 * kHPlane + o * kWin] = m3;
+      h[4 * kHPlane + o * kWin] = m4;
     }
   }
   __syncthreads();
   // Column blur and the SSIM terms: 3 channels x 16 columns x 4 runs of 4 pixels.
-  float* s_abc = s_buf;  // [A, B, C, SSIM][channel][256]
+  float* s_abc = s_buf;  // [A, B, C, SSIM][channel][kAbc]
   const float c1 = f.loss[1], c2 = f.loss[2];
   if (lid < 3u * kTile * kQuads) {
     const uint32_t col = lid % kTile, c = (lid / kTile) % 3u, q = lid / (3u * kTile);
-    const float* h = s_h + c * 5u * kHPlane + q * kRun * kTile + col;
+    const float* h = s_h + c * 5u * kHPlane + col * kWin + q * kRun;
     float mom[5][kRun];
 #pragma unroll
-    for (int j = 0; j < 5; ++j) blur_run(h + j * kHPlane, kTile, mom[j]);
+    for (int j = 0; j < 5; ++j) blur_column(h + j * kHPlane, mom[j]);
 #pragma unroll
     for (int o = 0; o < kRun; ++o) {
       const float mx = mom[0][o], my = mom[1][o], exx = mom[2][o], eyy = mom[3][o], exy = mom[4][o];
@@ -182,11 +203,11 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
       const float d_cxy = 2.0f * l * inv;
       const float d_vx = -ssim * (m * inv);
       const uint32_t pixel = (q * kRun + o) * kTile + col;
-      s_abc[c * 256u + pixel] =
+      s_abc[c * kAbc + pixel] =
           2.0f * my * cs * inv - ssim * 2.0f * mx * (vv * inv) - 2.0f * mx * d_vx - my * d_cxy;
-      s_abc[(3u + c) * 256u + pixel] = d_vx;
-      s_abc[(6u + c) * 256u + pixel] = d_cxy;
-      s_abc[(9u + c) * 256u + pixel] = ssim;
+      s_abc[(3u + c) * kAbc + pixel] = d_vx;
+      s_abc[(6u + c) * kAbc + pixel] = d_cxy;
+      s_abc[(9u + c) * kAbc + pixel] = ssim;
     }
   }
   __syncthreads();
@@ -200,10 +221,10 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
     float A[3], B[3], C[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      A[c] = s_abc[c * 256 + lid];
-      B[c] = s_abc[(3 + c) * 256 + lid];
-      C[c] = s_abc[(6 + c) * 256 + lid];
-      const float ssim = s_abc[(9 + c) * 256 + lid];
+      A[c] = s_abc[c * kAbc + lid];
+      B[c] = s_abc[(3 + c) * kAbc + lid];
+      C[c] = s_abc[(6 + c) * kAbc + lid];
+      const float ssim = s_abc[(9 + c) * kAbc + lid];
       ssim_sum += ssim;
       wsum += w * ssim;
     }
@@ -232,7 +253,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   // s_m: the 9 planes (A, B, C x rgb) of the window; after the row blur it holds the
   // 9 blurred planes of the tile's 256 pixels.
   __shared__ float s_m[9 * kPlane];
-  __shared__ float s_h[9 * kHPlane];
+  __shared__ __align__(16) float s_h[9 * kHPlane];
   const uint32_t gt = blockIdx.x;
   if (gt >= a.vt->total_tiles) return;
   const uint32_t v = view_of_tile(a.vt, gt);
@@ -274,17 +295,17 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
     float out[kRun];
     blur_run(s_m + p * kPlane + row * kS + q * kRun, 1, out);
 #pragma unroll
-    for (int o = 0; o < kRun; ++o) s_h[p * kHPlane + row * kTile + q * kRun + o] = out[o];
+    for (int o = 0; o < kRun; ++o) s_h[p * kHPlane + (q * kRun + o) * kWin + row] = out[o];
   }
   __syncthreads();
   // Column blur: 9 planes x 16 columns x 4 runs.
-  float* s_g = s_m;  // [plane][256]
+  float* s_g = s_m;  // [plane][kAbc]
   for (uint32_t e = lid; e < 9u * kTile * kQuads; e += 256u) {
     const uint32_t col = e % kTile, p = (e / kTile) % 9u, q = e / (9u * kTile);
     float out[kRun];
-    blur_run(s_h + p * kHPlane + q * kRun * kTile + col, kTile, out);
+    blur_column(s_h + p * kHPlane + col * kWin + q * kRun, out);
 #pragma unroll
-    for (int o = 0; o < kRun; ++o) s_g[p * 256u + (q * kRun + o) * kTile + col] = out[o];
+    for (int o = 0; o < kRun; ++o) s_g[p * kAbc + (q * kRun + o) * kTile + col] = out[o];
   }
   __syncthreads();
   const uint32_t lx = lid % kTile, ly = lid / kTile;
@@ -297,7 +318,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   float ds[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
-    ds[c] = s_g[c * 256 + lid] + 2.0f * xs[c] * s_g[(3 + c) * 256 + lid] + ys[c] * s_g[(6 + c) * 256 + lid];
+    ds[c] = s_g[c * kAbc + lid] + 2.0f * xs[c] * s_g[(3 + c) * kAbc + lid] + ys[c] * s_g[(6 + c) * kAbc + lid];
   float4 pg = a.rb.pixel_grad[pix];
   const float s = f.loss[0] * f.background[3];
   pg.x -= s * ds[0];

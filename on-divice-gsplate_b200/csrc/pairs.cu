@@ -18,9 +18,9 @@ struct EmitArgs {
   uint32_t cap, n_items, pair_capacity;
   const uint32_t* sorted_vals;
   const uint32_t* sorted_offsets;
+  const uint32_t* total;  // the scan's total: the end of the last item's pairs
   const float4* splat;
   const float4* foot;
-  const uint32_t* tiles;
   uint32_t* offsets;
   uint32_t* keys;
   uint32_t* values;
@@ -32,14 +32,16 @@ struct EmitArgs {
 __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.n_items) return;
-  const uint32_t g = a.sorted_vals[k];
-  const uint32_t count = a.tiles[g];
+  // The item's tile count from consecutive scan offsets (coalesced): items that emit
+  // nothing (the invisible ones, sorted last) leave before any gather.
+  uint32_t p = a.sorted_offsets[k];
+  const uint32_t count = (k + 1u < a.n_items ? a.sorted_offsets[k + 1u] : *a.total) - p;
   if (count == 0u) return;
+  const uint32_t g = a.sorted_vals[k];
   const uint32_t v = g / a.cap;
   const gs_frame_data& f = a.frames[v];
   const float4 q0 = a.splat[size_t(g) * 3u];
   const float4 fp = a.foot[g];
-  uint32_t p = a.sorted_offsets[k];
   a.offsets[g] = p;
   const uint32_t end = min(p + count, a.pair_capacity);
   const uint32_t tile_base = a.vt->tile_base[v];
@@ -109,11 +111,12 @@ __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ key
 }  // namespace
 
 void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
-                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, uint32_t pair_capacity, uint32_t* keys,
-                 uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads, uint32_t* mismatch, cudaStream_t st) {
+                 const uint32_t* sorted_vals, const uint32_t* sorted_offsets, const uint32_t* total,
+                 uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
+                 uint32_t* mismatch, cudaStream_t st) {
   if (n_items == 0u) return;
-  EmitArgs a{sp.frames, sp.vt, cap, n_items, pair_capacity, sorted_vals, sorted_offsets,
-             vb.splat, vb.foot, vb.tiles, vb.offsets, keys, values, pair_gaussian, pair_grads, mismatch};
+  EmitArgs a{sp.frames, sp.vt,   cap,       n_items, pair_capacity, sorted_vals, sorted_offsets, total,
+             vb.splat,  vb.foot, vb.offsets, keys,   values,        pair_gaussian, pair_grads,   mismatch};
   k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 
