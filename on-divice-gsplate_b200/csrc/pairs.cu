@@ -29,52 +29,84 @@ struct EmitArgs {
   uint32_t* mismatch;
 };
 
+// Pairs a warp stages in shared memory before writing them out: a warp's items are
+// consecutive in depth order, so their pairs form one contiguous range, written with
+// coalesced stores instead of one scattered run per lane.
+constexpr uint32_t kEmitStage = 512;
+
 __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
+  __shared__ uint32_t s_tile[4][kEmitStage];
+  __shared__ uint32_t s_owner[4][kEmitStage];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.n_items) return;
-  // The item's tile count from consecutive scan offsets (coalesced): items that emit
-  // nothing (the invisible ones, sorted last) leave before any gather.
-  uint32_t p = a.sorted_offsets[k];
-  const uint32_t count = (k + 1u < a.n_items ? a.sorted_offsets[k + 1u] : *a.total) - p;
-  if (count == 0u) return;
-  const uint32_t g = a.sorted_vals[k];
-  const uint32_t v = g / a.cap;
-  const gs_frame_data& f = a.frames[v];
-  const float4 q0 = a.splat[size_t(g) * 3u];
-  const float4 fp = a.foot[g];
-  a.offsets[g] = p;
-  const uint32_t end = min(p + count, a.pair_capacity);
-  const uint32_t tile_base = a.vt->tile_base[v];
-  const uint32_t width = f.image[0], height = f.image[1], tiles_x = f.image[2];
-  uint32_t wanted = 0u;
-  const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
-  if (rows.x <= rows.y) {
-    for (uint32_t ty = uint32_t(rows.x) / kTile; ty <= uint32_t(rows.y) / kTile; ++ty) {
-      const uint2 span = footprint_row_tiles(q0.x, q0.y, fp.x, fp.y, fp.z, fp.w, rows, ty, width);
-      wanted += span.y - span.x;
-      for (uint32_t x = span.x; x < span.y && p < end; ++x) {
-        a.keys[p] = tile_base + ty * tiles_x + x;
-        a.values[p] = p;
-        a.pair_gaussian[p] = g;
-        ++p;
+  if (blockIdx.x * blockDim.x + warp * 32u >= a.n_items) return;  // the whole warp
+  // The item's pairs [p, p + count) from consecutive scan offsets (coalesced): items that
+  // emit nothing (the invisible ones, sorted last) need no gather.
+  uint32_t p = 0u, count = 0u;
+  if (k < a.n_items) {
+    p = a.sorted_offsets[k];
+    count = (k + 1u < a.n_items ? a.sorted_offsets[k + 1u] : *a.total) - p;
+  }
+  const uint32_t wfirst = __shfl_sync(0xffffffffu, p, 0);
+  const uint32_t wend = min(__reduce_max_sync(0xffffffffu, count ? p + count : 0u), a.pair_capacity);
+  if (wend <= wfirst) {
+    if (count != 0u) a.offsets[a.sorted_vals[k]] = p;  // all past the capacity
+    return;
+  }
+  const bool staged = wend - wfirst <= kEmitStage;
+  uint32_t* st_tile = s_tile[warp];
+  uint32_t* st_owner = s_owner[warp];
+  if (count != 0u) {
+    const uint32_t g = a.sorted_vals[k];
+    const uint32_t v = g / a.cap;
+    const gs_frame_data& f = a.frames[v];
+    const float4 q0 = a.splat[size_t(g) * 3u];
+    const float4 fp = a.foot[g];
+    a.offsets[g] = p;
+    const uint32_t end = min(p + count, a.pair_capacity);
+    const uint32_t tile_base = a.vt->tile_base[v];
+    const uint32_t width = f.image[0], height = f.image[1], tiles_x = f.image[2];
+    auto put = [&](uint32_t q, uint32_t tile) {
+      if (staged) {
+        st_tile[q - wfirst] = tile;
+        st_owner[q - wfirst] = g;
+      } else {
+        a.keys[q] = tile;
+        a.values[q] = q;
+        a.pair_gaussian[q] = g;
+      }
+    };
+    uint32_t wanted = 0u;
+    const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
+    if (rows.x <= rows.y) {
+      for (uint32_t ty = uint32_t(rows.x) / kTile; ty <= uint32_t(rows.y) / kTile; ++ty) {
+        const uint2 span = footprint_row_tiles(q0.x, q0.y, fp.x, fp.y, fp.z, fp.w, rows, ty, width);
+        wanted += span.y - span.x;
+        for (uint32_t x = span.x; x < span.y && p < end; ++x) put(p++, tile_base + ty * tiles_x + x);
+      }
+    }
+    if (wanted != count) {
+      // The count and the walk disagree (never expected: same inputs, same arithmetic).
+      // Pad the rest into the unused tile after the last one, with zero gradient.
+      atomicAdd(a.mismatch, 1u);
+      const uint32_t pad_tile = a.vt->total_tiles;
+      for (; p < end; ++p) {
+        put(p, pad_tile);
+        if (a.pair_grads != nullptr) {
+          const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+          a.pair_grads[size_t(p) * 3u] = z;
+          a.pair_grads[size_t(p) * 3u + 1u] = z;
+          a.pair_grads[size_t(p) * 3u + 2u] = z;
+        }
       }
     }
   }
-  if (wanted == count) return;
-  // The count and the walk disagree (never expected: same inputs, same arithmetic).
-  // Pad the rest into the unused tile after the last one, with zero gradient.
-  atomicAdd(a.mismatch, 1u);
-  const uint32_t pad_tile = a.vt->total_tiles;
-  for (; p < end; ++p) {
-    a.keys[p] = pad_tile;
-    a.values[p] = p;
-    a.pair_gaussian[p] = g;
-    if (a.pair_grads != nullptr) {
-      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-      a.pair_grads[size_t(p) * 3u] = z;
-      a.pair_grads[size_t(p) * 3u + 1u] = z;
-      a.pair_grads[size_t(p) * 3u + 2u] = z;
-    }
+  if (!staged) return;
+  __syncwarp();
+  for (uint32_t q = wfirst + lane; q < wend; q += 32u) {
+    a.keys[q] = st_tile[q - wfirst];
+    a.values[q] = q;
+    a.pair_gaussian[q] = st_owner[q - wfirst];
   }
 }
 
