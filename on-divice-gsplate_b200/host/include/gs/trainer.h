@@ -269,6 +269,11 @@ class Trainer {
   // The tuning in use ("fpx=2 bpx=4 batch=64 digits=8 deterministic"), in place of the
   // reference's backward-variant name.
   std::string reduction() const;
+  // Testing: runs the backward (and the passes it shares knobs with) under the tuning
+  // `name` names, in reduction()'s form: any of fpx=1|2|4, bpx=1|2|4, batch=32|64,
+  // digits=4..8 and deterministic|atomic, the others kept (trainer.h:324 picks a backward
+  // variant by name). False, and nothing changed, for a name it cannot parse.
+  bool select_backward(const std::string& name);
   const std::vector<RetuneResult>& retunes() const { return retunes_; }
 
  private:

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -171,6 +172,34 @@ std::string Trainer::reduction() const {
   return "fpx=" + std::to_string(t.forward_pixels) + " bpx=" + std::to_string(t.backward_pixels) +
          " batch=" + std::to_string(t.backward_batch) + " digits=" + std::to_string(t.sort_digit_bits) +
          (t.deterministic ? " deterministic" : " atomic");
+}
+
+bool Trainer::select_backward(const std::string& name) {
+  gs_tuning t;
+  if (gs_get_tuning(gpu_, &t) != GS_OK) return false;
+  size_t pos = 0;
+  while (pos < name.size()) {
+    const size_t end = std::min(name.find(' ', pos), name.size());
+    const std::string word = name.substr(pos, end - pos);
+    pos = end + 1;
+    if (word.empty()) continue;
+    if (word == "deterministic" || word == "atomic") {
+      t.deterministic = word == "deterministic" ? 1u : 0u;
+      continue;
+    }
+    const size_t eq = word.find('=');
+    if (eq == std::string::npos) return false;
+    const std::string key = word.substr(0, eq);
+    char* rest = nullptr;
+    const unsigned long v = std::strtoul(word.c_str() + eq + 1, &rest, 10);
+    if (rest == word.c_str() + eq + 1 || *rest != '\0') return false;
+    if (key == "fpx" && (v == 1 || v == 2 || v == 4)) t.forward_pixels = uint32_t(v);
+    else if (key == "bpx" && (v == 1 || v == 2 || v == 4)) t.backward_pixels = uint32_t(v);
+    else if (key == "batch" && (v == 32 || v == 64)) t.backward_batch = uint32_t(v);
+    else if (key == "digits" && v >= 4 && v <= 8) t.sort_digit_bits = uint32_t(v);
+    else return false;
+  }
+  return gs_set_tuning(gpu_, &t) == GS_OK;
 }
 
 void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std::array<float, 3>>& backgrounds,

@@ -11,6 +11,8 @@
 //   gs_refine_selftest motion-gradient <nodes>
 //   gs_refine_selftest motion-recovery
 //   gs_refine_selftest motion-batched
+//   gs_refine_selftest variants     select_backward: every tuning gives the first step's
+//                                   gradients of the default one (test_trainer.cpp:56-125)
 // Each prints one JSON line with what it measured and exits 1 when its check fails.
 #include <algorithm>
 #include <array>
@@ -494,6 +496,42 @@ int motion_batched() {
              : 1;
 }
 
+int variants() {
+  gs::Dataset ds = test_dataset(64, 48, 1, true, 7);
+  const gs::SplatScene scene = test_scene(200, 2, 11);
+  const float bg[3] = {0.2f, 0.5f, 0.7f};
+  gs::TrainOptions o = frozen_options(2, true);
+  const char* names[] = {"fpx=2 bpx=4 batch=64 digits=8 deterministic", "fpx=1 bpx=1 batch=32 digits=4 deterministic",
+                         "fpx=4 bpx=2 batch=64 digits=6 deterministic", "fpx=2 bpx=4 batch=32 digits=7 atomic"};
+  std::vector<float> ref;
+  double worst = 0.0;
+  bool ok = true;
+  for (const char* name : names) {
+    gs::CudaContext ctx;
+    gs::Trainer t(ctx, ds, scene, o);
+    ok = ok && t.select_backward(name) && t.reduction() == name;
+    t.step_on(0, bg);
+    const std::vector<float> g = t.first_step_gradients().params;
+    if (ref.empty()) {
+      ref = g;
+      continue;
+    }
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < g.size(); ++i) {
+      num += (double(g[i]) - ref[i]) * (double(g[i]) - ref[i]);
+      den += double(ref[i]) * ref[i];
+    }
+    worst = std::max(worst, std::sqrt(num / std::max(den, 1e-300)));
+  }
+  gs::CudaContext ctx;
+  gs::Trainer t(ctx, ds, scene, o);
+  const std::string before = t.reduction();
+  const bool rejected = !t.select_backward("bpx=3") && !t.select_backward("fast") && t.reduction() == before;
+  std::printf("{\"variants\": 4, \"worst_rel_l2\": %.3g, \"names_ok\": %d, \"rejects_unknown\": %d}\n", worst,
+              int(ok), int(rejected));
+  return ok && rejected && worst < 1e-5 ? 0 : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -506,6 +544,7 @@ int main(int argc, char** argv) {
     if (mode == "motion-gradient" && argc > 2) return motion_gradient(uint32_t(std::atoi(argv[2])));
     if (mode == "motion-recovery") return motion_recovery();
     if (mode == "motion-batched") return motion_batched();
+    if (mode == "variants") return variants();
     std::fprintf(stderr, "usage: gs_refine_selftest pose-gradient <lambda> | pose-recovery | exposure-recovery | align\n");
     return 2;
   } catch (const std::exception& e) {

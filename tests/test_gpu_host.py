@@ -207,3 +207,11 @@ def test_gs_train_with_motion(tmp_path):
     assert len(data["nodes"]) == 16 and len(data["frames"]) == 24
     assert all(len(f["turn"]) == 16 and len(f["shift"]) == 16 for f in data["frames"])
     assert np.isfinite(np.array([f["shift"] for f in data["frames"]])).all()
+
+
+def test_trainer_select_backward_variants():
+    """select_backward (trainer.h:324; variant equality, test_trainer.cpp:56-125): every
+    tuning, deterministic or atomic, gives the default's first-step gradients (within float
+    summation order), and unknown names are refused."""
+    rc, out = refine_selftest("variants")
+    assert rc == 0, out
