@@ -410,10 +410,13 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy).
         const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
         const float lx = -ca * dx, ly = -cb * dx, mx = -cb, my = -cc;
-        const float hx = -0.5f * dx * dx, ndx = -dx;
+        // The lane's pixels share dx, so the mean and conic sums need only
+        // sd = sum dpow, st = sum dpow dy and sty = sum dpow dy^2 (formed after the loop):
+        // dmean = (lx sd + mx st, ly sd + my st), dconic = (-dx^2/2 sd, -dx st, -sty/2).
+        float sd = 0.0f, st = 0.0f, sty = 0.0f;
         float c[12];
 #pragma unroll
-        for (int k = 0; k < 12; ++k) c[k] = 0.0f;
+        for (int k = 5; k < 12; ++k) c[k] = 0.0f;
         bool has = false;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
@@ -436,11 +439,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           const float t = dpow * dy;
           const float dmx = fmaf(t, mx, dpow * lx);  // dpow (lx + mx dy)
           const float dmy = fmaf(t, my, dpow * ly);
-          c[0] += dmx;
-          c[1] += dmy;
-          c[2] = fmaf(dpow, hx, c[2]);
-          c[3] = fmaf(t, ndx, c[3]);
-          c[4] = fmaf(t, -0.5f * dy, c[4]);
+          sd += dpow;
+          st += t;
+          sty = fmaf(t, dy, sty);
           c[5] = fmaf(G, dl, c[5]);
           c[6] += weight * dl0[p];
           c[7] += weight * dl1[p];
@@ -451,6 +452,11 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           R[p] = rest;
         }
         if (__any_sync(0xffffffffu, has)) {
+          c[0] = fmaf(lx, sd, mx * st);
+          c[1] = fmaf(ly, sd, my * st);
+          c[2] = (-0.5f * dx * dx) * sd;
+          c[3] = -dx * st;
+          c[4] = -0.5f * sty;
           // Reduce-scatter of 12 slots (11 values and a zero): after the exchanges over
           // lane bits 4, 3, 2, 1 (6, 3, 2 and 1 shuffles; the 3 slots left after bit 3 are
           // padded to 4) and a final add over bit 0, lane l holds the warp sum of value
