@@ -121,6 +121,7 @@ struct gs_context {
   size_t pixel_cap = 0, tile_cap = 0;
   uint32_t* target = nullptr;
   float4 *pixel_grad = nullptr, *pixel_out = nullptr, *ssim_maps = nullptr;
+  float* ssim_last = nullptr;
   uint32_t *pixel_count = nullptr, *image = nullptr;
   float* pixel_dot = nullptr;
   uint2* ranges = nullptr;
@@ -173,7 +174,8 @@ struct gs_context {
     for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.dir_grad, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
-    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial, &motion_partial})
+    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial, &motion_partial,
+                     &ssim_last})
       dev_free(*p);
     dev_free(motion_rest);
     dev_free(motion_bind);
@@ -265,7 +267,8 @@ struct gs_context {
       dev_alloc(target, pixels);
       dev_alloc(pixel_grad, pixels);
       dev_alloc(pixel_out, pixels);
-      dev_alloc(ssim_maps, pixels * 3);
+      dev_alloc(ssim_maps, pixels * 2);
+      dev_alloc(ssim_last, pixels);
       dev_alloc(pixel_count, pixels);
       dev_alloc(image, pixels);
       dev_alloc(pixel_dot, pixels);
@@ -574,6 +577,7 @@ struct gs_context {
     rb.tile_loss = tile_loss;
     rb.tile_count = tile_count;
     rb.ssim_maps = ssim_maps;
+    rb.ssim_last = ssim_last;
     return rb;
   }
 

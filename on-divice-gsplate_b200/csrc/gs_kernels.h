@@ -96,7 +96,10 @@ struct RasterBuffers {
   float* pixel_dot = nullptr;
   float* tile_loss = nullptr;               // 16 per global tile
   uint32_t* tile_count = nullptr;
-  float4* ssim_maps = nullptr;              // 3 per pixel
+  // The SSIM gradient maps w A, w B, w C (rgb each) of every pixel, 36 bytes:
+  // ssim_maps[2 p] = (A rgb, B r), ssim_maps[2 p + 1] = (B g, B b, C r, C g), ssim_last[p] = C b.
+  float4* ssim_maps = nullptr;
+  float* ssim_last = nullptr;
 };
 // px: pixels per thread (1, 2 or 4).
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,

@@ -228,9 +228,9 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
       ssim_sum += ssim;
       wsum += w * ssim;
     }
-    a.rb.ssim_maps[pix * 3u] = make_float4(w * A[0], w * A[1], w * A[2], 0.0f);
-    a.rb.ssim_maps[pix * 3u + 1u] = make_float4(w * B[0], w * B[1], w * B[2], 0.0f);
-    a.rb.ssim_maps[pix * 3u + 2u] = make_float4(w * C[0], w * C[1], w * C[2], 0.0f);
+    a.rb.ssim_maps[pix * 2u] = make_float4(w * A[0], w * A[1], w * A[2], w * B[0]);
+    a.rb.ssim_maps[pix * 2u + 1u] = make_float4(w * B[1], w * B[2], w * C[0], w * C[1]);
+    a.rb.ssim_last[pix] = w * C[2];
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -273,20 +273,25 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
     const uint32_t row = e / kWin, col = e % kWin;
     const int gx = ox + int(col), gy = oy + int(row);
     const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
-    float4 m[3] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    float4 m0 = make_float4(0.f, 0.f, 0.f, 0.f), m1 = m0;
+    float m2 = 0.0f;
     if (in) {
-      const size_t q = (pbase + size_t(gy) * W + size_t(gx)) * 3u;
-      m[0] = a.rb.ssim_maps[q];
-      m[1] = a.rb.ssim_maps[q + 1u];
-      m[2] = a.rb.ssim_maps[q + 2u];
+      const size_t q = pbase + size_t(gy) * W + size_t(gx);
+      m0 = a.rb.ssim_maps[q * 2u];
+      m1 = a.rb.ssim_maps[q * 2u + 1u];
+      m2 = a.rb.ssim_last[q];
     }
+    // Planes A rgb, B rgb, C rgb.
     const uint32_t at = row * kS + col;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      s_m[(3 * q) * kPlane + at] = m[q].x;
-      s_m[(3 * q + 1) * kPlane + at] = m[q].y;
-      s_m[(3 * q + 2) * kPlane + at] = m[q].z;
-    }
+    s_m[at] = m0.x;
+    s_m[kPlane + at] = m0.y;
+    s_m[2 * kPlane + at] = m0.z;
+    s_m[3 * kPlane + at] = m0.w;
+    s_m[4 * kPlane + at] = m1.x;
+    s_m[5 * kPlane + at] = m1.y;
+    s_m[6 * kPlane + at] = m1.z;
+    s_m[7 * kPlane + at] = m1.w;
+    s_m[8 * kPlane + at] = m2;
   }
   __syncthreads();
   // Row blur: 9 planes x 26 rows x 4 runs.
