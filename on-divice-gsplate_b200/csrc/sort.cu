@@ -111,9 +111,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
                                                        const uint32_t* __restrict__ pass_offsets, uint32_t* lookback,
                                                        uint32_t* ticket, uint32_t* err) {
   __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_wc[kWarps][kRadix];  // per-warp digit counts, then per-warp exclusive offsets
-  __shared__ uint32_t s_dstart[kRadix];      // block-local start of each digit
-  __shared__ uint32_t s_gbase[kRadix];       // global position of each digit's first key of this block
+  __shared__ uint32_t s_wc[kWarps][kRadix];  // per-warp digit counts, then each warp's first block position per digit
+  __shared__ uint32_t s_delta[kRadix];       // global position minus block position, per digit
   __shared__ uint32_t s_warp[kWarps];
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[kSortTile];
@@ -157,16 +156,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
   }
   __syncthreads();
 
-  // Digit `tid`: per-warp exclusive offsets, block count, block-local start.
+  // Digit `tid`: block count, block-local start, then each warp's first block position
+  // (one shared read per key in the scatter below).
   uint32_t count = 0u;
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
-    const uint32_t c = s_wc[w][tid];
-    s_wc[w][tid] = count;
-    count += c;
-  }
+  for (int w = 0; w < kWarps; ++w) count += s_wc[w][tid];
   uint32_t block_total;
-  s_dstart[tid] = block_exclusive_scan<uint32_t>(count, s_warp, block_total);
+  const uint32_t dstart = block_exclusive_scan<uint32_t>(count, s_warp, block_total);
+  {
+    uint32_t running = dstart;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = s_wc[w][tid];
+      s_wc[w][tid] = running;
+      running += c;
+    }
+  }
 
   // Decoupled look-back on digit `tid`.
   uint32_t prefix = 0u;
@@ -192,15 +197,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
     }
     st_relaxed(&lookback[size_t(tile) * kRadix + tid], kPrefix | ((prefix + count) & kValueMask));
   }
-  s_gbase[tid] = pass_offsets[tid] + prefix;
+  s_delta[tid] = pass_offsets[tid] + prefix - dstart;
   __syncthreads();
 
 #pragma unroll
   for (int j = 0; j < kIpt; ++j) {
     const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
     if (idx < n) {
-      const uint32_t d = (key[j] >> shift) & mask;
-      const uint32_t pos = s_dstart[d] + s_wc[warp][d] + rank[j];
+      const uint32_t pos = s_wc[warp][(key[j] >> shift) & mask] + rank[j];
       s_keys[pos] = key[j];
       s_vals[pos] = val[j];
     }
@@ -209,8 +213,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
   const uint32_t tile_n = min(kSortTile, n - base);
   for (uint32_t p = tid; p < tile_n; p += kThreads) {
     const uint32_t k = s_keys[p];
-    const uint32_t d = (k >> shift) & mask;
-    const uint32_t out = s_gbase[d] + (p - s_dstart[d]);
+    const uint32_t out = s_delta[(k >> shift) & mask] + p;
     keys_out[out] = k;
     vals_out[out] = s_vals[p];
   }

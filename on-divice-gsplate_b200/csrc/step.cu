@@ -139,29 +139,75 @@ __device__ __forceinline__ void for_terms(std::integer_sequence<int, Ks...>, F&&
 }
 
 // View-independent quantities of a slot's covariance.
+// A slot's rotation and scale: M = R S (Sigma = M M^T).
+struct Shape {
+  float qn[4], qlen, R[3][3], s[3], M[3][3];
+};
+
+__device__ __forceinline__ void slot_shape(float4 p1, float4 q, Shape& S) {
+  S.qlen = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-12f);
+  S.qn[0] = q.x / S.qlen;
+  S.qn[1] = q.y / S.qlen;
+  S.qn[2] = q.z / S.qlen;
+  S.qn[3] = q.w / S.qlen;
+  quat_to_matrix(S.qn[0], S.qn[1], S.qn[2], S.qn[3], S.R);
+  S.s[0] = expf(p1.x);
+  S.s[1] = expf(p1.y);
+  S.s[2] = expf(p1.z);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S.M[r][c] = S.R[r][c] * S.s[c];
+}
+
+// What the per-view backward needs of a slot: its 3D covariance and opacity.
 struct Geometry {
-  float qn[4], qlen, R[3][3], s[3], M[3][3], Sig[3][3], opacity;
+  float Sig[3][3], opacity;
 };
 
 __device__ __forceinline__ void slot_geometry(float4 p0, float4 p1, float4 q, Geometry& G) {
-  G.qlen = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-12f);
-  G.qn[0] = q.x / G.qlen;
-  G.qn[1] = q.y / G.qlen;
-  G.qn[2] = q.z / G.qlen;
-  G.qn[3] = q.w / G.qlen;
-  quat_to_matrix(G.qn[0], G.qn[1], G.qn[2], G.qn[3], G.R);
-  G.s[0] = expf(p1.x);
-  G.s[1] = expf(p1.y);
-  G.s[2] = expf(p1.z);
+  Shape S;
+  slot_shape(p1, q, S);
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) G.M[r][c] = G.R[r][c] * G.s[c];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) G.Sig[r][c] = G.M[r][0] * G.M[c][0] + G.M[r][1] * G.M[c][1] + G.M[r][2] * G.M[c][2];
+    for (int c = 0; c < 3; ++c) G.Sig[r][c] = S.M[r][0] * S.M[c][0] + S.M[r][1] * S.M[c][1] + S.M[r][2] * S.M[c][2];
   G.opacity = sigmoidf(p0.w);
+}
+
+// The covariance's gradient summed over the views, dSigma (symmetric: 00, 01, 02, 11, 12,
+// 22), back to the log scales and the quaternion (train_step.glsl:206-219): dM = 2 dSigma M,
+// dL/dlog s_c = s_c sum_r dM_rc R_rc, dL/dR = dM S, then the quaternion's tangent part.
+// The map is linear in dSigma, so one pass after the views equals one per view.
+__device__ __forceinline__ void scale_rotation_backward(float4 p1, float4 q, const float dsig[6], float g16[16]) {
+  Shape S;
+  slot_shape(p1, q, S);
+  const float dS[3][3] = {{dsig[0], dsig[1], dsig[2]}, {dsig[1], dsig[3], dsig[4]}, {dsig[2], dsig[4], dsig[5]}};
+  float dM[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dM[r][c] = 2.0f * (dS[r][0] * S.M[0][c] + dS[r][1] * S.M[1][c] + dS[r][2] * S.M[2][c]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    g16[4 + c] += (dM[0][c] * S.R[0][c] + dM[1][c] * S.R[1][c] + dM[2][c] * S.R[2][c]) * S.s[c];
+  float gR[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gR[r][c] = dM[r][c] * S.s[c];
+  const float w = S.qn[0], x = S.qn[1], y = S.qn[2], z = S.qn[3];
+  float dq[4];
+  dq[0] = 2.0f * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
+  dq[1] = 2.0f * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0f * x * gR[1][1] - w * gR[1][2] + z * gR[2][0] +
+                  w * gR[2][1] - 2.0f * x * gR[2][2]);
+  dq[2] = 2.0f * (-2.0f * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] - w * gR[2][0] +
+                  z * gR[2][1] - 2.0f * y * gR[2][2]);
+  dq[3] = 2.0f * (-2.0f * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0f * z * gR[1][1] +
+                  y * gR[1][2] + x * gR[2][0] + y * gR[2][1]);
+  const float qd = S.qn[0] * dq[0] + S.qn[1] * dq[1] + S.qn[2] * dq[2] + S.qn[3] * dq[3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) g16[8 + k] += (dq[k] - S.qn[k] * qd) / S.qlen;
 }
 
 // The views slot i was seen in, as a bit mask: every view's tile count is loaded at once.
@@ -181,9 +227,11 @@ __device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t 
 }
 
 // One view's projection backward (train_step.glsl:82-219) of a slot: adds the gradient of
-// the 14 geometry + DC parameters to g16 (without the SH view-direction term, which
-// k_step_sh computes), updates the densification statistics, and returns the clamped
-// colour gradient and the view direction. drew: bit 0 any pair gradient, bit 1 a non-zero
+// the position, opacity and DC parameters to g16 (without the SH view-direction term, which
+// k_step_sh computes) and the 3D covariance's gradient to dsig (when non-null; the caller
+// takes it to the log scales and the quaternion once, scale_rotation_backward), updates
+// the densification statistics, and returns the clamped colour gradient and the view
+// direction. drew: bit 0 any pair gradient, bit 1 a non-zero
 // colour gradient. With POSE it also adds the slot's share of the camera pose gradient to
 // pose (dL/dd, dL/dw; train_step.glsl:196-202).
 // With MOTION and dm non-null the slot is moved with the subject in this view
@@ -193,7 +241,8 @@ __device__ __forceinline__ void view_colour_grad(float4 a1, float4 a2, uint32_t 
 // is added by the caller) and the turn of its orientation dL/dturn (world axes).
 template <int DEG, bool POSE = false, bool MOTION = false>
 __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0, const Geometry& G, float4 a0, float4 a1,
-                                              float4 a2, uint32_t clamped, float radius, float g16[16], float4& st,
+                                              float4 a2, uint32_t clamped, float radius, float g16[16], float* dsig,
+                                              float4& st,
                                               float dcol[3], float dir[3], float& dir_len, uint32_t& drew,
                                               float* pose = nullptr, const Deformed* dm = nullptr,
                                               float* share = nullptr) {
@@ -359,36 +408,15 @@ __device__ __forceinline__ void view_backward(const gs_frame_data& f, float4 p0,
     pose[5] += t[0] * dt[1] - t[1] * dt[0] + (x10 - x01);
   }
 
-  // 3D covariance -> log scale and rotation; dSigma = T^T G2 T folded into dM = 2 dSigma M.
-  float dM[3][3];
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    float dS[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) dS[c] = T[0][r] * G2T[0][c] + T[1][r] * G2T[1][c];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) dM[r][c] = 2.0f * (dS[0] * G.M[0][c] + dS[1] * G.M[1][c] + dS[2] * G.M[2][c]);
+  // 3D covariance: dSigma = T^T G2 T, summed over the views (scale_rotation_backward).
+  if (dsig != nullptr) {
+    dsig[0] += T[0][0] * G2T[0][0] + T[1][0] * G2T[1][0];
+    dsig[1] += T[0][0] * G2T[0][1] + T[1][0] * G2T[1][1];
+    dsig[2] += T[0][0] * G2T[0][2] + T[1][0] * G2T[1][2];
+    dsig[3] += T[0][1] * G2T[0][1] + T[1][1] * G2T[1][1];
+    dsig[4] += T[0][1] * G2T[0][2] + T[1][1] * G2T[1][2];
+    dsig[5] += T[0][2] * G2T[0][2] + T[1][2] * G2T[1][2];
   }
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-    g16[4 + c] += (dM[0][c] * G.R[0][c] + dM[1][c] * G.R[1][c] + dM[2][c] * G.R[2][c]) * G.s[c];
-  float gR[3][3];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gR[r][c] = dM[r][c] * G.s[c];
-  const float w = G.qn[0], x = G.qn[1], y = G.qn[2], z = G.qn[3];
-  float dq[4];
-  dq[0] = 2.0f * (-z * gR[0][1] + y * gR[0][2] + z * gR[1][0] - x * gR[1][2] - y * gR[2][0] + x * gR[2][1]);
-  dq[1] = 2.0f * (y * gR[0][1] + z * gR[0][2] + y * gR[1][0] - 2.0f * x * gR[1][1] - w * gR[1][2] + z * gR[2][0] +
-                  w * gR[2][1] - 2.0f * x * gR[2][2]);
-  dq[2] = 2.0f * (-2.0f * y * gR[0][0] + x * gR[0][1] + w * gR[0][2] + x * gR[1][0] + z * gR[1][2] - w * gR[2][0] +
-                  z * gR[2][1] - 2.0f * y * gR[2][2]);
-  dq[3] = 2.0f * (-2.0f * z * gR[0][0] - w * gR[0][1] + x * gR[0][2] + w * gR[1][0] - 2.0f * z * gR[1][1] +
-                  y * gR[1][2] + x * gR[2][0] + y * gR[2][1]);
-  const float qd = G.qn[0] * dq[0] + G.qn[1] * dq[1] + G.qn[2] * dq[2] + G.qn[3] * dq[3];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) g16[8 + k] += (dq[k] - G.qn[k] * qd) / G.qlen;
 }
 
 __device__ __forceinline__ void adam_params(const StepArgs& a, const gs_frame_data& f0, uint32_t i, float4 p0,
@@ -563,7 +591,7 @@ __global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
 // Part 2 (train_step.glsl:72-240): every view's projection backward summed, plus the SH
 // view-direction term from part 1, then Adam on the 16 parameters.
 template <int DEG, bool MOTION>
-__global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
+__global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
   if (*a.d_pairs > a.accept) return;
@@ -577,6 +605,7 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
   uint32_t drew = 0u;
   Geometry G;
   slot_geometry(p0, p1, q, G);
+  float dsig[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float4 st = a.stats[i];
   // Views in order; the next view's loads are issued before this view's arithmetic.
   uint32_t mask = seen_views(a.tiles, a.n_views, a.cap, i);
@@ -611,12 +640,13 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
       if ((s_frames[v].model[3] & GS_FLAG_MOTION) != 0u) {
         Deformed dm;
         deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, dm);
-        view_backward<DEG, false, true>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, st, dcol,
-                                        dir, dir_len, drew, nullptr, &dm);
+        view_backward<DEG, false, true>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, dsig, st,
+                                        dcol, dir, dir_len, drew, nullptr, &dm);
         continue;
       }
     }
-    view_backward<DEG>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, st, dcol, dir, dir_len, drew);
+    view_backward<DEG>(s_frames[v], p0, G, a0, a1, a2, __float_as_uint(cw), radius, g16, dsig, st, dcol, dir, dir_len,
+                       drew);
   }
   if (DEG > 0) {
     const float4 pd = a.dir_grad[i];
@@ -624,7 +654,10 @@ __global__ void __launch_bounds__(128, 4) k_step_geometry(StepArgs a) {
     g16[1] += pd.y;
     g16[2] += pd.z;
   }
-  if (seen) a.stats[i] = st;
+  if (seen) {
+    scale_rotation_backward(p1, q, dsig, g16);
+    a.stats[i] = st;
+  }
   const gs_frame_data& f0 = s_frames[0];
   const bool sparse = (f0.model[3] & GS_FLAG_SPARSE_ADAM) != 0u;
   if (!sparse || (drew & 1u)) adam_params(a, f0, i, p0, p1, q, p3, g16);
@@ -666,13 +699,14 @@ __global__ void __launch_bounds__(128) k_pose_grad(StepArgs a, float* __restrict
         if ((s_frame.model[3] & GS_FLAG_MOTION) != 0u) {
           Deformed dm;
           deform(a.motion, a.motion.views + size_t(v) * kMaxMotionNodes, i, p0.x, p0.y, p0.z, dm);
-          view_backward<DEG, true, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, st, dcol, dir, dir_len, drew,
-                                         pose, &dm);
+          view_backward<DEG, true, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, nullptr, st, dcol, dir, dir_len,
+                                         drew, pose, &dm);
           done = true;
         }
       }
       if (!done)
-        view_backward<DEG, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, st, dcol, dir, dir_len, drew, pose);
+        view_backward<DEG, true>(s_frame, p0, G, a0, a1, a2, clamped, 0.0f, g16, nullptr, st, dcol, dir, dir_len, drew,
+                                 pose);
     }
   }
 #pragma unroll
@@ -772,7 +806,7 @@ __global__ void __launch_bounds__(128) k_motion_grad(StepArgs a, float* __restri
         uint32_t drew = 0u;
         view_backward<DEG, false, true>(s_frame, p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u],
                                         a.grad2d[g * 3u + 2u], __float_as_uint(a.splat[g * 3u + 2u].w), 0.0f, g16,
-                                        st, dcol, dir, dir_len, drew, nullptr, &dm, share);
+                                        nullptr, st, dcol, dir, dir_len, drew, nullptr, &dm, share);
         if constexpr (K > 0) {
           // The SH view-direction term of dL/dx: U (dd - dir (dir . dd)) / |x - c|.
           float dd[3] = {0.f, 0.f, 0.f};
