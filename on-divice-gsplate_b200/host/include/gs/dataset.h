@@ -51,7 +51,7 @@ void compute_camera_bounds(Dataset& dataset);
 // short side is `target_width` (never enlarged), masks into alpha (255 without masks),
 // every 8th frame held out, unreadable frames skipped and listed (throws when fewer than
 // 2 or half remain). Images are PNG (8/16-bit) or binary PPM/PGM; JPEG frames and depth
-// maps are not decoded by this build (JPEG frames are skipped like unreadable ones).
+// maps are not decoded by libgs_host (JPEG frames are skipped like unreadable ones).
 Dataset load_dataset(const std::string& directory, uint32_t target_width);
 
 struct InitOptions {

@@ -170,7 +170,7 @@ Image decode_image(const std::vector<uint8_t>& bytes, uint32_t channels) {
   static const uint8_t kPng[8] = {137, 80, 78, 71, 13, 10, 26, 10};
   if (bytes.size() >= 8 && std::memcmp(bytes.data(), kPng, 8) == 0) return decode_png(bytes, channels);
   if (bytes.size() >= 3 && bytes[0] == 'P' && (bytes[1] == '5' || bytes[1] == '6')) return decode_pnm(bytes, channels);
-  if (bytes.size() >= 3 && bytes[0] == 0xff && bytes[1] == 0xd8) throw std::runtime_error("JPEG is not decoded by this build");
+  if (bytes.size() >= 3 && bytes[0] == 0xff && bytes[1] == 0xd8) throw std::runtime_error("JPEG images are not decoded (no JPEG decoder in libgs_host)");
   throw std::runtime_error("unknown image format");
 }
 

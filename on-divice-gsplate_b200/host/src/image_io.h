@@ -17,7 +17,7 @@ struct Image {
 // PNG (8 or 16 bits per sample, grey / grey+alpha / RGB / RGBA / palette, not interlaced)
 // or binary PPM (P6) / PGM (P5), converted to `channels` (1: grey or the alpha channel's
 // source for masks, 4: RGBA with alpha 255 where the file has none). Throws
-// std::runtime_error for other formats (JPEG is not decoded by this build).
+// std::runtime_error for other formats (libgs_host has no JPEG decoder).
 Image decode_image(const std::vector<uint8_t>& bytes, uint32_t channels);
 
 // Area resampling (each output pixel is the coverage-weighted mean of the input pixels it

@@ -2,7 +2,7 @@
 
 Writes a small transforms.json capture with PNG images of every colour type the loader
 reads (RGB, RGBA 16-bit, palette, grey + alpha) using every PNG row filter, grey masks, a
-point-cloud PLY and one JPEG frame (which this build does not decode), then checks what
+point-cloud PLY and one JPEG frame (which libgs_host does not decode), then checks what
 bin/gs_host_selftest reports against the reference's rules (dataset.cpp:85-223, 291-523):
 short side resized to the target width by area, intrinsics scaled with it, masks in alpha,
 every 8th frame held out, unreadable frames skipped and listed, points merged per voxel to
