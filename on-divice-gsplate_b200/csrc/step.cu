@@ -26,29 +26,61 @@ struct PairSumArgs {
   uint32_t accept;
 };
 
-// Items in depth order, so consecutive threads sum consecutive runs of pairs (the emit
-// order); an item's count is the gap to the next item's first pair. Items that drew no
-// pair are skipped: the step reads grad2d only where tiles > 0.
-__global__ void __launch_bounds__(128) k_pair_sum(PairSumArgs a) {
+// Items in depth order, so the 32 items of a warp own one contiguous run of pairs (the
+// emit order); an item's count is the gap to the next item's first pair. The warp streams
+// that run through shared memory kSumChunk pairs at a time, with coalesced loads and the
+// next chunk's loads in flight while the lanes add the current one; each lane adds its own
+// item's pairs one after another from zero, the order of train_pair_sum.comp:24-29. Items
+// that drew no pair are skipped: the step reads grad2d only where tiles > 0.
+constexpr uint32_t kSumChunk = 64;
+constexpr uint32_t kSumLoads = kSumChunk * 3u / 32u;  // float4 per lane per chunk
+constexpr uint32_t kSumWarps = 8;
+
+__global__ void __launch_bounds__(kSumWarps * 32) k_pair_sum(PairSumArgs a) {
+  __shared__ float4 s_chunk[kSumWarps][kSumChunk * 3u];
   const uint32_t total = *a.d_pairs;
   if (total > a.accept) return;
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.n_items) return;
-  const uint32_t first = a.first[idx];
-  const uint32_t count = (idx + 1u < a.n_items ? a.first[idx + 1u] : total) - first;
-  if (count == 0u) return;
-  const size_t g = a.order[idx];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t base = (blockIdx.x * kSumWarps + warp) * 32u;
+  if (base >= a.n_items) return;
+  const uint32_t idx = base + lane;
+  // Lanes past the last item own the empty run [total, total).
+  const uint32_t first = idx < a.n_items ? a.first[idx] : total;
+  uint32_t end = __shfl_down_sync(0xffffffffu, first, 1);
+  if (lane == 31u) end = base + 32u < a.n_items ? a.first[base + 32u] : total;
+  const uint32_t r0 = __shfl_sync(0xffffffffu, first, 0), r1 = __shfl_sync(0xffffffffu, end, 31);
+  if (r0 == r1) return;
+  float4* buf = s_chunk[warp];
+  const float4* src = a.pair_grads;
+  float4 v[kSumLoads];
+  auto load = [&](uint32_t c0) {
+    const uint32_t n = min(kSumChunk, r1 - c0) * 3u;
+    const float4* p = src + size_t(c0) * 3u;
+#pragma unroll
+    for (uint32_t j = 0; j < kSumLoads; ++j) {
+      const uint32_t k = lane + 32u * j;
+      v[j] = k < n ? p[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
   float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0, s2 = s0;
-  {
-#pragma unroll 4
-    for (uint32_t k = 0; k < count; ++k) {
-      const size_t q = (size_t(first) + k) * 3u;
-      const float4 x = a.pair_grads[q], y = a.pair_grads[q + 1u], z = a.pair_grads[q + 2u];
+  load(r0);
+  for (uint32_t c0 = r0; c0 < r1; c0 += kSumChunk) {
+    __syncwarp();
+#pragma unroll
+    for (uint32_t j = 0; j < kSumLoads; ++j) buf[lane + 32u * j] = v[j];
+    __syncwarp();
+    if (r1 - c0 > kSumChunk) load(c0 + kSumChunk);
+    const uint32_t lo = max(first, c0), hi = min(end, c0 + kSumChunk);
+    for (uint32_t q = lo; q < hi; ++q) {
+      const float4* t = buf + (q - c0) * 3u;
+      const float4 x = t[0], y = t[1], z = t[2];
       s0.x += x.x; s0.y += x.y; s0.z += x.z; s0.w += x.w;
       s1.x += y.x; s1.y += y.y; s1.z += y.z; s1.w += y.w;
       s2.x += z.x; s2.y += z.y; s2.z += z.z; s2.w += z.w;
     }
   }
+  if (end == first) return;
+  const size_t g = a.order[idx];
   a.grad2d[g * 3u] = s0;
   a.grad2d[g * 3u + 1u] = s1;
   a.grad2d[g * 3u + 2u] = s2;
@@ -1136,7 +1168,8 @@ void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* de
                      const float4* pair_grads, const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
   if (n_items == 0u) return;
   PairSumArgs a{n_items, depth_order, first, pair_grads, vb.grad2d, d_pairs, accept};
-  k_pair_sum<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
+  const uint32_t per_block = kSumWarps * 32u;
+  k_pair_sum<<<(n_items + per_block - 1u) / per_block, per_block, 0, st>>>(a);
 }
 
 template <bool MOTION>
