@@ -261,8 +261,8 @@ int gs_motion_gradient(gs_context* ctx, uint32_t view, double* out, uint32_t cou
    runtimes whose pool owns all device memory and forbids allocations outside it, plugins
    that get only the buffers such a runtime passes them, loops that cannot afford an
    allocation's device synchronisation — this sorts n (key, value) pairs already in device
-   memory, in place, stably by key bits [0, key_bits), with the library's onesweep radix
-   sort, and allocates nothing: its scratch is a static device array sized for
+   memory, in place, stably by key bits [0, key_bits), with the library's radix sort, and
+   allocates nothing: its scratch is a static device array sized for
    GS_SORT_NOALLOC_MAX_ITEMS pairs (about 8.3 MB, held by every GPU that loads the library
    until exit). Larger n is rejected with GS_ERR_INVALID.
    - `stream` is a cudaStream_t (NULL: the legacy default stream) on the current device;

@@ -187,7 +187,7 @@ struct gs_context {
     h_motion_grad = nullptr;
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
                          &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
-                         &d_scalars, &sort.hist, &sort.lookback, &sort.ticket, &sort.err, &dens.spawn,
+                         &d_scalars, &sort.hist, &sort.tile_counts, &sort.ticket, &sort.err, &dens.spawn,
                          &dens.release, &dens.wants, &dens.free_pos, &dens.spawn_pos, &dens.free_list,
                          &dens.counters})
       dev_free(*p);
@@ -249,9 +249,9 @@ struct gs_context {
     dev_alloc(pose_partial, size_t(views) * gsk::pose_blocks(model.cap) * 8u);
     GS_CUDA_TRY(cudaMemsetAsync(vb.tiles, 0, n * sizeof(uint32_t), stream));
     const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
-    if (sort_tiles > sort.lookback_tiles) {
-      dev_alloc(sort.lookback, size_t(sort_tiles) * 256);
-      sort.lookback_tiles = sort_tiles;
+    if (sort_tiles > sort.count_tiles) {
+      dev_alloc(sort.tile_counts, size_t(sort_tiles) * 256);
+      sort.count_tiles = sort_tiles;
     }
     const uint32_t scan_tiles = uint32_t((n + gsk::kScanTile - 1) / gsk::kScanTile);
     if (scan_tiles > sort.scan_tiles) {
@@ -296,9 +296,9 @@ struct gs_context {
     dev_alloc(pair_gaussian, n);
     dev_alloc(pair_grads, n * 3);
     const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
-    if (sort_tiles > sort.lookback_tiles) {
-      dev_alloc(sort.lookback, size_t(sort_tiles) * 256);
-      sort.lookback_tiles = sort_tiles;
+    if (sort_tiles > sort.count_tiles) {
+      dev_alloc(sort.tile_counts, size_t(sort_tiles) * 256);
+      sort.count_tiles = sort_tiles;
     }
     pair_cap = n;
   }

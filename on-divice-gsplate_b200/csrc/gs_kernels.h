@@ -54,8 +54,8 @@ void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, con
 // ---- sort.cu ----
 struct SortScratch {
   uint32_t* hist = nullptr;           // passes x 256 (up to 8 passes: 32-bit keys at 4-bit digits)
-  uint32_t* lookback = nullptr;       // tiles x 256 status words
-  uint32_t lookback_tiles = 0;
+  uint32_t* tile_counts = nullptr;    // 256 x tiles: per-tile digit counts, then the tiles' starts
+  uint32_t count_tiles = 0;
   unsigned long long* scan_lookback = nullptr;
   uint32_t scan_tiles = 0;
   uint32_t* ticket = nullptr;         // 1 word

@@ -6,8 +6,8 @@
 // get only the buffers it passes them, and tight loops where an allocation's implicit
 // device synchronisation costs more than the sort. For them this entry point sorts
 // buffers the caller already owns and takes its scratch — the alternate key/value
-// buffers, the digit histograms, the look-back words, the tile ticket and the error word
-// — from one file-scope device array of fixed size instead of allocating it. Every GPU
+// buffers, the digit histograms and the per-tile digit counts — from one file-scope
+// device array of fixed size instead of allocating it. Every GPU
 // that loads the library holds that array (about 8.3 MB) until the process exits.
 //
 // The first call on a device does the set-up (the array's device address, looked up with
@@ -26,10 +26,8 @@ constexpr uint32_t kMaxTiles = (kMaxItems + gsk::kSortTile - 1u) / gsk::kSortTil
 constexpr size_t kAltKeys = 0;
 constexpr size_t kAltVals = kAltKeys + kMaxItems;
 constexpr size_t kHist = kAltVals + kMaxItems;
-constexpr size_t kLookback = kHist + 4 * 256;
-constexpr size_t kTicket = kLookback + size_t(kMaxTiles) * 256;
-constexpr size_t kErr = kTicket + 1;
-constexpr size_t kWords = kErr + 1;
+constexpr size_t kTileCounts = kHist + 4 * 256;
+constexpr size_t kWords = kTileCounts + size_t(kMaxTiles) * 256;
 
 // The scratch. Host code must not take this name as a device address: it is a host-side
 // stand-in for the symbol. The device address comes from cudaGetSymbolAddress, per device.
@@ -77,26 +75,19 @@ extern "C" int gs_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   gsk::SortScratch s;
   s.hist = base + kHist;
-  s.lookback = base + kLookback;
-  s.lookback_tiles = kMaxTiles;
-  s.ticket = base + kTicket;
-  s.err = base + kErr;
-  // The array keeps the previous call's contents: the error word starts at zero here; the
-  // histograms, look-back words and ticket are cleared by the sort itself.
-  e = cudaMemsetAsync(s.err, 0, sizeof(uint32_t), st);
-  if (e != cudaSuccess) return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: ") + cudaGetErrorString(e));
+  s.tile_counts = base + kTileCounts;
+  s.count_tiles = kMaxTiles;
+  // The array keeps the previous call's contents; the sort clears its histograms and
+  // overwrites the tile counts it reads, so nothing needs clearing here.
   const bool in_alt = gsk::radix_sort_pairs(s, keys, values, base + kAltKeys, base + kAltVals, nullptr, n,
                                             int(key_bits), st, nullptr);
   if (in_alt) {
     cudaMemcpyAsync(keys, base + kAltKeys, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(values, base + kAltVals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
   }
-  uint32_t err = 0;
-  e = cudaMemcpyAsync(&err, s.err, sizeof(err), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  e = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: ") + cudaGetErrorString(e));
-  if (err != 0u) return failed(GS_ERR_TIMEOUT, "gs_sort_pairs_noalloc: a bounded look-back wait gave up");
   gsk::set_last_error("");
   return GS_OK;
 }

@@ -3,16 +3,18 @@
 // The reference sorts with a 3-kernel LSD radix sort of 4-bit digits (count, single
 // workgroup scan, scatter: engine/src/radix_sort.cpp:57-108, radix_{count,scan,scatter}.comp)
 // and scans with scan_local/blocks/add. Here:
-//  - radix_sort_pairs: onesweep LSD sort, digits of 4 to 8 bits (8 by default; the width is
-//    a tuning knob). One kernel computes every pass's
-//    digit histogram; each pass is then one kernel in which a block ranks its 3840 keys
-//    (warp match + per-warp counters, stable), publishes its digit counts and looks back
-//    over its predecessors' (decoupled look-back) for its global digit offsets, then
-//    scatters through shared memory so each digit run is written contiguously.
-//  - exclusive_scan: single-pass scan with decoupled look-back.
-// Blocks take their tile from an atomic ticket, so every predecessor a block waits on is
-// already running; each wait is still bounded (kSpinLimit polls), after which the block
-// records an error word the host turns into GS_ERR_TIMEOUT, and carries on.
+//  - radix_sort_pairs: LSD sort, digits of 4 to 8 bits (8 by default; the width is a tuning
+//    knob). One kernel computes every pass's digit histogram. Each pass then counts the
+//    digits of every 3840-key tile (k_tile_counts), turns each digit's row of tile counts
+//    into the tiles' global starts (k_tile_scan, one block per digit), and ranks and
+//    scatters (k_onesweep): a block ranks its tile's keys (warp match + per-warp counters,
+//    stable) and writes each digit run contiguously through shared memory. No block waits
+//    on another: a decoupled look-back over the previous tiles' counts was measured slower
+//    here, its polls of the same few status lines serialising in L2.
+//  - exclusive_scan: single-pass scan with decoupled look-back. Blocks take their tile from
+//    an atomic ticket, so every predecessor a block waits on is already running; each wait
+//    is still bounded (kSpinLimit polls), after which the block records an error word the
+//    host turns into GS_ERR_TIMEOUT, and carries on.
 #include <cuda/atomic>
 
 #include "gs_kernels.h"
@@ -26,14 +28,6 @@ constexpr int kIpt = 15;  // keys per thread
 constexpr int kRadix = 256;  // digit tables are sized for 8-bit digits; narrower digits use a prefix
 constexpr int kMaxPasses = 8;  // 32-bit keys at 4-bit digits
 constexpr uint32_t kSpinLimit = 1u << 22;
-constexpr uint32_t kAgg = 1u << 30, kPrefix = 2u << 30, kValueMask = (1u << 30) - 1u;
-
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
-  return cuda::atomic_ref<const uint32_t, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
-}
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
-  cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_relaxed);
-}
 __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
   return cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
 }
@@ -103,14 +97,73 @@ __global__ void __launch_bounds__(kThreads) k_histogram_scan(uint32_t* hist, int
   }
 }
 
+// Per-tile digit counts of one pass, digit-major: counts[d * stride + tile].
+__global__ void __launch_bounds__(kThreads) k_tile_counts(const uint32_t* __restrict__ keys, const uint32_t* d_count,
+                                                          uint32_t n_max, int shift, uint32_t mask,
+                                                          uint32_t* __restrict__ counts, uint32_t stride) {
+  __shared__ uint32_t s_count[kRadix];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t n = count_of(d_count, n_max);
+  const uint32_t base = tile * kSortTile;
+  if (base >= n) return;
+  s_count[tid] = 0u;
+  __syncthreads();
+  const uint32_t wbase = base + uint32_t(warp) * 32u * kIpt;
+  uint32_t key[kIpt];
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
+    key[j] = idx < n ? keys[idx] : 0u;
+  }
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
+    if (idx < n) atomicAdd(&s_count[(key[j] >> shift) & mask], 1u);
+  }
+  __syncthreads();
+  counts[size_t(tid) * stride + tile] = s_count[tid];
+}
+
+// Digit `blockIdx.x`: its counts over the live tiles become each tile's global start,
+// pass_offsets[d] plus the counts of the tiles before it (in place).
+constexpr int kRowIpt = 8;
+__global__ void __launch_bounds__(kThreads) k_tile_scan(uint32_t* __restrict__ counts, uint32_t stride,
+                                                        const uint32_t* d_count, uint32_t n_max,
+                                                        const uint32_t* __restrict__ pass_offsets) {
+  __shared__ uint32_t s_warp[kWarps];
+  const uint32_t n = count_of(d_count, n_max);
+  const uint32_t live = (n + kSortTile - 1u) / kSortTile;
+  uint32_t* row = counts + size_t(blockIdx.x) * stride;
+  uint32_t carry = pass_offsets[blockIdx.x];
+  for (uint32_t chunk = 0; chunk < live; chunk += kThreads * kRowIpt) {
+    uint32_t x[kRowIpt], sum = 0u;
+#pragma unroll
+    for (int k = 0; k < kRowIpt; ++k) {
+      const uint32_t t = chunk + uint32_t(threadIdx.x) * kRowIpt + k;
+      x[k] = t < live ? row[t] : 0u;
+      sum += x[k];
+    }
+    uint32_t total;
+    uint32_t run = carry + block_exclusive_scan<uint32_t>(sum, s_warp, total);
+#pragma unroll
+    for (int k = 0; k < kRowIpt; ++k) {
+      const uint32_t t = chunk + uint32_t(threadIdx.x) * kRowIpt + k;
+      if (t < live) row[t] = run;
+      run += x[k];
+    }
+    carry += total;
+  }
+}
+
+// One pass: each block ranks its tile's keys (warp match + per-warp counters, stable) and
+// scatters them through shared memory to its digits' global starts from k_tile_scan.
 __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out, const uint32_t* d_count,
                                                        uint32_t n_max, int shift, uint32_t mask,
-                                                       const uint32_t* __restrict__ pass_offsets, uint32_t* lookback,
-                                                       uint32_t* ticket, uint32_t* err) {
-  __shared__ uint32_t s_tile;
+                                                       const uint32_t* __restrict__ starts, uint32_t stride) {
   __shared__ uint32_t s_wc[kWarps][kRadix];  // per-warp digit counts, then each warp's first block position per digit
   __shared__ uint32_t s_delta[kRadix];       // global position minus block position, per digit
   __shared__ uint32_t s_warp[kWarps];
@@ -118,13 +171,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
   __shared__ uint32_t s_vals[kSortTile];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int k = tid; k < kWarps * kRadix; k += kThreads) (&s_wc[0][0])[k] = 0u;
-  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
-  __syncthreads();
-  const uint32_t tile = s_tile;
+  const uint32_t tile = blockIdx.x;
   const uint32_t n = count_of(d_count, n_max);
   const uint32_t base = tile * kSortTile;
-  if (base >= n) return;  // every later tile is empty too: nobody waits on this one
+  if (base >= n) return;
+  for (int k = tid; k < kWarps * kRadix; k += kThreads) (&s_wc[0][0])[k] = 0u;
+  __syncthreads();
 
   uint32_t key[kIpt], val[kIpt];
   uint16_t rank[kIpt];
@@ -158,6 +210,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
 
   // Digit `tid`: block count, block-local start, then each warp's first block position
   // (one shared read per key in the scatter below).
+  const uint32_t start = starts[size_t(tid) * stride + tile];
   uint32_t count = 0u;
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) count += s_wc[w][tid];
@@ -172,39 +225,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
       running += c;
     }
   }
-
-  // Decoupled look-back on digit `tid`.
-  uint32_t prefix = 0u;
-  if (tile == 0u) {
-    st_relaxed(&lookback[tid], kPrefix | count);
-  } else {
-    st_relaxed(&lookback[size_t(tile) * kRadix + tid], kAgg | count);
-    uint32_t j = tile - 1u, spins = 0u;
-    for (;;) {
-      const uint32_t w = ld_relaxed(&lookback[size_t(j) * kRadix + tid]);
-      const uint32_t status = w & ~kValueMask;
-      if (status == 0u) {
-        if (++spins > kSpinLimit) {
-          atomicExch(err, 1u);
-          break;
-        }
-        if (spins > 64u) __nanosleep(64);
-        continue;
-      }
-      prefix += w & kValueMask;
-      if (status == kPrefix || j == 0u) break;
-      --j;
-    }
-    st_relaxed(&lookback[size_t(tile) * kRadix + tid], kPrefix | ((prefix + count) & kValueMask));
+  s_delta[tid] = start - dstart;
+  if (tid == 0) {
+    s_warp[0] = uint32_t(shift);
+    s_warp[1] = n;
   }
-  s_delta[tid] = pass_offsets[tid] + prefix - dstart;
   __syncthreads();
+  // The shift and count read back from shared memory keep the scatter's digit and bounds
+  // arithmetic below the barrier (computed earlier, they would hold registers through the
+  // scan).
+  const uint32_t shift2 = s_warp[0], n2 = s_warp[1];
 
 #pragma unroll
   for (int j = 0; j < kIpt; ++j) {
     const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
-    if (idx < n) {
-      const uint32_t pos = s_wc[warp][(key[j] >> shift) & mask] + rank[j];
+    if (idx < n2) {
+      const uint32_t pos = s_wc[warp][(key[j] >> shift2) & mask] + rank[j];
       s_keys[pos] = key[j];
       s_vals[pos] = val[j];
     }
@@ -294,15 +330,16 @@ bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint
   const uint32_t hist_blocks = min((n_max + kThreads - 1u) / kThreads, 148u * 8u);
   k_histogram<<<hist_blocks, kThreads, 0, st>>>(keys, d_count, n_max, passes, bits, digit_bits, s.hist);
   k_histogram_scan<<<1, kThreads, 0, st>>>(s.hist, passes);
-  if (launches) *launches += 2 + passes;
+  if (launches) *launches += 2 + 3 * passes;
   uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_alt, *dst_v = vals_alt;
   for (int p = 0; p < passes; ++p) {
     const int shift = digit_bits * p;
     const int width = min(digit_bits, bits - shift);
-    cudaMemsetAsync(s.ticket, 0, sizeof(uint32_t), st);
-    cudaMemsetAsync(s.lookback, 0, sizeof(uint32_t) * size_t(tiles) * kRadix, st);
-    k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, (1u << width) - 1u,
-                                           s.hist + p * kRadix, s.lookback, s.ticket, s.err);
+    const uint32_t mask = (1u << width) - 1u;
+    k_tile_counts<<<tiles, kThreads, 0, st>>>(src_k, d_count, n_max, shift, mask, s.tile_counts, tiles);
+    k_tile_scan<<<mask + 1u, kThreads, 0, st>>>(s.tile_counts, tiles, d_count, n_max, s.hist + p * kRadix);
+    k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, mask, s.tile_counts,
+                                           tiles);
     uint32_t* t = src_k;
     src_k = dst_k;
     dst_k = t;
