@@ -4,10 +4,11 @@
 // workgroup scan, scatter: engine/src/radix_sort.cpp:57-108, radix_{count,scan,scatter}.comp)
 // and scans with scan_local/blocks/add. Here:
 //  - radix_sort_pairs: LSD sort, digits of 4 to 8 bits (8 by default; the width is a tuning
-//    knob). One kernel computes every pass's digit histogram. Each pass then counts the
-//    digits of every 3840-key tile (k_tile_counts), turns each digit's row of tile counts
-//    into the tiles' global starts (k_tile_scan, one block per digit), and ranks and
-//    scatters (k_onesweep): a block ranks its tile's keys (same-digit lanes from one ballot
+//    knob), three kernels a pass. k_tile_counts counts the digits of every 3840-key tile;
+//    k_tile_scan turns each digit's row of tile counts into the tiles' starts within the
+//    digit and the digit's total (one block per digit); k_onesweep ranks and scatters: a
+//    block adds the totals of the smaller digits (one scan) to its tiles' starts, ranks its
+//    tile's keys (same-digit lanes from one ballot
 //    per digit bit, per-warp counters, stable) and writes each digit run contiguously
 //    through shared memory. The ballots replace __match_any_sync, whose pipe was measured
 //    87% busy with 8-bit digits (up to 32 distinct values per warp). No block waits
@@ -28,7 +29,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kIpt = 15;  // keys per thread
 constexpr int kRadix = 256;  // digit tables are sized for 8-bit digits; narrower digits use a prefix
-constexpr int kMaxPasses = 8;  // 32-bit keys at 4-bit digits
 constexpr uint32_t kSpinLimit = 1u << 22;
 __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
   return cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
@@ -65,40 +65,6 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* s_warp, T& total) {
   return warp_prefix + x - v;
 }
 
-// Digit of pass p: bits [digit_bits p, min(digit_bits (p + 1), bits)) of the key.
-__device__ __forceinline__ uint32_t pass_mask(int bits, int digit_bits, int p) {
-  return (1u << min(digit_bits, bits - digit_bits * p)) - 1u;
-}
-
-__global__ void __launch_bounds__(kThreads) k_histogram(const uint32_t* __restrict__ keys, const uint32_t* d_count,
-                                                        uint32_t n_max, int passes, int bits, int digit_bits,
-                                                        uint32_t* __restrict__ hist) {
-  __shared__ uint32_t s_hist[kMaxPasses][kRadix];
-  for (int k = threadIdx.x; k < passes * kRadix; k += kThreads) (&s_hist[0][0])[k] = 0u;
-  __syncthreads();
-  const uint32_t n = count_of(d_count, n_max);
-  for (uint32_t idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
-    const uint32_t key = keys[idx];
-    for (int p = 0; p < passes; ++p)
-      atomicAdd(&s_hist[p][(key >> (digit_bits * p)) & pass_mask(bits, digit_bits, p)], 1u);
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < passes * kRadix; k += kThreads) {
-    const uint32_t c = (&s_hist[0][0])[k];
-    if (c) atomicAdd(&hist[k], c);
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) k_histogram_scan(uint32_t* hist, int passes) {
-  __shared__ uint32_t s_warp[kWarps];
-  for (int p = 0; p < passes; ++p) {
-    uint32_t total;
-    const uint32_t v = hist[p * kRadix + threadIdx.x];
-    const uint32_t ex = block_exclusive_scan<uint32_t>(v, s_warp, total);
-    hist[p * kRadix + threadIdx.x] = ex;
-  }
-}
-
 // Per-tile digit counts of one pass, digit-major: counts[d * stride + tile].
 __global__ void __launch_bounds__(kThreads) k_tile_counts(const uint32_t* __restrict__ keys, const uint32_t* d_count,
                                                           uint32_t n_max, int shift, uint32_t mask,
@@ -127,18 +93,22 @@ __global__ void __launch_bounds__(kThreads) k_tile_counts(const uint32_t* __rest
   counts[size_t(tid) * stride + tile] = s_count[tid];
 }
 
-// Digit `blockIdx.x`: its counts over the live tiles become each tile's global start,
-// pass_offsets[d] plus the counts of the tiles before it (in place).
-constexpr int kRowIpt = 8;
-__global__ void __launch_bounds__(kThreads) k_tile_scan(uint32_t* __restrict__ counts, uint32_t stride,
-                                                        const uint32_t* d_count, uint32_t n_max,
-                                                        const uint32_t* __restrict__ pass_offsets) {
-  __shared__ uint32_t s_warp[kWarps];
+// Digit `blockIdx.x`: its counts over the live tiles become each tile's start within the
+// digit (the counts of the tiles before it, in place), and the digit's total goes to
+// totals[d]. One 1024-thread block per digit: a row of up to 9216 tiles in one sweep.
+constexpr int kRowThreads = 1024;
+constexpr int kRowIpt = 9;
+__global__ void __launch_bounds__(kRowThreads) k_tile_scan(uint32_t* __restrict__ counts, uint32_t stride,
+                                                           const uint32_t* d_count, uint32_t n_max,
+                                                           uint32_t* __restrict__ totals) {
+  __shared__ uint32_t s_warp[kRowThreads / 32];
+  __shared__ uint32_t s_carry;
   const uint32_t n = count_of(d_count, n_max);
   const uint32_t live = (n + kSortTile - 1u) / kSortTile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t* row = counts + size_t(blockIdx.x) * stride;
-  uint32_t carry = pass_offsets[blockIdx.x];
-  for (uint32_t chunk = 0; chunk < live; chunk += kThreads * kRowIpt) {
+  uint32_t carry = 0u;
+  for (uint32_t chunk = 0; chunk < live; chunk += kRowThreads * kRowIpt) {
     uint32_t x[kRowIpt], sum = 0u;
 #pragma unroll
     for (int k = 0; k < kRowIpt; ++k) {
@@ -146,16 +116,37 @@ __global__ void __launch_bounds__(kThreads) k_tile_scan(uint32_t* __restrict__ c
       x[k] = t < live ? row[t] : 0u;
       sum += x[k];
     }
-    uint32_t total;
-    uint32_t run = carry + block_exclusive_scan<uint32_t>(sum, s_warp, total);
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t w = s_warp[lane];
+      uint32_t wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - w;  // exclusive prefix of the warps
+    }
+    __syncthreads();
+    uint32_t run = carry + s_warp[warp] + incl - sum;
 #pragma unroll
     for (int k = 0; k < kRowIpt; ++k) {
       const uint32_t t = chunk + uint32_t(threadIdx.x) * kRowIpt + k;
       if (t < live) row[t] = run;
       run += x[k];
     }
-    carry += total;
+    if (threadIdx.x == kRowThreads - 1) s_carry = run;  // the last thread ends the chunk
+    __syncthreads();
+    carry = s_carry;
   }
+  if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
 // One pass: each block ranks its tile's keys (warp match + per-warp counters, stable) and
@@ -165,10 +156,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out, const uint32_t* d_count,
                                                        uint32_t n_max, int shift, uint32_t mask,
-                                                       const uint32_t* __restrict__ starts, uint32_t stride) {
+                                                       const uint32_t* __restrict__ starts, uint32_t stride,
+                                                       const uint32_t* __restrict__ totals) {
   __shared__ uint32_t s_wc[kWarps][kRadix];  // per-warp digit counts, then each warp's first block position per digit
   __shared__ uint32_t s_delta[kRadix];       // global position minus block position, per digit
-  __shared__ uint32_t s_warp[kWarps];
+  __shared__ unsigned long long s_warp[kWarps];
   __shared__ uint32_t s_keys[kSortTile];
   __shared__ uint32_t s_vals[kSortTile];
 
@@ -219,12 +211,18 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
 
   // Digit `tid`: block count, block-local start, then each warp's first block position
   // (one shared read per key in the scatter below).
+  // The digit's global start: the totals of the smaller digits (one scan over the block,
+  // packed with the block's own counts) plus the counts of the earlier tiles.
   const uint32_t start = starts[size_t(tid) * stride + tile];
+  const uint32_t total = uint32_t(tid) <= mask ? totals[tid] : 0u;
   uint32_t count = 0u;
 #pragma unroll
   for (int w = 0; w < kWarps; ++w) count += s_wc[w][tid];
-  uint32_t block_total;
-  const uint32_t dstart = block_exclusive_scan<uint32_t>(count, s_warp, block_total);
+  unsigned long long both_total;
+  const unsigned long long both =
+      block_exclusive_scan<unsigned long long>((static_cast<unsigned long long>(total) << 32) | count, s_warp,
+                                               both_total);
+  const uint32_t dstart = uint32_t(both), digit_base = uint32_t(both >> 32);
   {
     uint32_t running = dstart;
 #pragma unroll
@@ -234,16 +232,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
       running += c;
     }
   }
-  s_delta[tid] = start - dstart;
-  if (tid == 0) {
-    s_warp[0] = uint32_t(shift);
-    s_warp[1] = n;
-  }
+  s_delta[tid] = digit_base + start - dstart;
+  if (tid == 0) s_warp[0] = static_cast<unsigned long long>(n) << 32 | uint32_t(shift);
   __syncthreads();
   // The shift and count read back from shared memory keep the scatter's digit and bounds
   // arithmetic below the barrier (computed earlier, they would hold registers through the
   // scan).
-  const uint32_t shift2 = s_warp[0], n2 = s_warp[1];
+  const uint32_t shift2 = uint32_t(s_warp[0]), n2 = uint32_t(s_warp[0] >> 32);
 
 #pragma unroll
   for (int j = 0; j < kIpt; ++j) {
@@ -335,20 +330,16 @@ bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint
   digit_bits = digit_bits < 4 ? 4 : (digit_bits > 8 ? 8 : digit_bits);
   const int passes = (bits + digit_bits - 1) / digit_bits;
   const uint32_t tiles = (n_max + kSortTile - 1u) / kSortTile;
-  cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * passes * kRadix, st);
-  const uint32_t hist_blocks = min((n_max + kThreads - 1u) / kThreads, 148u * 8u);
-  k_histogram<<<hist_blocks, kThreads, 0, st>>>(keys, d_count, n_max, passes, bits, digit_bits, s.hist);
-  k_histogram_scan<<<1, kThreads, 0, st>>>(s.hist, passes);
-  if (launches) *launches += 2 + 3 * passes;
+  if (launches) *launches += 3 * passes;
   uint32_t *src_k = keys, *src_v = vals, *dst_k = keys_alt, *dst_v = vals_alt;
   for (int p = 0; p < passes; ++p) {
     const int shift = digit_bits * p;
     const int width = min(digit_bits, bits - shift);
     const uint32_t mask = (1u << width) - 1u;
     k_tile_counts<<<tiles, kThreads, 0, st>>>(src_k, d_count, n_max, shift, mask, s.tile_counts, tiles);
-    k_tile_scan<<<mask + 1u, kThreads, 0, st>>>(s.tile_counts, tiles, d_count, n_max, s.hist + p * kRadix);
+    k_tile_scan<<<mask + 1u, kRowThreads, 0, st>>>(s.tile_counts, tiles, d_count, n_max, s.hist + p * kRadix);
     k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, mask, s.tile_counts,
-                                           tiles);
+                                           tiles, s.hist + p * kRadix);
     uint32_t* t = src_k;
     src_k = dst_k;
     dst_k = t;
