@@ -8,12 +8,12 @@
 //    k_tile_scan turns each digit's row of tile counts into the tiles' starts within the
 //    digit and the digit's total (one block per digit); k_onesweep ranks and scatters: a
 //    block adds the totals of the smaller digits (one scan) to its tiles' starts, ranks its
-//    tile's keys (same-digit lanes from one ballot
-//    per digit bit, per-warp counters, stable) and writes each digit run contiguously
-//    through shared memory. The ballots replace __match_any_sync, whose pipe was measured
-//    87% busy with 8-bit digits (up to 32 distinct values per warp). No block waits
-//    on another: a decoupled look-back over the previous tiles' counts was measured slower
-//    here, its polls of the same few status lines serialising in L2.
+//    tile's keys (same-digit lanes from one ballot per digit bit, per-warp counters,
+//    stable) and writes each digit run contiguously through shared memory. The ballots
+//    replace __match_any_sync, whose pipe was measured 87% busy with 8-bit digits (up to 32
+//    distinct values per warp). No block waits on another: a decoupled look-back over the
+//    previous tiles' counts was measured slower here, its polls of the same few status
+//    lines serialising in L2.
 //  - exclusive_scan: single-pass scan with decoupled look-back. Blocks take their tile from
 //    an atomic ticket, so every predecessor a block waits on is already running; each wait
 //    is still bounded (kSpinLimit polls), after which the block records an error word the
