@@ -67,6 +67,11 @@ constexpr int kPlane = kWin * kS;       // 702
 constexpr int kHRow = kWin * kTile;     // one plane after the row blur: 16 columns x 26 rows, column-major
 constexpr int kHPlane = kHRow + 16;     // padded so neighbouring planes fall on other banks (even: 8-byte aligned)
 constexpr int kAbc = kTilePixels + 16;  // stride of the per-pixel planes after the column blur
+// Threads of an SSIM block: ten warps, so the row blur of k_ssim (312 runs) takes one round
+// and those of k_ssim_grad (936 row runs, 576 column runs) three and two; the per-pixel
+// phases use the first 256.
+constexpr uint32_t kLossThreads = 320;
+constexpr uint32_t kLossWarps = kLossThreads / 32;
 
 // Blur of 4 consecutive outputs from `src` (14 inputs, `stride` apart) into out[4].
 __device__ __forceinline__ void blur4(const float x[kSpan], float out[kRun]) {
@@ -99,12 +104,12 @@ __device__ __forceinline__ void blur_column(const float* src, float out[kRun]) {
   blur4(x, out);
 }
 
-__global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
+__global__ void __launch_bounds__(kLossThreads) k_ssim(LossArgs a) {
   // s_buf: render rgb and target rgb planes of the window (26 x kS each); after the row
   // blur it holds A, B, C and SSIM per channel for the tile's 256 pixels.
   __shared__ float s_buf[6 * kPlane];
   __shared__ __align__(16) float s_h[3 * 5 * kHPlane];  // [channel][moment] after the row blur
-  __shared__ float s_sum[8][2];
+  __shared__ float s_sum[kLossWarps][2];
   const uint32_t gt = blockIdx.x;
   if (gt >= a.vt->total_tiles) return;
   const uint32_t v = view_of_tile(a.vt, gt);
@@ -126,7 +131,7 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   }
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
-  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
+  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += kLossThreads) {
     const uint32_t row = e / kWin, col = e % kWin;
     const int gx = ox + int(col), gy = oy + int(row);
     const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   }
   __syncthreads();
   // Row blur of the five moments: 3 channels x 26 rows x 4 runs.
-  for (uint32_t e = lid; e < 3u * kWin * kQuads; e += 256u) {
+  for (uint32_t e = lid; e < 3u * kWin * kQuads; e += kLossThreads) {
     const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, c = e / (kQuads * kWin);
     const float* xs = s_buf + c * kPlane + row * kS + q * kRun;
     const float* ys = s_buf + (3u + c) * kPlane + row * kS + q * kRun;
@@ -213,7 +218,7 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   __syncthreads();
   const uint32_t lx = lid % kTile, ly = lid / kTile;
   const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
-  const bool inside = px < W && py < H;
+  const bool inside = lid < kTilePixels && px < W && py < H;
   const size_t pix = pbase + size_t(py) * W + px;
   float ssim_sum = 0.0f, wsum = 0.0f;
   if (inside) {
@@ -244,12 +249,12 @@ __global__ void __launch_bounds__(256) k_ssim(LossArgs a) {
   __syncthreads();
   if (lid < 2u) {
     float s = 0.0f;
-    for (int w8 = 0; w8 < 8; ++w8) s += s_sum[w8][lid];
+    for (uint32_t w8 = 0; w8 < kLossWarps; ++w8) s += s_sum[w8][lid];
     a.rb.tile_loss[size_t(gt) * 16u + (lid == 0 ? 2u : 4u)] = s;
   }
 }
 
-__global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
+__global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
   // s_m: the 9 planes (A, B, C x rgb) of the window; after the row blur it holds the
   // 9 blurred planes of the tile's 256 pixels.
   __shared__ float s_m[9 * kPlane];
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   const uint32_t lid = threadIdx.x;
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
-  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += 256u) {
+  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += kLossThreads) {
     const uint32_t row = e / kWin, col = e % kWin;
     const int gx = ox + int(col), gy = oy + int(row);
     const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   }
   __syncthreads();
   // Row blur: 9 planes x 26 rows x 4 runs.
-  for (uint32_t e = lid; e < 9u * kWin * kQuads; e += 256u) {
+  for (uint32_t e = lid; e < 9u * kWin * kQuads; e += kLossThreads) {
     const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, p = e / (kQuads * kWin);
     float out[kRun];
     blur_run(s_m + p * kPlane + row * kS + q * kRun, 1, out);
@@ -305,7 +310,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   __syncthreads();
   // Column blur: 9 planes x 16 columns x 4 runs.
   float* s_g = s_m;  // [plane][kAbc]
-  for (uint32_t e = lid; e < 9u * kTile * kQuads; e += 256u) {
+  for (uint32_t e = lid; e < 9u * kTile * kQuads; e += kLossThreads) {
     const uint32_t col = e % kTile, p = (e / kTile) % 9u, q = e / (9u * kTile);
     float out[kRun];
     blur_column(s_h + p * kHPlane + col * kWin + q * kRun, out);
@@ -315,7 +320,7 @@ __global__ void __launch_bounds__(256) k_ssim_grad(LossArgs a) {
   __syncthreads();
   const uint32_t lx = lid % kTile, ly = lid / kTile;
   const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
-  if (px >= W || py >= H) return;
+  if (lid >= kTilePixels || px >= W || py >= H) return;
   const size_t pix = pbase + size_t(py) * W + px;
   const float4 o = a.rb.pixel_out[pix];
   const float3 y = target_colour(f, target[size_t(py) * W + px]);
@@ -373,12 +378,12 @@ __global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const 
 
 void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
-  k_ssim<<<sp.tile_cap, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
+  k_ssim<<<sp.tile_cap, kLossThreads, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
 }
 
 void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
-  k_ssim_grad<<<sp.tile_cap, 256, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
+  k_ssim_grad<<<sp.tile_cap, kLossThreads, 0, st>>>(LossArgs{sp.frames, sp.vt, rb});
 }
 
 void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, uint32_t stride,
