@@ -501,8 +501,10 @@ __device__ __forceinline__ void copy_frames(const StepArgs& a, gs_frame_data* s_
 // which goes through the normalisation into the position gradient (summed over views,
 // stored for part 2). Then Adam on the 3K coefficients, 3 coefficients' moments loaded
 // together so each thread keeps 18 loads in flight (the SH values are already loaded).
+// Capped at 128 registers (4 blocks per SM, a few spills): 55 us faster on 8 views of 1M
+// slots than 3 blocks at 168 registers; at 5 blocks (96 registers) the spills cost more.
 template <int DEG, bool MOTION>
-__global__ void __launch_bounds__(128, 3) k_step_sh(StepArgs a) {
+__global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
   if (*a.d_pairs > a.accept) return;
