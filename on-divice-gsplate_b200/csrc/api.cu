@@ -62,7 +62,9 @@ uint32_t bits_for(uint32_t n) {
   return bits;
 }
 
-constexpr uint64_t kMaxPairs = (1ull << 30) - 1ull;  // look-back words carry 30-bit counts
+// Pairs a step may hold: below 2^30, so 32-bit pair positions, digit starts and scanned
+// offsets never wrap (48 GB of per-pair gradients at the limit).
+constexpr uint64_t kMaxPairs = (1ull << 30) - 1ull;
 
 }  // namespace
 
@@ -413,7 +415,7 @@ struct gs_context {
       const uint32_t err = h_scalars[2];  // copied with the step's scalars
       if (err != 0u) {
         GS_CUDA_TRY(cudaMemset(sort.err, 0, sizeof(uint32_t)));
-        fail(GS_ERR_TIMEOUT, "a bounded device-side wait (sort/scan look-back) gave up; results discarded");
+        fail(GS_ERR_TIMEOUT, "a bounded device-side wait (the offset scan's look-back) gave up; results discarded");
       }
       const uint64_t pairs = h_scalars[0];
       last_pairs = pairs;
