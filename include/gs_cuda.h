@@ -38,7 +38,7 @@ extern "C" {
 #define GS_ERR_INVALID 1   /* invalid argument */
 #define GS_ERR_NO_MEMORY 2 /* device or host allocation failed */
 #define GS_ERR_CAPACITY 3  /* more pairs than the largest buffer the library will allocate */
-#define GS_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (the offset scan's look-back) */
+#define GS_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (no kernel of the library waits on another) */
 #define GS_ERR_CUDA 5      /* any other CUDA error */
 
 #define GS_MAX_VIEWS 16

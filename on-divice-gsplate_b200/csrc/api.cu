@@ -415,7 +415,7 @@ struct gs_context {
       const uint32_t err = h_scalars[2];  // copied with the step's scalars
       if (err != 0u) {
         GS_CUDA_TRY(cudaMemset(sort.err, 0, sizeof(uint32_t)));
-        fail(GS_ERR_TIMEOUT, "a bounded device-side wait (the offset scan's look-back) gave up; results discarded");
+        fail(GS_ERR_TIMEOUT, "a bounded device-side wait gave up; results discarded");
       }
       const uint64_t pairs = h_scalars[0];
       last_pairs = pairs;

@@ -110,32 +110,56 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   }
 }
 
-// Grid-stride over the stored pairs (the grid is sized for the SMs, not the capacity). At
-// each tile boundary that is also a view boundary the view spans are written too.
+// Grid-stride over the stored pairs, four consecutive keys per thread from one 16-byte
+// load (the grid is sized for the SMs, not the capacity). At each tile boundary that is
+// also a view boundary the view spans are written too.
+__device__ __forceinline__ void range_edge(uint32_t s, uint32_t prev, uint32_t tile, uint2* ranges, const ViewTable* vt,
+                                           uint32_t* view_span) {
+  ranges[prev].y = s;
+  ranges[tile].x = s;
+  const uint32_t v = view_of_tile(vt, tile), vp = view_of_tile(vt, prev);
+  if (v != vp) {
+    view_span[v] = s;
+    view_span[kMaxViews + vp] = s;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count,
                                                 uint32_t capacity, uint2* __restrict__ ranges, const ViewTable* vt,
                                                 uint32_t* __restrict__ view_span) {
   const uint32_t count = min(*d_count, capacity);
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
-    const uint32_t tile = keys[s];
-    if (s == 0u) {
-      ranges[tile].x = 0u;
-      view_span[view_of_tile(vt, tile)] = 0u;
+  if (count == 0u) return;
+  const uint32_t groups = (count + 3u) / 4u;
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+    const uint32_t s0 = 4u * q;
+    uint32_t k[4];
+    if (s0 + 4u <= count) {
+      const uint4 v = *reinterpret_cast<const uint4*>(keys + s0);
+      k[0] = v.x;
+      k[1] = v.y;
+      k[2] = v.z;
+      k[3] = v.w;
     } else {
-      const uint32_t prev = keys[s - 1u];
-      if (prev != tile) {
-        ranges[prev].y = s;
-        ranges[tile].x = s;
-        const uint32_t v = view_of_tile(vt, tile), vp = view_of_tile(vt, prev);
-        if (v != vp) {
-          view_span[v] = s;
-          view_span[kMaxViews + vp] = s;
-        }
-      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) k[j] = s0 + j < count ? keys[s0 + j] : 0u;
     }
-    if (s == count - 1u) {
-      ranges[tile].y = count;
-      view_span[kMaxViews + view_of_tile(vt, tile)] = count;
+    uint32_t prev = s0 > 0u ? keys[s0 - 1u] : 0u;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t s = s0 + uint32_t(j);
+      if (s >= count) break;
+      const uint32_t tile = k[j];
+      if (s == 0u) {
+        ranges[tile].x = 0u;
+        view_span[view_of_tile(vt, tile)] = 0u;
+      } else if (prev != tile) {
+        range_edge(s, prev, tile, ranges, vt, view_span);
+      }
+      if (s == count - 1u) {
+        ranges[tile].y = count;
+        view_span[kMaxViews + view_of_tile(vt, tile)] = count;
+      }
+      prev = tile;
     }
   }
 }
@@ -155,8 +179,8 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
                    const ViewTable* vt, uint32_t* view_span, cudaStream_t st) {
   if (pair_capacity == 0u) return;
-  k_ranges<<<min((pair_capacity + 255u) / 256u, 148u * 16u), 256, 0, st>>>(sorted_keys, d_count, pair_capacity,
-                                                                          ranges, vt, view_span);
+  k_ranges<<<min((pair_capacity + 1023u) / 1024u, 148u * 8u), 256, 0, st>>>(sorted_keys, d_count, pair_capacity,
+                                                                              ranges, vt, view_span);
 }
 
 }  // namespace gsk

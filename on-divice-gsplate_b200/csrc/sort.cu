@@ -14,12 +14,9 @@
 //    distinct values per warp). No block waits on another: a decoupled look-back over the
 //    previous tiles' counts was measured slower here, its polls of the same few status
 //    lines serialising in L2.
-//  - exclusive_scan: single-pass scan with decoupled look-back. Blocks take their tile from
-//    an atomic ticket, so every predecessor a block waits on is already running; each wait
-//    is still bounded (kSpinLimit polls), after which the block records an error word the
-//    host turns into GS_ERR_TIMEOUT, and carries on.
-#include <cuda/atomic>
-
+//  - exclusive_scan: three kernels (tile sums with the gathered values staged in the
+//    output, one block scanning the tile sums, then each tile's own scan), again with no
+//    block waiting on another, so no kernel of the sort or the scan spins on a flag.
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -29,14 +26,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kIpt = 15;  // keys per thread
 constexpr int kRadix = 256;  // digit tables are sized for 8-bit digits; narrower digits use a prefix
-constexpr uint32_t kSpinLimit = 1u << 22;
-__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
-  return cuda::atomic_ref<const unsigned long long, cuda::thread_scope_device>(*p).load(cuda::memory_order_relaxed);
-}
-__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
-  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_relaxed);
-}
-
 __device__ __forceinline__ uint32_t count_of(const uint32_t* d_count, uint32_t n_max) {
   return d_count != nullptr ? min(*d_count, n_max) : n_max;
 }
@@ -261,61 +250,104 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
 
 constexpr int kScanIpt = 8;
 
-__global__ void __launch_bounds__(kThreads) k_scan(const uint32_t* __restrict__ in, const uint32_t* __restrict__ gather,
-                                                   uint32_t* __restrict__ out, uint32_t n, uint32_t* d_total,
-                                                   unsigned long long* lookback, uint32_t* ticket, uint32_t* err) {
-  __shared__ uint32_t s_tile;
-  __shared__ unsigned long long s_warp[kWarps];
-  __shared__ unsigned long long s_prefix;
-  const int tid = threadIdx.x;
-  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+// Exclusive scan in three kernels, none waiting on another. k_scan_sums: each 2048-item
+// tile gathers its values (through `gather` when given) into out[] and writes its sum;
+// k_scan_tiles: one block turns the tile sums into tile starts (64-bit) and the total;
+// k_scan_apply: each tile scans its gathered values from out[] and adds its start.
+__global__ void __launch_bounds__(kThreads) k_scan_sums(const uint32_t* __restrict__ in,
+                                                        const uint32_t* __restrict__ gather, uint32_t* __restrict__ out,
+                                                        uint32_t n, unsigned long long* __restrict__ tile_sums) {
+  __shared__ uint32_t s_warp[kWarps];
+  const uint32_t base = blockIdx.x * kScanTile;
+  uint32_t sum = 0u;
+#pragma unroll
+  for (int j = 0; j < kScanIpt; ++j) {
+    const uint32_t idx = base + uint32_t(j) * kThreads + threadIdx.x;  // coalesced
+    if (idx < n) {
+      const uint32_t x = in[gather != nullptr ? gather[idx] : idx];
+      out[idx] = x;
+      sum += x;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31u) == 0u) s_warp[threadIdx.x >> 5] = sum;
   __syncthreads();
-  const uint32_t tile = s_tile;
-  const uint32_t base = tile * kScanTile;
-  if (base >= n) return;
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < kWarps; ++w) t += s_warp[w];
+    tile_sums[blockIdx.x] = t;
+  }
+}
+
+constexpr int kTileScanThreads = 1024;
+constexpr int kTileScanIpt = 4;
+
+__global__ void __launch_bounds__(kTileScanThreads) k_scan_tiles(unsigned long long* __restrict__ tile_sums,
+                                                                 uint32_t tiles, uint32_t* d_total) {
+  __shared__ unsigned long long s_warp[kTileScanThreads / 32];
+  __shared__ unsigned long long s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long carry = 0;
+  for (uint32_t chunk = 0; chunk < tiles; chunk += kTileScanThreads * kTileScanIpt) {
+    unsigned long long x[kTileScanIpt], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kTileScanIpt; ++k) {
+      const uint32_t t = chunk + uint32_t(threadIdx.x) * kTileScanIpt + k;
+      x[k] = t < tiles ? tile_sums[t] : 0ull;
+      sum += x[k];
+    }
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned long long w = s_warp[lane];
+      unsigned long long wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      s_warp[lane] = wi - w;
+    }
+    __syncthreads();
+    unsigned long long run = carry + s_warp[warp] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kTileScanIpt; ++k) {
+      const uint32_t t = chunk + uint32_t(threadIdx.x) * kTileScanIpt + k;
+      if (t < tiles) tile_sums[t] = run;
+      run += x[k];
+    }
+    if (threadIdx.x == kTileScanThreads - 1) s_carry = run;
+    __syncthreads();
+    carry = s_carry;
+  }
+  if (threadIdx.x == 0 && d_total != nullptr) *d_total = uint32_t(carry);
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan_apply(uint32_t* __restrict__ out, uint32_t n,
+                                                         const unsigned long long* __restrict__ tile_starts) {
+  __shared__ unsigned long long s_warp[kWarps];
+  const uint32_t base = blockIdx.x * kScanTile;
   uint32_t x[kScanIpt];
   unsigned long long sum = 0;
 #pragma unroll
   for (int j = 0; j < kScanIpt; ++j) {
-    const uint32_t idx = base + uint32_t(tid) * kScanIpt + j;
-    x[j] = idx < n ? in[gather != nullptr ? gather[idx] : idx] : 0u;
+    const uint32_t idx = base + uint32_t(threadIdx.x) * kScanIpt + j;
+    x[j] = idx < n ? out[idx] : 0u;
     sum += x[j];
   }
   unsigned long long block_total;
-  const unsigned long long ex = block_exclusive_scan<unsigned long long>(sum, s_warp, block_total);
-  constexpr unsigned long long kA = 1ull << 62, kP = 2ull << 62, kM = (1ull << 62) - 1ull;
-  if (tid == 0) {
-    unsigned long long prefix = 0;
-    if (tile == 0u) {
-      st_relaxed64(&lookback[0], kP | block_total);
-    } else {
-      st_relaxed64(&lookback[tile], kA | block_total);
-      uint32_t j = tile - 1u, spins = 0u;
-      for (;;) {
-        const unsigned long long w = ld_relaxed64(&lookback[j]);
-        const unsigned long long status = w & ~kM;
-        if (status == 0ull) {
-          if (++spins > kSpinLimit) {
-            atomicExch(err, 1u);
-            break;
-          }
-          if (spins > 64u) __nanosleep(64);
-          continue;
-        }
-        prefix += w & kM;
-        if (status == kP || j == 0u) break;
-        --j;
-      }
-      st_relaxed64(&lookback[tile], kP | ((prefix + block_total) & kM));
-    }
-    s_prefix = prefix;
-    if (d_total != nullptr && base + kScanTile >= n) *d_total = uint32_t(prefix + block_total);
-  }
-  __syncthreads();
-  unsigned long long run = s_prefix + ex;
+  unsigned long long run =
+      tile_starts[blockIdx.x] + block_exclusive_scan<unsigned long long>(sum, s_warp, block_total);
 #pragma unroll
   for (int j = 0; j < kScanIpt; ++j) {
-    const uint32_t idx = base + uint32_t(tid) * kScanIpt + j;
+    const uint32_t idx = base + uint32_t(threadIdx.x) * kScanIpt + j;
     if (idx < n) out[idx] = uint32_t(run);
     run += x[j];
   }
@@ -357,10 +389,10 @@ void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* ga
     return;
   }
   const uint32_t tiles = (n + kScanTile - 1u) / kScanTile;
-  cudaMemsetAsync(s.ticket, 0, sizeof(uint32_t), st);
-  cudaMemsetAsync(s.scan_lookback, 0, sizeof(unsigned long long) * tiles, st);
-  k_scan<<<tiles, kThreads, 0, st>>>(in, gather, out, n, d_total, s.scan_lookback, s.ticket, s.err);
-  if (launches) *launches += 1;
+  k_scan_sums<<<tiles, kThreads, 0, st>>>(in, gather, out, n, s.scan_lookback);
+  k_scan_tiles<<<1, kTileScanThreads, 0, st>>>(s.scan_lookback, tiles, d_total);
+  k_scan_apply<<<tiles, kThreads, 0, st>>>(out, n, s.scan_lookback);
+  if (launches) *launches += 3;
 }
 
 }  // namespace gsk
