@@ -179,6 +179,7 @@ struct gs_context {
     for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial, &motion_partial,
                      &ssim_last})
       dev_free(*p);
+    dev_free(vb.spans);
     dev_free(motion_rest);
     dev_free(motion_bind);
     dev_free(d_motion_views);
@@ -239,6 +240,7 @@ struct gs_context {
     const size_t n = size_t(views) * model.cap;
     dev_alloc(vb.splat, n * 3);
     dev_alloc(vb.foot, n);
+    dev_alloc(vb.spans, n);
     dev_alloc(vb.tiles, n);
     dev_alloc(vb.offsets, n);
     dev_alloc(vb.grad2d, n * 3);

@@ -175,6 +175,39 @@ __device__ __forceinline__ uint2 footprint_row_tiles(float mx, float my, float a
   return make_uint2(uint32_t(cols.x) / kTile, uint32_t(cols.y) / kTile + 1u);
 }
 
+// Tile count of the ellipse, and its tile-row spans packed for the pair emission:
+// x = first tile row | rows << 16 | bit 31 when the spans below are complete; y, z, w hold
+// rows 0-5 as 16 bits each, first tile (10 bits) | tiles in the row (6 bits) << 10. More
+// than 6 rows, a first tile past 1023 or a row of 64 tiles or more leave bit 31 clear (the
+// emission walks the rows again).
+__device__ __forceinline__ uint32_t footprint_count_spans(float mx, float my, float a, float b, float c, float t,
+                                                          uint32_t width, uint32_t height, uint4& packed) {
+  const int2 rows = footprint_rows(mx, my, c, t, height);
+  uint32_t tiles = 0u;
+  packed = make_uint4(0u, 0u, 0u, 0u);
+  if (rows.x <= rows.y) {
+    const uint32_t ty0 = uint32_t(rows.x) / kTile, ty1 = uint32_t(rows.y) / kTile;
+    const uint32_t n_rows = ty1 - ty0 + 1u;
+    bool complete = n_rows <= 6u;
+    unsigned long long lo = 0ull;
+    uint32_t hi = 0u;
+    for (uint32_t ty = ty0; ty <= ty1; ++ty) {
+      const uint2 span = footprint_row_tiles(mx, my, a, b, c, t, rows, ty, width);
+      const uint32_t w = span.y - span.x;
+      tiles += w;
+      complete = complete && span.x < 1024u && w < 64u;
+      if (complete) {
+        const uint32_t r = ty - ty0, v = span.x | w << 10;
+        if (r < 4u) lo |= static_cast<unsigned long long>(v) << (16u * r);
+        else hi |= v << (16u * (r - 4u));
+      }
+    }
+    packed = make_uint4(ty0 | min(n_rows, 255u) << 16 | (complete ? 1u << 31 : 0u), uint32_t(lo), uint32_t(lo >> 32),
+                        hi);
+  }
+  return tiles;
+}
+
 // Tile count of the ellipse (train_project.comp:75-81).
 __device__ __forceinline__ uint32_t footprint_count(float mx, float my, float a, float b, float c, float t,
                                                     uint32_t width, uint32_t height) {

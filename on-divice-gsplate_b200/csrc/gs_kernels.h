@@ -30,6 +30,7 @@ struct Model {
 struct ViewBuffers {
   float4* splat = nullptr;   // 3 per g: (mean xy, depth, opacity), (conic abc, radius), (rgb, clamp bits)
   float4* foot = nullptr;    // 1 per g: dilated 2D covariance abc, footprint threshold
+  uint4* spans = nullptr;    // 1 per g: the footprint's tile-row spans, packed (footprint_count_spans)
   uint32_t* tiles = nullptr; // tiles touched
   uint32_t* offsets = nullptr;  // first pair, pre-sort order
   float4* grad2d = nullptr;  // 3 per g: summed pair gradients (train_pair_sum layout)

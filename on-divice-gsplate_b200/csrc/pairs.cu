@@ -1,9 +1,10 @@
 // Pair emission and tile ranges.
 //
 // launch_emit: train_emit.comp:26-64. Items come in depth order (the depth sort of every
-// (view, slot)); each writes its (tile, gaussian) pairs at its scanned offset, walking
-// the same footprint rows train_project counted (train_common.glsl:185-213) from the
-// stored records. The pair key is the global tile (view tile base + tile), so one stable
+// (view, slot)); each writes its (tile, gaussian) pairs at its scanned offset, over the
+// same footprint rows train_project counted (train_common.glsl:185-213): the row spans the
+// projection packed while counting, or, for footprints too large to pack, the same walk
+// again from the stored records. The pair key is the global tile (view tile base + tile), so one stable
 // sort by key leaves every tile's pairs front to back, ties in slot order — the order a
 // (tile, depth16, index) sort gives (test_trainer.cpp:197-233).
 // launch_ranges: train_ranges.comp:14-29 over the sorted keys.
@@ -21,6 +22,7 @@ struct EmitArgs {
   const uint32_t* total;  // the scan's total: the end of the last item's pairs
   const float4* splat;
   const float4* foot;
+  const uint4* spans;
   uint32_t* offsets;
   uint32_t* keys;
   uint32_t* values;
@@ -60,8 +62,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
     const uint32_t g = a.sorted_vals[k];
     const uint32_t v = g / a.cap;
     const gs_frame_data& f = a.frames[v];
-    const float4 q0 = a.splat[size_t(g) * 3u];
-    const float4 fp = a.foot[g];
+    const uint4 packed = a.spans[g];
     a.offsets[g] = p;
     const uint32_t end = min(p + count, a.pair_capacity);
     const uint32_t tile_base = a.vt->tile_base[v];
@@ -77,12 +78,27 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
       }
     };
     uint32_t wanted = 0u;
-    const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
-    if (rows.x <= rows.y) {
-      for (uint32_t ty = uint32_t(rows.x) / kTile; ty <= uint32_t(rows.y) / kTile; ++ty) {
-        const uint2 span = footprint_row_tiles(q0.x, q0.y, fp.x, fp.y, fp.z, fp.w, rows, ty, width);
-        wanted += span.y - span.x;
-        for (uint32_t x = span.x; x < span.y && p < end; ++x) put(p++, tile_base + ty * tiles_x + x);
+    if (packed.x >> 31) {
+      // The row spans the projection packed while counting (footprint_count_spans).
+      const uint32_t ty0 = packed.x & 0xffffu, n_rows = (packed.x >> 16) & 0xffu;
+      const unsigned long long lo = packed.y | static_cast<unsigned long long>(packed.z) << 32;
+      for (uint32_t r = 0; r < n_rows; ++r) {
+        const uint32_t bits = r < 4u ? uint32_t(lo >> (16u * r)) & 0xffffu : (packed.w >> (16u * (r - 4u))) & 0xffffu;
+        const uint32_t x0 = bits & 1023u, x1 = x0 + (bits >> 10);
+        wanted += x1 - x0;
+        const uint32_t row = tile_base + (ty0 + r) * tiles_x;
+        for (uint32_t x = x0; x < x1 && p < end; ++x) put(p++, row + x);
+      }
+    } else {
+      const float4 q0 = a.splat[size_t(g) * 3u];
+      const float4 fp = a.foot[g];
+      const int2 rows = footprint_rows(q0.x, q0.y, fp.z, fp.w, height);
+      if (rows.x <= rows.y) {
+        for (uint32_t ty = uint32_t(rows.x) / kTile; ty <= uint32_t(rows.y) / kTile; ++ty) {
+          const uint2 span = footprint_row_tiles(q0.x, q0.y, fp.x, fp.y, fp.z, fp.w, rows, ty, width);
+          wanted += span.y - span.x;
+          for (uint32_t x = span.x; x < span.y && p < end; ++x) put(p++, tile_base + ty * tiles_x + x);
+        }
       }
     }
     if (wanted != count) {
@@ -171,8 +187,9 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
                  uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
                  uint32_t* mismatch, cudaStream_t st) {
   if (n_items == 0u) return;
-  EmitArgs a{sp.frames, sp.vt,   cap,       n_items, pair_capacity, sorted_vals, sorted_offsets, total,
-             vb.splat,  vb.foot, vb.offsets, keys,   values,        pair_gaussian, pair_grads,   mismatch};
+  EmitArgs a{sp.frames, sp.vt,    cap,        n_items, pair_capacity, sorted_vals, sorted_offsets,
+             total,     vb.splat, vb.foot,    vb.spans, vb.offsets, keys,  values,       pair_gaussian,
+             pair_grads, mismatch};
   k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 

@@ -5,9 +5,12 @@
 // the views of a slot chunk are neighbouring blocks, so a chunk's parameters (four
 // coalesced float4 planes, the SH planes when visible) come from HBM once per step and
 // from L2 for the other views. HBM-bound: per slot and view it writes 48 B of splat
-// record, 16 B of footprint, a tile count and a depth key/value pair. At 72 registers
-// 7 blocks fit per SM; a thread per slot looping over the views (128 registers, 4 blocks
-// per SM) measured 0.54 ms against 0.43 ms for 8 views of 1M slots.
+// record, 16 B of footprint, a tile count and a depth key/value pair, and for slots with
+// pairs the tile-row spans the count walked, packed for the pair emission (which then
+// reads 16 B instead of repeating the walk's divisions and square roots). Capped at 72
+// registers, 7 blocks per SM. A thread per slot looping over the views (128 registers,
+// 4 blocks per SM) measured 0.54 ms against 0.43 ms for 8 views of 1M slots (0.48 ms with
+// the spans, which take 0.09 ms off the emission).
 //
 // With MOTION (any view of the step has GS_FLAG_MOTION) a slot is first moved with the
 // subject in the views that have the flag (train_project.comp:36-41): its position by the
@@ -26,6 +29,7 @@ struct ProjectArgs {
   const float* SH;
   float4* splat;
   float4* foot;
+  uint4* spans;
   uint32_t* tiles;
   uint32_t* dkeys;
   uint32_t* dvals;
@@ -34,7 +38,7 @@ struct ProjectArgs {
 };
 
 template <int DEG, bool MOTION>
-__global__ void __launch_bounds__(128) k_project(ProjectArgs a) {
+__global__ void __launch_bounds__(128, 7) k_project(ProjectArgs a) {
   // Block b projects 128 slots into one view: view b % n_views of slot chunk b / n_views,
   // so the views of a chunk run in neighbouring blocks and re-read its parameters from L2.
   __shared__ gs_frame_data s_frame;
@@ -75,6 +79,7 @@ __global__ void __launch_bounds__(128) k_project(ProjectArgs a) {
     const size_t g = size_t(v) * a.cap + i;
     float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0, o2 = o0, o3 = o0;
     uint32_t tiles = 0u;
+    uint4 spans = make_uint4(0u, 0u, 0u, 0u);
     float x0 = p0.x, x1 = p0.y, x2 = p0.z;
     float W[3][3];  // rest frame -> camera, for the covariance
     float U[3][3];  // the orientation's turn (MOTION only)
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(128) k_project(ProjectArgs a) {
         const float lambda = mid + sqrtf(fmaxf(0.1f, mid * mid - det));
         const float sigma = sqrtf(lambda);
         const float thr = footprint_threshold(opacity);
-        tiles = footprint_count(mx, my, ca, cb, cc, thr, f.image[0], f.image[1]);
+        tiles = footprint_count_spans(mx, my, ca, cb, cc, thr, f.image[0], f.image[1], spans);
         if (tiles > 0u) {
           o3 = make_float4(ca, cb, cc, thr);
           float dx = x0 - f.cam_pos[0], dy = x1 - f.cam_pos[1], dz = x2 - f.cam_pos[2];
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(128) k_project(ProjectArgs a) {
     a.splat[g * 3u + 1u] = o1;
     a.splat[g * 3u + 2u] = o2;
     a.foot[g] = o3;
+    if (tiles > 0u) a.spans[g] = spans;  // emission reads it only for slots with pairs
     a.tiles[g] = tiles;
     const uint32_t key =
         tiles > 0u ? uint32_t(clampf(log2f(o0.z / kNear) / kLogRange, 0.0f, 1.0f) * 65535.0f) : 0xffffu;
@@ -208,7 +214,7 @@ void launch_project(const StepPointers& sp, const Model& m, uint32_t degree, con
                     uint32_t* depth_keys, uint32_t* depth_vals, bool zero_grad2d, const Motion* motion,
                     cudaStream_t st) {
   if (m.slots == 0 || sp.n_views == 0) return;
-  ProjectArgs a{sp.frames, sp.n_views, m.slots, m.cap, m.P, m.SH, vb.splat, vb.foot, vb.tiles,
+  ProjectArgs a{sp.frames, sp.n_views, m.slots, m.cap, m.P, m.SH, vb.splat, vb.foot, vb.spans, vb.tiles,
                 depth_keys, depth_vals, zero_grad2d ? vb.grad2d : nullptr, motion ? *motion : Motion{}};
   const dim3 grid(((m.slots + 127u) / 128u) * sp.n_views), block(128);
   if (motion != nullptr) project_degree<true>(degree, grid, block, st, a);
