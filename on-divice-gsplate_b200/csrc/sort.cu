@@ -138,8 +138,35 @@ __global__ void __launch_bounds__(kRowThreads) k_tile_scan(uint32_t* __restrict_
   if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
-// One pass: each block ranks its tile's keys (warp match + per-warp counters, stable) and
-// scatters them through shared memory to its digits' global starts from k_tile_scan.
+// Ranks of a warp's keys within its digit runs (stable), counting into the warp's row of
+// s_wc. kFull: every key of the tile is valid (all tiles but the last), so no lane test.
+template <bool kFull>
+__device__ __forceinline__ void rank_keys(const uint32_t (&key)[kIpt], uint16_t (&rank)[kIpt], uint32_t* wc,
+                                          uint32_t lane, uint32_t wbase, uint32_t n, int shift, uint32_t mask) {
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < kIpt; ++j) {
+    const bool valid = kFull || wbase + uint32_t(j) * 32u + lane < n;
+    const uint32_t digit = valid ? (key[j] >> shift) & mask : uint32_t(kRadix);
+    // The lanes holding the same digit, from one ballot per digit bit.
+    uint32_t peers = kFull ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const bool bit = (digit >> b) & 1u;
+      const uint32_t set = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? set : ~set;
+    }
+    uint32_t before = 0u;
+    if (valid) before = wc[digit];
+    __syncwarp();
+    if (valid && lane == uint32_t(__ffs(peers) - 1)) wc[digit] = before + __popc(peers);
+    __syncwarp();
+    rank[j] = uint16_t(before + __popc(peers & lanemask_lt));
+  }
+}
+
+// One pass: each block ranks its tile's keys (same-digit lanes from ballots, per-warp
+// counters, stable) and scatters them through shared memory to its digits' global starts.
 __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
@@ -175,33 +202,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __rest
       val[j] = 0u;
     }
   }
-  const uint32_t lanemask_lt = (1u << lane) - 1u;
-#pragma unroll
-  for (int j = 0; j < kIpt; ++j) {
-    const uint32_t idx = wbase + uint32_t(j) * 32u + lane;
-    const bool valid = idx < n;
-    const uint32_t digit = valid ? (key[j] >> shift) & mask : uint32_t(kRadix);
-    // The lanes holding the same digit, from one ballot per digit bit.
-    uint32_t peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const bool bit = (digit >> b) & 1u;
-      const uint32_t set = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? set : ~set;
-    }
-    uint32_t before = 0u;
-    if (valid) before = s_wc[warp][digit];
-    __syncwarp();
-    if (valid && lane == __ffs(peers) - 1) s_wc[warp][digit] = before + __popc(peers);
-    __syncwarp();
-    rank[j] = uint16_t(before + __popc(peers & lanemask_lt));
-  }
+  if (base + kSortTile <= n) rank_keys<true>(key, rank, s_wc[warp], lane, wbase, n, shift, mask);
+  else rank_keys<false>(key, rank, s_wc[warp], lane, wbase, n, shift, mask);
   __syncthreads();
 
-  // Digit `tid`: block count, block-local start, then each warp's first block position
-  // (one shared read per key in the scatter below).
-  // The digit's global start: the totals of the smaller digits (one scan over the block,
-  // packed with the block's own counts) plus the counts of the earlier tiles.
+  // Digit `tid`: block count and block-local start, then each warp's first block position
+  // (one shared read per key in the scatter below). The digit's global start is the totals
+  // of the smaller digits (one scan over the block, packed with the block's own counts)
+  // plus the counts of the earlier tiles.
   const uint32_t start = starts[size_t(tid) * stride + tile];
   const uint32_t total = uint32_t(tid) <= mask ? totals[tid] : 0u;
   uint32_t count = 0u;
