@@ -108,19 +108,23 @@ def test_sixteen_ragged_views_match_oracle(ctx):
     assert rel_l2(gsh, refsh) < 1e-3
 
 
-def test_one_gaussian_covers_every_tile(ctx):
+@pytest.mark.parametrize("width,height,focal", [(100, 70, 80.0), (1200, 64, 400.0)])
+def test_one_gaussian_covers_every_tile(ctx, width, height, focal):
+    """A footprint larger than the view: more than 6 tile rows (100x70), or rows of 75
+    tiles (1200x64), both beyond what the projection packs for the pair emission, which
+    then walks the rows again."""
     scene = S.make_test_scene(1, 0, 3)
     scene.params[0, 0:3] = 0.0
     scene.params[0, 4:7] = np.log(2.0)  # far wider than the view
     scene.params[0, 3] = 2.0
-    cam = S.front_camera(100, 70, 80.0)
+    cam = S.front_camera(width, height, focal)
     opt = F.frozen_options(0, False)
     fr = frame_for(scene, cam, opt, (0.0, 0.0, 0.0))
-    target = np.full((70, 100, 4), 200, np.uint8)
+    target = np.full((height, width, 4), 200, np.uint8)
     ctx.model_init(scene.params, scene.sh)
     ctx.set_views([fr], [target])
     res = ctx.step(True)
-    tiles = ((100 + 15) // 16) * ((70 + 15) // 16)
+    tiles = ((width + 15) // 16) * ((height + 15) // 16)
     assert res.pairs[0] == tiles and ctx.snapshot("tiles")[0] == tiles
     r = O.forward_view(fr, scene.params, scene.sh, target, ssim=True, backward=False,
                        projected=ctx.snapshot("projected"), depth_keys=ctx.snapshot("depth_key"))
