@@ -135,9 +135,8 @@ struct gs_context {
   float4* pair_grads = nullptr;
   const uint32_t* sorted_keys = nullptr;
   const uint32_t* sorted_values = nullptr;
-  // scalars: [0] pairs (the scan's total), [1] emit mismatches (whole run)
-  // Step scalars: [0] pairs, [1] emit mismatches (accumulate), [2] the sort's error word,
-  // [3] unused, [4 + v] first pair of view v, [4 + kMaxViews + v] its end.
+  // Step scalars: [0] pairs, [1] emit mismatches (accumulate), [2] and [3] unused,
+  // [4 + v] first pair of view v, [4 + kMaxViews + v] its end.
   static constexpr uint32_t kScalars = 4 + 2 * GS_MAX_VIEWS;
   uint32_t* d_scalars = nullptr;
   uint32_t* h_scalars = nullptr;  // pinned
@@ -190,7 +189,7 @@ struct gs_context {
     h_motion_grad = nullptr;
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
                          &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
-                         &d_scalars, &sort.hist, &sort.tile_counts, &sort.ticket, &sort.err, &dens.spawn,
+                         &d_scalars, &sort.hist, &sort.tile_counts, &dens.spawn,
                          &dens.release, &dens.wants, &dens.free_pos, &dens.spawn_pos, &dens.free_list,
                          &dens.counters})
       dev_free(*p);
@@ -327,7 +326,6 @@ struct gs_context {
   void enqueue_step(bool train, uint32_t degree) {
     GS_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(uint32_t) * gsk::kQueueCount, stream));
     record(train, degree);
-    GS_CUDA_TRY(cudaMemcpyAsync(d_scalars + 2, sort.err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
     GS_CUDA_TRY(cudaMemcpyAsync(h_scalars, d_scalars, kScalars * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     GS_CUDA_TRY(cudaMemcpyAsync(h_view_sums, d_view_sums, sizeof(double) * kViewSums * n_views,
                                 cudaMemcpyDeviceToHost, stream));
@@ -414,11 +412,6 @@ struct gs_context {
       GS_CUDA_TRY(cudaEventRecord(ev1, stream));
       GS_CUDA_TRY(cudaStreamSynchronize(stream));
       check_launch("step");
-      const uint32_t err = h_scalars[2];  // copied with the step's scalars
-      if (err != 0u) {
-        GS_CUDA_TRY(cudaMemset(sort.err, 0, sizeof(uint32_t)));
-        fail(GS_ERR_TIMEOUT, "a bounded device-side wait gave up; results discarded");
-      }
       const uint64_t pairs = h_scalars[0];
       last_pairs = pairs;
       max_pairs_seen = std::max(max_pairs_seen, pairs);
@@ -687,8 +680,8 @@ struct gs_context {
         ++launches;
       }
     }
-    gsk::launch_loss_reduce(sp, tile_loss, d_view_sums, kViewSums, stream);
-    ++launches;
+    gsk::launch_loss_reduce(sp, tile_loss, d_view_sums, kViewSums, d_view_sums + kViewSums * GS_MAX_VIEWS, stream);
+    launches += 2;
     mark(4);
     if (train) {
       const int px = tuning.backward_pixels ? int(tuning.backward_pixels) : 4;
@@ -927,12 +920,10 @@ int gs_create(int device, gs_context** out) {
       dev_alloc(c->d_queue, gsk::kQueueCount);
       c->sm_count = prop.multiProcessorCount;
       dev_alloc(c->d_scalars, gs_context::kScalars);
-      dev_alloc(c->d_view_sums, gs_context::kViewSums * GS_MAX_VIEWS);
+      // The views' sums, then the loss reduction's per-slice scratch.
+      dev_alloc(c->d_view_sums, (gs_context::kViewSums + gsk::kLossParts * 16u) * GS_MAX_VIEWS);
       dev_alloc(c->sort.hist, 8 * 256);
-      dev_alloc(c->sort.ticket, 1);
-      dev_alloc(c->sort.err, 1);
       GS_CUDA_TRY(cudaMemset(c->d_scalars, 0, gs_context::kScalars * sizeof(uint32_t)));
-      GS_CUDA_TRY(cudaMemset(c->sort.err, 0, sizeof(uint32_t)));
     } catch (...) {
       delete c;
       throw;

@@ -59,8 +59,6 @@ struct SortScratch {
   uint32_t count_tiles = 0;
   unsigned long long* scan_lookback = nullptr;
   uint32_t scan_tiles = 0;
-  uint32_t* ticket = nullptr;         // 1 word
-  uint32_t* err = nullptr;            // 1 word: a bounded wait gave up
 };
 constexpr uint32_t kSortTile = 256 * 15;
 constexpr uint32_t kScanTile = 256 * 8;
@@ -115,9 +113,11 @@ void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const
 // ---- loss.cu ----
 void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
 void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);
-// view_sums[v * stride + 0..15]: the view's 16 tile sums.
+// view_sums[v * stride + 0..15]: the view's 16 tile sums; parts: scratch of
+// n_views * kLossParts * 16 doubles.
+constexpr uint32_t kLossParts = 16;
 void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, uint32_t stride,
-                        cudaStream_t st);
+                        double* parts, cudaStream_t st);
 
 // ---- step.cu ----
 void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* depth_order, const uint32_t* first,

@@ -339,16 +339,21 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
 }
 
 // The 16 tile sums of each view (Trainer::read_slot, trainer.cpp:778-795), in double and
-// a fixed order, into view_sums[v * stride + 0..15].
-__global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const float* __restrict__ tile_loss,
-                                                     double* __restrict__ view_sums, uint32_t stride) {
+// a fixed order: kLossParts blocks per view sum consecutive slices of the view's tiles
+// (k_loss_partial), then one warp per view adds the slices in order (k_loss_final) into
+// view_sums[v * stride + 0..15]. The slices depend only on the view's own tile count, so
+// a view's sums do not depend on the other views of the step.
+__global__ void __launch_bounds__(256) k_loss_partial(const ViewTable* vt, const float* __restrict__ tile_loss,
+                                                      double* __restrict__ parts) {
   __shared__ double s[8][16];
-  const uint32_t v = blockIdx.x;
+  const uint32_t v = blockIdx.x / kLossParts, part = blockIdx.x % kLossParts;
+  const uint32_t t0 = vt->tile_base[v], t1 = vt->tile_base[v + 1];
+  const uint32_t chunk = (t1 - t0 + kLossParts - 1u) / kLossParts;
+  const uint32_t first = min(t1, t0 + part * chunk), last = min(t1, first + chunk);
   double acc[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) acc[k] = 0.0;
-  const uint32_t t0 = vt->tile_base[v], t1 = vt->tile_base[v + 1];
-  for (uint32_t t = t0 + threadIdx.x; t < t1; t += 256u) {
+  for (uint32_t t = first + threadIdx.x; t < last; t += 256u) {
     const float4* row = reinterpret_cast<const float4*>(tile_loss + size_t(t) * 16u);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -370,8 +375,17 @@ __global__ void __launch_bounds__(256) k_loss_reduce(const ViewTable* vt, const 
   if (threadIdx.x < 16u) {
     double sum = 0.0;
     for (int w = 0; w < 8; ++w) sum += s[w][threadIdx.x];
-    view_sums[size_t(v) * stride + threadIdx.x] = sum;
+    parts[(size_t(v) * kLossParts + part) * 16u + threadIdx.x] = sum;
   }
+}
+
+__global__ void __launch_bounds__(32) k_loss_final(const double* __restrict__ parts, double* __restrict__ view_sums,
+                                                   uint32_t stride) {
+  const uint32_t v = blockIdx.x;
+  if (threadIdx.x >= 16u) return;
+  double sum = 0.0;
+  for (uint32_t part = 0; part < kLossParts; ++part) sum += parts[(size_t(v) * kLossParts + part) * 16u + threadIdx.x];
+  view_sums[size_t(v) * stride + threadIdx.x] = sum;
 }
 
 }  // namespace
@@ -387,9 +401,10 @@ void launch_ssim_grad(const StepPointers& sp, const RasterBuffers& rb, cudaStrea
 }
 
 void launch_loss_reduce(const StepPointers& sp, const float* tile_loss, double* view_sums, uint32_t stride,
-                        cudaStream_t st) {
+                        double* parts, cudaStream_t st) {
   if (sp.n_views == 0u) return;
-  k_loss_reduce<<<sp.n_views, 256, 0, st>>>(sp.vt, tile_loss, view_sums, stride);
+  k_loss_partial<<<sp.n_views * kLossParts, 256, 0, st>>>(sp.vt, tile_loss, parts);
+  k_loss_final<<<sp.n_views, 32, 0, st>>>(parts, view_sums, stride);
 }
 
 }  // namespace gsk
