@@ -197,3 +197,40 @@ def test_full_size_batched_equals_single_views_and_is_bit_stable(ctx, full_size)
         ctx.set_views([frames[v]], [targets[v]])
         s = ctx.step(False)
         assert list(s.losses[0]) == list(a.losses[v]) and s.pairs[0] == a.pairs[v]
+
+
+def test_sixteen_full_views_multi_chunk_scans(ctx, full_size):
+    """GS_MAX_VIEWS views of 1080x1920 over the 1M-gaussian model: 16M (view, slot) items
+    and about 65M pairs, so the offset scan's tile-sum scan and the pair sort's per-digit
+    tile scans each run over more than one chunk. The pair list must still be a stable
+    sort by tile with consistent ranges and per-view counts, and a view's losses must not
+    depend on the other views of the step."""
+    scene, frames8, targets8 = full_size
+    cams = S.orbit_cameras(16, 3.0, 0.5, 1080, 1920, 1400.0)
+    opt = F.TrainOptions(iterations=30000, sh_degree=3, sh_degree_interval=0, masked=False,
+                         random_background=False, lambda_dssim=0.2, lambda_dssim_end=-1.0)
+    frames = [frame_for(scene, c, opt, (0.0, 0.0, 0.0)) for c in cams]
+    targets = [targets8[v % 8] for v in range(16)]
+    ctx.model_init(scene.params, scene.sh)
+    ctx.set_views(frames, targets)
+    res = ctx.step(False)
+    pairs = [int(res.pairs[v]) for v in range(16)]
+    total = sum(pairs)
+    assert res.overflow == 0 and res.tile_mismatch == 0
+    assert total > 9216 * 3840  # more pair-sort tiles than one k_tile_scan chunk
+    for v in (0, 7, 15):
+        assert int(ctx.snapshot("tiles", v).astype(np.int64).sum()) == pairs[v]
+        rg = ctx.snapshot("ranges", v).reshape(-1, 2).astype(np.int64)
+        assert int((rg[:, 1] - rg[:, 0]).sum()) == pairs[v]
+    order = ctx.snapshot("render_order", 0).astype(np.int64)
+    tile = ctx.snapshot("pair_tile", 0).astype(np.int64)
+    assert order.size == total and np.array_equal(np.sort(order), np.arange(total))
+    t = tile[order]
+    assert (np.diff(t) >= 0).all()
+    same = np.diff(t) == 0
+    assert (np.diff(order)[same] > 0).all()
+    for v in (3, 12):
+        ctx.model_init(scene.params, scene.sh)
+        ctx.set_views([frames[v]], [targets[v]])
+        s = ctx.step(False)
+        assert list(s.losses[0]) == list(res.losses[v]) and s.pairs[0] == res.pairs[v]
