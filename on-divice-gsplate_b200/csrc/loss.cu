@@ -8,8 +8,9 @@
 // lambda / (3 pixels) (G*A + 2 x G*B + y G*C) from dL/dC, then refreshes dL/dC . C.
 //
 // Both blurs are register-blocked: a thread produces 4 consecutive outputs of a row (or
-// column) from the 14 inputs it loads once, so shared-memory traffic per output is 3.5
-// loads per plane instead of 11, and sums run over the taps in window order. The row
+// column) from the 14 inputs it loads once (8 from 18 in k_ssim_grad, whose blurs carry
+// one plane), so shared-memory traffic per output is 3.5 (2.25) loads per plane instead of
+// 11, and sums run over the taps in window order. The row
 // blur's results are kept column-major (26 rows of a column contiguous): a warp's stores
 // (8 rows x 4 runs) then fall on 32 different banks, and the column blur reads its 14
 // rows as 7 aligned 8-byte loads.
@@ -68,7 +69,7 @@ constexpr int kHRow = kWin * kTile;     // one plane after the row blur: 16 colu
 constexpr int kHPlane = kHRow + 16;     // padded so neighbouring planes fall on other banks (even: 8-byte aligned)
 constexpr int kAbc = kTilePixels + 16;  // stride of the per-pixel planes after the column blur
 // Threads of an SSIM block: ten warps, so the row blur of k_ssim (312 runs) takes one round
-// and those of k_ssim_grad (936 row runs, 576 column runs) three and two; the per-pixel
+// and those of k_ssim_grad (468 row runs, 288 column runs of 8) two and one; the per-pixel
 // phases use the first 256.
 constexpr uint32_t kLossThreads = 320;
 constexpr uint32_t kLossWarps = kLossThreads / 32;
@@ -84,13 +85,6 @@ __device__ __forceinline__ void blur4(const float x[kSpan], float out[kRun]) {
   }
 }
 
-__device__ __forceinline__ void blur_run(const float* src, int stride, float out[kRun]) {
-  float x[kSpan];
-#pragma unroll
-  for (int k = 0; k < kSpan; ++k) x[k] = src[k * stride];
-  blur4(x, out);
-}
-
 // Column blur: 14 contiguous inputs at an 8-byte-aligned address.
 __device__ __forceinline__ void blur_column(const float* src, float out[kRun]) {
   float x[kSpan];
@@ -102,6 +96,22 @@ __device__ __forceinline__ void blur_column(const float* src, float out[kRun]) {
     x[2 * k + 1] = v.y;
   }
   blur4(x, out);
+}
+
+// The gradient kernel blurs single planes, so a thread can carry 8 outputs of a run (18
+// loads for 8 outputs, 2.25 per output) without running out of registers.
+constexpr int kRun8 = 8;
+constexpr int kSpan8 = kRun8 + 2 * kR;  // 18
+constexpr int kRuns8 = kTile / kRun8;   // 2
+
+__device__ __forceinline__ void blur8(const float x[kSpan8], float out[kRun8]) {
+#pragma unroll
+  for (int o = 0; o < kRun8; ++o) {
+    float sum = 0.0f;
+#pragma unroll
+    for (int k = 0; k <= 2 * kR; ++k) sum += c_window[k] * x[o + k];
+    out[o] = sum;
+  }
 }
 
 __global__ void __launch_bounds__(kLossThreads) k_ssim(LossArgs a) {
@@ -299,23 +309,33 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
     s_m[8 * kPlane + at] = m2;
   }
   __syncthreads();
-  // Row blur: 9 planes x 26 rows x 4 runs.
-  for (uint32_t e = lid; e < 9u * kWin * kQuads; e += kLossThreads) {
-    const uint32_t q = e % kQuads, row = (e / kQuads) % kWin, p = e / (kQuads * kWin);
-    float out[kRun];
-    blur_run(s_m + p * kPlane + row * kS + q * kRun, 1, out);
+  // Row blur: 9 planes x 26 rows x 2 runs of 8.
+  for (uint32_t e = lid; e < 9u * kWin * kRuns8; e += kLossThreads) {
+    const uint32_t q = e % kRuns8, row = (e / kRuns8) % kWin, p = e / (kRuns8 * kWin);
+    const float* src = s_m + p * kPlane + row * kS + q * kRun8;
+    float x[kSpan8], out[kRun8];
 #pragma unroll
-    for (int o = 0; o < kRun; ++o) s_h[p * kHPlane + (q * kRun + o) * kWin + row] = out[o];
+    for (int k = 0; k < kSpan8; ++k) x[k] = src[k];
+    blur8(x, out);
+#pragma unroll
+    for (int o = 0; o < kRun8; ++o) s_h[p * kHPlane + (q * kRun8 + o) * kWin + row] = out[o];
   }
   __syncthreads();
-  // Column blur: 9 planes x 16 columns x 4 runs.
+  // Column blur: 9 planes x 16 columns x 2 runs of 8 (18 contiguous inputs, 8-byte loads).
   float* s_g = s_m;  // [plane][kAbc]
-  for (uint32_t e = lid; e < 9u * kTile * kQuads; e += kLossThreads) {
+  for (uint32_t e = lid; e < 9u * kTile * kRuns8; e += kLossThreads) {
     const uint32_t col = e % kTile, p = (e / kTile) % 9u, q = e / (9u * kTile);
-    float out[kRun];
-    blur_column(s_h + p * kHPlane + col * kWin + q * kRun, out);
+    const float2* src = reinterpret_cast<const float2*>(s_h + p * kHPlane + col * kWin + q * kRun8);
+    float x[kSpan8], out[kRun8];
 #pragma unroll
-    for (int o = 0; o < kRun; ++o) s_g[p * kAbc + (q * kRun + o) * kTile + col] = out[o];
+    for (int k = 0; k < kSpan8 / 2; ++k) {
+      const float2 v = src[k];
+      x[2 * k] = v.x;
+      x[2 * k + 1] = v.y;
+    }
+    blur8(x, out);
+#pragma unroll
+    for (int o = 0; o < kRun8; ++o) s_g[p * kAbc + (q * kRun8 + o) * kTile + col] = out[o];
   }
   __syncthreads();
   const uint32_t lx = lid % kTile, ly = lid / kTile;
