@@ -69,6 +69,7 @@ bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint
                       const uint32_t* d_count, uint32_t n_max, int bits, cudaStream_t st, int* launches,
                       int digit_bits = 8);
 // Exclusive scan of in[gather ? gather[k] : k] for k < n; *d_total (if non-null) = the sum.
+// out must not alias in or gather (it first holds the gathered values).
 void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* gather, uint32_t* out, uint32_t n,
                     uint32_t* d_total, cudaStream_t st, int* launches);
 
