@@ -42,7 +42,7 @@ __device__ __forceinline__ void turn_matrix(float wx, float wy, float wz, float 
 }
 
 // Where slot i (rest position p) is in a view: x, the orientation's turn U and A = dx/dp
-// (train_motion.glsl:37-50).
+// (train_motion.glsl:33-49).
 struct Deformed {
   float x[3];
   float U[3][3];

@@ -355,7 +355,7 @@ uint64_t gso_emit(const gso_frame* f, const float* projected, const uint32_t* ti
   }
   uint32_t bad = 0;
   const uint32_t pad_tile = f->image[2] * f->image[3];
-  /* train_emit.comp:156-194 */
+  /* train_emit.comp:26-63 */
   PAR_FOR
   for (int64_t kk = 0; kk < (int64_t)n; ++kk) {
     const uint32_t i = order[kk];
@@ -639,7 +639,7 @@ void gso_ssim_grad(const gso_frame* f, const float* ssim_input, const float* ssi
   for (size_t p = 0; p < n; ++p) {
     const uint32_t x = (uint32_t)(p % width), y = (uint32_t)(p / width);
     const uint32_t t = (y / TILE) * tiles_x + x / TILE;
-    /* train_ssim_grad.comp:168-170 */
+    /* train_ssim_grad.comp:26-28 (tiles without splats keep their L1 gradient when the target is masked) */
     if ((f->model[3] & GSO_FLAG_MASKED) && ranges[2u * t + 1u] <= ranges[2u * t]) continue;
     float* pg = pixel_grad + p * 4u;
     float dot = 0.0f;

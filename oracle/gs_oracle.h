@@ -7,15 +7,19 @@
  * (engine/shaders/train_*.comp, train_common.glsl) in fp32 with no floating-point
  * contraction, and its FP64 CPU forward + loss (engine/src/train_selftest.cpp:38-283).
  *
- * Parity pinning: the reference ships no golden vectors and its GPU path (Vulkan) cannot
- * run here; its CPU self-test code does not build standalone (it pulls Vulkan headers and
- * generated SPIR-V). The oracle is therefore pinned against the reference's own
- * known-answer tests, restated in tests/test_oracle.py: FP64 central finite differences
- * of the restated reference_loss (train_selftest.cpp:356-446, tolerance
- * |err| <= 5% |fd| + 2e-6), pair order (test_trainer.cpp:197-233), footprint exactness
- * (test_trainer.cpp:235-289), forward image vs the FP64 reference within 2.5/255
- * (test_trainer.cpp:34) and the SSIM window constants (train_common.glsl:61-62 vs
- * train_selftest.cpp:176-181).
+ * Parity pinning: the reference's FP64 CPU forward + loss (train_selftest.cpp:27-283) is
+ * compiled from a reference checkout into oracle/_ref/libgs_ref.so (Makefile `ref`,
+ * ref_shim.cpp). tests/test_oracle_ref.py checks that gso_reference_loss and
+ * gso_reference_ssim reproduce it bit for bit (loss, FP64 image, SSIM) on the reference's own
+ * test scene and on workload-shaped scenes, that the fp32 passes here render within its
+ * 2.5/255 image and 1e-4 loss bars (test_trainer.cpp:34-35), and that the analytic gradients
+ * pass its finite-difference rule (train_selftest.cpp:418-446) against central differences
+ * of the reference's own loss. The reference has no CPU code for the sort, the backward,
+ * Adam or densify (its GPU path is Vulkan, which cannot run here); those passes are pinned by
+ * the reference's known-answer tests, restated in tests/test_oracle.py: pair order
+ * (test_trainer.cpp:197-233), footprint exactness (test_trainer.cpp:235-289), densify
+ * capacity (test_trainer.cpp:866-888), the stable depth sort (test_engine.cpp:27-68) and the
+ * SSIM window constants (train_common.glsl:61-62 vs train_selftest.cpp:176-181).
  *
  * Layouts are the reference's: 16 floats of parameters per slot (train_common.glsl:3-8),
  * `sh_stride` floats of SH beyond DC per slot ([coeff][rgb]), 16 floats of projected
@@ -60,10 +64,10 @@ typedef struct gso_frame {
 void gso_project(const gso_frame* f, const float* params, const float* sh, uint32_t n, float* projected,
                  uint32_t* tiles, uint32_t* depth_keys);
 
-/* The tile walk of train_emit.comp:167-180 over stored projected records: tile counts. */
+/* The tile walk of train_emit.comp:36-50 (train_common.glsl:176-213) over stored projected records: tile counts. */
 void gso_footprint_counts(const gso_frame* f, const float* projected, uint32_t n, uint32_t* tiles);
 
-/* Tiles of one gaussian in emission order (train_emit.comp:169-179); returns the count,
+/* Tiles of one gaussian in emission order (train_emit.comp:38-49); returns the count,
    writes at most `max` ids. */
 uint32_t gso_footprint_tiles(const gso_frame* f, const float* proj16, uint32_t* out, uint32_t max);
 
@@ -116,10 +120,10 @@ void gso_project_backward(const gso_frame* f, const float* params, const float* 
                           const float* grad_sum, const float* projected, float* stats, float* grad16,
                           float* sh_input, uint8_t* drew);
 
-/* train_step_sh.comp:36-38: the SH-rest gradient from sh_input, accumulated (+=). */
+/* train_step_sh.comp:32-34: the SH-rest gradient from sh_input, accumulated (+=). */
 void gso_sh_gradient(const gso_frame* f, const float* params, const float* sh_input, float* grad_sh);
 
-/* Adam of train_step.glsl:62-68, 222-236 and train_step_sh.comp:25-47 for every slot,
+/* Adam of train_step.glsl:62-68, 222-236 and train_step_sh.comp:25-43 for every slot,
    from accumulated gradients. Sparse Adam skips the 16 parameters of slots without
    drew bit 0 and the SH of slots without drew bit 1. */
 void gso_adam(const gso_frame* f, float* params, float* sh, float* m, float* v, float* m_sh, float* v_sh,

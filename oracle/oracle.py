@@ -284,16 +284,23 @@ def footprint_tiles(frame: np.ndarray, proj16: np.ndarray) -> np.ndarray:
     return out[:k].copy()
 
 
+def _camera_vector(camera: dict) -> np.ndarray:
+    """The camera as 19 doubles, each rounded to float first: gs::Camera stores floats
+    (engine/include/gs/camera.h:10-16), so the reference's FP64 code sees float values."""
+    v = np.concatenate([np.asarray(camera["rotation"], np.float64).reshape(9),
+                        np.asarray(camera["translation"], np.float64).reshape(3),
+                        np.asarray(camera["position"], np.float64).reshape(3),
+                        np.array([camera["fx"], camera["fy"], camera["cx"], camera["cy"]], np.float64)])
+    return v.astype(np.float32).astype(np.float64)
+
+
 def reference_loss(camera: dict, width: int, height: int, params64: np.ndarray, sh64: np.ndarray, degree: int,
                    target: np.ndarray, bg, masked: bool, lam: float, want_image: bool = False, head=None,
                    want_signature: bool = False):
     """FP64 forward + loss of train_selftest.cpp:211-283. With want_signature, also the hash
     of its blend decisions (equal hashes: no alpha / transmittance / clamp cut-off crossed)."""
     L = lib()
-    cam = np.concatenate([np.asarray(camera["rotation"], np.float64).reshape(9),
-                          np.asarray(camera["translation"], np.float64).reshape(3),
-                          np.asarray(camera["position"], np.float64).reshape(3),
-                          np.array([camera["fx"], camera["fy"], camera["cx"], camera["cy"]], np.float64)])
+    cam = _camera_vector(camera)
     n = params64.shape[0]
     stride = sh64.shape[1] if sh64.ndim == 2 else 0
     img = np.zeros((width * height, 3), np.float64) if want_image else None
@@ -316,3 +323,61 @@ def ssim_window() -> np.ndarray:
 
 def pcg_hash(v: int) -> int:
     return int(lib().gso_pcg_hash(v))
+
+
+# The reference's own FP64 CPU forward + loss (engine/src/train_selftest.cpp:27-283),
+# compiled from a reference checkout by `make -C oracle ref` into oracle/_ref/ (see
+# ref_shim.cpp). It pins the restatement above: gso_reference_loss / gso_reference_ssim must
+# reproduce it, and finite differences of it check the analytic gradients.
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libgs_ref.so")
+REFERENCE_SOURCE = os.path.join(os.environ.get("GS_REFERENCE", "/root/reference"), "engine", "src",
+                                "train_selftest.cpp")
+_ref = None
+
+
+def ref_lib():
+    """The reference's CPU library, built first if a reference checkout is present; None if
+    neither the library nor a checkout is present."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB_PATH):
+            if not os.path.exists(REFERENCE_SOURCE):
+                return None
+            import subprocess
+
+            subprocess.run(["make", "-s", "-C", HERE, "ref",
+                            f"REFERENCE={os.path.dirname(os.path.dirname(os.path.dirname(REFERENCE_SOURCE)))}"],
+                           check=True)
+        L = ctypes.CDLL(REF_LIB_PATH)
+        u32 = ctypes.c_uint32
+        L.gsr_reference_loss.argtypes = [_f64p, u32, u32, _f64p, _vp, u32, ctypes.c_int, ctypes.c_int, _u8p,
+                                         _f32p, ctypes.c_int, ctypes.c_double, _vp, _vp]
+        L.gsr_reference_loss.restype = ctypes.c_double
+        L.gsr_reference_ssim.argtypes = [_f64p, _f64p, u32, u32, _vp]
+        L.gsr_reference_ssim.restype = ctypes.c_double
+        _ref = L
+    return _ref
+
+
+
+
+def ref_reference_loss(camera: dict, width: int, height: int, params64: np.ndarray, sh64: np.ndarray, degree: int,
+                       target: np.ndarray, bg, masked: bool, lam: float, want_image: bool = False, head=None):
+    """gs::reference_loss itself (the reference's code), same arguments as reference_loss."""
+    L = ref_lib()
+    n = params64.shape[0]
+    stride = sh64.shape[1] if sh64.ndim == 2 else 0
+    img = np.zeros((width * height, 3), np.float64) if want_image else None
+    h = None if head is None else np.asarray(head, np.float64)
+    loss = L.gsr_reference_loss(_camera_vector(camera), width, height, np.ascontiguousarray(params64, np.float64),
+                                _ptr(np.ascontiguousarray(sh64, np.float64)) if stride else None, n, stride, degree,
+                                np.ascontiguousarray(target.reshape(-1), np.uint8), np.asarray(bg, np.float32),
+                                int(masked), float(lam), _ptr(img), _ptr(h))
+    return (loss, img) if want_image else loss
+
+
+def ref_reference_ssim(x: np.ndarray, y: np.ndarray, width: int, height: int, weights=None) -> float:
+    """gs::reference_ssim itself (x, y: (pixels, 3) float64)."""
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    return float(ref_lib().gsr_reference_ssim(np.ascontiguousarray(x, np.float64), np.ascontiguousarray(y, np.float64),
+                                              width, height, _ptr(w)))

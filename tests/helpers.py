@@ -24,20 +24,30 @@ GROUPS = {"position": [0, 1, 2], "opacity": [3], "log_scale": [4, 5, 6], "rotati
 
 def fd_check(scene: S.Scene, cam: F.Camera, target: np.ndarray, grad16: np.ndarray, grad_sh: np.ndarray,
              bg, masked: bool, lam: float, eps: float = 1e-5, params: list | None = None,
-             skip_crossings: bool = False) -> dict:
+             skip_crossings: bool = False, loss_impl=None) -> dict:
     """check_gradients (train_selftest.cpp:418-446): central finite differences of the FP64
     reference loss, |err| <= 5% |fd| + 2e-6, per parameter group. `params`: optional list of
     (slot, offset) to check (offset < 0: SH coefficient -1 - offset); default all.
     skip_crossings: leave out parameters whose stencil changes any blend decision of the FP64
     forward (an alpha or transmittance cut-off, a clamp or the depth order), where central
-    differences measure a jump, not the derivative; they are counted as `skipped`."""
+    differences measure a jump, not the derivative; they are counted as `skipped`.
+    loss_impl: the FP64 loss to differentiate (default the oracle's restatement; the
+    reference's own, O.ref_reference_loss, where it is built). Decision signatures always
+    come from the restatement, which reproduces the reference bit for bit."""
     p64, s64 = params64(scene)
     W, H = cam.width, cam.height
     camd = cam.as_dict()
     stride = scene.sh.shape[1]
 
     def loss():
-        return O.reference_loss(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam, want_signature=True)
+        if loss_impl is None:
+            return O.reference_loss(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam, want_signature=True)
+        value = loss_impl(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam)
+        sig = 0
+        if skip_crossings:
+            _, sig = O.reference_loss(camd, W, H, p64, s64, scene.degree, target, bg, masked, lam,
+                                      want_signature=True)
+        return value, sig
 
     _, sig0 = loss()
 
