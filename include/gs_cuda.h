@@ -256,8 +256,7 @@ int gs_set_view_motion(gs_context* ctx, uint32_t view, const float* nodes20);
    (train_step.glsl:270-337, train_motion_sum.comp). */
 int gs_motion_gradient(gs_context* ctx, uint32_t view, double* out, uint32_t count);
 
-/* No counterpart in the reference: its RadixSort allocates its own temporary buffers
-   (engine/src/radix_sort.cpp:37-39). For callers that cannot allocate device memory —
+/* No counterpart in the reference. For callers that cannot allocate device memory —
    runtimes whose pool owns all device memory and forbids allocations outside it, plugins
    that get only the buffers such a runtime passes them, loops that cannot afford an
    allocation's device synchronisation — this sorts n (key, value) pairs already in device

@@ -54,8 +54,14 @@ extern "C" int gs_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t 
                                       std::to_string(kMaxItems));
   if (key_bits == 0u || key_bits > 32u) return failed(GS_ERR_INVALID, "gs_sort_pairs_noalloc: key_bits must be 1..32");
   if (n > 0u && (keys == nullptr || values == nullptr)) return failed(GS_ERR_INVALID, "gs_sort_pairs_noalloc: null buffer");
+  // A launch error the caller left pending on this thread is not this call's: report it as
+  // such and leave it in place, rather than return it later as a failed sort.
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: a CUDA error was pending before the call: ") +
+                                   cudaGetErrorString(e));
   int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
+  e = cudaGetDevice(&device);
   if (e != cudaSuccess) return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: ") + cudaGetErrorString(e));
   if (device < 0 || device >= kMaxDevices) return failed(GS_ERR_INVALID, "gs_sort_pairs_noalloc: device index too large");
   uint32_t* base = nullptr;
@@ -81,12 +87,17 @@ extern "C" int gs_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t 
   // overwrites the tile counts it reads, so nothing needs clearing here.
   const bool in_alt = gsk::radix_sort_pairs(s, keys, values, base + kAltKeys, base + kAltVals, nullptr, n,
                                             int(key_bits), st, nullptr);
+  e = cudaGetLastError();  // the sort's launches
+  if (e != cudaSuccess)
+    return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: sort launch: ") + cudaGetErrorString(e));
   if (in_alt) {
-    cudaMemcpyAsync(keys, base + kAltKeys, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(values, base + kAltVals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    e = cudaMemcpyAsync(keys, base + kAltKeys, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(values, base + kAltVals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess)
+      return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: copy back: ") + cudaGetErrorString(e));
   }
   e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return failed(GS_ERR_CUDA, std::string("gs_sort_pairs_noalloc: ") + cudaGetErrorString(e));
   gsk::set_last_error("");
   return GS_OK;

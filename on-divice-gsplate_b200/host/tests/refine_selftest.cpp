@@ -13,6 +13,10 @@
 //   gs_refine_selftest motion-batched
 //   gs_refine_selftest variants     select_backward: every tuning gives the first step's
 //                                   gradients of the default one (test_trainer.cpp:56-125)
+//   gs_refine_selftest converge [views-per-step]
+//                                   fit_known_scene (train_selftest.cpp:692-739): held-out
+//                                   PSNR above 35 dB and 8 dB above the start
+//                                   (test_trainer.cpp:890-897)
 // Each prints one JSON line with what it measured and exits 1 when its check fails.
 #include <algorithm>
 #include <array>
@@ -532,6 +536,58 @@ int variants() {
   return ok && rejected && worst < 1e-5 ? 0 : 1;
 }
 
+// The reference's known-scene fit (fit_known_scene, train_selftest.cpp:692-739): 24 masked
+// views of 96x72 rendered from a 60-gaussian SH-1 scene over black (colour un-premultiplied,
+// the render's alpha as the mask), training 600 steps from the truth with its positions
+// moved by 0.05 N(0, 1), colours cleared and opacity logits at -1, under the default options
+// with SH degree steps every 200 and no densification. Passes when the held-out PSNR ends
+// above 35 dB and 8 dB above where it started (test_trainer.cpp:890-897). With views > 1
+// the steps are batched, views_per_step views each, for the same number of steps.
+int converge(uint32_t views) {
+  const int degree = 1;
+  const uint32_t steps = 600;
+  gs::Dataset ds = test_dataset(96, 72, 24, true, 9);
+  const gs::SplatScene truth = test_scene(60, degree, 21);
+  {
+    gs::CudaContext ctx;
+    gs::Trainer renderer(ctx, ds, truth, frozen_options(degree, false));
+    const float black[3] = {0.0f, 0.0f, 0.0f};
+    for (gs::DatasetFrame& f : ds.frames) {
+      const std::vector<uint8_t> img = renderer.render(gs::dataset_camera(ds, f), black);
+      for (size_t p = 0; p < img.size() / 4; ++p) {
+        const float a = float(img[p * 4 + 3]) / 255.0f;
+        for (int c = 0; c < 3; ++c)
+          f.rgba[p * 4 + c] = a > 0.0f ? uint8_t(std::min(255.0f, float(img[p * 4 + c]) / a + 0.5f)) : uint8_t(0);
+        f.rgba[p * 4 + 3] = img[p * 4 + 3];
+      }
+    }
+  }
+  gs::SplatScene init = truth;
+  std::mt19937 rng(4);
+  std::normal_distribution<float> noise(0.0f, 1.0f);
+  for (float& v : init.positions) v += 0.05f * noise(rng);
+  std::fill(init.sh_dc.begin(), init.sh_dc.end(), 0.0f);
+  std::fill(init.sh_rest.begin(), init.sh_rest.end(), 0.0f);
+  std::fill(init.opacity_logits.begin(), init.opacity_logits.end(), -1.0f);
+  gs::TrainOptions o;
+  o.iterations = steps;
+  o.sh_degree = degree;
+  o.sh_degree_interval = std::max(1u, steps / 3);
+  o.densify_from = o.densify_until = 1000000;
+  o.opacity_reset_interval = 0;
+  o.max_gaussians = 2000;
+  o.views_per_step = views;
+  gs::CudaContext ctx;
+  gs::Trainer trainer(ctx, ds, init, o);
+  const double before = trainer.evaluate().psnr;
+  while (!trainer.finished()) trainer.step();
+  const double after = trainer.evaluate().psnr;
+  const bool ok = after > before + 8.0 && after > 35.0;
+  std::printf("{\"views_per_step\": %u, \"steps\": %u, \"psnr_before\": %.3f, \"psnr_after\": %.3f}\n", views,
+              trainer.stats().step, before, after);
+  return ok ? 0 : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -545,6 +601,7 @@ int main(int argc, char** argv) {
     if (mode == "motion-recovery") return motion_recovery();
     if (mode == "motion-batched") return motion_batched();
     if (mode == "variants") return variants();
+    if (mode == "converge") return converge(argc > 2 ? uint32_t(std::atoi(argv[2])) : 1u);
     std::fprintf(stderr, "usage: gs_refine_selftest pose-gradient <lambda> | pose-recovery | exposure-recovery | align\n");
     return 2;
   } catch (const std::exception& e) {

@@ -1,0 +1,99 @@
+"""Value parity at the kernel-scale workload (GPU only): 1,000,000 gaussians, SH degree 3,
+means in a radius-2 ball, log-scales N(-5, 0.5), one 1080x1920 view from (0, 0, 3) with
+fx = fy = 1400, the target rendered from an independent seed-1 set, loss 0.8 L1 + 0.2 D-SSIM.
+These are the sizes the benchmark times (one view of its step).
+
+The oracle is fed the GPU's projection and depth keys (the reference keeps train_project and
+train_emit consistent the same way, train_common.glsl:163-168), then checked:
+- pair list (tile, gaussian), render order, per-gaussian offsets and tile ranges bit-exact;
+- rendered colour within 1e-4 max abs where the contributor counts agree (at least 99.95%
+  of the pixels), final transmittance within 1e-5, loss sums within 1e-4 relative;
+- per-pair gradients (mean2d, conic, opacity, colour, |dmean|) within 1e-3 relative L2;
+- the parameter gradients of the whole step against the oracle's own full step (its own
+  projection) within 1e-3 relative L2 per group, SH included.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from gs_b200 import frame as F
+from gs_b200 import scenes as S
+from helpers import GROUPS, frame_for, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+N, W, H, FOCAL = 1_000_000, 1080, 1920, 1400.0
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from gs_b200.cuda import Context
+
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def config3(ctx):
+    scene = S.make_scene(N, 0, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
+    truth = S.make_scene(N, 1, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
+    cam = S.front_camera(W, H, FOCAL)
+    opt = F.frozen_options(3, False)
+    opt.lambda_dssim, opt.lambda_dssim_end = 0.2, -1.0
+    ctx.model_init(truth.params, truth.sh)
+    target = ctx.render(frame_for(truth, cam, opt, (0, 0, 0), ssim=False)).reshape(H, W, 4).copy()
+    target[..., 3] = 255
+    fr = frame_for(scene, cam, opt, (0, 0, 0))
+    ctx.model_init(scene.params, scene.sh)
+    ctx.set_views([fr], [target])
+    res = ctx.step(True)
+    assert res.overflow == 0 and res.tile_mismatch == 0
+    snap = {k: ctx.snapshot(k) for k in ("projected", "depth_key", "tiles", "offsets", "pair_tile", "pair_gaussian",
+                                         "render_order", "ranges", "pixel_count", "pixel_out", "pixel_grad",
+                                         "pair_grads")}
+    g16, gsh = ctx.first_step_gradients()
+    r = O.forward_view(fr, scene.params, scene.sh, target, projected=snap["projected"], depth_keys=snap["depth_key"])
+    return scene, fr, target, res, snap, g16, gsh, r
+
+
+def test_pairs_order_and_ranges_bit_exact(config3):
+    _, _, _, res, snap, _, _, r = config3
+    assert res.pairs[0] == r.pairs > 3_000_000
+    np.testing.assert_array_equal(snap["tiles"], r.tiles)
+    np.testing.assert_array_equal(snap["pair_tile"], r.pair_tile[: r.pairs])
+    np.testing.assert_array_equal(snap["pair_gaussian"], r.pair_gaussian[: r.pairs])
+    np.testing.assert_array_equal(snap["render_order"], r.render_order[: r.pairs])
+    drawn = snap["tiles"] > 0
+    np.testing.assert_array_equal(snap["offsets"][drawn], r.offsets[drawn])
+    ntiles = ((W + 15) // 16) * ((H + 15) // 16)
+    np.testing.assert_array_equal(snap["ranges"].reshape(-1), r.ranges[: 2 * ntiles])
+
+
+def test_image_transmittance_and_loss(config3):
+    _, _, _, res, snap, _, _, r = config3
+    same = snap["pixel_count"] == r.pixel_count
+    assert same.mean() >= 0.9995, same.mean()
+    assert np.abs(snap["pixel_out"][same, :3] - r.ssim_input[same, :3]).max() <= 1e-4
+    assert np.abs(snap["pixel_grad"][same, 3] - r.pixel_grad[same, 3]).max() <= 1e-5
+    assert rel_l2(snap["pixel_grad"][same, :3], r.pixel_grad[same, :3]) < 1e-3
+    sums = np.array(res.losses[0][:8])
+    for k in (0, 1, 2, 3, 4, 5):
+        assert abs(sums[k] - r.sums[k]) <= 1e-4 * abs(r.sums[k]) + 1e-6, k
+
+
+def test_pair_gradients(config3):
+    _, _, _, _, snap, _, _, r = config3
+    got, ref = snap["pair_grads"], r.pair_grads[: r.pairs]
+    for name, cols in {"mean2d": [0, 1], "conic": [2, 3, 4], "opacity": [5], "colour": [6, 7, 8],
+                       "abs_mean": [9, 10]}.items():
+        assert rel_l2(got[:, cols], ref[:, cols]) < 1e-3, name
+
+
+def test_parameter_gradients(config3):
+    scene, fr, target, _, _, g16, gsh, _ = config3
+    model = O.Model.create(scene.params, scene.sh)
+    _, ref16, refsh, _ = O.train_step(model, [fr], [target])
+    for name, cols in GROUPS.items():
+        assert rel_l2(g16[:, cols], ref16[:, cols]) < 1e-3, name
+    assert rel_l2(gsh, refsh) < 1e-3

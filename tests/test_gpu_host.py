@@ -1,9 +1,11 @@
-"""gs_train and gs_render (the C++ host layer over libgs_cuda) on a GPU.
+"""gs_train, gs_render and gs::Trainer (the C++ host layer over libgs_cuda) on a GPU.
 
-Short synthetic orbit runs (the reference's convergence check trains until held-out PSNR
-is high, test_trainer.cpp:890-897; here the runs are short, so the check is that held-out
-PSNR rises and densification ran), plain and batched, and a headless render of the PLY
-the trainer wrote through the --views camera-file mode.
+- The reference's convergence check through gs::Trainer: its known-scene fit
+  (fit_known_scene, train_selftest.cpp:692-739) must end with held-out PSNR above 35 dB and
+  8 dB above the start (test_training_converges, test_trainer.cpp:890-897), plain and batched.
+- Short synthetic orbit runs of gs_train, plain and batched (held-out PSNR rises and
+  densification runs), and a headless render of the PLY the trainer wrote through the
+  --views camera-file mode.
 """
 import json
 import os
@@ -215,3 +217,14 @@ def test_trainer_select_backward_variants():
     summation order), and unknown names are refused."""
     rc, out = refine_selftest("variants")
     assert rc == 0, out
+
+
+@pytest.mark.parametrize("views", ["1", "4"])
+def test_training_converges(views):
+    """test_training_converges (test_trainer.cpp:890-897) through gs::Trainer: the known-scene
+    fit of train_selftest.cpp:692-739 (96x72, 24 masked views, 60 gaussians, 600 steps) ends
+    with held-out PSNR above 35 dB and 8 dB above its start; also with 4 views per step."""
+    rc, out = refine_selftest("converge", views)
+    assert rc == 0, out
+    m = json.loads(next(line for line in out.splitlines() if line.startswith('{"views_per_step"')))
+    assert m["psnr_after"] > 35.0 and m["psnr_after"] > m["psnr_before"] + 8.0, out

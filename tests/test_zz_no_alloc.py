@@ -97,3 +97,50 @@ def test_noalloc_sort_rejects_oversized_input():
     code = lib.gs_sort_pairs_noalloc(None, None, (1 << 20) + 1, 16, None)
     assert code == cuda.GS_ERR_INVALID
     assert b"maximum" in lib.gs_last_error()
+
+
+def test_noalloc_sort_trivial_sizes_and_bad_widths():
+    """n = 0 and n = 1 succeed and leave the buffers as they were (the first call on the
+    device still does its set-up); key widths outside 1..32 are refused."""
+    import torch
+
+    from gs_b200 import cuda
+
+    lib = cuda.load()
+    for n in (0, 1):
+        keys = torch.tensor([7, 3], dtype=torch.int32, device="cuda")
+        values = torch.tensor([11, 12], dtype=torch.int32, device="cuda")
+        code = lib.gs_sort_pairs_noalloc(ctypes.c_void_p(keys.data_ptr()), ctypes.c_void_p(values.data_ptr()), n, 8,
+                                         None)
+        assert code == cuda.GS_OK, lib.gs_last_error().decode()
+        assert keys.tolist() == [7, 3] and values.tolist() == [11, 12]
+    keys = torch.zeros(4, dtype=torch.int32, device="cuda")
+    for bits in (0, 33):
+        code = lib.gs_sort_pairs_noalloc(ctypes.c_void_p(keys.data_ptr()), ctypes.c_void_p(keys.data_ptr()), 4, bits,
+                                         None)
+        assert code == cuda.GS_ERR_INVALID
+        assert b"key_bits" in lib.gs_last_error()
+
+
+def test_noalloc_sort_on_a_side_stream():
+    """A sort issued on a stream other than the default one, after work queued on it."""
+    import torch
+
+    from gs_b200 import cuda
+
+    lib = cuda.load()
+    rng = np.random.default_rng(8)
+    n = 70001
+    keys_np = rng.integers(0, 1 << 13, n, dtype=np.uint64).astype(np.uint32)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        keys = torch.from_numpy(keys_np.view(np.int32)).cuda(non_blocking=False)
+        values = torch.arange(n, dtype=torch.int32, device="cuda")
+        keys.add_(0)  # queued on the side stream ahead of the sort
+        code = lib.gs_sort_pairs_noalloc(ctypes.c_void_p(keys.data_ptr()), ctypes.c_void_p(values.data_ptr()), n, 13,
+                                         ctypes.c_void_p(side.cuda_stream))
+    assert code == cuda.GS_OK, lib.gs_last_error().decode()
+    side.synchronize()
+    expect = np.argsort(keys_np, kind="stable").astype(np.uint32)
+    np.testing.assert_array_equal(values.cpu().numpy().view(np.uint32), expect)
+    np.testing.assert_array_equal(keys.cpu().numpy().view(np.uint32), keys_np[expect])
