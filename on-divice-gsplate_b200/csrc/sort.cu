@@ -6,14 +6,15 @@
 //  - radix_sort_pairs: LSD sort, digits of 4 to 8 bits (8 by default; the width is a tuning
 //    knob), three kernels a pass. k_tile_counts counts the digits of every 3840-key tile;
 //    k_tile_scan turns each digit's row of tile counts into the tiles' starts within the
-//    digit and the digit's total (one block per digit); k_onesweep ranks and scatters: a
+//    digit and the digit's total (one block per digit); k_rank_scatter ranks and scatters: a
 //    block adds the totals of the smaller digits (one scan) to its tiles' starts, ranks its
 //    tile's keys (same-digit lanes from one ballot per digit bit, per-warp counters,
 //    stable) and writes each digit run contiguously through shared memory. The ballots
 //    replace __match_any_sync, whose pipe was measured 87% busy with 8-bit digits (up to 32
 //    distinct values per warp). No block waits on another: a decoupled look-back over the
 //    previous tiles' counts was measured slower here, its polls of the same few status
-//    lines serialising in L2.
+//    lines serialising in L2. So this is a reduce-then-scan sort, not a single-pass
+//    (onesweep) one: the look-back was built, measured and dropped.
 //  - exclusive_scan: three kernels (tile sums with the gathered values staged in the
 //    output, one block scanning the tile sums, then each tile's own scan), again with no
 //    block waiting on another, so no kernel of the sort or the scan spins on a flag.
@@ -167,7 +168,7 @@ __device__ __forceinline__ void rank_keys(const uint32_t (&key)[kIpt], uint16_t 
 
 // One pass: each block ranks its tile's keys (same-digit lanes from ballots, per-warp
 // counters, stable) and scatters them through shared memory to its digits' global starts.
-__global__ void __launch_bounds__(kThreads, 4) k_onesweep(const uint32_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kThreads, 4) k_rank_scatter(const uint32_t* __restrict__ keys_in,
                                                        const uint32_t* __restrict__ vals_in,
                                                        uint32_t* __restrict__ keys_out,
                                                        uint32_t* __restrict__ vals_out, const uint32_t* d_count,
@@ -378,7 +379,7 @@ bool radix_sort_pairs(const SortScratch& s, uint32_t* keys, uint32_t* vals, uint
     const uint32_t mask = (1u << width) - 1u;
     k_tile_counts<<<tiles, kThreads, 0, st>>>(src_k, d_count, n_max, shift, mask, s.tile_counts, tiles);
     k_tile_scan<<<mask + 1u, kRowThreads, 0, st>>>(s.tile_counts, tiles, d_count, n_max, s.hist + p * kRadix);
-    k_onesweep<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, mask, s.tile_counts,
+    k_rank_scatter<<<tiles, kThreads, 0, st>>>(src_k, src_v, dst_k, dst_v, d_count, n_max, shift, mask, s.tile_counts,
                                            tiles, s.hist + p * kRadix);
     uint32_t* t = src_k;
     src_k = dst_k;

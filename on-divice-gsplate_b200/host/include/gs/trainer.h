@@ -24,6 +24,7 @@
 
 #include <array>
 #include <cstdint>
+#include <memory>
 #include <random>
 #include <string>
 #include <utility>
@@ -277,19 +278,9 @@ class Trainer {
   const std::vector<RetuneResult>& retunes() const { return retunes_; }
 
  private:
-  struct PoseFix {
-    float rotation[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // applied after the dataset's rotation (camera axes)
-    float shift[3] = {0, 0, 0};
-    double m[6] = {}, v[6] = {};  // Adam moments: shift xyz, turn xyz
-    uint32_t updates = 0;
-  };
-  struct NodeMotion {
-    float turn[3] = {0, 0, 0};  // axis-angle, radians
-    float shift[3] = {0, 0, 0};
-    double m[6] = {};           // Adam: shift xyz, turn xyz
-    double v[2] = {};           // one second moment per vector: shift, turn
-  };
-  using ViewMotion = std::vector<NodeMotion>;
+  // Pose, exposure and subject-motion state: the capture order, the camera corrections,
+  // the gains and the node rig (host/src/refinement.h, host/src/node_rig.h).
+  struct Corrections;
 
   void next_view(size_t& frame, float background[3]);
   void run_step(const std::vector<size_t>& frames, const std::vector<std::array<float, 3>>& backgrounds,
@@ -297,36 +288,33 @@ class Trainer {
   void write_frame(gs_frame_data& f, const Camera& camera, const float background[3], uint32_t step, bool ssim,
                    bool masked, uint32_t flags = 0u, const float* gain = nullptr) const;
   // One held-out measurement (forward only) or alignment probe of `camera` against the
-  // dataset's image `frame` (or `rgba`, another dataset's, when not null) over black, the
-  // subject moved by `motion` when not null.
+  // dataset's image `frame` (or `rgba`, another dataset's, when not null) over black; with
+  // `moved` (a node table, gs_set_view_motion's layout) the subject moves by it.
   void run_eval_view(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3], uint32_t flags,
-                     const ViewMotion* motion, gs_step_result& r);
+                     const std::vector<float>* moved, gs_step_result& r);
   EvalResult evaluate_views(const Dataset& ds, bool own);
-  std::vector<uint8_t> render_with(const Camera& camera, const float background[3], const ViewMotion* motion);
-  // Subject motion.
-  void place_nodes(const SplatScene& initial);  // k-means over the initial gaussians, then gs_motion_nodes
-  void bind_motion();                           // gs_motion_bind
-  bool refines_motion_at(uint32_t step) const { return !nodes_.empty() && step >= options_.motion_from; }
-  bool uses_motion() const;                     // some view's motion has been trained
-  ViewMotion view_motion(size_t frame) const;   // its own once trained, else between its neighbours'
-  void start_motion(size_t frame);              // before a training view's first motion update
-  void set_motion_table(uint32_t view, const ViewMotion& motion);  // gs_set_view_motion
-  void update_motion(const double* grad, size_t frame);            // Adam step from the image gradient + penalties
-  void update_motion_stats();
+  std::vector<uint8_t> render_with(const Camera& camera, const float background[3], const std::vector<float>* moved);
+  // Subject motion (trainer_refine.cpp).
+  void build_rig(const SplatScene& initial);  // the nodes over the initial gaussians, then gs_motion_nodes
+  void bind_motion();                         // gs_motion_bind
+  bool refines_motion_at(uint32_t step) const;
+  bool moves_subject() const;                 // some view's motion has been learned
+  std::vector<float> motion_table(size_t frame) const;  // its node table (estimated when not learned)
+  void upload_motion(uint32_t view, const std::vector<float>& table);
+  // Pose and exposure (trainer_refine.cpp).
   bool refines_pose_at(uint32_t step) const { return options_.refine_poses && step >= options_.pose_from; }
   bool refines_exposure_at(uint32_t step) const {
     return options_.refine_exposure && step >= options_.exposure_from;
   }
-  void update_pose(const double grad[6], size_t frame);
-  static void apply_pose_step(PoseFix& fix, const double step[6]);
-  static Camera with_fix(Camera camera, const PoseFix& fix);  // [R | t] -> [E R | E t + d]
-  PoseFix align_camera(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3],
-                       const ViewMotion* motion, const PoseFix* start);
-  PoseFix neighbour_fix(size_t frame) const;
-  void update_pose_stats();
-  void update_exposure(const double fit[8], size_t frame);
-  std::array<float, 3> exposure_gain(size_t frame) const;
-  void update_exposure_stats();
+  double rate_fade(float final_fraction) const;  // final_fraction ^ (step / iterations)
+  // After a training step that kept its update: each view's pose, gain and motion learn
+  // from the step's gradients and sums; the spreads in the statistics follow.
+  void learn_corrections(const std::vector<size_t>& frames, const gs_step_result& r, bool pose, bool exposure,
+                         bool motion);
+  // A held-out view's camera aligned to its image (evaluate_views): the correction found,
+  // applied to `given`.
+  Camera align_view(const Camera& given, size_t frame, const uint8_t* rgba, const float gain[3],
+                    const std::vector<float>* moved, bool own);
   uint32_t sh_degree_at(uint32_t step) const;
   double lambda_at(uint32_t step) const;
   bool uses_ssim() const;
@@ -349,17 +337,9 @@ class Trainer {
   PassTimes profile_;
   std::vector<RetuneResult> retunes_;
   std::vector<uint8_t> frame_bytes_;  // the last step's first FrameData (densify thresholds)
-  static constexpr size_t kNone = ~size_t(0);
-  std::vector<size_t> train_before_, train_after_;  // each frame's nearest training frames in capture order
-  std::vector<PoseFix> pose_fix_;                    // per dataset frame
+  std::unique_ptr<Corrections> fix_;
+  std::vector<MotionNode> nodes_;          // the rig's nodes, as motion_nodes() reports them
   double last_pose_grad_[6] = {0, 0, 0, 0, 0, 0};
-  std::vector<std::array<double, 3>> gain_log_;  // per frame: log gain per channel, as measured (blended)
-  std::vector<uint32_t> gain_updates_;
-  std::vector<MotionNode> nodes_;
-  std::vector<std::vector<uint32_t>> node_neighbors_;  // up to 6 nearest, per node
-  float node_spacing_ = 1.0f;                          // median node radius
-  std::vector<ViewMotion> motion_;                     // per dataset frame (empty without nodes)
-  std::vector<uint32_t> motion_updates_;               // per dataset frame
   std::vector<double> last_motion_grad_;
   uint32_t bound_at_ = 0;  // step of the latest binding
 };

@@ -2,8 +2,8 @@
 // (next_view, :911-924), FrameData (write_frame, :440-547), statistics (read_slot /
 // set_view_stats, :778-805), the densify and opacity-reset schedule (after_step,
 // :932-945; densify, :1083-1119; reset_opacity, :1121-1128), evaluation (evaluate_views,
-// :1244-1292) and export (export_scene, :1773-1800). Pose and exposure refinement are in
-// refine.cpp, subject motion in motion.cpp.
+// :1244-1292) and export (export_scene, :1773-1800). Pose and exposure refinement and
+// subject motion are in trainer_refine.cpp.
 #include "gs/trainer.h"
 
 #include <algorithm>
@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "corrections.h"
 #include "frame.h"
 #include "gs_cuda.h"
 
@@ -67,21 +68,10 @@ Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, c
     if (!f.holdout) train_frames_.push_back(i);
   }
   if (train_frames_.empty()) throw std::runtime_error("Trainer: no training frames");
-  // Each frame's nearest training frames in capture order (trainer.cpp:314-329).
-  const size_t nf = dataset_.frames.size();
-  train_before_.assign(nf, kNone);
-  train_after_.assign(nf, kNone);
-  for (size_t f = 0, last = kNone; f < nf; ++f) {
-    train_before_[f] = last;
-    if (!dataset_.frames[f].holdout) last = f;
-  }
-  for (size_t f = nf, last = kNone; f-- > 0;) {
-    train_after_[f] = last;
-    if (!dataset_.frames[f].holdout) last = f;
-  }
-  pose_fix_.assign(nf, PoseFix{});
-  gain_log_.assign(nf, {0.0, 0.0, 0.0});
-  gain_updates_.assign(nf, 0u);
+  fix_ = std::make_unique<Corrections>();
+  fix_->order.build(dataset_.frames.size(), train_frames_);
+  fix_->poses.reset(dataset_.frames.size());
+  fix_->gains.reset(dataset_.frames.size());
   sh_stride_ = uint32_t(sh_rest_coeffs(options_.sh_degree) * 3);
   capacity_ = std::max(std::max(options_.max_gaussians, initial.count), 1u);
 
@@ -109,7 +99,7 @@ Trainer::Trainer(CudaContext& ctx, Dataset dataset, const SplatScene& initial, c
       ptr.push_back(f.rgba.data());
     }
     check(gs_dataset_set(gpu_, uint32_t(ptr.size()), w.data(), h.data(), ptr.data()), "Trainer: gs_dataset_set");
-    if (options_.refine_motion) place_nodes(initial);
+    if (options_.refine_motion) build_rig(initial);
   } catch (...) {
     gs_destroy(gpu_);
     gpu_ = nullptr;
@@ -214,16 +204,17 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   const bool pose = refines_pose_at(step), exposure = refines_exposure_at(step), motion = refines_motion_at(step);
   for (uint32_t v = 0; v < k; ++v) {
     cams[v] = camera_for(frames[v]);
-    const std::array<float, 3> gain = exposure_gain(frames[v]);
-    if (motion) start_motion(frames[v]);
+    float gain[3];
+    view_gain(frames[v], gain);
+    if (motion) fix_->rig.begin(frames[v], fix_->order);
     const uint32_t flags =
         (pose ? GS_FLAG_POSE_GRAD : 0u) | (motion ? GS_FLAG_MOTION | GS_FLAG_MOTION_GRAD : 0u);
-    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked, flags, gain.data());
+    write_frame(fd[v], cams[v], backgrounds[v].data(), step, ssim, options_.masked, flags, gain);
     images[v] = uint32_t(frames[v]);
   }
   check(gs_set_views_dataset(gpu_, k, fd.data(), images.data()), "Trainer::step: gs_set_views_dataset");
   if (motion)
-    for (uint32_t v = 0; v < k; ++v) set_motion_table(v, motion_[frames[v]]);
+    for (uint32_t v = 0; v < k; ++v) upload_motion(v, fix_->rig.table(fix_->rig.pose(frames[v])));
   if (retune_due(step)) {
     gs_tuning chosen;
     check(gs_autotune(gpu_, 2, &chosen), "Trainer::step: gs_autotune");
@@ -232,21 +223,7 @@ void Trainer::run_step(const std::vector<size_t>& frames, const std::vector<std:
   gs_step_result r;
   check(gs_step(gpu_, GS_STEP_TRAIN | (profile ? GS_STEP_PROFILE : 0u), &r), "Trainer::step: gs_step");
   // A step whose pairs did not fit left the model alone: no pose or gain update either.
-  if (!r.overflow) {
-    std::vector<double> motion_grad(nodes_.size() * 6);
-    for (uint32_t v = 0; v < k; ++v) {
-      if (pose) update_pose(r.pose_grad[v], frames[v]);
-      if (exposure) update_exposure(r.fit[v], frames[v]);
-      if (motion) {
-        check(gs_motion_gradient(gpu_, v, motion_grad.data(), uint32_t(nodes_.size())),
-              "Trainer::step: gs_motion_gradient");
-        update_motion(motion_grad.data(), frames[v]);
-      }
-    }
-    if (pose) update_pose_stats();
-    if (exposure) update_exposure_stats();
-    if (motion) update_motion_stats();
-  }
+  if (!r.overflow && (pose || exposure || motion)) learn_corrections(frames, r, pose, exposure, motion);
   // Statistics: the views' sums (read_slot / set_view_stats), averaged over the views.
   const double lambda = lambda_at(step);
   ViewLosses mean;
@@ -354,39 +331,40 @@ std::vector<uint8_t> Trainer::render(const Camera& camera, const float backgroun
   return render_with(camera, background, nullptr);
 }
 
-std::vector<uint8_t> Trainer::render_with(const Camera& camera, const float background[3], const ViewMotion* motion) {
+std::vector<uint8_t> Trainer::render_with(const Camera& camera, const float background[3],
+                                          const std::vector<float>* moved) {
   gs_frame_data f;
-  const bool moved = motion != nullptr && !nodes_.empty();
+  const bool moving = moved != nullptr && !nodes_.empty();
   detail::frame_geometry(f, camera, stats_.slots, sh_stride_, int(sh_degree_at(stats_.step)),
-                         moved ? GS_FLAG_MOTION : 0u, background);
-  if (moved) set_motion_table(0, *motion);  // gs_render moves the subject by view 0's motion
+                         moving ? GS_FLAG_MOTION : 0u, background);
+  if (moving) upload_motion(0, *moved);  // gs_render moves the subject by view 0's motion
   std::vector<uint8_t> out(size_t(camera.width) * camera.height * 4);
   check(gs_render(gpu_, &f, out.data()), "Trainer::render");
   return out;
 }
 
 std::vector<uint8_t> Trainer::render_view(size_t frame, const float background[3]) {
-  if (!uses_motion()) return render_with(camera_for(frame), background, nullptr);
-  const ViewMotion motion = view_motion(frame);
-  return render_with(camera_for(frame), background, &motion);
+  if (!moves_subject()) return render_with(camera_for(frame), background, nullptr);
+  const std::vector<float> table = motion_table(frame);
+  return render_with(camera_for(frame), background, &table);
 }
 
 void Trainer::run_eval_view(const Camera& camera, size_t frame, const uint8_t* rgba, const float gain[3],
-                            uint32_t flags, const ViewMotion* motion, gs_step_result& r) {
+                            uint32_t flags, const std::vector<float>* moved, gs_step_result& r) {
   // A measurement renders forward only with SSIM; an alignment probe trains with only the
   // camera moving (pose gradient, the model untouched) on L1 (trainer.cpp:1180-1183, 1250).
   const float black[3] = {0.0f, 0.0f, 0.0f};
   const bool align = (flags & GS_FLAG_POSE_ONLY) != 0u;
-  const bool moved = motion != nullptr && !nodes_.empty();
+  const bool moving = moved != nullptr && !nodes_.empty();
   gs_frame_data f;
-  write_frame(f, camera, black, stats_.step, !align, options_.masked, flags | (moved ? GS_FLAG_MOTION : 0u), gain);
+  write_frame(f, camera, black, stats_.step, !align, options_.masked, flags | (moving ? GS_FLAG_MOTION : 0u), gain);
   if (rgba != nullptr) {  // another dataset's image, uploaded with the step
     check(gs_set_views(gpu_, 1, &f, &rgba), "Trainer::evaluate: gs_set_views");
   } else {
     const uint32_t image = uint32_t(frame);
     check(gs_set_views_dataset(gpu_, 1, &f, &image), "Trainer::evaluate: gs_set_views_dataset");
   }
-  if (moved) set_motion_table(0, *motion);
+  if (moving) upload_motion(0, *moved);
   check(gs_step(gpu_, align ? GS_STEP_TRAIN : 0u, &r), "Trainer::evaluate: gs_step");
 }
 
@@ -407,10 +385,11 @@ EvalResult Trainer::evaluate_views(const Dataset& ds, bool own) {
   EvalResult result;
   const bool align = options_.refine_poses && options_.eval_pose_steps > 0;
   double sums[5] = {0, 0, 0, 0, 0}, unaligned = 0.0;
-  const bool moving = own && uses_motion();
-  auto measure = [&](const Camera& cam, size_t i, const float gain[3], const ViewMotion* motion, double* psnr_out) {
+  const bool moving = own && moves_subject();
+  auto measure = [&](const Camera& cam, size_t i, const float gain[3], const std::vector<float>* moved,
+                     double* psnr_out) {
     gs_step_result r;
-    run_eval_view(cam, i, own ? nullptr : ds.frames[i].rgba.data(), gain, 0u, motion, r);
+    run_eval_view(cam, i, own ? nullptr : ds.frames[i].rgba.data(), gain, 0u, moved, r);
     const ViewLosses l = view_losses(r.losses[0], cam.width, cam.height, lambda_at(stats_.step), true);
     if (psnr_out) {
       *psnr_out += l.psnr;
@@ -428,19 +407,16 @@ EvalResult Trainer::evaluate_views(const Dataset& ds, bool own) {
     if (!ds.frames[i].holdout) continue;
     float gain[3] = {1.0f, 1.0f, 1.0f};
     if (own) view_gain(i, gain);
-    ViewMotion motion;
-    if (moving) motion = view_motion(i);
-    const ViewMotion* m = moving ? &motion : nullptr;
+    std::vector<float> table;
+    if (moving) table = motion_table(i);
+    const std::vector<float>* m = moving ? &table : nullptr;
     const Camera given = dataset_camera(ds, ds.frames[i]);
-    PoseFix fix{};
+    Camera seen = given;
     if (align) {
       measure(given, i, gain, m, &unaligned);
-      // A view aligned before starts where it got to; otherwise between its neighbours.
-      const PoseFix start = !own ? PoseFix{} : pose_fix_[i].updates > 0 ? pose_fix_[i] : neighbour_fix(i);
-      fix = align_camera(given, i, own ? nullptr : ds.frames[i].rgba.data(), gain, m, &start);
-      if (own) pose_fix_[i] = fix;
+      seen = align_view(given, i, own ? nullptr : ds.frames[i].rgba.data(), gain, m, own);
     }
-    measure(with_fix(given, fix), i, gain, m, nullptr);
+    measure(seen, i, gain, m, nullptr);
     ++result.views;
   }
   if (result.views > 0) {

@@ -10,9 +10,14 @@
 //                                  estimate_head over the float32 xyz triples in <xyz> with
 //                                  world up (ux, uy, uz), then the head and exposure words of
 //                                  a FrameData for the test camera with gains (0.8, 1, 1.25)
+//   gs_host_selftest refine        the pose, exposure and motion-rig arithmetic of the
+//                                  trainer's corrections (rotations, rigid corrections, Adam,
+//                                  capture-order blends, centred gains, node placement and
+//                                  the rig energies' gradients against central differences)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -20,6 +25,8 @@
 #include <zlib.h>
 
 #include "../src/frame.h"
+#include "../src/node_rig.h"
+#include "../src/refinement.h"
 #include "gs/camera.h"
 #include "gs/dataset.h"
 #include "gs/splat_scene.h"
@@ -219,6 +226,156 @@ int head_summary(const std::string& path, const float up[3], float weight) {
   return 0;
 }
 
+int refine_checks() {
+  using namespace gs::refine;
+  std::mt19937 rng(12);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  auto close = [](double a, double b, double tol) { return std::fabs(a - b) <= tol; };
+  double worst = 0.0;
+  // Rotations: exp/log round trip, composition against matrices, slerp end points and middle.
+  for (int trial = 0; trial < 200; ++trial) {
+    const Vec3 w{1.5 * u(rng), 1.5 * u(rng), 1.5 * u(rng)};
+    const Vec3 back = Rotation::exp(w).log();
+    for (int c = 0; c < 3; ++c) worst = std::max(worst, std::fabs(back[c] - w[c]));
+    const Rotation a = Rotation::exp(w), b = Rotation::exp({u(rng), u(rng), u(rng)});
+    double A[9], B[9], AB[9];
+    a.to_matrix(A);
+    b.to_matrix(B);
+    a.after(b).to_matrix(AB);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += A[r * 3 + k] * B[k * 3 + c];
+        worst = std::max(worst, std::fabs(v - AB[r * 3 + c]));
+      }
+    const Rotation s0 = Rotation::slerp(a, b, 0.0), s1 = Rotation::slerp(a, b, 1.0);
+    const Rotation mid = Rotation::slerp(a, b, 0.5);
+    expect(close(s0.after(Rotation{{a.q[0], -a.q[1], -a.q[2], -a.q[3]}}).degrees(), 0.0, 1e-6), "slerp at 0");
+    expect(close(s1.after(Rotation{{b.q[0], -b.q[1], -b.q[2], -b.q[3]}}).degrees(), 0.0, 1e-6), "slerp at 1");
+    const double ab = b.after(Rotation{{a.q[0], -a.q[1], -a.q[2], -a.q[3]}}).degrees();
+    const double am = mid.after(Rotation{{a.q[0], -a.q[1], -a.q[2], -a.q[3]}}).degrees();
+    expect(close(am, 0.5 * ab, 1e-6), "slerp halfway");
+  }
+  expect(worst < 1e-9, "rotation round trips: " + std::to_string(worst));
+  // A correction followed by a step equals the camera composed by hand.
+  {
+    gs::Camera cam = gs::camera_from_c2w_gl(std::array<float, 16>{0.8f, 0.0f, 0.6f, 1.0f, 0.0f, 1.0f, 0.0f, 0.5f,
+                                                                  -0.6f, 0.0f, 0.8f, 2.0f, 0, 0, 0, 1}
+                                                .data(),
+                                            100.0f, 100.0f, 32.0f, 24.0f, 64, 48);
+    RigidFix fix;
+    fix = fix.then({0.01, -0.02, 0.03}, {0.02, 0.01, -0.03});
+    fix = fix.then({-0.005, 0.0, 0.01}, {0.0, 0.04, 0.0});
+    const gs::Camera got = fix.apply(cam);
+    double U[9];
+    fix.turn.to_matrix(U);
+    for (int r = 0; r < 3; ++r) {
+      double t = fix.shift[r];
+      for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+        for (int k = 0; k < 3; ++k) v += U[r * 3 + k] * cam.rotation[k * 3 + c];
+        expect(close(v, got.rotation[r * 3 + c], 1e-6), "corrected rotation");
+        t += U[r * 3 + c] * cam.translation[c];
+      }
+      expect(close(t, got.translation[r], 1e-6), "corrected translation");
+    }
+    for (int c = 0; c < 3; ++c) {
+      double p = 0.0;
+      for (int r = 0; r < 3; ++r) p -= double(got.rotation[r * 3 + c]) * got.translation[r];
+      expect(close(p, got.position[c], 1e-5), "corrected centre");
+    }
+  }
+  // Adam's first step is the rate against the gradient's sign.
+  {
+    Adam<6> adam;
+    const std::array<double, 6> step = adam.step({3.0, -1e-8, 0.0, 2.0, -5.0, 1e3}, {1, 2, 3, 4, 5, 6});
+    const double want[6] = {-1.0, 2.0, 0.0, -4.0, 5.0, -6.0};
+    for (int i = 0; i < 6; ++i) expect(close(step[i], want[i], 1e-9), "Adam first step");
+  }
+  // Capture order: the nearest usable trained frames on either side, never the frame itself.
+  CaptureOrder order;
+  order.build(10, {1, 3, 4, 7});
+  auto all = [](size_t) { return true; };
+  CaptureOrder::Span s = order.around(5, all);
+  expect(s.lo == 4 && s.hi == 7 && close(s.t, 1.0 / 3.0, 1e-12), "span of 5");
+  s = order.around(0, all);
+  expect(s.lo == CaptureOrder::kNone && s.hi == 1 && s.t == 1.0, "span of 0");
+  s = order.around(9, all);
+  expect(s.lo == 7 && s.hi == CaptureOrder::kNone && s.t == 0.0, "span of 9");
+  s = order.around(3, all);
+  expect(s.lo == 1 && s.hi == 4, "span of a trained frame");
+  s = order.around(5, [](size_t f) { return f != 4; });
+  expect(s.lo == 3 && s.hi == 7, "span skipping an unusable frame");
+  // Gains: centred on the measured trained views, blended for the others.
+  {
+    GainTable g;
+    g.reset(10);
+    const double f1[8] = {1000, 1000, 1000, 600, 2000, 1000, 500, 0};  // gains 2, 1, 0.5
+    const double f3[8] = {1000, 1000, 1000, 600, 1000, 1000, 1000, 0};  // gains 1, 1, 1
+    g.observe(1, f1, 0.3);
+    g.observe(3, f3, 0.3);
+    const double few[8] = {1000, 1000, 1000, 10, 9000, 9000, 9000, 0};  // too few pixels: ignored
+    g.observe(3, few, 0.3);
+    const std::array<float, 3> a = g.gains(1, order), b = g.gains(3, order), m = g.gains(2, order);
+    expect(close(a[0], std::sqrt(2.0), 1e-5) && close(a[1], 1.0, 1e-6) && close(a[2], std::sqrt(0.5), 1e-5),
+           "centred gains of frame 1");
+    expect(close(double(a[0]) * b[0], 1.0, 1e-5) && close(double(a[2]) * b[2], 1.0, 1e-5), "centred gains of frame 3");
+    expect(close(m[0], 1.0, 1e-5), "frame 2 halfway between 1 and 3 in log gain");
+    const GainTable::Spread spread = g.spread(order);
+    expect(spread.updates == 2 && spread.low <= spread.high, "gain spread");
+  }
+  // The rig: placement, and its energies' gradients against central differences.
+  double grad_err = 0.0;
+  {
+    std::vector<float> xyz;
+    std::normal_distribution<float> n(0.0f, 0.3f);
+    for (int i = 0; i < 6000; ++i) {
+      const float cx = i % 2 ? 1.0f : -1.0f;
+      xyz.insert(xyz.end(), {cx + n(rng), n(rng), 0.5f * n(rng)});
+    }
+    NodeRig rig;
+    rig.place(xyz, 24, 10, 0.1f);
+    expect(rig.size() == 24 && rig.spacing() > 0.0f, "rig size");
+    for (const NodeRig::Node& node : rig.nodes()) expect(node.radius > 0.0f, "node radius");
+    for (size_t f : {1, 3, 7})
+      for (size_t k = 0; k < rig.size(); ++k)
+        rig.set(f, k, {0.05 * u(rng), 0.05 * u(rng), 0.05 * u(rng)}, {0.02 * u(rng), 0.02 * u(rng), 0.02 * u(rng)});
+    RigEnergy w;
+    w.decay = 0.3;
+    w.rigidity = 0.7;
+    w.smoothness = 0.2;
+    w.centring = 0.4;
+    // Frame 4: shifts anywhere, turns at zero (where a turn applied on top of the node's and
+    // the rotation vector agree to first order).
+    for (size_t k = 0; k < rig.size(); ++k) rig.set(4, k, {0.0, 0.0, 0.0}, {0.03 * u(rng), 0.03 * u(rng), 0.03 * u(rng)});
+    const std::vector<double> grad = rig.energy_gradient(4, w, order);
+    double scale = 0.0;
+    for (double v : grad) scale = std::max(scale, std::fabs(v));
+    const double h = 1e-6;
+    for (size_t k = 0; k < rig.size(); ++k)
+      for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < 3; ++c) {
+          NodeMotion m = rig.pose(4)[k];
+          Vec3& x = part == 0 ? m.shift : m.turn;
+          const double saved = x[c];
+          x[c] = saved + h;
+          rig.set(4, k, m.turn, m.shift);
+          const double up = rig.energy(4, w, order);
+          x[c] = saved - h;
+          rig.set(4, k, m.turn, m.shift);
+          const double down = rig.energy(4, w, order);
+          x[c] = saved;
+          rig.set(4, k, m.turn, m.shift);
+          grad_err = std::max(grad_err, std::fabs((up - down) / (2.0 * h) - grad[k * 6 + part * 3 + c]) / scale);
+        }
+    const std::vector<float> table = rig.table(rig.pose(4));
+    expect(table.size() == rig.size() * 20, "node table size");
+  }
+  expect(grad_err < 1e-5, "rig energy gradient vs central differences: " + std::to_string(grad_err));
+  std::printf("{\"rotation_err\": %.3g, \"rig_gradient_err\": %.3g}\n", worst, grad_err);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -226,6 +383,7 @@ int main(int argc, char** argv) {
     const std::string mode = argc > 1 ? argv[1] : "";
     if (mode == "scene" && argc > 2) return scene_checks(argv[2]);
     if (mode == "frame") return frame_words();
+    if (mode == "refine") return refine_checks();
     if (mode == "camera") return camera_floats();
     if (mode == "dataset" && argc > 4) return dataset_summary(argv[2], uint32_t(std::atoi(argv[3])), uint32_t(std::atoi(argv[4])));
     if (mode == "head" && argc > 6) {

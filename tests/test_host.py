@@ -6,6 +6,7 @@ other writers are available here), axis conversion, and the
 FrameData the C++ trainer writes compared word for word with the Python mirror
 (gs_b200.frame.make_frame, itself pinned to the oracle by the GPU parity tests).
 """
+import json
 import os
 import struct
 import subprocess
@@ -137,3 +138,12 @@ def test_no_head_region_for_small_or_sparse_subjects(tmp_path):
     assert not got["found"] and got["frame_head"] == [0, 0, 0, 1]
     f.write_bytes(standing_person(rng)[:150].tobytes())  # under 200 points
     assert not json.loads(run("head", str(f), "0", "1", "0", "3.0"))["found"]
+
+
+def test_refinement_arithmetic():
+    """The trainer's pose, exposure and motion-rig arithmetic on the CPU: rotation
+    exp/log/composition/slerp, a correction followed by steps against the composed camera,
+    Adam's first step, capture-order spans, centred and blended gains, node placement, and
+    the rig energies' gradients against central differences (to 1e-5 of the largest)."""
+    m = json.loads(run("refine").strip().splitlines()[-1])
+    assert m["rotation_err"] < 1e-9 and m["rig_gradient_err"] < 1e-5
