@@ -20,6 +20,11 @@ struct DatasetFrame {
   // reference's datasets share one resolution; batched training mixes them.
   uint32_t width = 0, height = 0;
   float fx = 0, fy = 0, cx = 0, cy = 0;
+  // Optional depth map (its own, usually lower, resolution): metres along the optical
+  // axis, 0 where missing, with an optional confidence per sample (0..255).
+  uint32_t depth_width = 0, depth_height = 0;
+  std::vector<float> depth;
+  std::vector<uint8_t> depth_confidence;
 };
 
 struct Dataset {
@@ -28,6 +33,7 @@ struct Dataset {
   uint32_t height = 0;
   float fx = 0, fy = 0, cx = 0, cy = 0;  // at training resolution
   bool has_masks = false;
+  bool has_depth = false;  // some frame names a depth map
   std::vector<DatasetFrame> frames;
   std::vector<float> points;          // optional sparse point cloud, xyz
   std::vector<uint8_t> point_colors;  // rgb per point
@@ -45,33 +51,39 @@ struct Dataset {
 void compute_camera_bounds(Dataset& dataset);
 
 // Loads `directory`/transforms.json (nerfstudio layout: w, h, fl_x[, fl_y, cx, cy],
-// frames with file_path, transform_matrix (OpenGL camera-to-world) and optional
-// mask_path; optional ply_file_path point cloud and gsplat_lab.world_up), as the
-// reference's load_dataset does (dataset.cpp:85-223): images resized by area so their
-// short side is `target_width` (never enlarged), masks into alpha (255 without masks),
-// every 8th frame held out, unreadable frames skipped and listed (throws when fewer than
-// 2 or half remain). Images are PNG (8/16-bit) or binary PPM/PGM; JPEG frames and depth
-// maps are not decoded by libgs_host (JPEG frames are skipped like unreadable ones).
+// frames with file_path, transform_matrix (OpenGL camera-to-world) and optional mask_path,
+// depth_file_path and depth_confidence_path; optional depth_unit_scale_factor (metres per
+// depth sample, default 0.001), ply_file_path point cloud and gsplat_lab.world_up), as the
+// reference's load_dataset does (dataset.cpp:85-223): images resized by area so their short
+// side is `target_width` (never enlarged), masks into alpha (255 without masks), every 8th
+// frame held out, unreadable frames skipped and listed (throws when fewer than 2 or half
+// remain), depth kept at its own resolution. Images are PNG (8/16-bit), binary PPM/PGM or
+// JPEG (decoded on the GPU by nvJPEG); depth maps are 16-bit PNG or PGM.
 Dataset load_dataset(const std::string& directory, uint32_t target_width);
 
 struct InitOptions {
   uint32_t max_gaussians = 150000;
+  bool subject_only = true;     // depth points only where the frame's mask covers them (with masks)
+  float min_confidence = 0.3f;  // depth samples below this confidence (0..1) are left out
   float initial_opacity = 0.2f;
   uint32_t seed = 1;
 };
 
 struct InitStats {
-  std::string source;  // "points" or "random"
+  std::string source;  // "depth", "points" or "random"
   size_t raw_points = 0;
-  float voxel_size = 0;
+  float voxel_size = 0;  // cell of the merge that brought the points under budget (0: none)
 };
 
-// Initial gaussians (SH degree 0) from the dataset's sparse points, or random points
-// around the cameras' centre (initialize_gaussians, dataset.cpp:291-523 without its depth
-// source): over budget the points are merged per voxel (cell size bisected in log space to
-// land under max_gaussians; the bracket widens until it does), ordered along a Morton curve, given isotropic scales from the
-// mean distance to their 3 nearest neighbours (clamped to [1e-4, 0.02] x the points'
-// robust extent), identity rotations and `initial_opacity`.
+// Initial gaussians (SH degree 0), the reference's sources in its order of preference
+// (initialize_gaussians, dataset.cpp:291-523): the training frames' depth maps
+// back-projected (confident samples, inside the subject mask with subject_only), else the
+// dataset's sparse points, else random points in a ball of half the camera extent around
+// the cameras' centre. Over budget the points are merged per occupied cell of a grid whose
+// cell size is fitted to land just under max_gaussians. They are then ordered along a
+// Morton curve and given identity rotations, `initial_opacity`, and isotropic scales from
+// the mean distance to their 3 nearest neighbours, clamped to [1e-4, 0.02] x the points'
+// robust extent (the 0.5%..99.5% box's diagonal).
 SplatScene initialize_gaussians(const Dataset& dataset, const InitOptions& options, InitStats* stats = nullptr);
 
 // Where a standing person's head is, from points on them (estimate_head,

@@ -5,9 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <array>
 #include <random>
 #include <stdexcept>
-#include <unordered_map>
 
 #include "frame.h"
 #include "gs_cuda.h"
@@ -154,20 +154,6 @@ std::string join(const std::string& dir, const std::string& file) {
   return dir.empty() || dir.back() == '/' ? dir + file : dir + "/" + file;
 }
 
-uint64_t cell_key(int64_t x, int64_t y, int64_t z) {
-  return (uint64_t(x) & 0x1fffffull) | (uint64_t(y) & 0x1fffffull) << 21 | (uint64_t(z) & 0x1fffffull) << 42;
-}
-
-// 10 bits of v spread to every third bit (Morton order).
-uint32_t spread3(uint32_t v) {
-  v &= 0x3ffu;
-  v = (v | (v << 16)) & 0x030000ffu;
-  v = (v | (v << 8)) & 0x0300f00fu;
-  v = (v | (v << 4)) & 0x030c30c3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
-
 }  // namespace
 
 Dataset load_dataset(const std::string& directory, uint32_t target_width) {
@@ -179,6 +165,7 @@ Dataset load_dataset(const std::string& directory, uint32_t target_width) {
   const double src_w = root.number_or("w", 0), src_h = root.number_or("h", 0);
   const double fl_x = root.number_or("fl_x", 0), fl_y = root.number_or("fl_y", fl_x);
   if (src_w <= 0 || src_h <= 0 || fl_x <= 0) throw std::runtime_error("transforms.json has no w/h/fl_x");
+  const double depth_unit = root.number_or("depth_unit_scale_factor", 0.001);  // metres per depth sample
   Dataset ds;
   if (const detail::Json* lab = root.find("gsplat_lab")) {
     const detail::Json* up = lab->find("world_up");
@@ -204,7 +191,7 @@ Dataset load_dataset(const std::string& directory, uint32_t target_width) {
   ds.cy = float(root.number_or("cy", src_h / 2) * s);
   const size_t n = frames->array.size();
   std::vector<DatasetFrame> all(n);
-  std::vector<std::string> images(n), masks(n);
+  std::vector<std::string> images(n), masks(n), depths(n), confidences(n);
   for (size_t i = 0; i < n; ++i) {
     const detail::Json& f = frames->array[i];
     images[i] = f.string_or("file_path", "");
@@ -217,9 +204,12 @@ Dataset load_dataset(const std::string& directory, uint32_t target_width) {
       for (int col = 0; col < 4; ++col) all[i].c2w[r * 4 + col] = float(m->array[size_t(r)].array[size_t(col)].number);
     }
     masks[i] = f.string_or("mask_path", "");
+    depths[i] = f.string_or("depth_file_path", "");
+    confidences[i] = f.string_or("depth_confidence_path", "");
     all[i].holdout = i % 8 == 0;
   }
   ds.has_masks = std::all_of(masks.begin(), masks.end(), [](const std::string& p) { return !p.empty(); });
+  ds.has_depth = std::any_of(depths.begin(), depths.end(), [](const std::string& p) { return !p.empty(); });
   for (size_t i = 0; i < n; ++i) {
     DatasetFrame& frame = all[i];
     try {
@@ -234,10 +224,29 @@ Dataset load_dataset(const std::string& directory, uint32_t target_width) {
       } else {
         for (size_t p = 0; p < size_t(ds.width) * ds.height; ++p) frame.rgba[p * 4 + 3] = 255;
       }
-      ds.frames.push_back(std::move(frame));
     } catch (const std::exception& e) {
       ds.skipped.push_back(images[i] + ": " + e.what());
+      continue;
     }
+    // Depth is optional per frame: one that cannot be read just adds no points.
+    if (!depths[i].empty()) {
+      try {
+        const detail::Depth16 d = detail::decode_depth16(read_file(join(directory, depths[i])));
+        frame.depth.resize(d.data.size());
+        for (size_t p = 0; p < d.data.size(); ++p) frame.depth[p] = float(double(d.data[p]) * depth_unit);
+        frame.depth_width = d.width;
+        frame.depth_height = d.height;
+        if (!confidences[i].empty()) {
+          detail::Image c = detail::decode_image(read_file(join(directory, confidences[i])), 1);
+          if (c.width == d.width && c.height == d.height) frame.depth_confidence = std::move(c.data);
+        }
+      } catch (const std::exception&) {
+        frame.depth.clear();
+        frame.depth_confidence.clear();
+        frame.depth_width = frame.depth_height = 0;
+      }
+    }
+    ds.frames.push_back(std::move(frame));
   }
   if (ds.frames.size() < 2 || ds.frames.size() * 2 < n)
     throw std::runtime_error("too few readable frames (" + std::to_string(ds.frames.size()) + "/" + std::to_string(n) +
@@ -266,176 +275,322 @@ Dataset load_dataset(const std::string& directory, uint32_t target_width) {
   return ds;
 }
 
-SplatScene initialize_gaussians(const Dataset& ds, const InitOptions& o, InitStats* stats) {
-  std::vector<float> pts, cols;  // colours in [0, 1]
-  std::string source = "points";
-  if (!ds.points.empty()) {
-    pts = ds.points;
-    for (uint8_t c : ds.point_colors) cols.push_back(float(c) / 255.0f);
-  } else {
-    source = "random";  // uniform in a ball of half the camera extent around the cameras' centre
-    std::mt19937 rng(o.seed);
-    std::uniform_real_distribution<float> u(-1.0f, 1.0f);
-    const float radius = 0.5f * ds.camera_extent;
-    for (uint32_t i = 0; i < o.max_gaussians; ++i) {
-      float p[3];
-      do
-        for (float& v : p) v = u(rng);
-      while (p[0] * p[0] + p[1] * p[1] + p[2] * p[2] > 1.0f);
-      for (int k = 0; k < 3; ++k) {
-        pts.push_back(ds.camera_center[k] + radius * p[k]);
-        cols.push_back(0.5f);
+namespace {
+
+// A coloured point set: xyz and rgb (0..1), three floats each per point.
+struct Cloud {
+  std::vector<float> xyz, rgb;
+  size_t size() const { return xyz.size() / 3; }
+};
+
+// The training frames' depth samples as world points, coloured by the frame's pixel there.
+Cloud depth_cloud(const Dataset& ds, const InitOptions& o) {
+  Cloud c;
+  const float floor_conf = std::clamp(o.min_confidence, 0.0f, 1.0f) * 255.0f;
+  const bool subject = o.subject_only && ds.has_masks;
+  for (const DatasetFrame& f : ds.frames) {
+    if (f.holdout || f.depth.empty()) continue;
+    const Camera cam = dataset_camera(ds, f);
+    for (uint32_t v = 0; v < f.depth_height; ++v)
+      for (uint32_t u = 0; u < f.depth_width; ++u) {
+        const size_t at = size_t(v) * f.depth_width + u;
+        const double z = f.depth[at];
+        if (!(z > 0.0)) continue;
+        if (!f.depth_confidence.empty() && float(f.depth_confidence[at]) < floor_conf) continue;
+        // The sample's centre in training pixels, and the pixel it lands in.
+        const double px = (u + 0.5) * cam.width / f.depth_width, py = (v + 0.5) * cam.height / f.depth_height;
+        const uint32_t ix = std::min(cam.width - 1, uint32_t(px)), iy = std::min(cam.height - 1, uint32_t(py));
+        const uint8_t* rgba = &f.rgba[(size_t(iy) * cam.width + ix) * 4];
+        if (subject && rgba[3] < 128) continue;
+        // OpenCV camera coordinates; the OpenGL camera-to-world takes (x, -y, -z).
+        const double x = (px - cam.cx) / cam.fx * z, y = (py - cam.cy) / cam.fy * z;
+        for (int r = 0; r < 3; ++r)
+          c.xyz.push_back(float(f.c2w[r * 4] * x - f.c2w[r * 4 + 1] * y - f.c2w[r * 4 + 2] * z + f.c2w[r * 4 + 3]));
+        for (int k = 0; k < 3; ++k) c.rgb.push_back(float(rgba[k]) / 255.0f);
       }
+  }
+  return c;
+}
+
+Cloud random_cloud(const Dataset& ds, uint32_t count, uint32_t seed) {
+  Cloud c;
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<float> u(-1.0f, 1.0f);
+  const float radius = 0.5f * ds.camera_extent;
+  while (c.size() < count) {
+    const float p[3] = {u(rng), u(rng), u(rng)};
+    if (p[0] * p[0] + p[1] * p[1] + p[2] * p[2] > 1.0f) continue;  // inside the unit ball
+    for (int k = 0; k < 3; ++k) {
+      c.xyz.push_back(ds.camera_center[k] + radius * p[k]);
+      c.rgb.push_back(0.5f);
     }
   }
-  const size_t raw = pts.size() / 3;
-  if (raw == 0) throw std::runtime_error("initialize_gaussians: no points");
+  return c;
+}
+
+// The diagonal of the box between each axis's 0.5% and 99.5% order statistics: the span
+// of the points without strays (depth smeared off an edge, flyers).
+float robust_extent(const std::vector<float>& xyz) {
+  const size_t n = xyz.size() / 3;
+  std::vector<float> axis(n);
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    for (size_t i = 0; i < n; ++i) axis[i] = xyz[i * 3 + k];
+    const size_t lo = n / 200, hi = n - 1 - n / 200;
+    std::nth_element(axis.begin(), axis.begin() + long(lo), axis.end());
+    const float a = axis[lo];
+    std::nth_element(axis.begin(), axis.begin() + long(hi), axis.end());
+    d2 += double(axis[hi] - a) * double(axis[hi] - a);
+  }
+  return float(std::sqrt(d2)) + 1e-6f;
+}
+
+// Grid cells of size `cell` from `origin`, 21 bits per axis in one 63-bit key.
+struct Grid {
+  float origin[3];
+  float cell;
+  uint64_t key(const float* p) const {
+    uint64_t out = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double c = std::floor((double(p[k]) - origin[k]) / cell);
+      out |= (uint64_t(int64_t(std::clamp(c, 0.0, double((1 << 21) - 1)))) & 0x1fffffu) << (21 * k);
+    }
+    return out;
+  }
+};
+
+// (cell key, point) of every point, sorted by key: a cell's points are one run.
+std::vector<std::pair<uint64_t, uint32_t>> by_cell(const std::vector<float>& xyz, const Grid& g) {
+  std::vector<std::pair<uint64_t, uint32_t>> keyed(xyz.size() / 3);
+  for (size_t i = 0; i < keyed.size(); ++i) keyed[i] = {g.key(&xyz[i * 3]), uint32_t(i)};
+  std::sort(keyed.begin(), keyed.end());
+  return keyed;
+}
+
+size_t occupied(const std::vector<float>& xyz, const Grid& g) {
+  std::vector<uint64_t> keys(xyz.size() / 3);
+  for (size_t i = 0; i < keys.size(); ++i) keys[i] = g.key(&xyz[i * 3]);
+  std::sort(keys.begin(), keys.end());
+  return size_t(std::unique(keys.begin(), keys.end()) - keys.begin());
+}
+
+// A cell size whose occupied-cell count is at most `budget` and close under it. The count
+// falls with the cell size roughly as a power law (size^-D, D the points' dimension), so
+// the size is found by false position on log(count) against log(size), kept inside a
+// bracket [small: count over budget, large: count within it] that every probe narrows.
+float fit_cell(const std::vector<float>& xyz, Grid g, float extent, size_t budget) {
+  auto count_at = [&](double cell) {
+    g.cell = float(cell);
+    return double(std::max<size_t>(occupied(xyz, g), 1));
+  };
+  double small = extent * 1e-4, large = extent;
+  double n_small = count_at(small), n_large = count_at(large);
+  if (n_small <= double(budget)) return float(small);
+  for (int i = 0; i < 60 && n_large > double(budget); ++i) n_large = count_at(large *= 2.0);
+  const double target = std::log(0.97 * double(budget));
+  for (int round = 0; round < 24; ++round) {
+    if (n_large >= 0.9 * double(budget) || large / small < 1.01) break;
+    // Where the line through the bracket's ends in log-log space meets the target, kept
+    // away from the ends (else the geometric middle).
+    const double ls = std::log(small), ll = std::log(large);
+    const double ys = std::log(n_small), yl = std::log(n_large);
+    double x = ys > yl ? ls + (ys - target) * (ll - ls) / (ys - yl) : 0.5 * (ls + ll);
+    const double margin = 0.05 * (ll - ls);
+    if (!(x > ls + margin && x < ll - margin)) x = 0.5 * (ls + ll);
+    const double cell = std::exp(x), n = count_at(cell);
+    if (n > double(budget)) {
+      small = cell;
+      n_small = n;
+    } else {
+      large = cell;
+      n_large = n;
+    }
+  }
+  return float(large);
+}
+
+// The points of each occupied cell replaced by their mean (position and colour).
+Cloud merge_cells(const Cloud& in, const Grid& g) {
+  const auto keyed = by_cell(in.xyz, g);
+  Cloud out;
+  for (size_t a = 0; a < keyed.size();) {
+    size_t b = a;
+    double sum[6] = {0, 0, 0, 0, 0, 0};
+    for (; b < keyed.size() && keyed[b].first == keyed[a].first; ++b)
+      for (int k = 0; k < 3; ++k) {
+        sum[k] += in.xyz[size_t(keyed[b].second) * 3 + k];
+        sum[3 + k] += in.rgb[size_t(keyed[b].second) * 3 + k];
+      }
+    const double n = double(b - a);
+    for (int k = 0; k < 3; ++k) {
+      out.xyz.push_back(float(sum[k] / n));
+      out.rgb.push_back(float(sum[3 + k] / n));
+    }
+    a = b;
+  }
+  return out;
+}
+
+// The points reordered along a Z-order (Morton) curve over their bounding box, 10 bits per
+// axis: points near in space are near in memory.
+Cloud morton_sorted(const Cloud& in) {
+  const size_t n = in.size();
   float lo[3], hi[3];
   for (int k = 0; k < 3; ++k) {
     lo[k] = INFINITY;
     hi[k] = -INFINITY;
   }
-  for (size_t i = 0; i < raw; ++i)
+  for (size_t i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], pts[i * 3 + k]);
-      hi[k] = std::max(hi[k], pts[i * 3 + k]);
+      lo[k] = std::min(lo[k], in.xyz[i * 3 + k]);
+      hi[k] = std::max(hi[k], in.xyz[i * 3 + k]);
     }
-  // The span without strays: the diagonal of the 0.5%..99.5% box.
-  float extent = 1e-6f;
-  {
-    std::vector<float> axis(raw);
-    double e2 = 0.0;
+  std::vector<std::pair<uint32_t, uint32_t>> code(n);
+  for (size_t i = 0; i < n; ++i) {
+    uint32_t q[3];
     for (int k = 0; k < 3; ++k) {
-      for (size_t i = 0; i < raw; ++i) axis[i] = pts[i * 3 + k];
-      const size_t a = raw / 200, b = raw - 1 - raw / 200;
-      std::nth_element(axis.begin(), axis.begin() + long(a), axis.end());
-      const float low = axis[a];
-      std::nth_element(axis.begin(), axis.begin() + long(b), axis.end());
-      e2 += double(axis[b] - low) * double(axis[b] - low);
+      const float t = (in.xyz[i * 3 + k] - lo[k]) / std::max(hi[k] - lo[k], 1e-6f);
+      q[k] = uint32_t(std::clamp(t, 0.0f, 1.0f) * 1023.0f);
     }
-    extent += float(std::sqrt(e2));
+    uint32_t z = 0;
+    for (int bit = 9; bit >= 0; --bit)
+      for (int k = 2; k >= 0; --k) z = z << 1 | ((q[k] >> bit) & 1u);
+    code[i] = {z, uint32_t(i)};
   }
-  auto cell_of = [&](const float* p, float cell, int64_t c[3]) {
-    for (int k = 0; k < 3; ++k) c[k] = int64_t(std::floor((p[k] - lo[k]) / cell));
-  };
-  auto occupied = [&](const std::vector<float>& p, float cell) {
-    std::vector<uint64_t> keys(p.size() / 3);
-    for (size_t i = 0; i < keys.size(); ++i) {
-      int64_t c[3];
-      cell_of(&p[i * 3], cell, c);
-      keys[i] = cell_key(c[0], c[1], c[2]);
+  std::sort(code.begin(), code.end());
+  Cloud out;
+  out.xyz.reserve(in.xyz.size());
+  out.rgb.reserve(in.rgb.size());
+  for (const auto& c : code)
+    for (int k = 0; k < 3; ++k) {
+      out.xyz.push_back(in.xyz[size_t(c.second) * 3 + k]);
+      out.rgb.push_back(in.rgb[size_t(c.second) * 3 + k]);
     }
-    std::sort(keys.begin(), keys.end());
-    return size_t(std::unique(keys.begin(), keys.end()) - keys.begin());
+  return out;
+}
+
+// A k-d tree over points (median splits on the widest axis) answering "the k nearest
+// other points" by branch-and-bound.
+class KdTree {
+ public:
+  explicit KdTree(const std::vector<float>& xyz) : xyz_(xyz), index_(xyz.size() / 3) {
+    for (size_t i = 0; i < index_.size(); ++i) index_[i] = uint32_t(i);
+    build(0, 0, index_.size());
+  }
+  // Squared distances to the (up to) 3 nearest points other than point `self`, ascending.
+  std::array<float, 3> nearest3(uint32_t self) const {
+    std::array<float, 3> best{INFINITY, INFINITY, INFINITY};
+    search(0, 0, index_.size(), &xyz_[size_t(self) * 3], self, best);
+    return best;
+  }
+
+ private:
+  struct Split {
+    int axis;
+    float value;
   };
-  // The cell size whose occupied-cell count lands just under `target` (log-space bisection;
-  // the large end is doubled first until it is under, so the budget always holds).
-  auto cell_for = [&](const std::vector<float>& p, size_t target) {
-    float small = extent * 1e-4f, large = extent * 0.1f;
-    for (int it = 0; it < 40 && occupied(p, large) > target; ++it) large *= 2.0f;
-    for (int it = 0; it < 12; ++it) {
-      const float mid = std::sqrt(small * large);
-      (occupied(p, mid) > target ? small : large) = mid;
+  // Node `node` holds points [a, b) of index_; its children are 2 node + 1 and 2 node + 2.
+  void build(size_t node, size_t a, size_t b) {
+    if (b - a <= kLeaf) return;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = a; i < b; ++i)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], xyz_[size_t(index_[i]) * 3 + k]);
+        hi[k] = std::max(hi[k], xyz_[size_t(index_[i]) * 3 + k]);
+      }
+    int axis = 0;
+    for (int k = 1; k < 3; ++k)
+      if (hi[k] - lo[k] > hi[axis] - lo[axis]) axis = k;
+    const size_t mid = (a + b) / 2;
+    std::nth_element(index_.begin() + long(a), index_.begin() + long(mid), index_.begin() + long(b),
+                     [&](uint32_t i, uint32_t j) { return xyz_[size_t(i) * 3 + axis] < xyz_[size_t(j) * 3 + axis]; });
+    if (splits_.size() <= node) splits_.resize(2 * node + 1);
+    splits_[node] = {axis, xyz_[size_t(index_[mid]) * 3 + axis]};
+    build(2 * node + 1, a, mid);
+    build(2 * node + 2, mid, b);
+  }
+  void search(size_t node, size_t a, size_t b, const float* q, uint32_t self, std::array<float, 3>& best) const {
+    if (b - a <= kLeaf) {
+      for (size_t i = a; i < b; ++i) {
+        if (index_[i] == self) continue;
+        const float* p = &xyz_[size_t(index_[i]) * 3];
+        const float d2 = (p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2]);
+        if (d2 < best[2]) {
+          best[2] = d2;
+          std::sort(best.begin(), best.end());
+        }
+      }
+      return;
     }
-    return large;
-  };
+    const Split s = splits_[node];
+    const size_t mid = (a + b) / 2;
+    const float gap = q[s.axis] - s.value;
+    const bool left_first = gap < 0.0f;
+    const size_t near = left_first ? 2 * node + 1 : 2 * node + 2, far = left_first ? 2 * node + 2 : 2 * node + 1;
+    search(near, left_first ? a : mid, left_first ? mid : b, q, self, best);
+    if (gap * gap < best[2]) search(far, left_first ? mid : a, left_first ? b : mid, q, self, best);
+  }
+  static constexpr size_t kLeaf = 16;
+  const std::vector<float>& xyz_;
+  std::vector<uint32_t> index_;
+  std::vector<Split> splits_;
+};
+
+}  // namespace
+
+SplatScene initialize_gaussians(const Dataset& ds, const InitOptions& o, InitStats* stats) {
+  Cloud cloud;
+  std::string source;
+  if (ds.has_depth) {
+    cloud = depth_cloud(ds, o);
+    source = "depth";
+  }
+  if (cloud.size() == 0 && !ds.points.empty()) {
+    cloud.xyz = ds.points;
+    for (uint8_t c : ds.point_colors) cloud.rgb.push_back(float(c) / 255.0f);
+    source = "points";
+  }
+  if (cloud.size() == 0) {
+    cloud = random_cloud(ds, o.max_gaussians, o.seed);
+    source = "random";
+  }
+  const size_t raw = cloud.size();
+  if (raw == 0) throw std::runtime_error("initialize_gaussians: no points");
+  const float extent = robust_extent(cloud.xyz);
   float voxel = 0.0f;
   if (raw > o.max_gaussians) {
-    voxel = cell_for(pts, o.max_gaussians);
-    struct Acc {
-      double p[3] = {0, 0, 0}, c[3] = {0, 0, 0};
-      uint32_t n = 0;
-    };
-    std::unordered_map<uint64_t, Acc> cells;
-    for (size_t i = 0; i < raw; ++i) {
-      int64_t c[3];
-      cell_of(&pts[i * 3], voxel, c);
-      Acc& a = cells[cell_key(c[0], c[1], c[2])];
-      for (int k = 0; k < 3; ++k) {
-        a.p[k] += pts[i * 3 + k];
-        a.c[k] += cols[i * 3 + k];
-      }
-      ++a.n;
-    }
-    std::vector<float> mp, mc;
-    for (const auto& kv : cells)
-      for (int k = 0; k < 3; ++k) {
-        mp.push_back(float(kv.second.p[k] / kv.second.n));
-        mc.push_back(float(kv.second.c[k] / kv.second.n));
-      }
-    pts.swap(mp);
-    cols.swap(mc);
+    Grid g{{INFINITY, INFINITY, INFINITY}, 0.0f};
+    for (size_t i = 0; i < raw; ++i)
+      for (int k = 0; k < 3; ++k) g.origin[k] = std::min(g.origin[k], cloud.xyz[i * 3 + k]);
+    voxel = fit_cell(cloud.xyz, g, extent, std::max<size_t>(o.max_gaussians, 1));
+    g.cell = voxel;
+    cloud = merge_cells(cloud, g);
   }
-  const size_t n = pts.size() / 3;
-  // Morton order: neighbours in space are neighbours in memory.
-  {
-    std::vector<std::pair<uint32_t, uint32_t>> order(n);
-    for (size_t i = 0; i < n; ++i) {
-      uint32_t code = 0;
-      for (int k = 0; k < 3; ++k) {
-        const float span = std::max(hi[k] - lo[k], 1e-6f);
-        code |= spread3(uint32_t(std::min(std::max((pts[i * 3 + k] - lo[k]) / span, 0.0f), 1.0f) * 1023.0f)) << k;
-      }
-      order[i] = {code, uint32_t(i)};
-    }
-    std::sort(order.begin(), order.end());
-    std::vector<float> p2(pts.size()), c2(cols.size());
-    for (size_t j = 0; j < n; ++j)
-      for (int k = 0; k < 3; ++k) {
-        p2[j * 3 + k] = pts[size_t(order[j].second) * 3 + k];
-        c2[j * 3 + k] = cols[size_t(order[j].second) * 3 + k];
-      }
-    pts.swap(p2);
-    cols.swap(c2);
-  }
-  // Scales: mean distance to the 3 nearest neighbours, found in a grid of about two
-  // points' spacing.
-  const float cell = 2.0f * (voxel > 0.0f ? voxel : cell_for(pts, std::max<size_t>(n / 2, 1)));
-  std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
-  for (uint32_t i = 0; i < n; ++i) {
-    int64_t c[3];
-    cell_of(&pts[size_t(i) * 3], cell, c);
-    grid[cell_key(c[0], c[1], c[2])].push_back(i);
-  }
+  cloud = morton_sorted(cloud);
+  const size_t n = cloud.size();
+  const KdTree tree(cloud.xyz);
   SplatScene scene;
   scene.convention = AxisConvention::RUB;
   scene.resize(uint32_t(n), 0);
   const float logit = std::log(o.initial_opacity / (1.0f - o.initial_opacity));
-  constexpr float kC0 = 0.28209479177387814f;  // SH DC basis value
-  for (uint32_t i = 0; i < n; ++i) {
-    const float* p = &pts[size_t(i) * 3];
-    int64_t c[3];
-    cell_of(p, cell, c);
-    float best[3] = {INFINITY, INFINITY, INFINITY};
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          const auto it = grid.find(cell_key(c[0] + dx, c[1] + dy, c[2] + dz));
-          if (it == grid.end()) continue;
-          for (uint32_t j : it->second) {
-            if (j == i) continue;
-            const float* q = &pts[size_t(j) * 3];
-            const float d2 = (p[0] - q[0]) * (p[0] - q[0]) + (p[1] - q[1]) * (p[1] - q[1]) + (p[2] - q[2]) * (p[2] - q[2]);
-            if (d2 < best[2]) {
-              best[2] = d2;
-              std::sort(best, best + 3);
-            }
-          }
-        }
-    float mean = 0.0f;
+  constexpr float kC0 = 0.28209479177387814f;  // the SH DC basis value
+  for (size_t i = 0; i < n; ++i) {
+    const std::array<float, 3> d2 = tree.nearest3(uint32_t(i));
+    double sum = 0.0;
     int found = 0;
-    for (float d2 : best)
-      if (std::isfinite(d2)) {
-        mean += std::sqrt(d2);
+    for (float v : d2)
+      if (std::isfinite(v)) {
+        sum += std::sqrt(double(v));
         ++found;
       }
-    const float scale = std::min(std::max(found > 0 ? mean / float(found) : cell, 1e-4f * extent), 0.02f * extent);
+    const float mean = found > 0 ? float(sum / found) : 0.01f * extent;
+    const float scale = std::clamp(mean, 1e-4f * extent, 0.02f * extent);
     for (int k = 0; k < 3; ++k) {
-      scene.positions[size_t(i) * 3 + k] = p[k];
-      scene.log_scales[size_t(i) * 3 + k] = std::log(scale);
-      scene.sh_dc[size_t(i) * 3 + k] = (cols[size_t(i) * 3 + k] - 0.5f) / kC0;
+      scene.positions[i * 3 + k] = cloud.xyz[i * 3 + k];
+      scene.log_scales[i * 3 + k] = std::log(scale);
+      scene.sh_dc[i * 3 + k] = (cloud.rgb[i * 3 + k] - 0.5f) / kC0;
     }
-    scene.rotations[size_t(i) * 4] = 1.0f;
+    scene.rotations[i * 4] = 1.0f;
     scene.opacity_logits[i] = logit;
   }
   if (stats != nullptr) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cctype>
 #include <stdexcept>
 
 #include <zlib.h>
@@ -29,10 +30,17 @@ void convert(const uint8_t* px, uint32_t src_channels, uint32_t channels, uint8_
   }
 }
 
-Image decode_png(const std::vector<uint8_t>& f, uint32_t channels) {
-  uint32_t w = 0, h = 0;
+// A PNG's unfiltered samples (big-endian when 16-bit) and the header fields that say how
+// to read them.
+struct PngRaster {
+  uint32_t w = 0, h = 0, samples = 0;
   int depth = 0, type = -1;
-  std::vector<uint8_t> idat, palette, palette_alpha;
+  std::vector<uint8_t> px, palette, palette_alpha;
+};
+
+PngRaster read_png(const std::vector<uint8_t>& f) {
+  PngRaster r;
+  std::vector<uint8_t> idat;
   for (size_t at = 8; at + 12 <= f.size();) {
     const uint32_t len = be32(&f[at]);
     if (at + 12 + size_t(len) > f.size()) throw std::runtime_error("PNG: truncated chunk");
@@ -40,15 +48,15 @@ Image decode_png(const std::vector<uint8_t>& f, uint32_t channels) {
     const uint8_t* d = &f[at + 8];
     if (std::memcmp(kind, "IHDR", 4) == 0) {
       if (len < 13) throw std::runtime_error("PNG: bad IHDR");
-      w = be32(d);
-      h = be32(d + 4);
-      depth = d[8];
-      type = d[9];
+      r.w = be32(d);
+      r.h = be32(d + 4);
+      r.depth = d[8];
+      r.type = d[9];
       if (d[12] != 0) throw std::runtime_error("PNG: interlaced images are not supported");
     } else if (std::memcmp(kind, "PLTE", 4) == 0) {
-      palette.assign(d, d + len);
+      r.palette.assign(d, d + len);
     } else if (std::memcmp(kind, "tRNS", 4) == 0) {
-      palette_alpha.assign(d, d + len);
+      r.palette_alpha.assign(d, d + len);
     } else if (std::memcmp(kind, "IDAT", 4) == 0) {
       idat.insert(idat.end(), d, d + len);
     } else if (std::memcmp(kind, "IEND", 4) == 0) {
@@ -56,29 +64,29 @@ Image decode_png(const std::vector<uint8_t>& f, uint32_t channels) {
     }
     at += 12 + size_t(len);
   }
-  if (w == 0 || h == 0) throw std::runtime_error("PNG: no IHDR");
-  uint32_t samples = 0;
-  switch (type) {
-    case 0: samples = 1; break;
-    case 2: samples = 3; break;
-    case 3: samples = 1; break;
-    case 4: samples = 2; break;
-    case 6: samples = 4; break;
+  if (r.w == 0 || r.h == 0) throw std::runtime_error("PNG: no IHDR");
+  switch (r.type) {
+    case 0: r.samples = 1; break;
+    case 2: r.samples = 3; break;
+    case 3: r.samples = 1; break;
+    case 4: r.samples = 2; break;
+    case 6: r.samples = 4; break;
     default: throw std::runtime_error("PNG: bad colour type");
   }
-  if (!(depth == 8 || (depth == 16 && type != 3))) throw std::runtime_error("PNG: only 8- and 16-bit samples are supported");
-  const size_t bpp = samples * size_t(depth / 8), stride = bpp * w;
-  std::vector<uint8_t> raw((stride + 1) * h);
+  if (!(r.depth == 8 || (r.depth == 16 && r.type != 3)))
+    throw std::runtime_error("PNG: only 8- and 16-bit samples are supported");
+  const size_t bpp = r.samples * size_t(r.depth / 8), stride = bpp * r.w;
+  std::vector<uint8_t> raw((stride + 1) * r.h);
   uLongf got = uLongf(raw.size());
   if (uncompress(raw.data(), &got, idat.data(), uLong(idat.size())) != Z_OK || got != raw.size())
     throw std::runtime_error("PNG: bad image data");
   // Undo the per-row filters (None, Sub, Up, Average, Paeth) in place.
-  std::vector<uint8_t> px(stride * h);
-  for (uint32_t y = 0; y < h; ++y) {
+  r.px.resize(stride * r.h);
+  for (uint32_t y = 0; y < r.h; ++y) {
     const uint8_t filter = raw[y * (stride + 1)];
     const uint8_t* in = &raw[y * (stride + 1) + 1];
-    uint8_t* row = &px[y * stride];
-    const uint8_t* up = y > 0 ? &px[(y - 1) * stride] : nullptr;
+    uint8_t* row = &r.px[y * stride];
+    const uint8_t* up = y > 0 ? &r.px[(y - 1) * stride] : nullptr;
     for (size_t i = 0; i < stride; ++i) {
       const int a = i >= bpp ? row[i - bpp] : 0, b = up ? up[i] : 0, c = (up && i >= bpp) ? up[i - bpp] : 0;
       int v = in[i];
@@ -97,23 +105,29 @@ Image decode_png(const std::vector<uint8_t>& f, uint32_t channels) {
       row[i] = uint8_t(v);
     }
   }
+  return r;
+}
+
+Image decode_png(const std::vector<uint8_t>& f, uint32_t channels) {
+  const PngRaster r = read_png(f);
+  const size_t bpp = r.samples * size_t(r.depth / 8);
   Image img;
-  img.width = w;
-  img.height = h;
+  img.width = r.w;
+  img.height = r.h;
   img.channels = channels;
-  img.data.resize(size_t(w) * h * channels);
-  for (size_t p = 0; p < size_t(w) * h; ++p) {
+  img.data.resize(size_t(r.w) * r.h * channels);
+  for (size_t p = 0; p < size_t(r.w) * r.h; ++p) {
     uint8_t s[4];
-    const uint32_t step = depth / 8;
-    for (uint32_t k = 0; k < samples; ++k) s[k] = px[p * bpp + k * step];  // 16-bit: the high byte
-    if (type == 3) {
+    const uint32_t step = uint32_t(r.depth / 8);
+    for (uint32_t k = 0; k < r.samples; ++k) s[k] = r.px[p * bpp + k * step];  // 16-bit: the high byte
+    if (r.type == 3) {
       const uint32_t i = s[0];
-      if (size_t(i) * 3 + 2 >= palette.size()) throw std::runtime_error("PNG: palette index out of range");
-      const uint8_t rgba[4] = {palette[i * 3], palette[i * 3 + 1], palette[i * 3 + 2],
-                               i < palette_alpha.size() ? palette_alpha[i] : uint8_t(255)};
+      if (size_t(i) * 3 + 2 >= r.palette.size()) throw std::runtime_error("PNG: palette index out of range");
+      const uint8_t rgba[4] = {r.palette[i * 3], r.palette[i * 3 + 1], r.palette[i * 3 + 2],
+                               i < r.palette_alpha.size() ? r.palette_alpha[i] : uint8_t(255)};
       convert(rgba, 4, channels, &img.data[p * channels]);
     } else {
-      convert(s, samples, channels, &img.data[p * channels]);
+      convert(s, r.samples, channels, &img.data[p * channels]);
     }
   }
   return img;
@@ -170,8 +184,47 @@ Image decode_image(const std::vector<uint8_t>& bytes, uint32_t channels) {
   static const uint8_t kPng[8] = {137, 80, 78, 71, 13, 10, 26, 10};
   if (bytes.size() >= 8 && std::memcmp(bytes.data(), kPng, 8) == 0) return decode_png(bytes, channels);
   if (bytes.size() >= 3 && bytes[0] == 'P' && (bytes[1] == '5' || bytes[1] == '6')) return decode_pnm(bytes, channels);
-  if (bytes.size() >= 3 && bytes[0] == 0xff && bytes[1] == 0xd8) throw std::runtime_error("JPEG images are not decoded (no JPEG decoder in libgs_host)");
+  if (bytes.size() >= 3 && bytes[0] == 0xff && bytes[1] == 0xd8) return decode_jpeg(bytes, channels);
   throw std::runtime_error("unknown image format");
+}
+
+Depth16 decode_depth16(const std::vector<uint8_t>& bytes) {
+  static const uint8_t kPng[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+  Depth16 d;
+  if (bytes.size() >= 8 && std::memcmp(bytes.data(), kPng, 8) == 0) {
+    const PngRaster r = read_png(bytes);
+    if (r.type != 0) throw std::runtime_error("depth PNG: not a single grey channel");
+    d.width = r.w;
+    d.height = r.h;
+    d.data.resize(size_t(r.w) * r.h);
+    for (size_t p = 0; p < d.data.size(); ++p)
+      d.data[p] = r.depth == 16 ? uint16_t(uint32_t(r.px[p * 2]) << 8 | r.px[p * 2 + 1]) : uint16_t(r.px[p]);
+    return d;
+  }
+  if (bytes.size() >= 3 && bytes[0] == 'P' && bytes[1] == '5') {
+    size_t at = 2;
+    uint32_t v[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+      while (at < bytes.size() && (std::isspace(bytes[at]) || bytes[at] == '#')) {
+        if (bytes[at] == '#')
+          while (at < bytes.size() && bytes[at] != '\n') ++at;
+        else
+          ++at;
+      }
+      while (at < bytes.size() && std::isdigit(bytes[at])) v[k] = v[k] * 10 + uint32_t(bytes[at++] - '0');
+    }
+    ++at;
+    const size_t each = v[2] > 255 ? 2 : 1;
+    if (v[2] == 0 || v[2] > 65535 || at + size_t(v[0]) * v[1] * each > bytes.size())
+      throw std::runtime_error("depth PGM: unsupported or truncated");
+    d.width = v[0];
+    d.height = v[1];
+    d.data.resize(size_t(v[0]) * v[1]);
+    for (size_t p = 0; p < d.data.size(); ++p)
+      d.data[p] = each == 2 ? uint16_t(uint32_t(bytes[at + 2 * p]) << 8 | bytes[at + 2 * p + 1]) : bytes[at + p];
+    return d;
+  }
+  throw std::runtime_error("depth map: not a 16-bit PNG or PGM");
 }
 
 std::vector<uint8_t> resize_area(const uint8_t* src, uint32_t w, uint32_t h, uint32_t channels, uint32_t out_w,

@@ -14,11 +14,26 @@ struct Image {
   std::vector<uint8_t> data;  // row-major, `channels` bytes per pixel
 };
 
-// PNG (8 or 16 bits per sample, grey / grey+alpha / RGB / RGBA / palette, not interlaced)
-// or binary PPM (P6) / PGM (P5), converted to `channels` (1: grey or the alpha channel's
-// source for masks, 4: RGBA with alpha 255 where the file has none). Throws
-// std::runtime_error for other formats (libgs_host has no JPEG decoder).
+// PNG (8 or 16 bits per sample, grey / grey+alpha / RGB / RGBA / palette, not interlaced),
+// binary PPM (P6) / PGM (P5) or JPEG (decoded on the GPU by nvJPEG: decode_jpeg), converted
+// to `channels` (1: grey or the alpha channel's source for masks, 4: RGBA with alpha 255
+// where the file has none). Throws std::runtime_error for other formats and for JPEG files
+// when no GPU can decode them.
 Image decode_image(const std::vector<uint8_t>& bytes, uint32_t channels);
+
+// A JPEG file decoded by nvJPEG on the current CUDA device (baseline and progressive,
+// any chroma subsampling), as `channels` (1: luma, 4: RGBA with alpha 255). The decode
+// runs on the GPU; the pixels come back to host memory. Throws std::runtime_error with
+// nvJPEG's status when the file or the device cannot be decoded.
+Image decode_jpeg(const std::vector<uint8_t>& bytes, uint32_t channels);
+
+// A depth map: a single-channel PNG (16- or 8-bit) or PGM (P5, maxval up to 65535), raw
+// samples in the file's units (the capture's depth_unit_scale_factor converts them).
+struct Depth16 {
+  uint32_t width = 0, height = 0;
+  std::vector<uint16_t> data;
+};
+Depth16 decode_depth16(const std::vector<uint8_t>& bytes);
 
 // Area resampling (each output pixel is the coverage-weighted mean of the input pixels it
 // covers), rounded to the nearest level.

@@ -189,18 +189,33 @@ int dataset_summary(const std::string& dir, uint32_t width, uint32_t max_init) {
   gs::InitStats st;
   const gs::SplatScene init = gs::initialize_gaussians(ds, io, &st);
   gs::write_file(dir + "/frame0.rgba", ds.frames.at(0).rgba);
+  // The initial gaussians' positions and log-scales (float32) for the caller to check.
+  std::vector<uint8_t> bytes(init.positions.size() * 4), scales(init.log_scales.size() * 4);
+  std::memcpy(bytes.data(), init.positions.data(), bytes.size());
+  std::memcpy(scales.data(), init.log_scales.data(), scales.size());
+  gs::write_file(dir + "/init.xyz", bytes);
+  gs::write_file(dir + "/init.logscale", scales);
   float smin = INFINITY, smax = -INFINITY;
   for (float v : init.log_scales) {
     smin = std::min(smin, v);
     smax = std::max(smax, v);
   }
   std::printf("{\"name\": \"%s\", \"width\": %u, \"height\": %u, \"fx\": %.6g, \"fy\": %.6g, \"cx\": %.6g, "
-              "\"cy\": %.6g, \"frames\": %zu, \"holdout\": %zu, \"skipped\": %zu, \"has_masks\": %s, \"points\": %zu, "
+              "\"cy\": %.6g, \"frames\": %zu, \"holdout\": %zu, \"skipped\": %zu, \"has_masks\": %s, \"has_depth\": %s, "
+              "\"points\": %zu, "
               "\"extent\": %.6g, \"names\": [",
               ds.name.c_str(), ds.width, ds.height, ds.fx, ds.fy, ds.cx, ds.cy, ds.frames.size(), ds.holdout_count(),
-              ds.skipped.size(), ds.has_masks ? "true" : "false", ds.points.size() / 3, ds.camera_extent);
+              ds.skipped.size(), ds.has_masks ? "true" : "false", ds.has_depth ? "true" : "false", ds.points.size() / 3,
+              ds.camera_extent);
   for (size_t i = 0; i < ds.frames.size(); ++i)
     std::printf("%s\"%s\"", i ? ", " : "", ds.frames[i].name.c_str());
+  std::printf("], \"skipped_why\": [");
+  for (size_t i = 0; i < ds.skipped.size(); ++i) {
+    std::string why = ds.skipped[i];
+    for (char& ch : why)
+      if (ch == '"' || ch == '\\') ch = '\'';
+    std::printf("%s\"%s\"", i ? ", " : "", why.c_str());
+  }
   std::printf("], \"init_source\": \"%s\", \"init_raw\": %zu, \"init_count\": %u, \"init_voxel\": %.6g, "
               "\"log_scale_min\": %.6g, \"log_scale_max\": %.6g, \"init_opacity_logit\": %.6g}\n",
               st.source.c_str(), st.raw_points, init.count, st.voxel_size, smin, smax,

@@ -2,11 +2,13 @@
 
 Writes a small transforms.json capture with PNG images of every colour type the loader
 reads (RGB, RGBA 16-bit, palette, grey + alpha) using every PNG row filter, grey masks, a
-point-cloud PLY and one JPEG frame (which libgs_host does not decode), then checks what
-bin/gs_host_selftest reports against the reference's rules (dataset.cpp:85-223, 291-523):
-short side resized to the target width by area, intrinsics scaled with it, masks in alpha,
-every 8th frame held out, unreadable frames skipped and listed, points merged per voxel to
-the budget.
+point-cloud PLY and one damaged JPEG frame, then checks what bin/gs_host_selftest reports
+against the reference's rules (dataset.cpp:85-223, 291-523): short side resized to the
+target width by area, intrinsics scaled with it, masks in alpha, every 8th frame held out,
+unreadable frames skipped and listed, points merged per voxel to the budget; and the depth
+source of the initial gaussians (16-bit PNG and PGM depth maps with confidence maps,
+back-projected through each frame's camera). Decoding real JPEG frames needs the GPU
+(nvJPEG): tests/test_gpu_jpeg.py.
 """
 import json
 import os
@@ -88,7 +90,7 @@ def make_capture(d, rng, with_points=True, n_frames=10):
             g = rng.integers(0, 256, (H, W, 2))
             full[..., 0] = full[..., 1] = full[..., 2] = g[..., 0]
             write_png(d / name, g, 4)
-        elif i == 8:  # a JPEG: not decoded here, so the frame is skipped
+        elif i == 8:  # a damaged JPEG: skipped
             name = f"img_{i:02d}.jpg"
             open(d / name, "wb").write(b"\xff\xd8\xff\xe0" + bytes(64))
         else:
@@ -169,3 +171,85 @@ def test_png_colour_types_decode_exactly(tmp_path):
         assert s["frames"] == 2
         got = np.frombuffer(open(tmp_path / "frame0.rgba", "rb").read(), np.uint8).reshape(H, W, 4)
         np.testing.assert_array_equal(got, rgba[i], err_msg=f"frame {i}")
+
+
+def _depth_frames(d, rng, meta, dw=15, dh=10):
+    """Adds a depth map (16-bit PNG, or 16-bit PGM for frame 4) and a confidence map to every
+    frame of the capture in `d`; returns them as {frame: (depth16, confidence)}."""
+    maps = {}
+    for i, fr in enumerate(meta["frames"]):
+        depth = (1500 + rng.integers(0, 1000, (dh, dw))).astype(np.uint16)
+        depth[rng.random((dh, dw)) < 0.1] = 0  # missing samples
+        conf = rng.integers(0, 256, (dh, dw, 1)).astype(np.uint8)
+        if i == 4:
+            name = f"depth_{i:02d}.pgm"
+            open(d / name, "wb").write(b"P5\n%d %d\n65535\n" % (dw, dh) + depth.astype(">u2").tobytes())
+        else:
+            name = f"depth_{i:02d}.png"
+            write_png(d / name, depth[..., None], 0, depth=16)
+        write_png(d / f"conf_{i:02d}.png", conf, 0)
+        fr["depth_file_path"] = name
+        fr["depth_confidence_path"] = f"conf_{i:02d}.png"
+        maps[i] = (depth, conf[..., 0])
+    meta["depth_unit_scale_factor"] = 0.001
+    (d / "transforms.json").write_text(json.dumps(meta))
+    return maps
+
+
+def test_depth_initialisation(tmp_path):
+    """initialize_gaussians from depth maps (dataset.cpp:297-320's source): every confident
+    sample of a training frame inside the subject mask, back-projected through the frame's
+    camera, and nothing else; log-scales from the 3 nearest neighbours."""
+    rng = np.random.default_rng(6)
+    rgba = make_capture(tmp_path, rng, with_points=True)
+    meta = json.loads((tmp_path / "transforms.json").read_text())
+    maps = _depth_frames(tmp_path, rng, meta)
+    s = load(tmp_path, 100, 100000)
+    assert s["has_depth"] and s["init_source"] == "depth"
+    want = []
+    fx, fy, cx, cy = 40.0, 41.0, 22.0, 15.5
+    for i, (depth, conf) in maps.items():
+        if i % 8 == 0 or i == 8:  # held out, or skipped (the JPEG frame)
+            continue
+        c2w = np.array(meta["frames"][i]["transform_matrix"])
+        dh, dw = depth.shape
+        for v in range(dh):
+            for u in range(dw):
+                z = np.float32(float(depth[v, u]) * 0.001)
+                if not z > 0 or conf[v, u] < np.float32(0.3) * np.float32(255.0):
+                    continue
+                px, py = (u + 0.5) * W / dw, (v + 0.5) * H / dh
+                if rgba[i][min(H - 1, int(py)), min(W - 1, int(px)), 3] < 128:
+                    continue
+                x, y = (px - cx) / fx * z, (py - cy) / fy * z
+                want.append(c2w[:3, 0] * x - c2w[:3, 1] * y - c2w[:3, 2] * z + c2w[:3, 3])
+    want = np.array(want)
+    got = np.frombuffer(open(tmp_path / "init.xyz", "rb").read(), np.float32).reshape(-1, 3)
+    assert s["init_raw"] == len(want) == len(got) > 100
+    order_w = np.lexsort(want.T[::-1])
+    order_g = np.lexsort(got.T[::-1])
+    np.testing.assert_allclose(got[order_g], want[order_w], atol=2e-5)
+    # Scales: the mean distance to the 3 nearest other points, clamped to [1e-4, 0.02] x
+    # the robust extent (0.5%..99.5% box diagonal).
+    d = np.sqrt(((got[:, None, :].astype(np.float64) - got[None, :, :]) ** 2).sum(-1))
+    np.fill_diagonal(d, np.inf)
+    mean3 = np.sort(d, axis=1)[:, :3].mean(1)
+    lo = np.sort(got, axis=0)[len(got) // 200]
+    hi = np.sort(got, axis=0)[len(got) - 1 - len(got) // 200]
+    extent = np.sqrt(((hi.astype(np.float64) - lo) ** 2).sum())
+    want_scale = np.log(np.clip(mean3, 1e-4 * extent, 0.02 * extent))
+    logscale = np.frombuffer(open(tmp_path / "init.logscale", "rb").read(), np.float32).reshape(-1, 3)
+    np.testing.assert_allclose(logscale[:, 0], want_scale, atol=1e-4)
+
+
+def test_depth_merge_to_budget(tmp_path):
+    """Over budget, depth points are merged per occupied cell to at most max_gaussians and
+    close under it (the cell size is fitted to the budget)."""
+    rng = np.random.default_rng(7)
+    make_capture(tmp_path, rng, with_points=False)
+    meta = json.loads((tmp_path / "transforms.json").read_text())
+    _depth_frames(tmp_path, rng, meta, dw=45, dh=30)
+    for budget in (50, 400, 1500):
+        s = load(tmp_path, 100, budget)
+        assert s["init_source"] == "depth" and s["init_raw"] > budget
+        assert 0.5 * budget <= s["init_count"] <= budget and s["init_voxel"] > 0, (budget, s["init_count"])

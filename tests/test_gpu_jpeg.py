@@ -1,0 +1,85 @@
+"""JPEG frames in capture folders, decoded on the GPU by nvJPEG (GPU only).
+
+The reference decodes its photos with stb_image (engine/src/image_io.cpp:27-30); here
+libgs_host hands JPEG files to nvJPEG. A capture of JPEG frames (baseline 4:4:4, baseline
+4:2:0 and progressive) is loaded through gs::load_dataset and each frame compared with an
+independent decoder's output (Pillow's libjpeg): JPEG decoders may differ in their inverse
+DCT's rounding and, with subsampled chroma, in how they upsample it, so the check is a
+small mean difference (and a tight maximum for 4:4:4), not bit equality.
+"""
+import io
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SELFTEST = os.path.join(ROOT, "on-divice-gsplate_b200", "bin", "gs_host_selftest")
+W, H = 96, 64
+
+
+def smooth_image(rng):
+    y, x = np.mgrid[0:H, 0:W].astype(np.float64)
+    img = np.stack([128 + 100 * np.sin(x / 13 + rng.uniform(0, 6)), 128 + 90 * np.cos(y / 9 + rng.uniform(0, 6)),
+                    128 + 80 * np.sin((x + y) / 17 + rng.uniform(0, 6))], -1)
+    cx, cy = rng.uniform(20, 76), rng.uniform(15, 50)
+    img[(x - cx) ** 2 + (y - cy) ** 2 < 150] = rng.uniform(0, 255, 3)
+    return np.clip(img, 0, 255).astype(np.uint8)
+
+
+@pytest.mark.parametrize("kind", ["444", "420", "progressive"])
+def test_jpeg_frames_decode_on_the_gpu(tmp_path, kind):
+    from PIL import Image
+
+    rng = np.random.default_rng(11)
+    frames, decoded = [], []
+    for i in range(4):
+        img = smooth_image(rng)
+        buf = io.BytesIO()
+        opts = {"quality": 92, "subsampling": 0 if kind == "444" else 2, "progressive": kind == "progressive"}
+        Image.fromarray(img).save(buf, "JPEG", **opts)
+        (tmp_path / f"f{i}.jpg").write_bytes(buf.getvalue())
+        decoded.append(np.asarray(Image.open(io.BytesIO(buf.getvalue())).convert("RGB")))
+        c2w = np.eye(4)
+        c2w[:3, 3] = [3 * np.sin(i), 0.5, 3 * np.cos(i)]
+        frames.append({"file_path": f"f{i}.jpg", "transform_matrix": c2w.tolist()})
+    meta = {"w": W, "h": H, "fl_x": 80.0, "frames": frames}
+    (tmp_path / "transforms.json").write_text(json.dumps(meta))
+    out = subprocess.run([SELFTEST, "dataset", str(tmp_path), "1000", "64"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    s = json.loads(out.stdout)
+    assert s["frames"] == 4 and s["skipped"] == 0, s
+    got = np.frombuffer((tmp_path / "frame0.rgba").read_bytes(), np.uint8).reshape(H, W, 4)
+    assert (got[..., 3] == 255).all()
+    diff = np.abs(got[..., :3].astype(int) - decoded[0].astype(int))
+    assert diff.mean() < (0.5 if kind == "444" else 2.0), diff.mean()
+    if kind == "444":
+        assert diff.max() <= 4, diff.max()
+
+
+def test_broken_jpeg_frames_are_skipped(tmp_path):
+    """A damaged JPEG is skipped and listed like any unreadable frame (the loader's rule for
+    damaged downloads), and the capture still loads."""
+    from PIL import Image
+
+    rng = np.random.default_rng(12)
+    frames = []
+    for i in range(4):
+        buf = io.BytesIO()
+        Image.fromarray(smooth_image(rng)).save(buf, "JPEG", quality=90)
+        data = buf.getvalue()
+        if i == 2:
+            data = data[:40]
+        (tmp_path / f"f{i}.jpg").write_bytes(data)
+        c2w = np.eye(4)
+        c2w[:3, 3] = [3 * np.sin(i), 0.5, 3 * np.cos(i)]
+        frames.append({"file_path": f"f{i}.jpg", "transform_matrix": c2w.tolist()})
+    (tmp_path / "transforms.json").write_text(json.dumps({"w": W, "h": H, "fl_x": 80.0, "frames": frames}))
+    out = subprocess.run([SELFTEST, "dataset", str(tmp_path), "1000", "64"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    s = json.loads(out.stdout)
+    assert s["frames"] == 3 and s["skipped"] == 1 and "f2.jpg" in s["skipped_why"][0]
