@@ -14,7 +14,12 @@ Adam on every parameter. Views are drawn in shuffled epochs over the 200 cameras
   one-view-per-step path (autotuned for itself) measured the same way.
 - e2e: the batched step through the C ABI as a caller drives it, wall clock: each step
   uploads its 8 targets from pinned host memory (gs_set_views) and reads the loss sums back.
-- roofline: the dominant pass of the batched step, from per-pass CUDA events.
+- roofline: the dominant pass of the batched step, timed by pass events recorded inside
+  the replayed graph. Raster passes are issue-bound, so their roofline is the
+  special-function unit (MUFU, 16 operations per clock per SM at the sampled clock) over the
+  step's pixel-pair evaluations E (one exponential per evaluation forward, an exponential
+  and a reciprocal backward); every pass also reports HBM GB/s from fixed per-unit bytes
+  (algorithmic_bytes) against the measured copy bandwidth.
 - cpu_baseline: the CPU oracle (a multithreaded restatement of the reference's passes) on
   plain steps of the same workload, host cores, bounded time.
 Inputs (732 MB of parameters and moments, 1.66 GB of targets) exceed the 126 MB L2, so no
@@ -139,22 +144,40 @@ def peaks() -> dict:
 
 
 def algorithmic_bytes(pass_name: str, n: int, views: int, pairs: int, pixels: int, stride: int) -> float:
-    """Bytes each pass must move at minimum (fp32), per step of `views` views."""
-    p_g = 4 * (16 + stride)  # parameters of one slot (4 float4 planes + SH)
+    """The bytes each pass must move at minimum (fp32) per step of `views` views: the fixed
+    per-unit figures of the path's byte model (per gaussian, per pair, per pixel), not what
+    this implementation happens to move.
+    - project: 236 B of parameters read per gaussian (SH3), 52 B written per (view, gaussian)
+      (44 B projected record, 4 B tile count, 4 B depth key);
+    - sort: 12 B per pair emitted (8 B key + 4 B payload) + 56 B per (view, gaussian) read by
+      the key build and scan, 96 B per pair for the key sort, 8 B per pair for the ranges;
+    - rasterize (forward): 40 B per pair (the gathered splat record) + 28 B per pixel;
+    - loss: 28 B per pixel (12 B render + 4 B target read, 12 B dL/dC written);
+    - backward: 40 B per pair + 44 B per pixel;
+    - optimize: 1,456 B per gaussian (parameters, m and v read and written, 6 x 236 B, +
+      40 B of 2D gradients)."""
+    p_g = 4 * (14 + stride)
     if pass_name == "project":
-        return n * p_g + n * views * (48 + 16 + 4 + 8)
+        return n * p_g + n * views * 52
     if pass_name == "sort":
-        # depth sort (2 passes x 8 B read + written), scan + emit (12 B per pair), pair sort, ranges
-        return n * views * 2 * 16 + pairs * 12 + pairs * 2 * 16 + pairs * 4
+        return pairs * 12 + n * views * 56 + pairs * 96 + pairs * 8
     if pass_name == "rasterize":
-        return pairs * (4 + 4 + 64) + pixels * (4 + 16 + 16 + 4 + 4 + 4)
+        return pairs * 40 + pixels * 28
     if pass_name == "loss":
-        return pixels * (16 + 4 + 48) + pixels * (48 + 16 + 16 + 4 + 16)
+        return pixels * 28
     if pass_name == "backward":
-        return pairs * (4 + 4 + 64 + 48) + pixels * (16 + 4 + 4)
+        return pairs * 40 + pixels * 44
     if pass_name == "optimize":
-        return pairs * 48 + n * views * 48 + n * (6 * p_g + 32)
+        return n * (6 * p_g + 40)
     return 0.0
+
+
+# Special-function (MUFU) operations per pixel-pair evaluation: the forward's exponential;
+# the backward's exponential and the reciprocal of (1 - alpha). B200 issues 16 MUFU
+# operations per clock per SM.
+MUFU_PER_EVALUATION = {"rasterize": 1, "backward": 2}
+MUFU_PER_CLOCK_PER_SM = 16
+SM_COUNT = 148
 
 
 def render_targets(ctx, truth, cams, opt):
@@ -167,8 +190,10 @@ def render_targets(ctx, truth, cams, opt):
     return out
 
 
-def measure(ctx, scene, cams, opt, views_per_step, steps, warmup, order, step0, dist=None, clocks=None):
-    """Device time of `steps` training steps of `views_per_step` views each (dataset targets)."""
+def measure(ctx, scene, cams, opt, views_per_step, steps, warmup, order, step0, dist=None, clocks=None, passes=None):
+    """Device time of `steps` training steps of `views_per_step` views each (dataset targets).
+    With `passes` (a list), each timed step's per-pass device times are appended to it (the
+    pass events are recorded inside the replayed graph)."""
     import torch
 
     step = step0
@@ -186,7 +211,9 @@ def measure(ctx, scene, cams, opt, views_per_step, steps, warmup, order, step0, 
     for _ in range(steps):
         idx = order.next(views_per_step)
         ctx.set_views_dataset([frame(scene, cams[i], opt, step) for i in idx], idx)
-        r = ctx.step(True)
+        r = ctx.step(True, profile=passes is not None)
+        if passes is not None:
+            passes.append([float(r.pass_ms[k]) for k in range(6)])
         gpu_ms += r.gpu_ms
         launches += r.kernels
         pairs += sum(int(r.pairs[v]) for v in range(views_per_step))
@@ -209,12 +236,15 @@ def max_over_ranks(values, dist, device="cuda"):
 
 
 def autotune(ctx, scene, cams, opt, views_per_step, order, step):
-    """gs_autotune on a step of `views_per_step` dataset views (the model is left as it was)."""
+    """gs_autotune on a step of `views_per_step` dataset views (the model is left as it was),
+    free to pick fixed-order or atomic gradient sums."""
     idx = order.next(views_per_step)
     ctx.set_views_dataset([frame(scene, cams[i], opt, step) for i in idx], idx)
+    ctx.set_tuning(tune_reduction=1)
     t = ctx.autotune(2)
-    return {"forward_pixels": t.forward_pixels, "backward_pixels": t.backward_pixels,
-            "backward_batch": t.backward_batch, "sort_digit_bits": t.sort_digit_bits}
+    return {"forward_pixels": t.forward_pixels, "forward_batch": t.forward_batch,
+            "backward_pixels": t.backward_pixels, "backward_batch": t.backward_batch,
+            "sort_digit_bits": t.sort_digit_bits, "deterministic": bool(t.deterministic)}
 
 
 def cpu_baseline(scene, targets, cams, opt, seconds: float = 20.0) -> dict:
@@ -349,18 +379,20 @@ def main() -> None:
     if not args.no_autotune:
         tunings["batched"] = autotune(ctx, scene, cams, opt, VIEWS_PER_STEP, order, step)
     clocks = ClockSampler(local)
+    step_passes = []
     gpu_ms, launches, pairs, step = measure(ctx, scene, cams, opt, VIEWS_PER_STEP, args.steps, args.warmup, order,
-                                            step, dist, clocks)
+                                            step, dist, clocks, step_passes)
     if args.mode == "batched":
         print(json.dumps({"mode": "batched", "views_per_s": VIEWS_PER_STEP * 1000.0 * args.steps / gpu_ms}), flush=True)
         ctx.close()
         return
-    # One profiled batched step: device time per pass.
-    idx = order.next(VIEWS_PER_STEP)
-    ctx.set_views_dataset([frame(scene, cams[i], opt, step) for i in idx], idx)
-    prof = ctx.step(True, profile=True)
-    step += 1
-    passes = {name: float(prof.pass_ms[k]) for k, name in enumerate(PASSES)}
+    # Device time per pass: the mean over the timed steps. The pixel-pair evaluations of the
+    # last timed step (the sum over its pixels of the last contributor's position in the
+    # tile's list: the forward's own count; the backward walks the same) go with that step's
+    # own pass times.
+    passes = {name: float(np.mean([p[k] for p in step_passes])) for k, name in enumerate(PASSES)}
+    last_passes = {name: step_passes[-1][k] for k, name in enumerate(PASSES)}
+    evaluations = sum(int(ctx.snapshot("pixel_count", v).astype(np.int64).sum()) for v in range(VIEWS_PER_STEP))
 
     # End to end: the caller's photos sit in pinned host memory; each step uploads its 8
     # targets (gs_set_views) and reads the loss sums back.
@@ -395,12 +427,33 @@ def main() -> None:
                 traffic = json.load(f).get(dom)
         except (OSError, ValueError):
             traffic = None
+        clk = clocks.summary()
+        sm_hz = (clk["sm_mhz"] or 1965.0) * 1e6
+        mufu_peak = MUFU_PER_CLOCK_PER_SM * SM_COUNT * sm_hz / 1e9  # Gop/s at the sampled clock
         per_pass = {}
         for name, ms in passes.items():
             b = algorithmic_bytes(name, scene.count, VIEWS_PER_STEP, int(pairs), pixels, stride)
             gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
-            per_pass[name] = {"ms": round(ms, 4), "gbs": round(gbs, 1) if gbs else None,
-                              "frac": round(gbs / pk["hbm_gbs"], 4) if gbs else None}
+            entry = {"ms": round(ms, 4), "gbs": round(gbs, 1) if gbs else None,
+                     "hbm_frac": round(gbs / pk["hbm_gbs"], 4) if gbs else None}
+            if name in MUFU_PER_EVALUATION and last_passes[name] > 0:
+                gops = evaluations * MUFU_PER_EVALUATION[name] / (last_passes[name] * 1e-3) / 1e9
+                entry.update({"mufu_gops": round(gops, 1), "mufu_frac": round(gops / mufu_peak, 4)})
+            per_pass[name] = entry
+        # The raster passes are bound by instruction issue on the SMs, not by HBM: their
+        # roofline is the special-function unit's rate at the sampled clock.
+        d = per_pass[dom]
+        if "mufu_gops" in d:
+            roof = {"bound": "sfu", "kernel": dom, "achieved": d["mufu_gops"], "peak": round(mufu_peak, 1),
+                    "unit": "Gop/s", "frac": d["mufu_frac"], "evaluations_per_step": evaluations,
+                    "mufu_per_evaluation": MUFU_PER_EVALUATION[dom],
+                    "hbm": {"achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": d["hbm_frac"]}}
+        else:
+            roof = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s",
+                    "frac": d["hbm_frac"]}
+        roof.update({"traffic": traffic, "peak_source": pk["source"], "per_pass": per_pass,
+                     "passes_from": "pass events inside the replayed graph, mean over the timed steps; the "
+                                    "SFU figures pair the last timed step's evaluations with its own pass times"})
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "views/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -415,13 +468,11 @@ def main() -> None:
                        "deterministic": bool(ctx.tuning().deterministic), "graph": True,
                        "autotuned": tunings},
             "passes_ms": {k: round(v, 4) for k, v in passes.items()},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_pass[dom]["gbs"], "peak": pk["hbm_gbs"],
-                         "unit": "GB/s", "frac": per_pass[dom]["frac"], "traffic": traffic,
-                         "peak_source": pk["source"], "per_pass": per_pass},
+            "roofline": roof,
             "e2e": {"value": round(e2e, 3), "unit": "views/s", "h2d_bytes_per_step": VIEWS_PER_STEP * WIDTH * HEIGHT * 4,
                     "d2h_bytes_per_step": 4 * (4 + 2 * 16) + 64 * VIEWS_PER_STEP},
             "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "clocks": clk,
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(scene, targets, cams, opt)

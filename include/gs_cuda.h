@@ -148,6 +148,8 @@ typedef struct gs_tuning {
                                  structure (views, slots, buffer sizes, SH degree, mode) holds */
   uint32_t backward_batch;    /* splats staged per round of the backward pass: 32 or 64 (0: default) */
   uint32_t sort_digit_bits;   /* radix digit width of the depth and pair sorts: 4..8 (0: default 8) */
+  uint32_t forward_batch;     /* splats staged per round of the forward pass: 64, 128 or 256 (0: default 256) */
+  uint32_t tune_reduction;    /* 1: gs_autotune may also switch `deterministic` (0: it keeps the caller's) */
 } gs_tuning;
 
 typedef struct gs_model_info {

@@ -90,7 +90,7 @@ struct gs_context {
   std::vector<PendingTarget> pending_targets;
   bool targets_uploaded = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t marks[7] = {};  // pass boundaries when profiling
+  cudaEvent_t marks[7] = {};  // pass boundaries, recorded by every step (event nodes inside a captured graph)
   bool profile = false;
   gsk::Model model;
   gs_tuning tuning{};
@@ -316,9 +316,7 @@ struct gs_context {
     return ms;
   }
 
-  void mark(int k) {
-    if (profile) GS_CUDA_TRY(cudaEventRecord(marks[k], stream));
-  }
+  void mark(int k) { GS_CUDA_TRY(cudaEventRecord(marks[k], stream)); }
 
   // Everything one step puts on the stream: the step table upload, the queue reset, the
   // launch sequence and the readback of the pair count and loss sums.
@@ -402,8 +400,9 @@ struct gs_context {
         targets_uploaded = true;
       }
       GS_CUDA_TRY(cudaEventRecord(ev0, stream));
-      // A profiled step runs directly: its pass events must be recorded by the stream.
-      if (tuning.graph && allow_graph && !profile) {
+      // The pass events are part of the step's launch sequence, so a graph replay records
+      // them too and a profiled step can run as a replay.
+      if (tuning.graph && allow_graph) {
         launch_graph(train, degree);
       } else {
         launches = 0;
@@ -497,13 +496,20 @@ struct gs_context {
           best = t;
         }
       };
-      const uint32_t fpx0 = best.forward_pixels;
+      if (start.tune_reduction) {  // fixed-order sums or atomics, then the rest under the faster
+        gs_tuning t = best;
+        t.deterministic = best.deterministic ? 0u : 1u;
+        consider(t);
+      }
+      const uint32_t fpx0 = best.forward_pixels, fb0 = best.forward_batch;
       for (uint32_t fpx : {1u, 2u, 4u})
-        if (fpx != fpx0) {
-          gs_tuning t = best;
-          t.forward_pixels = fpx;
-          consider(t);
-        }
+        for (uint32_t fb : {128u, 256u})
+          if (fpx != fpx0 || fb != fb0) {
+            gs_tuning t = best;
+            t.forward_pixels = fpx;
+            t.forward_batch = fb;
+            consider(t);
+          }
       const uint32_t bpx0 = best.backward_pixels, batch0 = best.backward_batch;
       for (uint32_t bpx : {2u, 4u})
         for (uint32_t batch : {32u, 64u})
@@ -668,7 +674,8 @@ struct gs_context {
       GS_CUDA_TRY(cudaStreamWaitEvent(stream, targets_ready,
                                       capture == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0u));
     }
-    gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2, stream);
+    gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2,
+                               tuning.forward_batch ? int(tuning.forward_batch) : 256, stream);
     ++launches;
     mark(3);
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
@@ -902,6 +909,7 @@ int gs_create(int device, gs_context** out) {
     c->tuning.backward_pixels = 4u;
     c->tuning.backward_batch = 64u;
     c->tuning.sort_digit_bits = 8u;
+    c->tuning.forward_batch = 256u;
     c->tuning.retry = 1u;
     c->tuning.graph = 0u;
     try {
@@ -1333,6 +1341,8 @@ int gs_set_tuning(gs_context* c, const gs_tuning* t) {
       fail(GS_ERR_INVALID, "gs_set_tuning: backward_batch must be 32 or 64");
     if (t->sort_digit_bits != 0 && (t->sort_digit_bits < 4 || t->sort_digit_bits > 8))
       fail(GS_ERR_INVALID, "gs_set_tuning: sort_digit_bits must be 4..8");
+    if (t->forward_batch != 0 && t->forward_batch != 64 && t->forward_batch != 128 && t->forward_batch != 256)
+      fail(GS_ERR_INVALID, "gs_set_tuning: forward_batch must be 64, 128 or 256");
     c->tuning = *t;
     if (c->tuning.min_pair_capacity == 0) c->tuning.min_pair_capacity = 1;
     c->drop_graph();

@@ -102,7 +102,7 @@ struct RasterBuffers {
   float* ssim_last = nullptr;
 };
 // px: pixels per thread (1, 2 or 4).
-void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,
+void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
                            cudaStream_t st);
 // Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
 // vb.grad2d (fast), staging `batch` (32 or 64) splats per round. Skipped on device when

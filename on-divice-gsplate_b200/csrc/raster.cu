@@ -18,8 +18,10 @@
 // tree per value), skipped when no lane touched the splat, and the warps' partials are
 // added in a fixed order, so the per-pair gradient is bit-stable. Deterministic mode
 // stores it at the pair's pre-sort index (pair_grads, summed per gaussian by
-// train_pair_sum's fixed order); fast mode adds it to the gaussian's accumulator with one
-// atomic per value and tile.
+// train_pair_sum's fixed order); fast mode adds it to the gaussian's accumulator with
+// three 16-byte vector atomics per tile (red.global.add.v4.f32). Fast mode also leaves out
+// the |dL/dmean2d| sums (pair values 9 and 10): they feed only the densify statistic
+// stats.w, which no densify decision reads (train_densify_mark.comp:22-57 uses x, y, z).
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -128,12 +130,14 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
   return item;
 }
 
-template <int PX>
+// FB splats are staged per round (64, 128 or 256: a tuning knob).
+template <int PX, int FB>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
-  __shared__ float4 s_a[256];  // staged splats (stage_splat)
-  __shared__ float4 s_b[256];
-  __shared__ float4 s_c[256];
+  static_assert(FB % 32 == 0 && FB <= 256, "whole warps of staged splats");
+  __shared__ float4 s_a[FB];  // staged splats (stage_splat)
+  __shared__ float4 s_b[FB];
+  __shared__ float4 s_c[FB];
   __shared__ float s_red[L::kWarps][16];
   __shared__ uint32_t s_max[L::kWarps];
 
@@ -159,11 +163,10 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
     last[p] = 0u;
   }
   const float block_h = float(4 * PX);
-  for (uint32_t start = range.x; start < range.y; start += 256u) {
+  for (uint32_t start = range.x; start < range.y; start += uint32_t(FB)) {
     if (__syncthreads_count(all_done) == L::kThreads) break;
 #pragma unroll
-    for (int r = 0; r < PX; ++r) {
-      const uint32_t slot = lid + uint32_t(r) * L::kThreads;
+    for (uint32_t slot = lid; slot < uint32_t(FB); slot += uint32_t(L::kThreads)) {
       const uint32_t k = start + slot;
       if (k < range.y) {
         const uint32_t g = a.rb.pair_gaussian[a.rb.values[k]];
@@ -177,17 +180,17 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
       }
     }
     __syncthreads();
-    const uint32_t n = min(256u, range.y - start);
+    const uint32_t n = min(uint32_t(FB), range.y - start);
     // The splats of this batch whose footprint reaches the warp's block, in order.
-    uint32_t masks[8];
+    uint32_t masks[FB / 32];
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < FB / 32; ++w) {
       const uint32_t j = uint32_t(w) * 32u + lane;
       masks[w] = __ballot_sync(0xffffffffu, j < n && block_reached(s_a[j], s_b[j], s_c[j], lay.bx, lay.by, block_h));
     }
     const uint32_t base = start - range.x;  // position in the tile's list of the batch's first splat
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < FB / 32; ++w) {
       uint32_t m = masks[w];
       while (m != 0u && !all_done) {
         const uint32_t j = uint32_t(w) * 32u + uint32_t(__ffs(m) - 1);
@@ -317,14 +320,15 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
   }
 }
 
-template <int PX>
+template <int PX, int FB>
 __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   const uint32_t total = a.vt->total_tiles;
-  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX>(a, gt);
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX, FB>(a, gt);
 }
 
 template <int BATCH, bool DET, int PX>
 __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt) {
+  constexpr bool ABS = DET;  // the |dL/dmean2d| sums (see the top of the file)
   using L = TileLayout<PX>;
   static_assert(BATCH <= L::kThreads, "one staged splat per thread");
   __shared__ float4 s_a[BATCH];
@@ -437,8 +441,6 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           const float dl = raw >= kMaxAlpha ? 0.0f : dlda;
           const float dpow = raw * dl;
           const float t = dpow * dy;
-          const float dmx = fmaf(t, mx, dpow * lx);  // dpow (lx + mx dy)
-          const float dmy = fmaf(t, my, dpow * ly);
           sd += dpow;
           st += t;
           sty = fmaf(t, dy, sty);
@@ -446,8 +448,10 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           c[6] += weight * dl0[p];
           c[7] += weight * dl1[p];
           c[8] += weight * dl2[p];
-          c[9] += fabsf(dmx);
-          c[10] += fabsf(dmy);
+          if constexpr (ABS) {
+            c[9] += fabsf(fmaf(t, mx, dpow * lx));  // |dpow (lx + mx dy)|
+            c[10] += fabsf(fmaf(t, my, dpow * ly));
+          }
           T[p] = __fmul_rn(T[p], one_minus);
           R[p] = rest;
         }
@@ -496,16 +500,33 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
       if (lane == 0) s_wrote[warp][w] = wrote;
     }
     __syncthreads();
-    for (uint32_t idx = lid; idx < nb * 12u; idx += L::kThreads) {
-      const uint32_t j = idx / 12u, k = idx - j * 12u;
-      float s = 0.0f;
+    if constexpr (DET) {
+      for (uint32_t idx = lid; idx < nb * 12u; idx += L::kThreads) {
+        const uint32_t j = idx / 12u, k = idx - j * 12u;
+        float s = 0.0f;
 #pragma unroll
-      for (int w8 = 0; w8 < L::kWarps; ++w8)
-        if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) s += s_part[w8][j][k];
-      if (DET) {
+        for (int w8 = 0; w8 < L::kWarps; ++w8)
+          if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) s += s_part[w8][j][k];
         a.pair_grads[size_t(s_dst[j]) * 12u + k] = s;
-      } else if (s != 0.0f) {
-        atomicAdd(a.grad2d + size_t(s_dst[j]) * 12u + k, s);
+      }
+    } else {
+      // One float4 of the gaussian's accumulator per thread: the warps' partials added in
+      // order, then one vector atomic (skipped for a splat no warp drew).
+      for (uint32_t idx = lid; idx < nb * 3u; idx += L::kThreads) {
+        const uint32_t j = idx / 3u, q = idx - j * 3u;
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool any = false;
+#pragma unroll
+        for (int w8 = 0; w8 < L::kWarps; ++w8)
+          if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) {
+            const float* part = &s_part[w8][j][q * 4u];
+            s.x += part[0];
+            s.y += part[1];
+            s.z += part[2];
+            s.w += part[3];
+            any = true;
+          }
+        if (any) atomicAdd(reinterpret_cast<float4*>(a.grad2d) + size_t(s_dst[j]) * 3u + q, s);
       }
     }
   }
@@ -553,25 +574,32 @@ void launch_bwd_batch(const RasterArgs& a, const StepPointers& sp, bool determin
   }
 }
 
-template <int PX>
+template <int PX, int FB>
 void launch_fwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_fwd<PX>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_fwd<PX, FB>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_fwd<PX><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_fwd<PX, FB><<<grid, 256 / PX, 0, st>>>(a);
+}
+
+template <int PX>
+void launch_fwd_batch(const RasterArgs& a, const StepPointers& sp, int batch, cudaStream_t st) {
+  if (batch >= 256) launch_fwd<PX, 256>(a, sp, st);
+  else if (batch >= 128) launch_fwd<PX, 128>(a, sp, st);
+  else launch_fwd<PX, 64>(a, sp, st);
 }
 
 }  // namespace
 
-void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px,
+void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
                            cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u};
-  if (px >= 4) launch_fwd<4>(a, sp, st);
-  else if (px == 2) launch_fwd<2>(a, sp, st);
-  else launch_fwd<1>(a, sp, st);
+  if (px >= 4) launch_fwd_batch<4>(a, sp, batch, st);
+  else if (px == 2) launch_fwd_batch<2>(a, sp, batch, st);
+  else launch_fwd_batch<1>(a, sp, batch, st);
 }
 
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,

@@ -50,7 +50,8 @@ class Tuning(ctypes.Structure):
     _fields_ = [("min_pair_capacity", ctypes.c_uint32), ("initial_pairs", ctypes.c_uint64),
                 ("deterministic", ctypes.c_uint32), ("forward_pixels", ctypes.c_uint32),
                 ("backward_pixels", ctypes.c_uint32), ("retry", ctypes.c_uint32), ("graph", ctypes.c_uint32),
-                ("backward_batch", ctypes.c_uint32), ("sort_digit_bits", ctypes.c_uint32)]
+                ("backward_batch", ctypes.c_uint32), ("sort_digit_bits", ctypes.c_uint32),
+                ("forward_batch", ctypes.c_uint32), ("tune_reduction", ctypes.c_uint32)]
 
 
 class ModelInfo(ctypes.Structure):

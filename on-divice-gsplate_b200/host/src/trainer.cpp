@@ -159,9 +159,9 @@ bool Trainer::retune_due(uint32_t s) const {
 std::string Trainer::reduction() const {
   gs_tuning t;
   if (gs_get_tuning(gpu_, &t) != GS_OK) return "unknown";
-  return "fpx=" + std::to_string(t.forward_pixels) + " bpx=" + std::to_string(t.backward_pixels) +
-         " batch=" + std::to_string(t.backward_batch) + " digits=" + std::to_string(t.sort_digit_bits) +
-         (t.deterministic ? " deterministic" : " atomic");
+  return "fpx=" + std::to_string(t.forward_pixels) + " fbatch=" + std::to_string(t.forward_batch) +
+         " bpx=" + std::to_string(t.backward_pixels) + " batch=" + std::to_string(t.backward_batch) +
+         " digits=" + std::to_string(t.sort_digit_bits) + (t.deterministic ? " deterministic" : " atomic");
 }
 
 bool Trainer::select_backward(const std::string& name) {
@@ -184,6 +184,7 @@ bool Trainer::select_backward(const std::string& name) {
     const unsigned long v = std::strtoul(word.c_str() + eq + 1, &rest, 10);
     if (rest == word.c_str() + eq + 1 || *rest != '\0') return false;
     if (key == "fpx" && (v == 1 || v == 2 || v == 4)) t.forward_pixels = uint32_t(v);
+    else if (key == "fbatch" && (v == 64 || v == 128 || v == 256)) t.forward_batch = uint32_t(v);
     else if (key == "bpx" && (v == 1 || v == 2 || v == 4)) t.backward_pixels = uint32_t(v);
     else if (key == "batch" && (v == 32 || v == 64)) t.backward_batch = uint32_t(v);
     else if (key == "digits" && v >= 4 && v <= 8) t.sort_digit_bits = uint32_t(v);

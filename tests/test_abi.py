@@ -34,7 +34,7 @@ def test_library_exports_every_symbol():
 def test_struct_layouts_match_header():
     # gs_frame_data is FrameData (train_common.glsl:15-37): 18 vec4 = 288 bytes.
     assert FRAME_DTYPE.itemsize == 288
-    assert ctypes.sizeof(cuda.Tuning) == 48
+    assert ctypes.sizeof(cuda.Tuning) == 56
     assert ctypes.sizeof(cuda.StepResult) == 16 + 8 * 16 + 8 * 8 * 16 + 4 + 4 + 24 + 8 * 8 * 16 + 6 * 8 * 16
 
 
