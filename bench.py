@@ -15,10 +15,10 @@ Adam on every parameter. Views are drawn in shuffled epochs over the 200 cameras
 - e2e: the batched step through the C ABI as a caller drives it, wall clock: each step
   uploads its 8 targets from pinned host memory (gs_set_views) and reads the loss sums back.
 - roofline: the dominant pass of the batched step, timed by pass events recorded inside
-  the replayed graph. Raster passes are issue-bound, so their roofline is the
-  special-function unit (MUFU, 16 operations per clock per SM at the sampled clock) over the
-  step's pixel-pair evaluations E (one exponential per evaluation forward, an exponential
-  and a reciprocal backward); every pass also reports HBM GB/s from fixed per-unit bytes
+  the replayed graph. Raster passes are issue-bound, so their roofline is the FP32 pipe
+  (128 lane operations per clock per SM at the sampled clock) over the work of the step's
+  pixel-pair evaluations E (FP32_PER_EVALUATION), with the special-function unit's share
+  beside it; every pass also reports HBM GB/s from fixed per-unit bytes
   (algorithmic_bytes) against the measured copy bandwidth.
 - cpu_baseline: the CPU oracle (a multithreaded restatement of the reference's passes) on
   plain steps of the same workload, host cores, bounded time.
@@ -172,11 +172,17 @@ def algorithmic_bytes(pass_name: str, n: int, views: int, pairs: int, pixels: in
     return 0.0
 
 
-# Special-function (MUFU) operations per pixel-pair evaluation: the forward's exponential;
-# the backward's exponential and the reciprocal of (1 - alpha). B200 issues 16 MUFU
-# operations per clock per SM.
+# Work per pixel-pair evaluation of the raster passes (E = the sum over pixels of the last
+# contributor's position in its tile's list): special-function (MUFU) operations (the
+# forward's exponential; the backward's exponential and its reciprocal of 1 - alpha) and
+# FP32 operations (an FMA counts as one). The backward's 60 FP32 operations are the path's
+# byte-and-work model; the forward's 15 are its exponent (3), alpha and the skip tests (4),
+# transmittance (2) and colour accumulation (6). B200 issues 16 MUFU and 128 FP32 lane
+# operations per clock per SM, so at these counts the FP32 pipe bounds both passes.
 MUFU_PER_EVALUATION = {"rasterize": 1, "backward": 2}
+FP32_PER_EVALUATION = {"rasterize": 15, "backward": 60}
 MUFU_PER_CLOCK_PER_SM = 16
+FP32_PER_CLOCK_PER_SM = 128
 SM_COUNT = 148
 
 
@@ -430,6 +436,7 @@ def main() -> None:
         clk = clocks.summary()
         sm_hz = (clk["sm_mhz"] or 1965.0) * 1e6
         mufu_peak = MUFU_PER_CLOCK_PER_SM * SM_COUNT * sm_hz / 1e9  # Gop/s at the sampled clock
+        fp32_peak = FP32_PER_CLOCK_PER_SM * SM_COUNT * sm_hz / 1e9
         per_pass = {}
         for name, ms in passes.items():
             b = algorithmic_bytes(name, scene.count, VIEWS_PER_STEP, int(pairs), pixels, stride)
@@ -437,16 +444,21 @@ def main() -> None:
             entry = {"ms": round(ms, 4), "gbs": round(gbs, 1) if gbs else None,
                      "hbm_frac": round(gbs / pk["hbm_gbs"], 4) if gbs else None}
             if name in MUFU_PER_EVALUATION and last_passes[name] > 0:
-                gops = evaluations * MUFU_PER_EVALUATION[name] / (last_passes[name] * 1e-3) / 1e9
-                entry.update({"mufu_gops": round(gops, 1), "mufu_frac": round(gops / mufu_peak, 4)})
+                per_s = evaluations / (last_passes[name] * 1e-3) / 1e9
+                mufu, fp32 = per_s * MUFU_PER_EVALUATION[name], per_s * FP32_PER_EVALUATION[name]
+                entry.update({"evaluations_g_per_s": round(per_s, 2), "mufu_gops": round(mufu, 1),
+                              "mufu_frac": round(mufu / mufu_peak, 4), "fp32_gops": round(fp32, 1),
+                              "fp32_frac": round(fp32 / fp32_peak, 4)})
             per_pass[name] = entry
         # The raster passes are bound by instruction issue on the SMs, not by HBM: their
-        # roofline is the special-function unit's rate at the sampled clock.
+        # roofline is the FP32 pipe's rate at the sampled clock over the evaluations' work.
         d = per_pass[dom]
-        if "mufu_gops" in d:
-            roof = {"bound": "sfu", "kernel": dom, "achieved": d["mufu_gops"], "peak": round(mufu_peak, 1),
-                    "unit": "Gop/s", "frac": d["mufu_frac"], "evaluations_per_step": evaluations,
-                    "mufu_per_evaluation": MUFU_PER_EVALUATION[dom],
+        if "fp32_gops" in d:
+            roof = {"bound": "fp32", "kernel": dom, "achieved": d["fp32_gops"], "peak": round(fp32_peak, 1),
+                    "unit": "Gop/s", "frac": d["fp32_frac"], "evaluations_per_step": evaluations,
+                    "fp32_per_evaluation": FP32_PER_EVALUATION[dom],
+                    "sfu": {"achieved": d["mufu_gops"], "peak": round(mufu_peak, 1), "unit": "Gop/s",
+                            "frac": d["mufu_frac"], "per_evaluation": MUFU_PER_EVALUATION[dom]},
                     "hbm": {"achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": d["hbm_frac"]}}
         else:
             roof = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s",

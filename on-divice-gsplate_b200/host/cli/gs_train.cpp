@@ -12,9 +12,10 @@
 //            [--motion-reg decay,rigidity,smoothness,center] [--motion-out motion.json]
 //            [--eval-rest <capture_dir>] (held-out views of a twin capture with the subject standing still:
 //            the model at rest against it)
-// <dataset> is a capture folder (transforms.json; PNG/PPM images, resized so the short side
-// is --width; initial gaussians from its point cloud or random, up to --init-gaussians,
-// 150000 by default; the reference's default options with the schedule scaled to --iters)
+// <dataset> is a capture folder (transforms.json; PNG/PPM/JPEG images, resized so the short
+// side is --width, optional depth maps; initial gaussians from the depth maps, its point
+// cloud or random, up to --init-gaussians, 150000 by default; the reference's default
+// options with the schedule scaled to --iters)
 // or a synthetic orbit capture:
 //   synthetic:orbit        ground truth of 100k gaussians (radius-1 ball, log-scales N(-4, 0.5),
 //                          SH 3 ~ N(0, 0.2)), 60 cameras on a circle of radius 3 at height 0.5,
