@@ -335,6 +335,8 @@ def main() -> None:
     ap.add_argument("--cameras", type=int, default=N_CAMERAS, help="orbit cameras (fewer: shorter setup)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tuning (profiling runs: timings under ncu would mislead the autotuner)")
+    ap.add_argument("--set", action="append", default=[], metavar="KNOB=VALUE",
+                    help="a gs_tuning field to set instead of autotuning it (profiling runs), e.g. deterministic=0")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -366,6 +368,10 @@ def main() -> None:
     ctx = Context(local)
     targets = render_targets(ctx, truth, cams, opt)
     ctx.set_tuning(graph=1)
+    fixed = {k: int(v) for k, v in (kv.split("=", 1) for kv in args.set)}
+    if fixed:
+        ctx.set_tuning(**fixed)
+        args.no_autotune = True
     ctx.model_init(scene.params, scene.sh)
     ctx.set_dataset(targets)
     order = ViewOrder(len(cams))
@@ -415,6 +421,14 @@ def main() -> None:
         step += 1
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+
+    # Densification runs every 100 steps of this schedule, outside the step's graph: one call
+    # on the statistics of the steps above, its cost spread over 100 steps.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    counters = ctx.densify(frame(scene, cams[0], opt, step))
+    torch.cuda.synchronize()
+    densify_ms = 1000.0 * (time.perf_counter() - t0)
 
     gpu_ms, plain_ms, e2e_s = max_over_ranks([gpu_ms, plain_ms, e2e_s], dist)
     ms_per_step = gpu_ms / args.steps
@@ -484,6 +498,10 @@ def main() -> None:
             "e2e": {"value": round(e2e, 3), "unit": "views/s", "h2d_bytes_per_step": VIEWS_PER_STEP * WIDTH * HEIGHT * 4,
                     "d2h_bytes_per_step": 4 * (4 + 2 * 16) + 64 * VIEWS_PER_STEP},
             "gpu_launches": launches,
+            "densify": {"ms": round(densify_ms, 3), "every_steps": 100, "spawned": int(counters[1]),
+                        "pruned": int(counters[2]),
+                        "views_per_s_with_densify": round(world * VIEWS_PER_STEP * 1000.0 /
+                                                          (ms_per_step + densify_ms / 100.0), 3)},
             "clocks": clk,
         }
         if not args.no_cpu_baseline and world == 1:

@@ -122,8 +122,8 @@ typedef enum gs_snapshot_kind {
   GS_SNAP_TILES = 3,        /* uint32 per slot: tiles touched */
   GS_SNAP_OFFSETS = 4,      /* uint32 per slot: first pair (pre-sort order) */
   GS_SNAP_PAIR_GRADS = 5,   /* 12 floats per pair, pre-sort order (deterministic mode) */
-  GS_SNAP_PAIR_TILE = 6,    /* uint32 per pair, pre-sort order: the view's tile */
-  GS_SNAP_RENDER_ORDER = 7, /* uint32 per pair: pre-sort index in render order */
+  GS_SNAP_PAIR_TILE = 6,    /* uint32 per pair, pre-sort order: the view's tile (not after an atomic training step) */
+  GS_SNAP_RENDER_ORDER = 7, /* uint32 per pair: pre-sort index in render order (not after an atomic training step) */
   GS_SNAP_DEPTH_KEY = 8,    /* uint32 per slot: 16-bit depth key */
   GS_SNAP_IMAGE = 9,        /* RGBA8 per pixel */
   GS_SNAP_RANGES = 10,      /* 2 uint32 per tile: [start, end) in render order, view-local */
@@ -150,6 +150,8 @@ typedef struct gs_tuning {
   uint32_t sort_digit_bits;   /* radix digit width of the depth and pair sorts: 4..8 (0: default 8) */
   uint32_t forward_batch;     /* splats staged per round of the forward pass: 64, 128 or 256 (0: default 256) */
   uint32_t tune_reduction;    /* 1: gs_autotune may also switch `deterministic` (0: it keeps the caller's) */
+  uint32_t stage_async;       /* 1: raster passes copy the next round of splats with cp.async while the
+                                 current one blends (double-buffered); 0: plain loads */
 } gs_tuning;
 
 typedef struct gs_model_info {

@@ -132,6 +132,8 @@ struct gs_context {
   // pairs
   uint64_t pair_cap = 0;
   uint32_t *keys = nullptr, *values = nullptr, *keys_alt = nullptr, *values_alt = nullptr, *pair_gaussian = nullptr;
+  uint32_t* sorted_g = nullptr;  // each sorted pair's gaussian, in render order (gathered by the ranges pass)
+  bool payload_gaussian = false;  // the latest step sorted each pair's gaussian instead of its pre-sort index
   float4* pair_grads = nullptr;
   const uint32_t* sorted_keys = nullptr;
   const uint32_t* sorted_values = nullptr;
@@ -189,6 +191,7 @@ struct gs_context {
     h_motion_grad = nullptr;
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
                          &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
+                         &sorted_g,
                          &d_scalars, &sort.hist, &sort.tile_counts, &dens.spawn,
                          &dens.release, &dens.wants, &dens.free_pos, &dens.spawn_pos, &dens.free_list,
                          &dens.counters})
@@ -297,6 +300,7 @@ struct gs_context {
     dev_alloc(keys_alt, n);
     dev_alloc(values_alt, n);
     dev_alloc(pair_gaussian, n);
+    dev_alloc(sorted_g, n);
     dev_alloc(pair_grads, n * 3);
     const uint32_t sort_tiles = uint32_t((n + gsk::kSortTile - 1) / gsk::kSortTile);
     if (sort_tiles > sort.count_tiles) {
@@ -501,6 +505,11 @@ struct gs_context {
         t.deterministic = best.deterministic ? 0u : 1u;
         consider(t);
       }
+      {  // splats staged with plain loads or with asynchronous copies
+        gs_tuning t = best;
+        t.stage_async = best.stage_async ? 0u : 1u;
+        consider(t);
+      }
       const uint32_t fpx0 = best.forward_pixels, fb0 = best.forward_batch;
       for (uint32_t fpx : {1u, 2u, 4u})
         for (uint32_t fb : {128u, 256u})
@@ -571,6 +580,7 @@ struct gs_context {
     gsk::RasterBuffers rb;
     rb.ranges = ranges;
     rb.values = sorted_values;
+    rb.gauss = payload_gaussian ? sorted_values : sorted_g;
     rb.pair_gaussian = pair_gaussian;
     rb.pixel_grad = pixel_grad;
     rb.pixel_out = pixel_out;
@@ -635,6 +645,10 @@ struct gs_context {
     const gsk::StepPointers sp = step_pointers();
     const uint32_t items = n_views * model.slots;
     const bool det = tuning.deterministic != 0u;
+    // An atomic training step needs no pre-sort pair index: the sort carries each pair's
+    // gaussian, which the raster passes stage from directly (no gather). Deterministic and
+    // forward-only steps keep the index (per-pair gradients, the render-order snapshots).
+    payload_gaussian = train && !det;
     GS_CUDA_TRY(cudaMemsetAsync(d_scalars, 0, sizeof(uint32_t), stream));  // [0] pairs; [1] mismatches accumulate
     const uint32_t motion = motion_mode();
     const gsk::Motion mo = motion_state();
@@ -653,7 +667,7 @@ struct gs_context {
     // Offsets of each item's pairs in depth order; the total is the step's pair count.
     gsk::exclusive_scan(sort, vb.tiles, depth_sorted_vals, sorted_offsets, items, d_scalars, stream, &launches);
     gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, d_scalars, uint32_t(pair_cap), keys,
-                     values, pair_gaussian, pair_grads, d_scalars + 1, stream);
+                     values, pair_gaussian, pair_grads, d_scalars + 1, payload_gaussian, stream);
     launches += items ? 1 : 0;
     const uint32_t max_tiles = uint32_t(tile_cap - 1);
     const int tile_bits = int(bits_for(max_tiles + 1));
@@ -664,7 +678,9 @@ struct gs_context {
     sorted_values = pairs_alt ? values_alt : values;
     GS_CUDA_TRY(cudaMemsetAsync(ranges, 0, sizeof(uint2) * (max_tiles + 1), stream));
     GS_CUDA_TRY(cudaMemsetAsync(d_scalars + 4, 0, 2 * GS_MAX_VIEWS * sizeof(uint32_t), stream));
-    gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, sp.vt, d_scalars + 4, stream);
+    const gsk::PairGather gather{sorted_values, pair_gaussian, sorted_g};
+    gsk::launch_ranges(sorted_keys, d_scalars, uint32_t(pair_cap), ranges, sp.vt, d_scalars + 4,
+                       payload_gaussian ? nullptr : &gather, stream);
     ++launches;
     mark(2);
     const gsk::RasterBuffers rb = raster_buffers();
@@ -675,7 +691,8 @@ struct gs_context {
                                       capture == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0u));
     }
     gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2,
-                               tuning.forward_batch ? int(tuning.forward_batch) : 256, stream);
+                               tuning.forward_batch ? int(tuning.forward_batch) : 256, tuning.stage_async != 0u,
+                               stream);
     ++launches;
     mark(3);
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
@@ -693,7 +710,8 @@ struct gs_context {
     if (train) {
       const int px = tuning.backward_pixels ? int(tuning.backward_pixels) : 4;
       const int batch = tuning.backward_batch ? int(tuning.backward_batch) : 64;
-      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, px, batch, d_scalars, uint32_t(pair_cap), stream);
+      gsk::launch_raster_backward(sp, vb, rb, pair_grads, det, px, batch, tuning.stage_async != 0u, d_scalars,
+                                  uint32_t(pair_cap), stream);
       ++launches;
       mark(5);
       if (det) {
@@ -1238,6 +1256,9 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
         break;
       }
       case GS_SNAP_PAIR_TILE: case GS_SNAP_RENDER_ORDER: {
+        if (c->payload_gaussian)
+          fail(GS_ERR_INVALID, "gs_snapshot: an atomic training step sorts gaussians, not pair indices: the pair "
+                               "tiles and the render order are kept by deterministic or forward-only steps");
         std::vector<uint32_t> k(pairs), v(pairs);
         d2h(k.data(), c->sorted_keys, pairs * 4);
         d2h(v.data(), c->sorted_values, pairs * 4);

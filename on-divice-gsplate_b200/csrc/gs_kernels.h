@@ -75,19 +75,30 @@ void exclusive_scan(const SortScratch& s, const uint32_t* in, const uint32_t* ga
 
 // ---- pairs.cu ----
 // total: the scan's total (the end of the last item's pairs).
+// values: each pair's pre-sort index, or (payload_gaussian) its gaussian g, which the sort
+// then carries to the raster passes directly (atomic training steps, which never need the
+// pre-sort index).
 void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
                  const uint32_t* sorted_vals, const uint32_t* sorted_offsets, const uint32_t* total,
                  uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
-                 uint32_t* mismatch, cudaStream_t st);
+                 uint32_t* mismatch, bool payload_gaussian, cudaStream_t st);
 // Tile ranges of the sorted pairs, and each view's span [view_span[v], view_span[kMaxViews + v])
-// of them (zeroed by the caller; views without pairs keep 0, 0).
+// of them (zeroed by the caller; views without pairs keep 0, 0). With `gather` non-null,
+// also sorted_g[s] = pair_gaussian[sorted_values[s]]: each sorted pair's gaussian, laid out
+// in render order for the raster passes' coalesced staging.
+struct PairGather {
+  const uint32_t* sorted_values = nullptr;
+  const uint32_t* pair_gaussian = nullptr;
+  uint32_t* sorted_g = nullptr;
+};
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
-                   const ViewTable* vt, uint32_t* view_span, cudaStream_t st);
+                   const ViewTable* vt, uint32_t* view_span, const PairGather* gather, cudaStream_t st);
 
 // ---- raster.cu ----
 struct RasterBuffers {
   const uint2* ranges = nullptr;
-  const uint32_t* values = nullptr;         // pre-sort pair index per sorted pair
+  const uint32_t* values = nullptr;         // per sorted pair: its pre-sort index (or g, see launch_emit)
+  const uint32_t* gauss = nullptr;          // per sorted pair: its gaussian g (render order)
   const uint32_t* pair_gaussian = nullptr;  // g per pre-sort pair
   float4* pixel_grad = nullptr;             // dL/dC rgb, final T
   float4* pixel_out = nullptr;              // rendered colour rgb (over the background), loss weight
@@ -101,15 +112,16 @@ struct RasterBuffers {
   float4* ssim_maps = nullptr;
   float* ssim_last = nullptr;
 };
-// px: pixels per thread (1, 2 or 4).
+// px: pixels per thread (1, 2 or 4); batch: splats staged per round (64, 128, 256);
+// async: stage the next round with cp.async while the current one blends.
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
-                           cudaStream_t st);
+                           bool async, cudaStream_t st);
 // Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
 // vb.grad2d (fast), staging `batch` (32 or 64) splats per round. Skipped on device when
 // *d_pairs > accept.
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
-                            float4* pair_grads, bool deterministic, int px, int batch, const uint32_t* d_pairs,
-                            uint32_t accept, cudaStream_t st);
+                            float4* pair_grads, bool deterministic, int px, int batch, bool async,
+                            const uint32_t* d_pairs, uint32_t accept, cudaStream_t st);
 
 // ---- loss.cu ----
 void launch_ssim(const StepPointers& sp, const RasterBuffers& rb, cudaStream_t st);

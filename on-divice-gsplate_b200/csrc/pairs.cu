@@ -29,6 +29,7 @@ struct EmitArgs {
   uint32_t* pair_gaussian;
   float4* pair_grads;
   uint32_t* mismatch;
+  bool payload_gaussian;  // values carry g instead of the pre-sort index
 };
 
 // Pairs a warp stages in shared memory before writing them out: a warp's items are
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
         st_owner[q - wfirst] = g;
       } else {
         a.keys[q] = tile;
-        a.values[q] = q;
+        a.values[q] = a.payload_gaussian ? g : q;
         a.pair_gaussian[q] = g;
       }
     };
@@ -120,9 +121,10 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   if (!staged) return;
   __syncwarp();
   for (uint32_t q = wfirst + lane; q < wend; q += 32u) {
+    const uint32_t owner = st_owner[q - wfirst];
     a.keys[q] = st_tile[q - wfirst];
-    a.values[q] = q;
-    a.pair_gaussian[q] = st_owner[q - wfirst];
+    a.values[q] = a.payload_gaussian ? owner : q;
+    a.pair_gaussian[q] = owner;
   }
 }
 
@@ -142,7 +144,7 @@ __device__ __forceinline__ void range_edge(uint32_t s, uint32_t prev, uint32_t t
 
 __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ keys, const uint32_t* d_count,
                                                 uint32_t capacity, uint2* __restrict__ ranges, const ViewTable* vt,
-                                                uint32_t* __restrict__ view_span) {
+                                                uint32_t* __restrict__ view_span, PairGather gather) {
   const uint32_t count = min(*d_count, capacity);
   if (count == 0u) return;
   const uint32_t groups = (count + 3u) / 4u;
@@ -158,6 +160,16 @@ __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ key
     } else {
 #pragma unroll
       for (int j = 0; j < 4; ++j) k[j] = s0 + j < count ? keys[s0 + j] : 0u;
+    }
+    if (gather.sorted_g != nullptr) {
+      if (s0 + 4u <= count) {
+        const uint4 v = *reinterpret_cast<const uint4*>(gather.sorted_values + s0);
+        *reinterpret_cast<uint4*>(gather.sorted_g + s0) =
+            make_uint4(gather.pair_gaussian[v.x], gather.pair_gaussian[v.y], gather.pair_gaussian[v.z],
+                       gather.pair_gaussian[v.w]);
+      } else {
+        for (uint32_t s = s0; s < count; ++s) gather.sorted_g[s] = gather.pair_gaussian[gather.sorted_values[s]];
+      }
     }
     uint32_t prev = s0 > 0u ? keys[s0 - 1u] : 0u;
 #pragma unroll
@@ -185,19 +197,19 @@ __global__ void __launch_bounds__(256) k_ranges(const uint32_t* __restrict__ key
 void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, uint32_t n_items,
                  const uint32_t* sorted_vals, const uint32_t* sorted_offsets, const uint32_t* total,
                  uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
-                 uint32_t* mismatch, cudaStream_t st) {
+                 uint32_t* mismatch, bool payload_gaussian, cudaStream_t st) {
   if (n_items == 0u) return;
   EmitArgs a{sp.frames, sp.vt,    cap,        n_items, pair_capacity, sorted_vals, sorted_offsets,
              total,     vb.splat, vb.foot,    vb.spans, vb.offsets, keys,  values,       pair_gaussian,
-             pair_grads, mismatch};
+             pair_grads, mismatch, payload_gaussian};
   k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 
 void launch_ranges(const uint32_t* sorted_keys, const uint32_t* d_count, uint32_t pair_capacity, uint2* ranges,
-                   const ViewTable* vt, uint32_t* view_span, cudaStream_t st) {
+                   const ViewTable* vt, uint32_t* view_span, const PairGather* gather, cudaStream_t st) {
   if (pair_capacity == 0u) return;
-  k_ranges<<<min((pair_capacity + 1023u) / 1024u, 148u * 8u), 256, 0, st>>>(sorted_keys, d_count, pair_capacity,
-                                                                              ranges, vt, view_span);
+  k_ranges<<<min((pair_capacity + 1023u) / 1024u, 148u * 8u), 256, 0, st>>>(
+      sorted_keys, d_count, pair_capacity, ranges, vt, view_span, gather ? *gather : PairGather{});
 }
 
 }  // namespace gsk

@@ -78,6 +78,33 @@ __device__ __forceinline__ float exp2_approx(float x) {
   return r;
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, cached in L2 only), grouped per
+// staged round: a round's copies are committed as one group, and waiting for all but the
+// newest group leaves the next round in flight while the current one is consumed.
+__device__ __forceinline__ void copy_async16(void* smem, const void* gmem) {
+  const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void copy_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+// Raw splat records of a staged round, component-major: q[0..2][slot] are the gaussian's
+// three splat float4s, q[3][slot] its footprint float4 (whose w is the threshold).
+template <int N>
+struct RawRound {
+  float4 q[4][N];
+};
+__device__ __forceinline__ void fetch_record_async(float4* q0, float4* q1, float4* q2, float4* qf, const float4* splat,
+                                                   const float4* foot, uint32_t g) {
+  copy_async16(q0, splat + size_t(g) * 3u);
+  copy_async16(q1, splat + size_t(g) * 3u + 1u);
+  copy_async16(q2, splat + size_t(g) * 3u + 2u);
+  copy_async16(qf, foot + g);
+}
+
 // Whether a staged splat's footprint ellipse reaches a pixel centre of the 8 x h block
 // whose first centre is (x0, y0): the maximum of the concave E over the block's rectangle
 // is 0 when the centre lies inside, else it lies on an edge facing the centre, at the
@@ -130,14 +157,19 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
   return item;
 }
 
-// FB splats are staged per round (64, 128 or 256: a tuning knob).
-template <int PX, int FB>
+// FB splats are staged per round (64, 128 or 256: a tuning knob). With ASYNC the records of
+// round i + 1 are copied with cp.async while round i blends (double-buffered raw records,
+// the gaussian indices loaded one round further ahead), and each thread turns the records it
+// copied into staged splats once they land.
+template <int PX, int FB, bool ASYNC>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
   static_assert(FB % 32 == 0 && FB <= 256, "whole warps of staged splats");
+  constexpr int kPer = (FB + L::kThreads - 1) / L::kThreads;  // slots per thread
   __shared__ float4 s_a[FB];  // staged splats (stage_splat)
   __shared__ float4 s_b[FB];
   __shared__ float4 s_c[FB];
+  __shared__ RawRound<ASYNC ? FB : 1> s_raw[ASYNC ? 2 : 1];
   __shared__ float s_red[L::kWarps][16];
   __shared__ uint32_t s_max[L::kWarps];
 
@@ -163,20 +195,70 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
     last[p] = 0u;
   }
   const float block_h = float(4 * PX);
+  uint32_t g_next[kPer];  // ASYNC: the gaussians of the round after the one in flight
+  uint32_t buf = 0u;
+  if constexpr (ASYNC) {
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const uint32_t slot = lid + uint32_t(r) * L::kThreads, k = range.x + slot;
+      if (slot < uint32_t(FB) && k < range.y)
+        fetch_record_async(&s_raw[0].q[0][slot], &s_raw[0].q[1][slot], &s_raw[0].q[2][slot], &s_raw[0].q[3][slot],
+                           a.splat, a.foot, a.rb.gauss[k]);
+    }
+    copy_async_commit();
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const uint32_t slot = lid + uint32_t(r) * L::kThreads, k = range.x + uint32_t(FB) + slot;
+      g_next[r] = slot < uint32_t(FB) && k < range.y ? a.rb.gauss[k] : 0u;
+    }
+  }
   for (uint32_t start = range.x; start < range.y; start += uint32_t(FB)) {
     if (__syncthreads_count(all_done) == L::kThreads) break;
+    if constexpr (ASYNC) {
+      // Round i + 1 into the other buffer (free: every warp has passed the barrier above),
+      // then round i's own copies, staged by the thread that made them.
+      const uint32_t nstart = start + uint32_t(FB);
 #pragma unroll
-    for (uint32_t slot = lid; slot < uint32_t(FB); slot += uint32_t(L::kThreads)) {
-      const uint32_t k = start + slot;
-      if (k < range.y) {
-        const uint32_t g = a.rb.pair_gaussian[a.rb.values[k]];
-        const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u],
-                     q2 = a.splat[size_t(g) * 3u + 2u];
-        float4 A, B, C;
-        stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
-        s_a[slot] = A;
-        s_b[slot] = B;
-        s_c[slot] = C;
+      for (int r = 0; r < kPer; ++r) {
+        const uint32_t slot = lid + uint32_t(r) * L::kThreads, k = nstart + slot;
+        if (slot < uint32_t(FB) && k < range.y)
+          fetch_record_async(&s_raw[buf ^ 1u].q[0][slot], &s_raw[buf ^ 1u].q[1][slot], &s_raw[buf ^ 1u].q[2][slot],
+                             &s_raw[buf ^ 1u].q[3][slot], a.splat, a.foot, g_next[r]);
+      }
+      copy_async_commit();
+#pragma unroll
+      for (int r = 0; r < kPer; ++r) {
+        const uint32_t slot = lid + uint32_t(r) * L::kThreads, k = nstart + uint32_t(FB) + slot;
+        g_next[r] = slot < uint32_t(FB) && k < range.y ? a.rb.gauss[k] : 0u;
+      }
+      copy_async_wait<1>();
+#pragma unroll
+      for (int r = 0; r < kPer; ++r) {
+        const uint32_t slot = lid + uint32_t(r) * L::kThreads;
+        if (slot < uint32_t(FB) && start + slot < range.y) {
+          float4 A, B, C;
+          stage_splat(s_raw[buf].q[0][slot], s_raw[buf].q[1][slot], s_raw[buf].q[2][slot], s_raw[buf].q[3][slot].w,
+                      A, B, C);
+          s_a[slot] = A;
+          s_b[slot] = B;
+          s_c[slot] = C;
+        }
+      }
+      buf ^= 1u;
+    } else {
+#pragma unroll
+      for (uint32_t slot = lid; slot < uint32_t(FB); slot += uint32_t(L::kThreads)) {
+        const uint32_t k = start + slot;
+        if (k < range.y) {
+          const uint32_t g = a.rb.gauss[k];
+          const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u],
+                       q2 = a.splat[size_t(g) * 3u + 2u];
+          float4 A, B, C;
+          stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
+          s_a[slot] = A;
+          s_b[slot] = B;
+          s_c[slot] = C;
+        }
       }
     }
     __syncthreads();
@@ -226,6 +308,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
       }
     }
   }
+  if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
 
   float vals[14];
 #pragma unroll
@@ -320,13 +403,15 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
   }
 }
 
-template <int PX, int FB>
+template <int PX, int FB, bool ASYNC>
 __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   const uint32_t total = a.vt->total_tiles;
-  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX, FB>(a, gt);
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX, FB, ASYNC>(a, gt);
 }
 
-template <int BATCH, bool DET, int PX>
+// ASYNC: the splat records of round i + 1 are copied with cp.async while round i is
+// differentiated (as in the forward).
+template <int BATCH, bool DET, int PX, bool ASYNC>
 __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt) {
   constexpr bool ABS = DET;  // the |dL/dmean2d| sums (see the top of the file)
   using L = TileLayout<PX>;
@@ -334,6 +419,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   __shared__ float4 s_a[BATCH];
   __shared__ float4 s_b[BATCH];
   __shared__ float4 s_c[BATCH];  // staged splats (stage_splat): s_a, s_b, s_c
+  __shared__ RawRound<ASYNC ? BATCH : 1> s_raw[ASYNC ? 2 : 1];
   __shared__ uint32_t s_dst[BATCH];
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
@@ -379,18 +465,62 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   const uint32_t wlast = __reduce_max_sync(0xffffffffu, my_last);
   const float block_h = float(4 * PX);
 
+  // ASYNC: this thread's slot of the round in flight (cur) and of the next one (nxt): the
+  // gaussian, and in deterministic mode the pair's pre-sort index (its gradient's place).
+  const bool stager = lid < uint32_t(BATCH);
+  uint32_t g_cur = 0u, pre_cur = 0u, g_nxt = 0u, pre_nxt = 0u, buf = 0u;
+  if constexpr (ASYNC) {
+    if (stager && lid < n) {
+      g_cur = a.rb.gauss[range.x + lid];
+      if (DET) pre_cur = a.rb.values[range.x + lid];
+      fetch_record_async(&s_raw[0].q[0][lid], &s_raw[0].q[1][lid], &s_raw[0].q[2][lid], &s_raw[0].q[3][lid], a.splat,
+                         a.foot, g_cur);
+    }
+    copy_async_commit();
+    if (stager && uint32_t(BATCH) + lid < n) {
+      g_nxt = a.rb.gauss[range.x + uint32_t(BATCH) + lid];
+      if (DET) pre_nxt = a.rb.values[range.x + uint32_t(BATCH) + lid];
+    }
+  }
   for (uint32_t start = 0; start < n; start += BATCH) {
     __syncthreads();
-    if (lid < uint32_t(BATCH) && start + lid < n) {
-      const uint32_t pre = a.rb.values[range.x + start + lid];
-      const uint32_t g = a.rb.pair_gaussian[pre];
+    if constexpr (ASYNC) {
+      // Round i + 1 into the other buffer (free: every warp has passed the barrier above),
+      // the round after it's indices, then round i's own copy, staged by this thread.
+      const bool next = stager && start + uint32_t(BATCH) + lid < n;
+      if (next)
+        fetch_record_async(&s_raw[buf ^ 1u].q[0][lid], &s_raw[buf ^ 1u].q[1][lid], &s_raw[buf ^ 1u].q[2][lid],
+                           &s_raw[buf ^ 1u].q[3][lid], a.splat, a.foot, g_nxt);
+      copy_async_commit();
+      uint32_t g_after = 0u, pre_after = 0u;
+      if (stager && start + 2u * uint32_t(BATCH) + lid < n) {
+        g_after = a.rb.gauss[range.x + start + 2u * uint32_t(BATCH) + lid];
+        if (DET) pre_after = a.rb.values[range.x + start + 2u * uint32_t(BATCH) + lid];
+      }
+      copy_async_wait<1>();
+      if (stager && start + lid < n) {
+        float4 A, B, C;
+        stage_splat(s_raw[buf].q[0][lid], s_raw[buf].q[1][lid], s_raw[buf].q[2][lid], s_raw[buf].q[3][lid].w, A, B, C);
+        s_a[lid] = A;
+        s_b[lid] = B;
+        s_c[lid] = C;
+        s_dst[lid] = DET ? pre_cur : g_cur;
+      }
+      g_cur = g_nxt;
+      pre_cur = pre_nxt;
+      g_nxt = g_after;
+      pre_nxt = pre_after;
+      buf ^= 1u;
+    } else if (stager && start + lid < n) {
+      const uint32_t k = range.x + start + lid;
+      const uint32_t g = a.rb.gauss[k];
       const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
       float4 A, B, C;
       stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
       s_a[lid] = A;
       s_b[lid] = B;
       s_c[lid] = C;
-      s_dst[lid] = DET ? pre : g;
+      s_dst[lid] = DET ? a.rb.values[k] : g;
     }
     __syncthreads();
     const uint32_t nb = min(uint32_t(BATCH), n - start);
@@ -530,16 +660,18 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
       }
     }
   }
+  if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
 }
 
 // 3 PX blocks of 256 / PX threads per SM: 12 two-warp blocks at 4 pixels per thread (at
 // most 85 registers; with no bound the compiler settled on 72 with spills, measured 1%
 // slower, and a 64-register cap 18% slower).
-template <int BATCH, bool DET, int PX>
+template <int BATCH, bool DET, int PX, bool ASYNC>
 __global__ void __launch_bounds__(256 / PX, 3 * PX) k_raster_bwd(RasterArgs a) {
   if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
   const uint32_t total = a.vt->total_tiles;
-  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_bwd_tile<BATCH, DET, PX>(a, gt);
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue))
+    raster_bwd_tile<BATCH, DET, PX, ASYNC>(a, gt);
 }
 
 // A persistent grid: as many blocks as fit on the GPU at once (at most one per tile).
@@ -551,65 +683,77 @@ uint32_t persistent_grid(Kernel kernel, int threads, const StepPointers& sp) {
   return min(sp.tile_cap, uint32_t(per_sm) * uint32_t(sp.sm_count));
 }
 
-template <int BATCH, bool DET, int PX>
+template <int BATCH, bool DET, int PX, bool ASYNC>
 void launch_bwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_bwd<BATCH, DET, PX>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_bwd<BATCH, DET, PX, ASYNC>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_bwd<BATCH, DET, PX><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_bwd<BATCH, DET, PX, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
+}
+
+template <int BATCH, bool DET, bool ASYNC>
+void launch_bwd_px(const RasterArgs& a, const StepPointers& sp, int px, cudaStream_t st) {
+  if (px >= 4) launch_bwd<BATCH, DET, 4, ASYNC>(a, sp, st);
+  else if (px == 2) launch_bwd<BATCH, DET, 2, ASYNC>(a, sp, st);
+  else launch_bwd<BATCH, DET, 1, ASYNC>(a, sp, st);
 }
 
 template <int BATCH>
-void launch_bwd_batch(const RasterArgs& a, const StepPointers& sp, bool deterministic, int px, cudaStream_t st) {
+void launch_bwd_batch(const RasterArgs& a, const StepPointers& sp, bool deterministic, int px, bool async,
+                      cudaStream_t st) {
   if (deterministic) {
-    if (px >= 4) launch_bwd<BATCH, true, 4>(a, sp, st);
-    else if (px == 2) launch_bwd<BATCH, true, 2>(a, sp, st);
-    else launch_bwd<BATCH, true, 1>(a, sp, st);
+    if (async) launch_bwd_px<BATCH, true, true>(a, sp, px, st);
+    else launch_bwd_px<BATCH, true, false>(a, sp, px, st);
   } else {
-    if (px >= 4) launch_bwd<BATCH, false, 4>(a, sp, st);
-    else if (px == 2) launch_bwd<BATCH, false, 2>(a, sp, st);
-    else launch_bwd<BATCH, false, 1>(a, sp, st);
+    if (async) launch_bwd_px<BATCH, false, true>(a, sp, px, st);
+    else launch_bwd_px<BATCH, false, false>(a, sp, px, st);
   }
 }
 
-template <int PX, int FB>
+template <int PX, int FB, bool ASYNC>
 void launch_fwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_fwd<PX, FB>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_fwd<PX, FB, ASYNC>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_fwd<PX, FB><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_fwd<PX, FB, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
+}
+
+template <int PX, bool ASYNC>
+void launch_fwd_batch(const RasterArgs& a, const StepPointers& sp, int batch, cudaStream_t st) {
+  if (batch >= 256) launch_fwd<PX, 256, ASYNC>(a, sp, st);
+  else if (batch >= 128) launch_fwd<PX, 128, ASYNC>(a, sp, st);
+  else launch_fwd<PX, 64, ASYNC>(a, sp, st);
 }
 
 template <int PX>
-void launch_fwd_batch(const RasterArgs& a, const StepPointers& sp, int batch, cudaStream_t st) {
-  if (batch >= 256) launch_fwd<PX, 256>(a, sp, st);
-  else if (batch >= 128) launch_fwd<PX, 128>(a, sp, st);
-  else launch_fwd<PX, 64>(a, sp, st);
+void launch_fwd_mode(const RasterArgs& a, const StepPointers& sp, int batch, bool async, cudaStream_t st) {
+  if (async) launch_fwd_batch<PX, true>(a, sp, batch, st);
+  else launch_fwd_batch<PX, false>(a, sp, batch, st);
 }
 
 }  // namespace
 
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
-                           cudaStream_t st) {
+                           bool async, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u};
-  if (px >= 4) launch_fwd_batch<4>(a, sp, batch, st);
-  else if (px == 2) launch_fwd_batch<2>(a, sp, batch, st);
-  else launch_fwd_batch<1>(a, sp, batch, st);
+  if (px >= 4) launch_fwd_mode<4>(a, sp, batch, async, st);
+  else if (px == 2) launch_fwd_mode<2>(a, sp, batch, async, st);
+  else launch_fwd_mode<1>(a, sp, batch, async, st);
 }
 
 void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb,
-                            float4* pair_grads, bool deterministic, int px, int batch, const uint32_t* d_pairs,
-                            uint32_t accept, cudaStream_t st) {
+                            float4* pair_grads, bool deterministic, int px, int batch, bool async,
+                            const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueBackward, rb, vb.splat, vb.foot,
                reinterpret_cast<float*>(pair_grads), reinterpret_cast<float*>(vb.grad2d), d_pairs, accept};
-  if (batch >= 64) launch_bwd_batch<64>(a, sp, deterministic, px, st);
-  else launch_bwd_batch<32>(a, sp, deterministic, px, st);
+  if (batch >= 64) launch_bwd_batch<64>(a, sp, deterministic, px, async, st);
+  else launch_bwd_batch<32>(a, sp, deterministic, px, async, st);
 }
 
 }  // namespace gsk

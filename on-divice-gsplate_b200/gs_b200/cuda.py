@@ -51,7 +51,8 @@ class Tuning(ctypes.Structure):
                 ("deterministic", ctypes.c_uint32), ("forward_pixels", ctypes.c_uint32),
                 ("backward_pixels", ctypes.c_uint32), ("retry", ctypes.c_uint32), ("graph", ctypes.c_uint32),
                 ("backward_batch", ctypes.c_uint32), ("sort_digit_bits", ctypes.c_uint32),
-                ("forward_batch", ctypes.c_uint32), ("tune_reduction", ctypes.c_uint32)]
+                ("forward_batch", ctypes.c_uint32), ("tune_reduction", ctypes.c_uint32),
+                ("stage_async", ctypes.c_uint32)]
 
 
 class ModelInfo(ctypes.Structure):

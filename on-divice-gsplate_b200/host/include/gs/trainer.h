@@ -171,7 +171,7 @@ struct TrainStats {
 
 struct RetuneResult {
   uint32_t step = 0;
-  std::string chosen;  // "fpx=2 fbatch=256 bpx=4 batch=64 digits=8 deterministic"
+  std::string chosen;  // "fpx=2 fbatch=256 bpx=4 batch=64 digits=8 sync deterministic"
 };
 
 struct EvalResult {
@@ -267,12 +267,12 @@ class Trainer {
   };
   DebugSnapshot debug_snapshot();
   uint32_t sh_stride() const { return sh_stride_; }
-  // The tuning in use ("fpx=2 fbatch=256 bpx=4 batch=64 digits=8 deterministic"), in place of the
+  // The tuning in use ("fpx=2 fbatch=256 bpx=4 batch=64 digits=8 sync deterministic"), in place of the
   // reference's backward-variant name.
   std::string reduction() const;
   // Testing: runs the backward (and the passes it shares knobs with) under the tuning
   // `name` names, in reduction()'s form: any of fpx=1|2|4, fbatch=64|128|256, bpx=1|2|4,
-  // batch=32|64, digits=4..8 and deterministic|atomic, the others kept (trainer.h:324 picks a backward
+  // batch=32|64, digits=4..8, sync|async and deterministic|atomic, the others kept (trainer.h:324 picks a backward
   // variant by name). False, and nothing changed, for a name it cannot parse.
   bool select_backward(const std::string& name);
   const std::vector<RetuneResult>& retunes() const { return retunes_; }

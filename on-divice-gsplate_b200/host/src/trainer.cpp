@@ -161,7 +161,8 @@ std::string Trainer::reduction() const {
   if (gs_get_tuning(gpu_, &t) != GS_OK) return "unknown";
   return "fpx=" + std::to_string(t.forward_pixels) + " fbatch=" + std::to_string(t.forward_batch) +
          " bpx=" + std::to_string(t.backward_pixels) + " batch=" + std::to_string(t.backward_batch) +
-         " digits=" + std::to_string(t.sort_digit_bits) + (t.deterministic ? " deterministic" : " atomic");
+         " digits=" + std::to_string(t.sort_digit_bits) + (t.stage_async ? " async" : " sync") +
+         (t.deterministic ? " deterministic" : " atomic");
 }
 
 bool Trainer::select_backward(const std::string& name) {
@@ -175,6 +176,10 @@ bool Trainer::select_backward(const std::string& name) {
     if (word.empty()) continue;
     if (word == "deterministic" || word == "atomic") {
       t.deterministic = word == "deterministic" ? 1u : 0u;
+      continue;
+    }
+    if (word == "async" || word == "sync") {
+      t.stage_async = word == "async" ? 1u : 0u;
       continue;
     }
     const size_t eq = word.find('=');
@@ -489,9 +494,13 @@ Trainer::DebugSnapshot Trainer::debug_snapshot() {
   fetch(GS_SNAP_PROJECTED, d.projected);
   fetch(GS_SNAP_TILES, d.tiles);
   fetch(GS_SNAP_OFFSETS, d.offsets);
-  if (options_.deterministic) fetch(GS_SNAP_PAIR_GRADS, d.pair_grads);
-  fetch(GS_SNAP_PAIR_TILE, d.pair_tile);
-  fetch(GS_SNAP_RENDER_ORDER, d.render_order);
+  gs_tuning t;
+  check(gs_get_tuning(gpu_, &t), "Trainer::debug_snapshot");
+  if (t.deterministic) {  // an atomic training step keeps neither per-pair gradients nor pair indices
+    fetch(GS_SNAP_PAIR_GRADS, d.pair_grads);
+    fetch(GS_SNAP_PAIR_TILE, d.pair_tile);
+    fetch(GS_SNAP_RENDER_ORDER, d.render_order);
+  }
   fetch(GS_SNAP_DEPTH_KEY, d.depth_key);
   return d;
 }

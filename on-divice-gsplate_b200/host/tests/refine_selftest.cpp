@@ -505,10 +505,10 @@ int variants() {
   const gs::SplatScene scene = test_scene(200, 2, 11);
   const float bg[3] = {0.2f, 0.5f, 0.7f};
   gs::TrainOptions o = frozen_options(2, true);
-  const char* names[] = {"fpx=2 fbatch=256 bpx=4 batch=64 digits=8 deterministic",
-                         "fpx=1 fbatch=64 bpx=1 batch=32 digits=4 deterministic",
-                         "fpx=4 fbatch=128 bpx=2 batch=64 digits=6 deterministic",
-                         "fpx=2 fbatch=256 bpx=4 batch=32 digits=7 atomic"};
+  const char* names[] = {"fpx=2 fbatch=256 bpx=4 batch=64 digits=8 sync deterministic",
+                         "fpx=1 fbatch=64 bpx=1 batch=32 digits=4 async deterministic",
+                         "fpx=4 fbatch=128 bpx=2 batch=64 digits=6 async deterministic",
+                         "fpx=2 fbatch=256 bpx=4 batch=32 digits=7 async atomic"};
   std::vector<float> ref;
   double worst = 0.0;
   bool ok = true;

@@ -97,10 +97,69 @@ def test_tunings_compute_the_same_gradients(ctx):
 
     ref16, refsh = grads(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8)
     for kw in (dict(forward_pixels=1), dict(forward_pixels=4), dict(backward_pixels=2, backward_batch=32),
-               dict(backward_pixels=1, backward_batch=64), dict(sort_digit_bits=5)):
-        base = dict(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8)
+               dict(backward_pixels=1, backward_batch=64), dict(sort_digit_bits=5), dict(forward_batch=64),
+               dict(forward_batch=128, forward_pixels=4), dict(stage_async=1), dict(stage_async=1, forward_batch=128),
+               dict(stage_async=1, backward_pixels=2, backward_batch=32), dict(deterministic=0),
+               dict(deterministic=0, stage_async=1, backward_pixels=1, backward_batch=32)):
+        base = dict(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8, forward_batch=256,
+                    stage_async=0, deterministic=1)
         base.update(kw)
         g16, gsh = grads(**base)
         assert rel_l2(g16, ref16) < 1e-5, kw
         assert rel_l2(gsh, refsh) < 1e-5, kw
-    ctx.set_tuning(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8)
+    ctx.set_tuning(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8, forward_batch=256,
+                   stage_async=0, deterministic=1)
+
+
+def test_async_staging_is_bit_identical(ctx):
+    """Copying the next round of splats with cp.async while the current one is used changes
+    when the records arrive, not what is computed: the forward's outputs, the per-pair
+    gradients and the moments equal the plain-load staging bit for bit, at every forward
+    batch and both backward batches (the batch changes how a tile's list is cut into rounds,
+    not the order or the sums), on a view whose tiles hold several rounds of splats."""
+    scene, cam, opt, target = view_and_target(n=60000)
+    frozen = F.frozen_options(1, False)
+    frozen.lambda_dssim, frozen.lambda_dssim_end = 0.2, -1.0
+    fr = frame_for(scene, cam, frozen, (0.1, 0.2, 0.3))
+    outs = {}
+    for fb, bb, stage in ((256, 64, 0), (256, 64, 1), (128, 32, 1), (64, 64, 1)):
+        ctx.set_tuning(forward_batch=fb, backward_batch=bb, stage_async=stage, deterministic=1)
+        ctx.model_init(scene.params, scene.sh)
+        ctx.set_views([fr], [target])
+        ctx.step(train=True)
+        outs[(fb, bb, stage)] = {k: ctx.snapshot(k) for k in ("pixel_count", "pixel_out", "pixel_grad", "pair_grads")}
+        outs[(fb, bb, stage)]["m"] = ctx.moments()["m"]
+    ref = outs[(256, 64, 0)]
+    assert (ref["pixel_count"] > 256).any()  # tiles with more than one forward round
+    for key, got in outs.items():
+        for k in ref:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} {key}")
+    ctx.set_tuning(forward_batch=256, backward_batch=64, stage_async=0, deterministic=1)
+
+
+def test_atomic_steps_sort_gaussians(ctx):
+    """An atomic training step sorts each pair's gaussian (no pre-sort index): the pair-order
+    snapshots are refused with a message, the tile ranges and gradients are those of the
+    deterministic step, and a forward-only step afterwards has the pair order again."""
+    from gs_b200.cuda import GsError
+
+    scene, cam, opt, target = view_and_target()
+    frozen = F.frozen_options(1, False)
+    fr = frame_for(scene, cam, frozen, (0, 0, 0))
+    ctx.set_tuning(deterministic=1)
+    ctx.model_init(scene.params, scene.sh)
+    ctx.set_views([fr], [target])
+    ctx.step(train=True)
+    ref_ranges, ref_g = ctx.snapshot("ranges"), ctx.first_step_gradients()[0]
+    ref_order = ctx.snapshot("render_order")
+    ctx.set_tuning(deterministic=0)
+    ctx.model_init(scene.params, scene.sh)
+    ctx.set_views([fr], [target])
+    ctx.step(train=True)
+    np.testing.assert_array_equal(ctx.snapshot("ranges"), ref_ranges)
+    assert rel_l2(ctx.first_step_gradients()[0], ref_g) < 1e-5
+    with pytest.raises(GsError, match="atomic training step"):
+        ctx.snapshot("render_order")
+    ctx.step(train=False)
+    np.testing.assert_array_equal(ctx.snapshot("render_order"), ref_order)
+    ctx.set_tuning(deterministic=1)
