@@ -17,9 +17,9 @@ Adam on every parameter. Views are drawn in shuffled epochs over the 200 cameras
 - roofline: the dominant pass of the batched step, timed by pass events recorded inside
   the replayed graph. Raster passes are issue-bound, so their roofline is the FP32 pipe
   (128 lane operations per clock per SM at the sampled clock) over the work of the step's
-  pixel-pair evaluations E (FP32_PER_EVALUATION), with the special-function unit's share
-  beside it; every pass also reports HBM GB/s from fixed per-unit bytes
-  (algorithmic_bytes) against the measured copy bandwidth.
+  blending evaluations C (FP32_PER_EVALUATION each; counted by one untimed counting
+  forward), with the special-function unit's share beside it; every pass also reports HBM
+  GB/s from fixed per-unit bytes (algorithmic_bytes) against the measured copy bandwidth.
 - cpu_baseline: the CPU oracle (a multithreaded restatement of the reference's passes) on
   plain steps of the same workload, host cores, bounded time.
 Inputs (732 MB of parameters and moments, 1.66 GB of targets) exceed the 126 MB L2, so no
@@ -172,13 +172,16 @@ def algorithmic_bytes(pass_name: str, n: int, views: int, pairs: int, pixels: in
     return 0.0
 
 
-# Work per pixel-pair evaluation of the raster passes (E = the sum over pixels of the last
-# contributor's position in its tile's list): special-function (MUFU) operations (the
+# Work per blending evaluation of the raster passes (a pixel-splat pair with alpha >= 1/255
+# in front of the pixel's stop: the evaluations whose arithmetic reaches the output; C,
+# counted by the library's counting forward): special-function (MUFU) operations (the
 # forward's exponential; the backward's exponential and its reciprocal of 1 - alpha) and
 # FP32 operations (an FMA counts as one). The backward's 60 FP32 operations are the path's
 # byte-and-work model; the forward's 15 are its exponent (3), alpha and the skip tests (4),
 # transmittance (2) and colour accumulation (6). B200 issues 16 MUFU and 128 FP32 lane
-# operations per clock per SM, so at these counts the FP32 pipe bounds both passes.
+# operations per clock per SM, so at these counts the FP32 pipe bounds both passes. E (the
+# sum over pixels of the last contributor's position in its tile's list) counts every pair
+# up to the stop, blending or not, and is reported beside C.
 MUFU_PER_EVALUATION = {"rasterize": 1, "backward": 2}
 FP32_PER_EVALUATION = {"rasterize": 15, "backward": 60}
 MUFU_PER_CLOCK_PER_SM = 16
@@ -398,13 +401,14 @@ def main() -> None:
         print(json.dumps({"mode": "batched", "views_per_s": VIEWS_PER_STEP * 1000.0 * args.steps / gpu_ms}), flush=True)
         ctx.close()
         return
-    # Device time per pass: the mean over the timed steps. The pixel-pair evaluations of the
-    # last timed step (the sum over its pixels of the last contributor's position in the
-    # tile's list: the forward's own count; the backward walks the same) go with that step's
-    # own pass times.
+    # Device time per pass: the mean over the timed steps. The evaluations of a step: one
+    # untimed counting forward on the next view set (no graph, not trained on).
     passes = {name: float(np.mean([p[k] for p in step_passes])) for k, name in enumerate(PASSES)}
-    last_passes = {name: step_passes[-1][k] for k, name in enumerate(PASSES)}
+    idx = order.next(VIEWS_PER_STEP)
+    ctx.set_views_dataset([frame(scene, cams[i], opt, step) for i in idx], idx)
+    ctx.step(False, count=True)
     evaluations = sum(int(ctx.snapshot("pixel_count", v).astype(np.int64).sum()) for v in range(VIEWS_PER_STEP))
+    blending = int(ctx.snapshot("contributions")[0])
 
     # End to end: the caller's photos sit in pinned host memory; each step uploads its 8
     # targets (gs_set_views) and reads the loss sums back.
@@ -457,8 +461,8 @@ def main() -> None:
             gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
             entry = {"ms": round(ms, 4), "gbs": round(gbs, 1) if gbs else None,
                      "hbm_frac": round(gbs / pk["hbm_gbs"], 4) if gbs else None}
-            if name in MUFU_PER_EVALUATION and last_passes[name] > 0:
-                per_s = evaluations / (last_passes[name] * 1e-3) / 1e9
+            if name in MUFU_PER_EVALUATION and ms > 0:
+                per_s = blending / (ms * 1e-3) / 1e9
                 mufu, fp32 = per_s * MUFU_PER_EVALUATION[name], per_s * FP32_PER_EVALUATION[name]
                 entry.update({"evaluations_g_per_s": round(per_s, 2), "mufu_gops": round(mufu, 1),
                               "mufu_frac": round(mufu / mufu_peak, 4), "fp32_gops": round(fp32, 1),
@@ -469,8 +473,8 @@ def main() -> None:
         d = per_pass[dom]
         if "fp32_gops" in d:
             roof = {"bound": "fp32", "kernel": dom, "achieved": d["fp32_gops"], "peak": round(fp32_peak, 1),
-                    "unit": "Gop/s", "frac": d["fp32_frac"], "evaluations_per_step": evaluations,
-                    "fp32_per_evaluation": FP32_PER_EVALUATION[dom],
+                    "unit": "Gop/s", "frac": d["fp32_frac"], "blending_evaluations_per_step": blending,
+                    "evaluations_per_step": evaluations, "fp32_per_evaluation": FP32_PER_EVALUATION[dom],
                     "sfu": {"achieved": d["mufu_gops"], "peak": round(mufu_peak, 1), "unit": "Gop/s",
                             "frac": d["mufu_frac"], "per_evaluation": MUFU_PER_EVALUATION[dom]},
                     "hbm": {"achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": d["hbm_frac"]}}
@@ -478,8 +482,8 @@ def main() -> None:
             roof = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "frac": d["hbm_frac"]}
         roof.update({"traffic": traffic, "peak_source": pk["source"], "per_pass": per_pass,
-                     "passes_from": "pass events inside the replayed graph, mean over the timed steps; the "
-                                    "SFU figures pair the last timed step's evaluations with its own pass times"})
+                     "passes_from": "pass events inside the replayed graph, mean over the timed steps; "
+                                    "evaluations from one counting forward on the next view set"})
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "views/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,

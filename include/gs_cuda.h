@@ -133,7 +133,9 @@ typedef enum gs_snapshot_kind {
   GS_SNAP_PAIR_GAUSSIAN = 14, /* uint32 per pair, pre-sort order: the slot */
   GS_SNAP_PIXEL_OUT = 15,     /* 4 floats per pixel: rendered rgb over the background, loss weight */
   GS_SNAP_SPAWN = 16,         /* uint32 per slot after gs_densify: 0 none, 1 clone, 2 split */
-  GS_SNAP_MOTION_BIND = 17    /* 8 uint32 per slot: 4 motion nodes, their 4 weights (float bits) */
+  GS_SNAP_MOTION_BIND = 17,   /* 8 uint32 per slot: 4 motion nodes, their 4 weights (float bits) */
+  GS_SNAP_CONTRIBUTIONS = 18  /* one uint64 (view 0): the pixel-splat evaluations that blended in the
+                                 latest GS_STEP_COUNT step, all its views together */
 } gs_snapshot_kind;
 
 /* Tuning knobs (Trainer options that shape buffers and kernels; trainer.h:150-165). */
@@ -200,6 +202,8 @@ int gs_set_views_dataset(gs_context* ctx, uint32_t n_views, const gs_frame_data*
 
 #define GS_STEP_TRAIN 1u   /* backward pass and Adam (else: forward and loss only) */
 #define GS_STEP_PROFILE 2u /* time each pass with CUDA events (pass_ms) */
+#define GS_STEP_COUNT 4u   /* count the evaluations that blend (GS_SNAP_CONTRIBUTIONS); runs without
+                              the step's graph, so time no step that counts */
 
 /* One step over the views set by gs_set_views: project -> key build + sort -> tile ranges
    -> rasterise -> L1 + SSIM -> backward -> Adam (trainer.cpp:825-831). With more than one

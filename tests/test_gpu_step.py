@@ -17,8 +17,11 @@ Tolerances:
   2^-20 covers sqrt (2^-23, halved through the quotient's denominator), the division
   (2 x 2^-24), the product with lr and one contraction, with margin.
 - Against the oracle's own gradients (which differ by summation order, within 1e-3 relative
-  L2 per group): moments, parameter updates and statistics within 1e-3 relative L2 per group
-  (v within 2e-3: it is quadratic in g); view counts exact on all but 1e-4 of the slots (a
+  L2 per group): moments and statistics within 1e-3 relative L2 per group (v within 2e-3:
+  it is quadratic in g); parameter updates within 2e-3, because Adam gives every element a
+  step of about lr whatever its gradient's size, so the elements with small gradients (and
+  the largest relative summation error) weigh as much in the update's L2 norm as the large
+  ones; view counts exact on all but 1e-4 of the slots (a
   slot at the edge of a view can gain or lose its last tile through a float of the
   projection); radii within 1e-5 relative.
 """
@@ -159,17 +162,17 @@ def test_first_step_moments_and_update_match_oracle(stepped):
 
 
 def test_second_step_matches_oracle(stepped):
-    """Step 1 from the GPU's state after step 0, on both sides: parameter updates, moments
-    and SH per group within 1e-3 relative L2 (v 2e-3)."""
+    """Step 1 from the GPU's state after step 0, on both sides: moments per group within
+    1e-3 relative L2 (v 2e-3), parameter and SH updates within 2e-3."""
     _, _, (_, s1, s2), model, _ = stepped
     n = s1["params"].shape[0]
     for name, cols in GROUPS.items():
         d_gpu = (s2["params"] - s1["params"])[:, cols]
         d_ref = (model.params[:n] - s1["params"])[:, cols]
-        assert rel_l2(d_gpu, d_ref) < 1e-3, name
+        assert rel_l2(d_gpu, d_ref) < 2e-3, name
         assert rel_l2(s2["m"][:, cols], model.m[:n, cols]) < 1e-3, name
         assert rel_l2(s2["v"][:, cols], model.v[:n, cols]) < 2e-3, name
-    assert rel_l2(s2["sh"] - s1["sh"], model.sh[:n] - s1["sh"]) < 1e-3
+    assert rel_l2(s2["sh"] - s1["sh"], model.sh[:n] - s1["sh"]) < 2e-3
     assert rel_l2(s2["m_sh"], model.m_sh[:n]) < 1e-3
     assert rel_l2(s2["v_sh"], model.v_sh[:n]) < 2e-3
 

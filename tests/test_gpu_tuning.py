@@ -163,3 +163,29 @@ def test_atomic_steps_sort_gaussians(ctx):
     ctx.step(train=False)
     np.testing.assert_array_equal(ctx.snapshot("render_order"), ref_order)
     ctx.set_tuning(deterministic=1)
+
+
+def test_counting_forward(ctx):
+    """GS_STEP_COUNT: the counting forward renders exactly what the plain one does, and its
+    count of blending evaluations is the same at every pixels-per-thread setting, positive
+    and below E (the sum of every pixel's last-contributor position, which also counts the
+    pairs a pixel skips)."""
+    scene, cam, opt, target = view_and_target()
+    frozen = F.frozen_options(1, False)
+    fr = frame_for(scene, cam, frozen, (0, 0, 0))
+    ctx.model_init(scene.params, scene.sh)
+    ctx.set_views([fr], [target])
+    ctx.step(train=False)
+    plain = {k: ctx.snapshot(k) for k in ("pixel_count", "pixel_out", "image")}
+    counts = []
+    for px in (1, 2, 4):
+        ctx.set_tuning(forward_pixels=px)
+        ctx.step(train=False, count=True)
+        for k in plain:
+            np.testing.assert_array_equal(ctx.snapshot(k), plain[k], err_msg=f"{k} at {px} pixels per thread")
+        counts.append(int(ctx.snapshot("contributions")[0]))
+    ctx.set_tuning(forward_pixels=2)
+    E = int(plain["pixel_count"].astype(np.int64).sum())
+    assert counts[0] == counts[1] == counts[2] and 0 < counts[0] < E, (counts, E)
+    # Every pixel with a last contributor blended at least once.
+    assert counts[0] >= int((plain["pixel_count"] > 0).sum())
