@@ -6,7 +6,10 @@ libgs_host hands JPEG files to nvJPEG. A capture of JPEG frames (baseline 4:4:4,
 independent decoder's output (Pillow's libjpeg). JPEG leaves decoders free in their inverse
 DCT's rounding and in how they upsample subsampled chroma (libjpeg interpolates, others
 replicate), so the check is on luma, which is never subsampled: mean difference under one
-level and at most 6 levels anywhere; and, for 4:4:4, RGB within a mean of one level.
+level and 99% of the pixels within 3 levels (luma computed from RGB also moves where a
+decoder's chroma pushes a saturated colour past 0 or 255 and it is clipped: a few pixels
+on the edge of the test image's disc); and, for 4:4:4, RGB within a mean of one level and 6
+levels everywhere.
 """
 import io
 import json
@@ -58,7 +61,7 @@ def test_jpeg_frames_decode_on_the_gpu(tmp_path, kind):
     assert (got[..., 3] == 255).all()
     luma = np.array([0.299, 0.587, 0.114])
     dy = np.abs(got[..., :3].astype(np.float64) @ luma - decoded[0].astype(np.float64) @ luma)
-    assert dy.mean() < 1.0 and dy.max() <= 6.0, (dy.mean(), dy.max())
+    assert dy.mean() < 1.0 and np.quantile(dy, 0.99) <= 3.0, (dy.mean(), np.quantile(dy, 0.99))
     if kind == "444":
         diff = np.abs(got[..., :3].astype(int) - decoded[0].astype(int))
         assert diff.mean() < 1.0 and diff.max() <= 6, (diff.mean(), diff.max())
