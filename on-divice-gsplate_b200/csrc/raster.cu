@@ -278,26 +278,20 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
 #pragma unroll
     for (int w = 0; w < FB / 32; ++w) {
       uint32_t m = masks[w];
-      while (m != 0u) {  // warp-uniform: the lanes stay converged for the votes below
-        if (__all_sync(0xffffffffu, all_done)) break;
+      while (m != 0u && !all_done) {
         const uint32_t j = uint32_t(w) * 32u + uint32_t(__ffs(m) - 1);
         m &= m - 1u;
         const uint32_t contributor = base + j + 1u;
         const float4 A = s_a[j];
         const float4 B = s_b[j];
-        const float2 bl = *reinterpret_cast<const float2*>(&s_c[j]);  // blue, exponent bound
-        const float blue = bl.x;
+        const float blue = s_c[j].x;
         const float dx = __fsub_rn(A.x, cx);
         const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
         all_done = true;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
-          // Row group p of the warp's block (8 x 4 pixels): where no lane's pixel is both
-          // still open and inside the splat's conservative exponent bound, no pixel can
-          // blend, and the whole warp skips the rest of the evaluation.
-          const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
-          const bool open = !done[p] && e >= bl.y;
-          if (__any_sync(0xffffffffu, open) && open) {
+          if (!done[p]) {
+            const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
             const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
             if (e <= 0.0f && alpha >= kMinAlpha) {
               const float next_T = __fmul_rn(T[p], __fsub_rn(1.0f, alpha));
@@ -553,8 +547,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
         const float4 A = s_a[j];
         const float4 B = s_b[j];
-        const float2 bl = *reinterpret_cast<const float2*>(&s_c[j]);  // blue, exponent bound
-        const float blue = bl.x;
+        const float blue = s_c[j].x;
         const float dx = __fsub_rn(A.x, cx);
         const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
         // The conic (a, b, c) back from the scaled exponent terms, for the mean gradient:
@@ -571,13 +564,9 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         bool has = false;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
-          // Row group p (8 x 4 pixels): skipped by the whole warp where no lane's pixel is in
-          // front of its stop and inside the splat's conservative exponent bound (as in the
-          // forward; such a pixel cannot blend).
+          if (pos > last[p]) continue;
           const float dy = __fsub_rn(A.y, cy[p]);
           const float e = splat_exponent(e0, e1, B.y, dy);
-          const bool open = pos <= last[p] && e >= bl.y;
-          if (!__any_sync(0xffffffffu, open) || !open) continue;
           const float G = exp2_approx(e);
           const float raw = __fmul_rn(A.z, G);
           const float alpha = fminf(kMaxAlpha, raw);

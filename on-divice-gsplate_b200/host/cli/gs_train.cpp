@@ -217,7 +217,11 @@ int main(int argc, char** argv) {
     gs::Trainer trainer(ctx, std::move(dataset), init, options);
     if (options.refine_motion)
       std::printf("motion: %zu nodes from step %u\n", trainer.motion_nodes().size(), options.motion_from);
-    std::vector<std::pair<uint32_t, double>> evals;
+    struct Eval {
+      uint32_t step;
+      double psnr, train_seconds;  // training time up to this evaluation (evaluations excluded)
+    };
+    std::vector<Eval> evals;
     double train_s = 0.0;
     while (!trainer.finished()) {
       const uint32_t chunk = std::min(eval_every > 0 ? eval_every : iterations, iterations - trainer.stats().step);
@@ -245,7 +249,7 @@ int main(int argc, char** argv) {
         const gs::EvalResult r = trainer.evaluate_at_rest(rest);
         std::printf("  at rest: held-out PSNR %.2f dB, SSIM %.4f over %u views\n", r.psnr, r.ssim, r.views);
       }
-      evals.push_back({s.step, e.psnr});
+      evals.push_back({s.step, e.psnr, train_s});
     }
     const gs::TrainStats& s = trainer.stats();
     const double views_per_s = double(s.views) / train_s;
@@ -304,12 +308,13 @@ int main(int argc, char** argv) {
       j << "{\"dataset\": \"" << source << "\", \"iterations\": " << s.step
         << ", \"views_per_step\": " << options.views_per_step << ", \"views\": " << s.views
         << ", \"train_seconds\": " << train_s << ", \"views_per_s\": " << views_per_s
-        << ", \"final_psnr\": " << (evals.empty() ? 0.0 : evals.back().second) << ", \"gaussians\": " << s.gaussians
+        << ", \"final_psnr\": " << (evals.empty() ? 0.0 : evals.back().psnr) << ", \"gaussians\": " << s.gaussians
         << ", \"spawned\": " << s.spawned << ", \"pruned\": " << s.pruned
         << ", \"overflow_steps\": " << s.overflow_steps << ", \"tuning\": \"" << trainer.reduction()
         << "\", \"eval\": [";
       for (size_t k = 0; k < evals.size(); ++k)
-        j << (k ? ", " : "") << "{\"step\": " << evals[k].first << ", \"psnr\": " << evals[k].second << "}";
+        j << (k ? ", " : "") << "{\"step\": " << evals[k].step << ", \"psnr\": " << evals[k].psnr
+          << ", \"train_seconds\": " << evals[k].train_seconds << "}";
       j << "]}\n";
     }
   } catch (const std::exception& e) {
