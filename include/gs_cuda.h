@@ -144,7 +144,9 @@ typedef struct gs_tuning {
   uint64_t initial_pairs;     /* pairs to allocate before the first count (0: 4 per slot and view) */
   uint32_t deterministic;     /* 1: per-pair gradients + fixed-order sum (bit-stable); 0: atomics */
   uint32_t forward_pixels;    /* pixels per thread in the forward pass: 1, 2 or 4 (0: default) */
-  uint32_t backward_pixels;   /* pixels per thread in the backward pass: 1, 2 or 4 (0: default) */
+  uint32_t backward_pixels;   /* pixels per thread in the backward pass: 1, 2 or 4 (a warp covers an
+                                 8 x 4, 8 x 8 or 8 x 16 block of a tile), or 8 (one warp per 16 x 16
+                                 tile; backward_batch does not apply) (0: default) */
   uint32_t retry;             /* 1 (default): grow the pair buffers and run again on overflow */
   uint32_t graph;             /* 1: capture the step as a CUDA graph and replay it while its launch
                                  structure (views, slots, buffer sizes, SH degree, mode) holds */

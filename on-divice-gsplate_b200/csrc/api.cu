@@ -536,6 +536,11 @@ struct gs_context {
             t.backward_batch = batch;
             consider(t);
           }
+      if (bpx0 != 8u) {  // one warp per tile (its rounds are 32 splats whatever backward_batch says)
+        gs_tuning t = best;
+        t.backward_pixels = 8u;
+        consider(t);
+      }
       const uint32_t digits0 = best.sort_digit_bits;
       for (uint32_t digits : {6u, 7u, 8u})
         if (digits != digits0) {
@@ -1377,9 +1382,11 @@ int gs_motion_gradient(gs_context* c, uint32_t view, double* out, uint32_t count
 int gs_set_tuning(gs_context* c, const gs_tuning* t) {
   return guarded([&] {
     if (c == nullptr || t == nullptr) fail(GS_ERR_INVALID, "gs_set_tuning: null argument");
-    for (uint32_t px : {t->forward_pixels, t->backward_pixels})
-      if (px != 0 && px != 1 && px != 2 && px != 4)
-        fail(GS_ERR_INVALID, "gs_set_tuning: pixels per thread must be 1, 2 or 4");
+    if (t->forward_pixels != 0 && t->forward_pixels != 1 && t->forward_pixels != 2 && t->forward_pixels != 4)
+      fail(GS_ERR_INVALID, "gs_set_tuning: forward_pixels must be 1, 2 or 4");
+    if (t->backward_pixels != 0 && t->backward_pixels != 1 && t->backward_pixels != 2 && t->backward_pixels != 4 &&
+        t->backward_pixels != 8)
+      fail(GS_ERR_INVALID, "gs_set_tuning: backward_pixels must be 1, 2, 4 or 8");
     if (t->backward_batch != 0 && t->backward_batch != 32 && t->backward_batch != 64)
       fail(GS_ERR_INVALID, "gs_set_tuning: backward_batch must be 32 or 64");
     if (t->sort_digit_bits != 0 && (t->sort_digit_bits < 4 || t->sort_digit_bits > 8))

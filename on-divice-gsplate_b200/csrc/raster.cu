@@ -106,12 +106,13 @@ __device__ __forceinline__ void fetch_record_async(float4* q0, float4* q1, float
   copy_async16(qf, foot + g);
 }
 
-// Whether a staged splat's footprint ellipse reaches a pixel centre of the 8 x h block
+// Whether a staged splat's footprint ellipse reaches a pixel centre of the w x h block
 // whose first centre is (x0, y0): the maximum of the concave E over the block's rectangle
 // is 0 when the centre lies inside, else it lies on an edge facing the centre, at the
 // unconstrained maximiser along that edge clamped to the edge.
-__device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 C, float x0, float y0, float h) {
-  const float dx0 = x0 - A.x, dx1 = dx0 + 7.0f, dy0 = y0 - A.y, dy1 = dy0 + (h - 1.0f);
+__device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 C, float x0, float y0, float h,
+                                              float w = 8.0f) {
+  const float dx0 = x0 - A.x, dx1 = dx0 + (w - 1.0f), dy0 = y0 - A.y, dy1 = dy0 + (h - 1.0f);
   const float ex = dx0 > 0.0f ? dx0 : fminf(dx1, 0.0f);  // facing vertical edge (0: none)
   const float ey = dy0 > 0.0f ? dy0 : fminf(dy1, 0.0f);  // facing horizontal edge (0: none)
   const float ha = A.w, hb = B.x, hc = B.y;
@@ -121,6 +122,43 @@ __device__ __forceinline__ bool block_reached(float4 A, float4 B, float4 C, floa
   const float eh = ey != 0.0f ? tx * (ha * tx + hb * ey) + hc * ey * ey : -3.0e38f;
   const float e = (ex == 0.0f && ey == 0.0f) ? 0.0f : fmaxf(ev, eh);
   return e >= C.y;
+}
+
+// Reduce-scatter of 12 slots (11 values and a zero) over a warp: after the exchanges over
+// lane bits 4, 3, 2, 1 (6, 3, 2 and 1 shuffles; the 3 slots left after bit 3 are padded
+// to 4) and a final add over bit 0, lane l holds in c[0] the warp sum of slot
+// g + 3 b3 + 6 b4, g = (l >> 1) & 3, when l is even and g < 3. Returns that slot, or 12
+// for the lanes that hold none.
+__device__ __forceinline__ uint32_t warp_reduce_scatter12(float c[12], uint32_t lane) {
+  const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const float send = b4 ? c[i] : c[i + 6];
+    const float keep = b4 ? c[i + 6] : c[i];
+    c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float send = b3 ? c[i] : c[i + 3];
+    const float keep = b3 ? c[i + 3] : c[i];
+    c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  {
+    const float send0 = b2 ? c[0] : c[2];
+    const float keep0 = b2 ? c[2] : c[0];
+    const float send1 = b2 ? c[1] : 0.0f;
+    const float keep1 = b2 ? 0.0f : c[1];
+    c[0] = keep0 + __shfl_xor_sync(0xffffffffu, send0, 4);
+    c[1] = keep1 + __shfl_xor_sync(0xffffffffu, send1, 4);
+  }
+  {
+    const float send = b1 ? c[0] : c[1];
+    const float keep = b1 ? c[1] : c[0];
+    c[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  c[0] += __shfl_xor_sync(0xffffffffu, c[0], 1);
+  const uint32_t group = (lane >> 1) & 3u;
+  return ((lane & 1u) == 0u && group < 3u) ? group + (b3 ? 3u : 0u) + (b4 ? 6u : 0u) : 12u;
 }
 
 // The tile and pixel layout of one block.
@@ -601,39 +639,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           c[2] = (-0.5f * dx * dx) * sd;
           c[3] = -dx * st;
           c[4] = -0.5f * sty;
-          // Reduce-scatter of 12 slots (11 values and a zero): after the exchanges over
-          // lane bits 4, 3, 2, 1 (6, 3, 2 and 1 shuffles; the 3 slots left after bit 3 are
-          // padded to 4) and a final add over bit 0, lane l holds the warp sum of value
-          // g + 3 b3 + 6 b4, g = (l >> 1) & 3, when g < 3.
-          const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
-#pragma unroll
-          for (int i = 0; i < 6; ++i) {
-            const float send = b4 ? c[i] : c[i + 6];
-            const float keep = b4 ? c[i + 6] : c[i];
-            c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-          }
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            const float send = b3 ? c[i] : c[i + 3];
-            const float keep = b3 ? c[i + 3] : c[i];
-            c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-          }
-          {
-            const float send0 = b2 ? c[0] : c[2];
-            const float keep0 = b2 ? c[2] : c[0];
-            const float send1 = b2 ? c[1] : 0.0f;
-            const float keep1 = b2 ? 0.0f : c[1];
-            c[0] = keep0 + __shfl_xor_sync(0xffffffffu, send0, 4);
-            c[1] = keep1 + __shfl_xor_sync(0xffffffffu, send1, 4);
-          }
-          {
-            const float send = b1 ? c[0] : c[1];
-            const float keep = b1 ? c[1] : c[0];
-            c[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-          }
-          c[0] += __shfl_xor_sync(0xffffffffu, c[0], 1);
-          const uint32_t group = (lane >> 1) & 3u;
-          if ((lane & 1u) == 0u && group < 3u) s_part[warp][j][group + (b3 ? 3u : 0u) + (b4 ? 6u : 0u)] = c[0];
+          const uint32_t slot = warp_reduce_scatter12(c, lane);
+          if (slot < 12u) s_part[warp][j][slot] = c[0];
           wrote |= 1u << (j & 31u);
         }
       }
@@ -673,6 +680,198 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
 }
 
+// One warp per 16x16 tile (backward_pixels = 8). Lane (c, r) = (lane & 7, lane >> 3) owns
+// the tile's pixels (8h + c, 4q + r), p = 2q + h for h in {0, 1} and q in 0..3: the two
+// half-tile warps of the 2-warp layout folded into one. Each warp takes tiles from the
+// queue on its own and stages 32 splats per round, one per lane, with no block barrier. A
+// splat reaching the tile is reduced once over the whole tile instead of once per half,
+// and its sum needs no second, cross-warp stage. The lane's pixels share one of two dx
+// values, so the mean and conic sums keep three per-lane sums per column half h:
+// u = sum G dl (dpow = opacity G dl), s1 = sum G dl dy and s2 = sum G dl dy^2.
+struct WarpTileSmem {
+  float4 a[32], b[32], c[32];  // staged splats (stage_splat)
+  uint32_t dst[32];            // pre-sort pair index (deterministic) or gaussian
+  float part[32][12];          // the round's per-splat tile sums
+};
+
+template <bool DET>
+__device__ __forceinline__ void raster_bwd_warp_tile(const RasterArgs& a, uint32_t gt, uint32_t lane,
+                                                     WarpTileSmem& sm) {
+  constexpr bool ABS = DET;  // the |dL/dmean2d| sums (see the top of the file)
+  const uint32_t v = view_of_tile(a.vt, gt);
+  const gs_frame_data& f = a.frames[v];
+  const uint32_t W = f.image[0], H = f.image[1];
+  const uint32_t t = gt - a.vt->tile_base[v];
+  const uint32_t tx = t % f.image[2], ty = t / f.image[2];
+  const uint2 range = a.rb.ranges[gt];
+  const uint32_t len = range.y - range.x;
+  const uint32_t n = min(len, a.rb.tile_count[gt]);
+  if (DET) {
+    // Pairs behind the tile's furthest last contributor draw nothing (train_backward_serial.glsl:58-66).
+    for (uint32_t k = range.x + n + lane; k < range.y; k += 32u) {
+      float4* o = reinterpret_cast<float4*>(a.pair_grads + size_t(a.rb.values[k]) * 12u);
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      o[0] = z;
+      o[1] = z;
+      o[2] = z;
+    }
+  }
+  if (n == 0u) return;
+
+  const uint32_t x0 = tx * kTile + (lane & 7u), y0 = ty * kTile + (lane >> 3);
+  const float cx0 = float(x0) + 0.5f, cx1 = float(x0 + 8u) + 0.5f;
+  float cy[4], dl0[8], dl1[8], dl2[8], R[8], T[8];
+  uint32_t last[8], my_last = 0u;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) cy[q] = float(y0 + 4u * uint32_t(q)) + 0.5f;
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    const uint32_t x = x0 + 8u * uint32_t(p & 1), y = y0 + 4u * uint32_t(p >> 1);
+    dl0[p] = dl1[p] = dl2[p] = R[p] = 0.0f;
+    T[p] = 1.0f;
+    last[p] = 0u;
+    if (x < W && y < H) {
+      const size_t pix = size_t(a.vt->pixel_base[v]) + size_t(y) * W + x;
+      const float4 pg = a.rb.pixel_grad[pix];
+      dl0[p] = pg.x;
+      dl1[p] = pg.y;
+      dl2[p] = pg.z;
+      R[p] = a.rb.pixel_dot[pix];
+      last[p] = a.rb.pixel_count[pix];
+      my_last = max(my_last, last[p]);
+    }
+  }
+  const uint32_t wlast = __reduce_max_sync(0xffffffffu, my_last);
+  const float bx = float(tx * kTile) + 0.5f, by = float(ty * kTile) + 0.5f;
+
+  for (uint32_t start = 0; start < n; start += 32u) {
+    __syncwarp();  // the previous round's reads of the staging buffers are done
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
+    if (start + lane < n) {
+      const uint32_t k = range.x + start + lane;
+      const uint32_t g = a.rb.gauss[k];
+      const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
+      stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
+      sm.a[lane] = A;
+      sm.b[lane] = B;
+      sm.c[lane] = C;
+      sm.dst[lane] = DET ? a.rb.values[k] : g;
+    }
+    __syncwarp();
+    const uint32_t nb = min(32u, n - start);
+    const uint32_t jmax = wlast > start ? min(nb, wlast - start) : 0u;
+    uint32_t m = __ballot_sync(0xffffffffu, lane < jmax && block_reached(A, B, C, bx, by, 16.0f, 16.0f));
+    uint32_t wrote = 0u;
+#pragma unroll 1
+    while (m != 0u) {
+      const uint32_t j = uint32_t(__ffs(m) - 1);
+      m &= m - 1u;
+      const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
+      const float4 SA = sm.a[j];
+      const float4 SB = sm.b[j];
+      const float blue = sm.c[j].x;
+      const float dx0 = __fsub_rn(SA.x, cx0), dx1 = __fsub_rn(SA.x, cx1);
+      const float e00 = __fmul_rn(__fmul_rn(SA.w, dx0), dx0), e10 = __fmul_rn(SB.x, dx0);
+      const float e01 = __fmul_rn(__fmul_rn(SA.w, dx1), dx1), e11 = __fmul_rn(SB.x, dx1);
+      // The conic (a, b, c) back from the scaled exponent terms, for the mean gradient:
+      // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy), lx = -ca dx, ly = -cb dx.
+      const float ca = SA.w * (-2.0f / kLog2e), cb = SB.x * (-1.0f / kLog2e), cc = SB.y * (-2.0f / kLog2e);
+      const float mx = -cb, my = -cc;
+      float u[2] = {0.0f, 0.0f}, s1[2] = {0.0f, 0.0f}, s2[2] = {0.0f, 0.0f};
+      float c[12];
+#pragma unroll
+      for (int k = 6; k < 12; ++k) c[k] = 0.0f;
+      bool has = false;
+#pragma unroll
+      for (int p = 0; p < 8; ++p) {
+        const int h = p & 1;
+        if (pos > last[p]) continue;
+        const float dy = __fsub_rn(SA.y, cy[p >> 1]);
+        const float e = splat_exponent(h ? e01 : e00, h ? e11 : e10, SB.y, dy);
+        const float G = exp2_approx(e);
+        const float raw = __fmul_rn(SA.z, G);
+        const float alpha = fminf(kMaxAlpha, raw);
+        if (e > 0.0f || alpha < kMinAlpha) continue;
+        has = true;
+        const float gc = dl0[p] * SB.z + dl1[p] * SB.w + dl2[p] * blue;
+        const float weight = alpha * T[p];
+        const float rest = R[p] - gc * weight;
+        const float one_minus = __fsub_rn(1.0f, alpha);
+        const float dlda = T[p] * gc - __fdividef(rest, one_minus);
+        // Opacity and exponent gradients vanish where alpha is clamped at 0.99.
+        const float dl = raw >= kMaxAlpha ? 0.0f : dlda;
+        const float gd = G * dl;  // dpow / opacity
+        const float tt = gd * dy;
+        u[h] += gd;
+        s1[h] += tt;
+        s2[h] = fmaf(tt, dy, s2[h]);
+        c[6] += weight * dl0[p];
+        c[7] += weight * dl1[p];
+        c[8] += weight * dl2[p];
+        if constexpr (ABS) {
+          const float dx = h ? dx1 : dx0;
+          c[9] += fabsf(fmaf(tt, mx, gd * (-ca * dx)));  // |dpow (lx + mx dy)| / opacity
+          c[10] += fabsf(fmaf(tt, my, gd * (-cb * dx)));
+        }
+        T[p] = __fmul_rn(T[p], one_minus);
+        R[p] = rest;
+      }
+      if (__any_sync(0xffffffffu, has)) {
+        const float op = SA.z;
+        const float sd0 = op * u[0], sd1 = op * u[1];
+        const float sdx = fmaf(dx0, sd0, dx1 * sd1);                // sum dpow dx
+        const float sdxx = fmaf(dx0 * dx0, sd0, (dx1 * dx1) * sd1);  // sum dpow dx^2
+        const float st = op * (s1[0] + s1[1]);                      // sum dpow dy
+        const float stx = op * fmaf(dx0, s1[0], dx1 * s1[1]);       // sum dpow dx dy
+        const float sty = op * (s2[0] + s2[1]);                     // sum dpow dy^2
+        c[0] = fmaf(-ca, sdx, mx * st);
+        c[1] = fmaf(-cb, sdx, my * st);
+        c[2] = -0.5f * sdxx;
+        c[3] = -stx;
+        c[4] = -0.5f * sty;
+        c[5] = u[0] + u[1];
+        if constexpr (ABS) {
+          c[9] *= op;
+          c[10] *= op;
+        }
+        const uint32_t slot = warp_reduce_scatter12(c, lane);
+        if (slot < 12u) sm.part[j][slot] = c[0];
+        wrote |= 1u << j;
+      }
+    }
+    __syncwarp();
+    // Three float4s per staged splat: stored at the pair (deterministic; zero for a splat
+    // that reached no pixel) or added to the gaussian's accumulator.
+    for (uint32_t idx = lane; idx < nb * 3u; idx += 32u) {
+      const uint32_t j = idx / 3u, qd = idx - 3u * j;
+      const bool drew = (wrote >> j) & 1u;
+      const float4 sum = drew ? *reinterpret_cast<const float4*>(&sm.part[j][4u * qd]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      if constexpr (DET) {
+        reinterpret_cast<float4*>(a.pair_grads + size_t(sm.dst[j]) * 12u)[qd] = sum;
+      } else if (drew) {
+        atomicAdd(reinterpret_cast<float4*>(a.grad2d) + size_t(sm.dst[j]) * 3u + qd, sum);
+      }
+    }
+  }
+}
+
+// Four independent warps per block, each with its own staging buffers; 5 blocks per SM
+// (96 registers, no spills; a 6-block bound spills).
+template <bool DET>
+__global__ void __launch_bounds__(128, 5) k_raster_bwd_warp(RasterArgs a) {
+  if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
+  __shared__ WarpTileSmem s_warp[4];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t total = a.vt->total_tiles;
+  for (;;) {
+    uint32_t gt = 0u;
+    if (lane == 0u) gt = atomicAdd(a.queue, 1u);
+    gt = __shfl_sync(0xffffffffu, gt, 0);
+    if (gt >= total) break;
+    raster_bwd_warp_tile<DET>(a, gt, lane, s_warp[warp]);
+  }
+}
+
 // 3 PX blocks of 256 / PX threads per SM: 12 two-warp blocks at 4 pixels per thread (at
 // most 85 registers; with no bound the compiler settled on 72 with spills, measured 1%
 // slower, and a 64-register cap 18% slower).
@@ -703,9 +902,20 @@ void launch_bwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   k_raster_bwd<BATCH, DET, PX, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
 }
 
+template <bool DET>
+void launch_bwd_warp(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
+  static uint32_t grid = 0, cap = 0;
+  if (grid == 0 || cap != sp.tile_cap) {
+    grid = persistent_grid(k_raster_bwd_warp<DET>, 128, sp);
+    cap = sp.tile_cap;
+  }
+  k_raster_bwd_warp<DET><<<grid, 128, 0, st>>>(a);
+}
+
 template <int BATCH, bool DET, bool ASYNC>
 void launch_bwd_px(const RasterArgs& a, const StepPointers& sp, int px, cudaStream_t st) {
-  if (px >= 4) launch_bwd<BATCH, DET, 4, ASYNC>(a, sp, st);
+  if (px >= 8) launch_bwd_warp<DET>(a, sp, st);
+  else if (px >= 4) launch_bwd<BATCH, DET, 4, ASYNC>(a, sp, st);
   else if (px == 2) launch_bwd<BATCH, DET, 2, ASYNC>(a, sp, st);
   else launch_bwd<BATCH, DET, 1, ASYNC>(a, sp, st);
 }

@@ -190,7 +190,7 @@ bool Trainer::select_backward(const std::string& name) {
     if (rest == word.c_str() + eq + 1 || *rest != '\0') return false;
     if (key == "fpx" && (v == 1 || v == 2 || v == 4)) t.forward_pixels = uint32_t(v);
     else if (key == "fbatch" && (v == 64 || v == 128 || v == 256)) t.forward_batch = uint32_t(v);
-    else if (key == "bpx" && (v == 1 || v == 2 || v == 4)) t.backward_pixels = uint32_t(v);
+    else if (key == "bpx" && (v == 1 || v == 2 || v == 4 || v == 8)) t.backward_pixels = uint32_t(v);
     else if (key == "batch" && (v == 32 || v == 64)) t.backward_batch = uint32_t(v);
     else if (key == "digits" && v >= 4 && v <= 8) t.sort_digit_bits = uint32_t(v);
     else return false;

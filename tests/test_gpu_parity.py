@@ -94,10 +94,16 @@ def _stage_oracle(ctx, fr, scene, target, ssim=True):
                           depth_keys=keys)
 
 
-def test_forward_loss_backward_match_oracle(ctx):
+@pytest.mark.parametrize("backward_pixels", [4, 8])
+def test_forward_loss_backward_match_oracle(ctx, backward_pixels):
+    """Backward at 4 pixels per thread (two warps per tile) and at 8 (one warp per tile)."""
     scene, cam, opt, target = cfg0_view()
     fr = frame_for(scene, cam, opt, (0.1, 0.2, 0.3))
-    res = gpu_step(ctx, scene, [fr], [target], train=True)
+    ctx.set_tuning(backward_pixels=backward_pixels)
+    try:
+        res = gpu_step(ctx, scene, [fr], [target], train=True)
+    finally:
+        ctx.set_tuning(backward_pixels=4)
     r = _stage_oracle(ctx, fr, scene, target)
     count = ctx.snapshot("pixel_count")
     same = count == r.pixel_count
@@ -190,16 +196,22 @@ def test_adjoint_sh3_against_oracle_and_fd(ctx):
         assert g["bad"] <= max(1, g["checked"] // 20), (name, g)
 
 
-def test_deterministic_mode_is_bit_stable(ctx):
+@pytest.mark.parametrize("backward_pixels", [4, 8])
+def test_deterministic_mode_is_bit_stable(ctx, backward_pixels):
     scene, cam, opt, target = cfg0_view()
     fr = frame_for(scene, cam, opt, (0.1, 0.2, 0.3))
-    gpu_step(ctx, scene, [fr], [target])
-    a = ctx.moments()
-    pa = ctx.snapshot("pair_grads")
-    gpu_step(ctx, scene, [fr], [target])
-    b = ctx.moments()
+    ctx.set_tuning(backward_pixels=backward_pixels)
+    try:
+        gpu_step(ctx, scene, [fr], [target])
+        a = ctx.moments()
+        pa = ctx.snapshot("pair_grads")
+        gpu_step(ctx, scene, [fr], [target])
+        b = ctx.moments()
+        pb = ctx.snapshot("pair_grads")
+    finally:
+        ctx.set_tuning(backward_pixels=4)
     np.testing.assert_array_equal(a["m"], b["m"])
-    np.testing.assert_array_equal(pa, ctx.snapshot("pair_grads"))
+    np.testing.assert_array_equal(pa, pb)
 
 
 def test_pair_overflow_retry(ctx):

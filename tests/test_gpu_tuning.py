@@ -73,7 +73,7 @@ def test_autotune_restores_the_model_and_picks_a_candidate(ctx):
         np.testing.assert_array_equal(before[1][k], after[1][k], err_msg=k)
     np.testing.assert_array_equal(before[2], after[2])
     assert t.forward_pixels in (1, 2, 4)
-    assert (t.backward_pixels, t.backward_batch) in ((2, 32), (2, 64), (4, 32), (4, 64))
+    assert (t.backward_pixels, t.backward_batch) in ((2, 32), (2, 64), (4, 32), (4, 64)) or t.backward_pixels == 8
     assert t.sort_digit_bits in (6, 7, 8)
     cur = ctx.tuning()
     assert (cur.forward_pixels, cur.backward_pixels, cur.backward_batch, cur.sort_digit_bits) == (
@@ -100,7 +100,8 @@ def test_tunings_compute_the_same_gradients(ctx):
                dict(backward_pixels=1, backward_batch=64), dict(sort_digit_bits=5), dict(forward_batch=64),
                dict(forward_batch=128, forward_pixels=4), dict(stage_async=1), dict(stage_async=1, forward_batch=128),
                dict(stage_async=1, backward_pixels=2, backward_batch=32), dict(deterministic=0),
-               dict(deterministic=0, stage_async=1, backward_pixels=1, backward_batch=32)):
+               dict(deterministic=0, stage_async=1, backward_pixels=1, backward_batch=32), dict(backward_pixels=8),
+               dict(backward_pixels=8, deterministic=0)):
         base = dict(forward_pixels=2, backward_pixels=4, backward_batch=64, sort_digit_bits=8, forward_batch=256,
                     stage_async=0, deterministic=1)
         base.update(kw)
