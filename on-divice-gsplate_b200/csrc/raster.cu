@@ -14,9 +14,10 @@
 // (same multiplications). Per splat it needs
 //   dL/dalpha_k = T_k (dL/dC . c_k) - R_{k+1} / (1 - alpha_k),  R_{k+1} = R_k - (dL/dC . c_k) alpha_k T_k.
 // A thread adds its PX pixels' gradients in registers; each warp then sums a splat's 11
-// values over its lanes with a reduce-scatter butterfly (13 shuffles instead of 55 for a
-// tree per value), skipped when no lane touched the splat, and the warps' partials are
-// added in a fixed order, so the per-pair gradient is bit-stable. Deterministic mode
+// values over its lanes (a reduce-scatter butterfly of 13 shuffles in deterministic mode;
+// in fast mode, 9 values through shared memory), skipped when no lane touched the splat,
+// and the warps' partials are added in a fixed order, so the per-pair gradient is
+// bit-stable. Deterministic mode
 // stores it at the pair's pre-sort index (pair_grads, summed per gaussian by
 // train_pair_sum's fixed order); fast mode adds it to the gaussian's accumulator with
 // three 16-byte vector atomics per tile (red.global.add.v4.f32). Fast mode also leaves out
@@ -159,6 +160,34 @@ __device__ __forceinline__ uint32_t warp_reduce_scatter12(float c[12], uint32_t 
   c[0] += __shfl_xor_sync(0xffffffffu, c[0], 1);
   const uint32_t group = (lane >> 1) & 3u;
   return ((lane & 1u) == 0u && group < 3u) ? group + (b3 ? 3u : 0u) + (b4 ? 6u : 0u) : 12u;
+}
+
+// The fast mode's sum of a splat's 9 gradient values (without the |dmean| sums) over a
+// warp's 32 lanes, through shared memory: each lane stores its values as a row of 12 floats
+// (three conflict-free 16-byte stores); lane v + 9h (v < 9, h < 3) adds value v down the
+// rows h, h + 3, h + 6, ... in two interleaved chains (the three groups' banks meet once);
+// lane v then adds the three groups. Fewer instructions than a shuffle butterfly, which
+// spends two selects per shuffle. Returns the warp sum of value `lane` for lanes below 9.
+// `rows` is the warp's own 32 x 12 scratch.
+__device__ __forceinline__ float warp_sum9_rows(float (*rows)[12], const float c[12], uint32_t lane) {
+  __syncwarp();  // the previous splat's rows have been read
+  float4* row = reinterpret_cast<float4*>(&rows[lane][0]);
+  row[0] = make_float4(c[0], c[1], c[2], c[3]);
+  row[1] = make_float4(c[4], c[5], c[6], c[7]);
+  row[2] = make_float4(c[8], 0.0f, 0.0f, 0.0f);
+  __syncwarp();
+  float even = 0.0f, odd = 0.0f;
+  if (lane < 27u) {
+    const uint32_t v = lane % 9u, h = lane / 9u;
+#pragma unroll
+    for (uint32_t i = 0; i < 10u; i += 2u) {
+      even += rows[3u * i + h][v];
+      odd += rows[3u * i + 3u + h][v];
+    }
+    if (30u + h < 32u) even += rows[30u + h][v];
+  }
+  const float sum = even + odd;
+  return sum + __shfl_down_sync(0xffffffffu, sum, 9) + __shfl_down_sync(0xffffffffu, sum, 18);
 }
 
 // The tile and pixel layout of one block.
@@ -328,23 +357,24 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         all_done = true;
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
-          if (!done[p]) {
+          {
+            // Predicated rather than branched: a pixel that is done, or skips this splat,
+            // adds zero weight and keeps T and its last contributor (bit for bit the same
+            // sums: x + 0 = x).
             const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
             const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
-            if (e <= 0.0f && alpha >= kMinAlpha) {
-              const float next_T = __fmul_rn(T[p], __fsub_rn(1.0f, alpha));
-              if (next_T < kMinTransmittance) {
-                done[p] = true;
-              } else {
-                const float weight = alpha * T[p];
-                C0[p] += B.z * weight;
-                C1[p] += B.w * weight;
-                C2[p] += blue * weight;
-                T[p] = next_T;
-                last[p] = contributor;
-                if constexpr (COUNT) ++blended;
-              }
-            }
+            const bool blend = !done[p] && e <= 0.0f && alpha >= kMinAlpha;
+            const float next_T = __fmul_rn(T[p], __fsub_rn(1.0f, alpha));
+            const bool stop = blend && next_T < kMinTransmittance;
+            const bool ok = blend && !stop;
+            done[p] = done[p] || stop;
+            const float weight = ok ? alpha * T[p] : 0.0f;
+            C0[p] += B.z * weight;
+            C1[p] += B.w * weight;
+            C2[p] += blue * weight;
+            T[p] = ok ? next_T : T[p];
+            last[p] = ok ? contributor : last[p];
+            if constexpr (COUNT) blended += ok ? 1u : 0u;
           }
           all_done = all_done && done[p];
         }
@@ -471,6 +501,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   __shared__ uint32_t s_dst[BATCH];
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
+  __shared__ __align__(16) float s_lanes[DET ? 1 : L::kWarps][DET ? 1 : 32][12];  // fast mode: warp_sum9_rows
 
   const uint32_t lid = threadIdx.x, lane = lid & 31u, warp = lid >> 5;
   const L lay(a.vt, a.frames, gt, warp);
@@ -639,8 +670,13 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
           c[2] = (-0.5f * dx * dx) * sd;
           c[3] = -dx * st;
           c[4] = -0.5f * sty;
-          const uint32_t slot = warp_reduce_scatter12(c, lane);
-          if (slot < 12u) s_part[warp][j][slot] = c[0];
+          if constexpr (ABS) {
+            const uint32_t slot = warp_reduce_scatter12(c, lane);
+            if (slot < 12u) s_part[warp][j][slot] = c[0];
+          } else {
+            const float sum = warp_sum9_rows(s_lanes[warp], c, lane);
+            if (lane < 12u) s_part[warp][j][lane] = lane < 9u ? sum : 0.0f;
+          }
           wrote |= 1u << (j & 31u);
         }
       }
@@ -692,6 +728,7 @@ struct WarpTileSmem {
   float4 a[32], b[32], c[32];  // staged splats (stage_splat)
   uint32_t dst[32];            // pre-sort pair index (deterministic) or gaussian
   float part[32][12];          // the round's per-splat tile sums
+  float lanes[32][12];         // the lanes' values of the splat being summed (fast mode)
 };
 
 template <bool DET>
@@ -834,8 +871,13 @@ __device__ __forceinline__ void raster_bwd_warp_tile(const RasterArgs& a, uint32
           c[9] *= op;
           c[10] *= op;
         }
-        const uint32_t slot = warp_reduce_scatter12(c, lane);
-        if (slot < 12u) sm.part[j][slot] = c[0];
+        if constexpr (ABS) {
+          const uint32_t slot = warp_reduce_scatter12(c, lane);
+          if (slot < 12u) sm.part[j][slot] = c[0];
+        } else {
+          const float sum = warp_sum9_rows(sm.lanes, c, lane);
+          if (lane < 12u) sm.part[j][lane] = lane < 9u ? sum : 0.0f;
+        }
         wrote |= 1u << j;
       }
     }
