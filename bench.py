@@ -18,8 +18,10 @@ Adam on every parameter. Views are drawn in shuffled epochs over the 200 cameras
   the replayed graph. Raster passes are issue-bound, so their roofline is the FP32 pipe
   (128 lane operations per clock per SM at the sampled clock) over the work of the step's
   blending evaluations C (FP32_PER_EVALUATION each; counted by one untimed counting
-  forward), with the special-function unit's share beside it; every pass also reports HBM
-  GB/s from fixed per-unit bytes (algorithmic_bytes) against the measured copy bandwidth.
+  forward), with the special-function unit's share beside it, and the issue slots they use
+  (warp instructions per launch from a committed ncu count over the pass time, against one
+  per SM sub-partition per clock); every pass also reports HBM GB/s from fixed per-unit
+  bytes (algorithmic_bytes) against the measured copy bandwidth.
 - cpu_baseline: the CPU oracle (a multithreaded restatement of the reference's passes) on
   plain steps of the same workload, host cores, bounded time.
 Inputs (732 MB of parameters and moments, 1.66 GB of targets) exceed the 126 MB L2, so no
@@ -187,6 +189,18 @@ FP32_PER_EVALUATION = {"rasterize": 15, "backward": 60}
 MUFU_PER_CLOCK_PER_SM = 16
 FP32_PER_CLOCK_PER_SM = 128
 SM_COUNT = 148
+
+
+def ncu_figures(pass_name: str, mode: str) -> dict:
+    """Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) and warp / thread
+    instruction counts of a pass's kernel on this workload, from the committed ncu summary
+    profiles/ncu_traffic.json ({pass: {"fast" | "deterministic": {...}}}); {} when absent."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            entry = json.load(f).get(pass_name, {})
+    except (OSError, ValueError):
+        return {}
+    return entry.get(mode, {}) if isinstance(entry, dict) else {}
 
 
 def render_targets(ctx, truth, cams, opt):
@@ -445,12 +459,9 @@ def main() -> None:
         pixels = VIEWS_PER_STEP * WIDTH * HEIGHT
         pk = peaks()
         dom = max(passes, key=passes.get)
-        traffic = None
-        try:
-            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-                traffic = json.load(f).get(dom)
-        except (OSError, ValueError):
-            traffic = None
+        mode = "deterministic" if ctx.tuning().deterministic else "fast"
+        prof = ncu_figures(dom, mode)
+        traffic = prof.get("traffic")
         clk = clocks.summary()
         sm_hz = (clk["sm_mhz"] or 1965.0) * 1e6
         mufu_peak = MUFU_PER_CLOCK_PER_SM * SM_COUNT * sm_hz / 1e9  # Gop/s at the sampled clock
@@ -481,7 +492,21 @@ def main() -> None:
         else:
             roof = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": pk["hbm_gbs"], "unit": "GB/s",
                     "frac": d["hbm_frac"]}
-        roof.update({"traffic": traffic, "peak_source": pk["source"], "per_pass": per_pass,
+        warp_inst = prof.get("warp_instructions")
+        if warp_inst and d["ms"]:
+            # Issue slots: one warp instruction per SM sub-partition (4 per SM) per clock.
+            issue_peak = 4 * SM_COUNT * sm_hz / 1e9
+            issued = warp_inst / (d["ms"] * 1e-3) / 1e9
+            roof["issue"] = {"achieved": round(issued, 1), "peak": round(issue_peak, 1),
+                             "unit": "G warp instructions/s", "frac": round(issued / issue_peak, 4),
+                             "warp_instructions_per_launch": warp_inst,
+                             "thread_instructions_per_blending_evaluation":
+                                 round(prof["thread_instructions"] / blending, 1) if blending else None,
+                             "thread_instructions_per_evaluation":
+                                 round(prof["thread_instructions"] / evaluations, 1) if evaluations else None,
+                             "from": "instruction counts of one launch of the same workload (ncu, "
+                                     "profiles/ncu_traffic.json) over this run's pass time"}
+        roof.update({"traffic": traffic, "traffic_mode": mode, "peak_source": pk["source"], "per_pass": per_pass,
                      "passes_from": "pass events inside the replayed graph, mean over the timed steps; "
                                     "evaluations from one counting forward on the next view set"})
         line = {
