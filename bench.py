@@ -291,6 +291,81 @@ def cpu_baseline(scene, targets, cams, opt, seconds: float = 20.0) -> dict:
                       f"{dt:.1f} s on {O.threads()} threads"}
 
 
+# The reference's own CPU forward + loss (gs::reference_loss: FP64, single thread, every
+# gaussian against every pixel) at the two small workloads it is tractable at: seeded scenes
+# of N gaussians in a radius-1 ball, SH degree D, log-scales N(mu, sigma), one front view.
+REFERENCE_LOSS_CONFIGS = {
+    "config1": dict(n=512, degree=3, mu=-2.5, sigma=0.3, width=128, height=128, focal=200.0),
+    "config0": dict(n=20000, degree=0, mu=-4.0, sigma=0.5, width=360, height=640, focal=500.0),
+}
+
+
+def reference_forward_loss(names=("config1",), repeats: int = 5) -> dict:
+    """Times the reference's own CPU code for the path (engine/src/train_selftest.cpp's
+    reference_loss, compiled unchanged into oracle/_ref/libgs_ref.so) on one host thread:
+    forward + L1/SSIM loss of one view, no backward. {} when the library was not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from gs_b200 import scenes as S
+
+    if O.ref_lib() is None:
+        return {}
+    out = {}
+    for name in names:
+        c = REFERENCE_LOSS_CONFIGS[name]
+        scene = S.make_scene(c["n"], 0, c["degree"], radius=1.0, log_scale_mu=c["mu"], log_scale_sigma=c["sigma"])
+        cam = S.front_camera(c["width"], c["height"], c["focal"])
+        target = np.zeros((c["height"], c["width"], 4), np.uint8)
+        target[..., 3] = 255
+        p64, s64 = scene.params.astype(np.float64), scene.sh.astype(np.float64)
+        times = []
+        for _ in range(repeats if name == "config1" else 1):
+            t0 = time.perf_counter()
+            O.ref_reference_loss(cam.as_dict(), c["width"], c["height"], p64, s64, c["degree"], target,
+                                 (0.0, 0.0, 0.0), False, 0.2)
+            times.append(time.perf_counter() - t0)
+        sec = float(np.median(times))
+        out[name] = {"gaussians": c["n"], "width": c["width"], "height": c["height"], "sh_degree": c["degree"],
+                     "seconds_per_view": round(sec, 4), "views_per_s": round(1.0 / sec, 4), "threads": 1,
+                     "work": "forward + loss only (the reference's CPU path has no backward)"}
+    return out
+
+
+def b200_small_configs(names=("config1", "config0"), steps: int = 50) -> dict:
+    """This path on the GPU at the same small workloads, for beside reference_forward_loss:
+    device time per view of a forward + loss step (no backward, as the reference's CPU code)
+    and of a full training step, graph replay, median over `steps` steps."""
+    from gs_b200 import frame as F
+    from gs_b200 import scenes as S
+    from gs_b200.cuda import Context
+
+    out = {}
+    ctx = Context(0)
+    ctx.set_tuning(graph=1)
+    for name in names:
+        c = REFERENCE_LOSS_CONFIGS[name]
+        scene = S.make_scene(c["n"], 0, c["degree"], radius=1.0, log_scale_mu=c["mu"], log_scale_sigma=c["sigma"])
+        cam = S.front_camera(c["width"], c["height"], c["focal"])
+        target = np.zeros((c["height"], c["width"], 4), np.uint8)
+        target[..., 3] = 255
+        opt = F.TrainOptions(sh_degree=c["degree"], sh_degree_interval=0, lambda_dssim=0.2, lambda_dssim_end=-1.0)
+        fr = F.make_frame(cam, scene.count, scene.sh.shape[1], 0, opt, (0.0, 0.0, 0.0), 3.3)
+        entry = {}
+        for label, train in (("forward_loss", False), ("train_step", True)):
+            ctx.model_init(scene.params, scene.sh)
+            ctx.set_views([fr], [target])
+            ms = []
+            for k in range(steps + 3):
+                r = ctx.step(train)
+                if k >= 3:
+                    ms.append(r.gpu_ms)
+            entry[label] = {"ms_per_view": round(float(np.median(ms)), 4),
+                            "views_per_s": round(1000.0 / float(np.median(ms)), 1)}
+        out[name] = entry
+    ctx.close()
+    return out
+
+
 def run_reference(args, rank: int) -> None:
     """--impl reference: the reference's CPU implementation of the path. Its own code is
     Vulkan compute (no graphics stack here), so the restated CPU oracle stands in for it:
@@ -352,10 +427,18 @@ def main() -> None:
     ap.add_argument("--cameras", type=int, default=N_CAMERAS, help="orbit cameras (fewer: shorter setup)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tuning (profiling runs: timings under ncu would mislead the autotuner)")
+    ap.add_argument("--reference-loss", action="store_true",
+                    help="time only the reference's own CPU forward + loss at configs 1 and 0 (about 2 min) "
+                         "and this path's step at the same workloads on the GPU")
     ap.add_argument("--set", action="append", default=[], metavar="KNOB=VALUE",
                     help="a gs_tuning field to set instead of autotuning it (profiling runs), e.g. deterministic=0")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.reference_loss:
+        line = {"reference_cpu_forward_loss": reference_forward_loss(("config1", "config0"))}
+        line["b200"] = b200_small_configs()
+        print(json.dumps(line), flush=True)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -535,6 +618,9 @@ def main() -> None:
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(scene, targets, cams, opt)
+            ref = reference_forward_loss()
+            if ref:
+                line["reference_cpu_forward_loss"] = ref
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
