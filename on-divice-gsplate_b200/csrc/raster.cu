@@ -359,20 +359,21 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         for (int p = 0; p < PX; ++p) {
           {
             // Predicated rather than branched: a pixel that is done, or skips this splat,
-            // adds zero weight and keeps T and its last contributor (bit for bit the same
-            // sums: x + 0 = x).
+            // blends it with alpha 0, which adds zero weight and keeps T (T (1 - 0) = T) and
+            // its last contributor, bit for bit. Where it blends, T (1 - alpha) is the same
+            // product the stop test formed.
             const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
             const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
             const bool blend = !done[p] && e <= 0.0f && alpha >= kMinAlpha;
-            const float next_T = __fmul_rn(T[p], __fsub_rn(1.0f, alpha));
-            const bool stop = blend && next_T < kMinTransmittance;
+            const bool stop = blend && __fmul_rn(T[p], __fsub_rn(1.0f, alpha)) < kMinTransmittance;
             const bool ok = blend && !stop;
             done[p] = done[p] || stop;
-            const float weight = ok ? alpha * T[p] : 0.0f;
+            const float ab = ok ? alpha : 0.0f;
+            const float weight = ab * T[p];
             C0[p] += B.z * weight;
             C1[p] += B.w * weight;
             C2[p] += blue * weight;
-            T[p] = ok ? next_T : T[p];
+            T[p] = __fmul_rn(T[p], __fsub_rn(1.0f, ab));
             last[p] = ok ? contributor : last[p];
             if constexpr (COUNT) blended += ok ? 1u : 0u;
           }
@@ -626,50 +627,67 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         // The lane's pixels share dx, so the mean and conic sums need only
         // sd = sum dpow, st = sum dpow dy and sty = sum dpow dy^2 (formed after the loop):
         // dmean = (lx sd + mx st, ly sd + my st), dconic = (-dx^2/2 sd, -dx st, -sty/2).
-        float sd = 0.0f, st = 0.0f, sty = 0.0f;
+        // With dpow = opacity G dl the loop sums u = sum G dl (also the opacity gradient)
+        // and st, sty over G dl; the opacity factor is applied once after it.
+        float u = 0.0f, st = 0.0f, sty = 0.0f;
         float c[12];
 #pragma unroll
-        for (int k = 5; k < 12; ++k) c[k] = 0.0f;
+        for (int k = 6; k < 12; ++k) c[k] = 0.0f;
         bool has = false;
+        float dy[PX], G[PX], raw[PX], alpha[PX];
+        bool blend[PX];
+#pragma unroll
+        for (int p = 0; p < PX; ++p) {  // the groups' exponentials, independent of each other
+          dy[p] = __fsub_rn(A.y, cy[p]);
+          const float e = splat_exponent(e0, e1, B.y, dy[p]);
+          G[p] = exp2_approx(e);
+          raw[p] = __fmul_rn(A.z, G[p]);
+          alpha[p] = fminf(kMaxAlpha, raw[p]);
+          blend[p] = pos <= last[p] && e <= 0.0f && alpha[p] >= kMinAlpha;
+          has = has || blend[p];
+        }
+        // Then the groups' adjoints, each skipped by the whole warp when no lane blends; a
+        // lane that does not blend takes alpha 0, which leaves its T and R as they are and
+        // adds nothing (its G dl is zeroed, so a G outside the footprint cannot make a NaN).
 #pragma unroll
         for (int p = 0; p < PX; ++p) {
-          if (pos > last[p]) continue;
-          const float dy = __fsub_rn(A.y, cy[p]);
-          const float e = splat_exponent(e0, e1, B.y, dy);
-          const float G = exp2_approx(e);
-          const float raw = __fmul_rn(A.z, G);
-          const float alpha = fminf(kMaxAlpha, raw);
-          if (e > 0.0f || alpha < kMinAlpha) continue;
-          has = true;
+          if (!__any_sync(0xffffffffu, blend[p])) continue;
+          const float ab = blend[p] ? alpha[p] : 0.0f;
           const float gc = dl0[p] * B.z + dl1[p] * B.w + dl2[p] * blue;
-          const float weight = alpha * T[p];
+          const float weight = ab * T[p];
           const float rest = R[p] - gc * weight;
-          const float one_minus = __fsub_rn(1.0f, alpha);
+          const float one_minus = __fsub_rn(1.0f, ab);
           const float dlda = T[p] * gc - __fdividef(rest, one_minus);
           // Opacity and exponent gradients vanish where alpha is clamped at 0.99.
-          const float dl = raw >= kMaxAlpha ? 0.0f : dlda;
-          const float dpow = raw * dl;
-          const float t = dpow * dy;
-          sd += dpow;
+          const float gd = (blend[p] && raw[p] < kMaxAlpha) ? G[p] * dlda : 0.0f;
+          const float t = gd * dy[p];
+          u += gd;
           st += t;
-          sty = fmaf(t, dy, sty);
-          c[5] = fmaf(G, dl, c[5]);
+          sty = fmaf(t, dy[p], sty);
           c[6] += weight * dl0[p];
           c[7] += weight * dl1[p];
           c[8] += weight * dl2[p];
           if constexpr (ABS) {
-            c[9] += fabsf(fmaf(t, mx, dpow * lx));  // |dpow (lx + mx dy)|
-            c[10] += fabsf(fmaf(t, my, dpow * ly));
+            c[9] += fabsf(fmaf(t, mx, gd * lx));  // |dpow (lx + mx dy)| / opacity
+            c[10] += fabsf(fmaf(t, my, gd * ly));
           }
           T[p] = __fmul_rn(T[p], one_minus);
           R[p] = rest;
         }
         if (__any_sync(0xffffffffu, has)) {
+          const float sd = A.z * u;
+          st *= A.z;
+          sty *= A.z;
           c[0] = fmaf(lx, sd, mx * st);
           c[1] = fmaf(ly, sd, my * st);
           c[2] = (-0.5f * dx * dx) * sd;
           c[3] = -dx * st;
           c[4] = -0.5f * sty;
+          c[5] = u;
+          if constexpr (ABS) {
+            c[9] *= A.z;
+            c[10] *= A.z;
+          }
           if constexpr (ABS) {
             const uint32_t slot = warp_reduce_scatter12(c, lane);
             if (slot < 12u) s_part[warp][j][slot] = c[0];
