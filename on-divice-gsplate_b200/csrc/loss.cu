@@ -73,6 +73,7 @@ constexpr int kAbc = kTilePixels + 16;  // stride of the per-pixel planes after 
 // phases use the first 256.
 constexpr uint32_t kLossThreads = 320;
 constexpr uint32_t kLossWarps = kLossThreads / 32;
+constexpr uint32_t kWindowLoads = (kWin * kWin + kLossThreads - 1) / kLossThreads;  // 3 window pixels a thread
 
 // Blur of 4 consecutive outputs from `src` (14 inputs, `stride` apart) into out[4].
 __device__ __forceinline__ void blur4(const float x[kSpan], float out[kRun]) {
@@ -141,21 +142,34 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim(LossArgs a) {
   }
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
-  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += kLossThreads) {
+  // Each thread's (up to) three window pixels, all loads issued before the first store.
+  float4 xo[kWindowLoads];
+  uint32_t yt[kWindowLoads];
+  bool in_image[kWindowLoads];
+#pragma unroll
+  for (uint32_t r = 0; r < kWindowLoads; ++r) {
+    const uint32_t e = lid + r * kLossThreads;
     const uint32_t row = e / kWin, col = e % kWin;
     const int gx = ox + int(col), gy = oy + int(row);
-    const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
-    float3 x = make_float3(0.f, 0.f, 0.f), y = x;
+    const bool in = e < uint32_t(kWin * kWin) && gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
+    xo[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    yt[r] = 0u;
+    in_image[r] = in;
     if (in) {
       const size_t local = size_t(gy) * W + size_t(gx);
-      const float4 o = a.rb.pixel_out[pbase + local];
-      x = make_float3(o.x, o.y, o.z);
-      y = target_colour(f, target[local]);
+      xo[r] = a.rb.pixel_out[pbase + local];
+      yt[r] = target[local];
     }
-    const uint32_t at = row * kS + col;
-    s_buf[at] = x.x;
-    s_buf[kPlane + at] = x.y;
-    s_buf[2 * kPlane + at] = x.z;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kWindowLoads; ++r) {
+    const uint32_t e = lid + r * kLossThreads;
+    if (e >= uint32_t(kWin * kWin)) break;
+    const float3 y = in_image[r] ? target_colour(f, yt[r]) : make_float3(0.f, 0.f, 0.f);
+    const uint32_t at = (e / kWin) * kS + e % kWin;
+    s_buf[at] = xo[r].x;
+    s_buf[kPlane + at] = xo[r].y;
+    s_buf[2 * kPlane + at] = xo[r].z;
     s_buf[3 * kPlane + at] = y.x;
     s_buf[4 * kPlane + at] = y.y;
     s_buf[5 * kPlane + at] = y.z;
@@ -284,29 +298,41 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
   const uint32_t lid = threadIdx.x;
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
-  for (uint32_t e = lid; e < uint32_t(kWin * kWin); e += kLossThreads) {
+  // Each thread's (up to) three window pixels: every load issued before the first store,
+  // so their latencies overlap instead of adding up.
+  float4 m0[kWindowLoads], m1[kWindowLoads];
+  float m2[kWindowLoads];
+#pragma unroll
+  for (uint32_t r = 0; r < kWindowLoads; ++r) {
+    const uint32_t e = lid + r * kLossThreads;
     const uint32_t row = e / kWin, col = e % kWin;
     const int gx = ox + int(col), gy = oy + int(row);
-    const bool in = gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
-    float4 m0 = make_float4(0.f, 0.f, 0.f, 0.f), m1 = m0;
-    float m2 = 0.0f;
+    const bool in = e < uint32_t(kWin * kWin) && gx >= 0 && gy >= 0 && gx < int(W) && gy < int(H);
+    m0[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    m1[r] = m0[r];
+    m2[r] = 0.0f;
     if (in) {
       const size_t q = pbase + size_t(gy) * W + size_t(gx);
-      m0 = a.rb.ssim_maps[q * 2u];
-      m1 = a.rb.ssim_maps[q * 2u + 1u];
-      m2 = a.rb.ssim_last[q];
+      m0[r] = a.rb.ssim_maps[q * 2u];
+      m1[r] = a.rb.ssim_maps[q * 2u + 1u];
+      m2[r] = a.rb.ssim_last[q];
     }
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kWindowLoads; ++r) {
+    const uint32_t e = lid + r * kLossThreads;
+    if (e >= uint32_t(kWin * kWin)) break;
     // Planes A rgb, B rgb, C rgb.
-    const uint32_t at = row * kS + col;
-    s_m[at] = m0.x;
-    s_m[kPlane + at] = m0.y;
-    s_m[2 * kPlane + at] = m0.z;
-    s_m[3 * kPlane + at] = m0.w;
-    s_m[4 * kPlane + at] = m1.x;
-    s_m[5 * kPlane + at] = m1.y;
-    s_m[6 * kPlane + at] = m1.z;
-    s_m[7 * kPlane + at] = m1.w;
-    s_m[8 * kPlane + at] = m2;
+    const uint32_t at = (e / kWin) * kS + e % kWin;
+    s_m[at] = m0[r].x;
+    s_m[kPlane + at] = m0[r].y;
+    s_m[2 * kPlane + at] = m0[r].z;
+    s_m[3 * kPlane + at] = m0[r].w;
+    s_m[4 * kPlane + at] = m1[r].x;
+    s_m[5 * kPlane + at] = m1[r].y;
+    s_m[6 * kPlane + at] = m1[r].z;
+    s_m[7 * kPlane + at] = m1[r].w;
+    s_m[8 * kPlane + at] = m2[r];
   }
   __syncthreads();
   // Row blur: 9 planes x 26 rows x 2 runs of 8.

@@ -488,6 +488,89 @@ __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
     raster_fwd_tile<PX, FB, ASYNC, COUNT>(a, gt);
 }
 
+// One staged splat's adjoint over a warp's PX row groups (train_common.glsl:215-253; the
+// front-to-back form described at the top of the file), at 1-based position `pos` of the
+// tile's list: updates each lane's T and R and, when some lane of the warp blends the
+// splat, forms the splat's gradient values over the lane's pixels in c (11 with the
+// |dmean| sums (ABS), else 9) and returns true.
+template <int PX, bool ABS>
+__device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, const float blue, const uint32_t pos,
+                                              const float cx, const float (&cy)[PX], const float (&dl0)[PX],
+                                              const float (&dl1)[PX], const float (&dl2)[PX],
+                                              const uint32_t (&last)[PX], float (&T)[PX], float (&R)[PX],
+                                              float (&c)[12]) {
+  const float dx = __fsub_rn(A.x, cx);
+  const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
+  // The conic (a, b, c) back from the scaled exponent terms, for the mean gradient:
+  // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy).
+  const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
+  const float lx = -ca * dx, ly = -cb * dx, mx = -cb, my = -cc;
+  // The lane's pixels share dx, so the mean and conic sums need only
+  // sd = sum dpow, st = sum dpow dy and sty = sum dpow dy^2 (formed after the loop):
+  // dmean = (lx sd + mx st, ly sd + my st), dconic = (-dx^2/2 sd, -dx st, -sty/2).
+  // With dpow = opacity G dl the loop sums u = sum G dl (also the opacity gradient)
+  // and st, sty over G dl; the opacity factor is applied once after it.
+  float u = 0.0f, st = 0.0f, sty = 0.0f;
+#pragma unroll
+  for (int k = 6; k < 12; ++k) c[k] = 0.0f;
+  bool has = false;
+  float dy[PX], G[PX], raw[PX], alpha[PX];
+  bool blend[PX];
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {  // the groups' exponentials, independent of each other
+    dy[p] = __fsub_rn(A.y, cy[p]);
+    const float e = splat_exponent(e0, e1, B.y, dy[p]);
+    G[p] = exp2_approx(e);
+    raw[p] = __fmul_rn(A.z, G[p]);
+    alpha[p] = fminf(kMaxAlpha, raw[p]);
+    blend[p] = pos <= last[p] && e <= 0.0f && alpha[p] >= kMinAlpha;
+    has = has || blend[p];
+  }
+  // Then the groups' adjoints, each skipped by the whole warp when no lane blends; a
+  // lane that does not blend takes alpha 0, which leaves its T and R as they are and
+  // adds nothing (its G dl is zeroed, so a G outside the footprint cannot make a NaN).
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    if (!__any_sync(0xffffffffu, blend[p])) continue;
+    const float ab = blend[p] ? alpha[p] : 0.0f;
+    const float gc = dl0[p] * B.z + dl1[p] * B.w + dl2[p] * blue;
+    const float weight = ab * T[p];
+    const float rest = R[p] - gc * weight;
+    const float one_minus = __fsub_rn(1.0f, ab);
+    const float dlda = T[p] * gc - __fdividef(rest, one_minus);
+    // Opacity and exponent gradients vanish where alpha is clamped at 0.99.
+    const float gd = (blend[p] && raw[p] < kMaxAlpha) ? G[p] * dlda : 0.0f;
+    const float t = gd * dy[p];
+    u += gd;
+    st += t;
+    sty = fmaf(t, dy[p], sty);
+    c[6] += weight * dl0[p];
+    c[7] += weight * dl1[p];
+    c[8] += weight * dl2[p];
+    if constexpr (ABS) {
+      c[9] += fabsf(fmaf(t, mx, gd * lx));  // |dpow (lx + mx dy)| / opacity
+      c[10] += fabsf(fmaf(t, my, gd * ly));
+    }
+    T[p] = __fmul_rn(T[p], one_minus);
+    R[p] = rest;
+  }
+  if (!__any_sync(0xffffffffu, has)) return false;
+  const float sd = A.z * u;
+  st *= A.z;
+  sty *= A.z;
+  c[0] = fmaf(lx, sd, mx * st);
+  c[1] = fmaf(ly, sd, my * st);
+  c[2] = (-0.5f * dx * dx) * sd;
+  c[3] = -dx * st;
+  c[4] = -0.5f * sty;
+  c[5] = u;
+  if constexpr (ABS) {
+    c[9] *= A.z;
+    c[10] *= A.z;
+  }
+  return true;
+}
+
 // ASYNC: the splat records of round i + 1 are copied with cp.async while round i is
 // differentiated (as in the forward).
 template <int BATCH, bool DET, int PX, bool ASYNC>
@@ -615,79 +698,8 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t j = uint32_t(w) * 32u + uint32_t(__ffs(m) - 1);
         m &= m - 1u;
         const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
-        const float4 A = s_a[j];
-        const float4 B = s_b[j];
-        const float blue = s_c[j].x;
-        const float dx = __fsub_rn(A.x, cx);
-        const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
-        // The conic (a, b, c) back from the scaled exponent terms, for the mean gradient:
-        // dmx = dpow (lx + mx dy), dmy = dpow (ly + my dy).
-        const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
-        const float lx = -ca * dx, ly = -cb * dx, mx = -cb, my = -cc;
-        // The lane's pixels share dx, so the mean and conic sums need only
-        // sd = sum dpow, st = sum dpow dy and sty = sum dpow dy^2 (formed after the loop):
-        // dmean = (lx sd + mx st, ly sd + my st), dconic = (-dx^2/2 sd, -dx st, -sty/2).
-        // With dpow = opacity G dl the loop sums u = sum G dl (also the opacity gradient)
-        // and st, sty over G dl; the opacity factor is applied once after it.
-        float u = 0.0f, st = 0.0f, sty = 0.0f;
         float c[12];
-#pragma unroll
-        for (int k = 6; k < 12; ++k) c[k] = 0.0f;
-        bool has = false;
-        float dy[PX], G[PX], raw[PX], alpha[PX];
-        bool blend[PX];
-#pragma unroll
-        for (int p = 0; p < PX; ++p) {  // the groups' exponentials, independent of each other
-          dy[p] = __fsub_rn(A.y, cy[p]);
-          const float e = splat_exponent(e0, e1, B.y, dy[p]);
-          G[p] = exp2_approx(e);
-          raw[p] = __fmul_rn(A.z, G[p]);
-          alpha[p] = fminf(kMaxAlpha, raw[p]);
-          blend[p] = pos <= last[p] && e <= 0.0f && alpha[p] >= kMinAlpha;
-          has = has || blend[p];
-        }
-        // Then the groups' adjoints, each skipped by the whole warp when no lane blends; a
-        // lane that does not blend takes alpha 0, which leaves its T and R as they are and
-        // adds nothing (its G dl is zeroed, so a G outside the footprint cannot make a NaN).
-#pragma unroll
-        for (int p = 0; p < PX; ++p) {
-          if (!__any_sync(0xffffffffu, blend[p])) continue;
-          const float ab = blend[p] ? alpha[p] : 0.0f;
-          const float gc = dl0[p] * B.z + dl1[p] * B.w + dl2[p] * blue;
-          const float weight = ab * T[p];
-          const float rest = R[p] - gc * weight;
-          const float one_minus = __fsub_rn(1.0f, ab);
-          const float dlda = T[p] * gc - __fdividef(rest, one_minus);
-          // Opacity and exponent gradients vanish where alpha is clamped at 0.99.
-          const float gd = (blend[p] && raw[p] < kMaxAlpha) ? G[p] * dlda : 0.0f;
-          const float t = gd * dy[p];
-          u += gd;
-          st += t;
-          sty = fmaf(t, dy[p], sty);
-          c[6] += weight * dl0[p];
-          c[7] += weight * dl1[p];
-          c[8] += weight * dl2[p];
-          if constexpr (ABS) {
-            c[9] += fabsf(fmaf(t, mx, gd * lx));  // |dpow (lx + mx dy)| / opacity
-            c[10] += fabsf(fmaf(t, my, gd * ly));
-          }
-          T[p] = __fmul_rn(T[p], one_minus);
-          R[p] = rest;
-        }
-        if (__any_sync(0xffffffffu, has)) {
-          const float sd = A.z * u;
-          st *= A.z;
-          sty *= A.z;
-          c[0] = fmaf(lx, sd, mx * st);
-          c[1] = fmaf(ly, sd, my * st);
-          c[2] = (-0.5f * dx * dx) * sd;
-          c[3] = -dx * st;
-          c[4] = -0.5f * sty;
-          c[5] = u;
-          if constexpr (ABS) {
-            c[9] *= A.z;
-            c[10] *= A.z;
-          }
+        if (splat_adjoint<PX, ABS>(s_a[j], s_b[j], s_c[j].x, pos, cx, cy, dl0, dl1, dl2, last, T, R, c)) {
           if constexpr (ABS) {
             const uint32_t slot = warp_reduce_scatter12(c, lane);
             if (slot < 12u) s_part[warp][j][slot] = c[0];
@@ -932,6 +944,106 @@ __global__ void __launch_bounds__(128, 5) k_raster_bwd_warp(RasterArgs a) {
   }
 }
 
+// Fast mode with independent warps. A work item is one warp's block of the tile layout of
+// raster_bwd_tile (TileLayout<PX>: an 8 x 4PX block, 8 / PX of them a tile). The warp
+// stages its own rounds of 32 splats from the tile's list, stops at its block's own
+// furthest last contributor, and adds each splat's sums into the gaussian's accumulator
+// with three 16-byte vector atomics, so no warp waits at a block barrier for another
+// warp's pixels or round. Staging the tile's list once per warp instead of once per tile
+// costs about 2% more instructions. (The deterministic mode adds the warps of a tile in a
+// fixed order instead, in raster_bwd_tile.)
+struct SplitSmem {
+  float4 a[32], b[32], c[32];  // the round's staged splats (stage_splat)
+  uint32_t dst[32];            // their gaussians
+  float part[32][12];          // the round's per-splat warp sums
+  float lanes[32][12];         // the lanes' values of the splat being summed (warp_sum9_rows)
+};
+
+template <int PX>
+__device__ __forceinline__ void raster_bwd_split(const RasterArgs& a, uint32_t item, uint32_t lane, SplitSmem& sm) {
+  using L = TileLayout<PX>;
+  const uint32_t gt = item / uint32_t(L::kWarps), warp = item - gt * uint32_t(L::kWarps);
+  const L lay(a.vt, a.frames, gt, warp);
+  const uint2 range = a.rb.ranges[gt];
+  const uint32_t n = min(range.y - range.x, a.rb.tile_count[gt]);
+  if (n == 0u) return;
+  float cx = 0.0f, cy[PX], dl0[PX], dl1[PX], dl2[PX], R[PX], T[PX];
+  uint32_t last[PX], my_last = 0u;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    const uint2 px = lay.pixel(lane, p);
+    cx = float(px.x) + 0.5f;
+    cy[p] = float(px.y) + 0.5f;
+    dl0[p] = dl1[p] = dl2[p] = R[p] = 0.0f;
+    T[p] = 1.0f;
+    last[p] = 0u;
+    if (px.x < lay.W && px.y < lay.H) {
+      const size_t pix = size_t(a.vt->pixel_base[lay.v]) + size_t(px.y) * lay.W + px.x;
+      const float4 pg = a.rb.pixel_grad[pix];
+      dl0[p] = pg.x;
+      dl1[p] = pg.y;
+      dl2[p] = pg.z;
+      R[p] = a.rb.pixel_dot[pix];
+      last[p] = a.rb.pixel_count[pix];
+      my_last = max(my_last, last[p]);
+    }
+  }
+  const uint32_t stop = min(n, __reduce_max_sync(0xffffffffu, my_last));
+  const float block_h = float(4 * PX);
+  for (uint32_t start = 0; start < stop; start += 32u) {
+    __syncwarp();  // the previous round's reads of the staging buffers are done
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
+    if (start + lane < stop) {
+      const uint32_t g = a.rb.gauss[range.x + start + lane];
+      const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
+      stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
+      sm.a[lane] = A;
+      sm.b[lane] = B;
+      sm.c[lane] = C;
+      sm.dst[lane] = g;
+    }
+    __syncwarp();
+    const uint32_t nb = min(32u, stop - start);
+    uint32_t m = __ballot_sync(0xffffffffu, lane < nb && block_reached(A, B, C, lay.bx, lay.by, block_h));
+    uint32_t wrote = 0u;
+#pragma unroll 1
+    while (m != 0u) {
+      const uint32_t j = uint32_t(__ffs(m) - 1);
+      m &= m - 1u;
+      float c[12];
+      if (splat_adjoint<PX, false>(sm.a[j], sm.b[j], sm.c[j].x, start + j + 1u, cx, cy, dl0, dl1, dl2, last, T, R,
+                                   c)) {
+        const float sum = warp_sum9_rows(sm.lanes, c, lane);
+        if (lane < 12u) sm.part[j][lane] = lane < 9u ? sum : 0.0f;
+        wrote |= 1u << j;
+      }
+    }
+    __syncwarp();
+    for (uint32_t idx = lane; idx < nb * 3u; idx += 32u) {
+      const uint32_t j = idx / 3u, q = idx - 3u * j;
+      if ((wrote >> j) & 1u)
+        atomicAdd(reinterpret_cast<float4*>(a.grad2d) + size_t(sm.dst[j]) * 3u + q,
+                  *reinterpret_cast<const float4*>(&sm.part[j][4u * q]));
+    }
+  }
+}
+
+// Four independent warps a block, each with its own staging buffers; 6 blocks per SM.
+template <int PX>
+__global__ void __launch_bounds__(128, 6) k_raster_bwd_split(RasterArgs a) {
+  if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
+  __shared__ __align__(16) SplitSmem s_warp[4];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t total = a.vt->total_tiles * uint32_t(TileLayout<PX>::kWarps);
+  for (;;) {
+    uint32_t item = 0u;
+    if (lane == 0u) item = atomicAdd(a.queue, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= total) break;
+    raster_bwd_split<PX>(a, item, lane, s_warp[warp]);
+  }
+}
+
 // 3 PX blocks of 256 / PX threads per SM: 12 two-warp blocks at 4 pixels per thread (at
 // most 85 registers; with no bound the compiler settled on 72 with spills, measured 1%
 // slower, and a 64-register cap 18% slower).
@@ -972,8 +1084,28 @@ void launch_bwd_warp(const RasterArgs& a, const StepPointers& sp, cudaStream_t s
   k_raster_bwd_warp<DET><<<grid, 128, 0, st>>>(a);
 }
 
+template <int PX>
+void launch_bwd_split(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
+  static uint32_t grid = 0, cap = 0;
+  if (grid == 0 || cap != sp.tile_cap) {
+    grid = persistent_grid(k_raster_bwd_split<PX>, 128, sp);
+    cap = sp.tile_cap;
+  }
+  k_raster_bwd_split<PX><<<grid, 128, 0, st>>>(a);
+}
+
+// Fast mode at 1, 2 or 4 pixels per thread: the independent-warp kernel (its rounds are 32
+// splats and it stages with plain loads, whatever backward_batch and stage_async say).
 template <int BATCH, bool DET, bool ASYNC>
 void launch_bwd_px(const RasterArgs& a, const StepPointers& sp, int px, cudaStream_t st) {
+  if constexpr (!DET) {
+    if (px < 8) {
+      if (px >= 4) launch_bwd_split<4>(a, sp, st);
+      else if (px == 2) launch_bwd_split<2>(a, sp, st);
+      else launch_bwd_split<1>(a, sp, st);
+      return;
+    }
+  }
   if (px >= 8) launch_bwd_warp<DET>(a, sp, st);
   else if (px >= 4) launch_bwd<BATCH, DET, 4, ASYNC>(a, sp, st);
   else if (px == 2) launch_bwd<BATCH, DET, 2, ASYNC>(a, sp, st);
