@@ -528,9 +528,11 @@ struct gs_context {
         consider(t);
       }
       const uint32_t bpx0 = best.backward_pixels, batch0 = best.backward_batch;
+      // (The fast backward stages 32 splats per warp whatever backward_batch says, so in
+      // fast mode only the pixels per thread are tried.)
       for (uint32_t bpx : {2u, 4u})
         for (uint32_t batch : {32u, 64u})
-          if (bpx != bpx0 || batch != batch0) {
+          if ((bpx != bpx0 || batch != batch0) && (best.deterministic || batch == batch0)) {
             gs_tuning t = best;
             t.backward_pixels = bpx;
             t.backward_batch = batch;

@@ -13,16 +13,19 @@
 // last contributor (pixel_count), reproducing the forward's transmittance bit for bit
 // (same multiplications). Per splat it needs
 //   dL/dalpha_k = T_k (dL/dC . c_k) - R_{k+1} / (1 - alpha_k),  R_{k+1} = R_k - (dL/dC . c_k) alpha_k T_k.
-// A thread adds its PX pixels' gradients in registers; each warp then sums a splat's 11
-// values over its lanes (a reduce-scatter butterfly of 13 shuffles in deterministic mode;
-// in fast mode, 9 values through shared memory), skipped when no lane touched the splat,
-// and the warps' partials are added in a fixed order, so the per-pair gradient is
-// bit-stable. Deterministic mode
-// stores it at the pair's pre-sort index (pair_grads, summed per gaussian by
-// train_pair_sum's fixed order); fast mode adds it to the gaussian's accumulator with
-// three 16-byte vector atomics per tile (red.global.add.v4.f32). Fast mode also leaves out
-// the |dL/dmean2d| sums (pair values 9 and 10): they feed only the densify statistic
-// stats.w, which no densify decision reads (train_densify_mark.comp:22-57 uses x, y, z).
+// A thread adds its PX pixels' gradients in registers (splat_adjoint); its warp then sums
+// the splat's values over its lanes, skipped when no lane touched the splat.
+// - Deterministic mode (raster_bwd_tile): the warps of a tile share each staged round; a
+//   warp sums a splat's 11 values with a reduce-scatter butterfly (13 shuffles), the warps'
+//   partials are added in a fixed order, and the pair's gradient is stored at its pre-sort
+//   index (pair_grads, summed per gaussian by train_pair_sum's fixed order): bit-stable.
+// - Fast mode (raster_bwd_split): each warp works on its own block of a tile, stages its
+//   own rounds and stops at its own last contributor; it sums 9 values through shared
+//   memory and adds them to the gaussian's accumulator with three 16-byte vector atomics
+//   (red.global.add.v4.f32). It leaves out the |dL/dmean2d| sums (pair values 9 and 10):
+//   they feed only the densify statistic stats.w, which no densify decision reads
+//   (train_densify_mark.comp:22-57 uses x, y, z).
+// - backward_pixels = 8 (raster_bwd_warp_tile): one warp per whole tile, either mode.
 #include "gs_kernels.h"
 
 namespace gsk {
@@ -573,8 +576,9 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
 
 // ASYNC: the splat records of round i + 1 are copied with cp.async while round i is
 // differentiated (as in the forward).
-template <int BATCH, bool DET, int PX, bool ASYNC>
+template <int BATCH, int PX, bool ASYNC>
 __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt) {
+  constexpr bool DET = true;  // this layout serves the deterministic mode (fast mode: raster_bwd_split)
   constexpr bool ABS = DET;  // the |dL/dmean2d| sums (see the top of the file)
   using L = TileLayout<PX>;
   static_assert(BATCH <= L::kThreads, "one staged splat per thread");
@@ -585,7 +589,6 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   __shared__ uint32_t s_dst[BATCH];
   __shared__ float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
-  __shared__ __align__(16) float s_lanes[DET ? 1 : L::kWarps][DET ? 1 : 32][12];  // fast mode: warp_sum9_rows
 
   const uint32_t lid = threadIdx.x, lane = lid & 31u, warp = lid >> 5;
   const L lay(a.vt, a.frames, gt, warp);
@@ -700,47 +703,23 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
         float c[12];
         if (splat_adjoint<PX, ABS>(s_a[j], s_b[j], s_c[j].x, pos, cx, cy, dl0, dl1, dl2, last, T, R, c)) {
-          if constexpr (ABS) {
-            const uint32_t slot = warp_reduce_scatter12(c, lane);
-            if (slot < 12u) s_part[warp][j][slot] = c[0];
-          } else {
-            const float sum = warp_sum9_rows(s_lanes[warp], c, lane);
-            if (lane < 12u) s_part[warp][j][lane] = lane < 9u ? sum : 0.0f;
-          }
+          const uint32_t slot = warp_reduce_scatter12(c, lane);
+          if (slot < 12u) s_part[warp][j][slot] = c[0];
           wrote |= 1u << (j & 31u);
         }
       }
       if (lane == 0) s_wrote[warp][w] = wrote;
     }
     __syncthreads();
-    if constexpr (DET) {
-      for (uint32_t idx = lid; idx < nb * 12u; idx += L::kThreads) {
-        const uint32_t j = idx / 12u, k = idx - j * 12u;
-        float s = 0.0f;
+    // The pair's gradient at its pre-sort index: the warps' partials added in order (zero
+    // for a splat no warp drew), for train_pair_sum's fixed-order sum per gaussian.
+    for (uint32_t idx = lid; idx < nb * 12u; idx += L::kThreads) {
+      const uint32_t j = idx / 12u, k = idx - j * 12u;
+      float s = 0.0f;
 #pragma unroll
-        for (int w8 = 0; w8 < L::kWarps; ++w8)
-          if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) s += s_part[w8][j][k];
-        a.pair_grads[size_t(s_dst[j]) * 12u + k] = s;
-      }
-    } else {
-      // One float4 of the gaussian's accumulator per thread: the warps' partials added in
-      // order, then one vector atomic (skipped for a splat no warp drew).
-      for (uint32_t idx = lid; idx < nb * 3u; idx += L::kThreads) {
-        const uint32_t j = idx / 3u, q = idx - j * 3u;
-        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool any = false;
-#pragma unroll
-        for (int w8 = 0; w8 < L::kWarps; ++w8)
-          if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) {
-            const float* part = &s_part[w8][j][q * 4u];
-            s.x += part[0];
-            s.y += part[1];
-            s.z += part[2];
-            s.w += part[3];
-            any = true;
-          }
-        if (any) atomicAdd(reinterpret_cast<float4*>(a.grad2d) + size_t(s_dst[j]) * 3u + q, s);
-      }
+      for (int w8 = 0; w8 < L::kWarps; ++w8)
+        if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) s += s_part[w8][j][k];
+      a.pair_grads[size_t(s_dst[j]) * 12u + k] = s;
     }
   }
   if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
@@ -1047,12 +1026,12 @@ __global__ void __launch_bounds__(128, 6) k_raster_bwd_split(RasterArgs a) {
 // 3 PX blocks of 256 / PX threads per SM: 12 two-warp blocks at 4 pixels per thread (at
 // most 85 registers; with no bound the compiler settled on 72 with spills, measured 1%
 // slower, and a 64-register cap 18% slower).
-template <int BATCH, bool DET, int PX, bool ASYNC>
+template <int BATCH, int PX, bool ASYNC>
 __global__ void __launch_bounds__(256 / PX, 3 * PX) k_raster_bwd(RasterArgs a) {
   if (*a.d_pairs > a.accept) return;  // more pairs than stored: the step's update is skipped
   const uint32_t total = a.vt->total_tiles;
   for (uint32_t gt = next_tile(a.queue); gt < total; gt = next_tile(a.queue))
-    raster_bwd_tile<BATCH, DET, PX, ASYNC>(a, gt);
+    raster_bwd_tile<BATCH, PX, ASYNC>(a, gt);
 }
 
 // A persistent grid: as many blocks as fit on the GPU at once (at most one per tile).
@@ -1064,14 +1043,14 @@ uint32_t persistent_grid(Kernel kernel, int threads, const StepPointers& sp) {
   return min(sp.tile_cap, uint32_t(per_sm) * uint32_t(sp.sm_count));
 }
 
-template <int BATCH, bool DET, int PX, bool ASYNC>
+template <int BATCH, int PX, bool ASYNC>
 void launch_bwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   static uint32_t grid = 0, cap = 0;
   if (grid == 0 || cap != sp.tile_cap) {
-    grid = persistent_grid(k_raster_bwd<BATCH, DET, PX, ASYNC>, 256 / PX, sp);
+    grid = persistent_grid(k_raster_bwd<BATCH, PX, ASYNC>, 256 / PX, sp);
     cap = sp.tile_cap;
   }
-  k_raster_bwd<BATCH, DET, PX, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
+  k_raster_bwd<BATCH, PX, ASYNC><<<grid, 256 / PX, 0, st>>>(a);
 }
 
 template <bool DET>
@@ -1094,22 +1073,23 @@ void launch_bwd_split(const RasterArgs& a, const StepPointers& sp, cudaStream_t 
   k_raster_bwd_split<PX><<<grid, 128, 0, st>>>(a);
 }
 
-// Fast mode at 1, 2 or 4 pixels per thread: the independent-warp kernel (its rounds are 32
-// splats and it stages with plain loads, whatever backward_batch and stage_async say).
+// 8 pixels per thread: one warp per tile, either mode. Fast mode at 1, 2 or 4: the
+// independent-warp kernel (its rounds are 32 splats and it stages with plain loads,
+// whatever backward_batch and stage_async say). Deterministic mode at 1, 2 or 4: the
+// block kernel, whose warps' partials are added in a fixed order.
 template <int BATCH, bool DET, bool ASYNC>
 void launch_bwd_px(const RasterArgs& a, const StepPointers& sp, int px, cudaStream_t st) {
-  if constexpr (!DET) {
-    if (px < 8) {
-      if (px >= 4) launch_bwd_split<4>(a, sp, st);
-      else if (px == 2) launch_bwd_split<2>(a, sp, st);
-      else launch_bwd_split<1>(a, sp, st);
-      return;
-    }
+  if (px >= 8) {
+    launch_bwd_warp<DET>(a, sp, st);
+  } else if constexpr (DET) {
+    if (px >= 4) launch_bwd<BATCH, 4, ASYNC>(a, sp, st);
+    else if (px == 2) launch_bwd<BATCH, 2, ASYNC>(a, sp, st);
+    else launch_bwd<BATCH, 1, ASYNC>(a, sp, st);
+  } else {
+    if (px >= 4) launch_bwd_split<4>(a, sp, st);
+    else if (px == 2) launch_bwd_split<2>(a, sp, st);
+    else launch_bwd_split<1>(a, sp, st);
   }
-  if (px >= 8) launch_bwd_warp<DET>(a, sp, st);
-  else if (px >= 4) launch_bwd<BATCH, DET, 4, ASYNC>(a, sp, st);
-  else if (px == 2) launch_bwd<BATCH, DET, 2, ASYNC>(a, sp, st);
-  else launch_bwd<BATCH, DET, 1, ASYNC>(a, sp, st);
 }
 
 template <int BATCH>
