@@ -153,7 +153,8 @@ typedef struct gs_tuning {
   uint32_t backward_batch;    /* splats staged per round of the deterministic backward: 32 or 64
                                  (0: default); the fast backward stages 32 per warp */
   uint32_t sort_digit_bits;   /* radix digit width of the depth and pair sorts: 4..8 (0: default 8) */
-  uint32_t forward_batch;     /* splats staged per round of the forward pass: 64, 128 or 256 (0: default 256) */
+  uint32_t forward_batch;     /* splats staged per round of the forward pass with stage_async: 64, 128 or
+                                 256 (0: default 256); without it each warp stages 32 per round */
   uint32_t tune_reduction;    /* 1: gs_autotune may also switch `deterministic` (0: it keeps the caller's) */
   uint32_t stage_async;       /* 1: raster passes copy the next round of splats with cp.async while the
                                  current one blends (double-buffered; the forward and the

@@ -131,6 +131,8 @@ struct gs_context {
   uint2* ranges = nullptr;
   float* tile_loss = nullptr;
   uint32_t* tile_count = nullptr;
+  float* tile_part = nullptr;
+  uint32_t* tile_done = nullptr;
   // pairs
   uint64_t pair_cap = 0;
   uint32_t *keys = nullptr, *values = nullptr, *keys_alt = nullptr, *values_alt = nullptr, *pair_gaussian = nullptr;
@@ -179,8 +181,8 @@ struct gs_context {
     for (float4** p : {&model.P, &model.M, &model.V, &model.stats, &vb.splat, &vb.foot, &vb.grad2d, &vb.dir_grad, &pixel_grad,
                        &pixel_out, &ssim_maps, &pair_grads})
       dev_free(*p);
-    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &pose_partial, &motion_partial,
-                     &ssim_last})
+    for (float** p : {&model.SH, &model.MSH, &model.VSH, &pixel_dot, &tile_loss, &tile_part, &pose_partial,
+                      &motion_partial, &ssim_last})
       dev_free(*p);
     dev_free(vb.spans);
     dev_free(motion_rest);
@@ -192,7 +194,7 @@ struct gs_context {
     h_motion_views = nullptr;
     h_motion_grad = nullptr;
     for (uint32_t** p : {&vb.tiles, &vb.offsets, &dkeys, &dvals, &dkeys_alt, &dvals_alt, &sorted_offsets, &target,
-                         &pixel_count, &image, &tile_count, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
+                         &pixel_count, &image, &tile_count, &tile_done, &keys, &values, &keys_alt, &values_alt, &pair_gaussian,
                          &sorted_g,
                          &d_scalars, &sort.hist, &sort.tile_counts, &dens.spawn,
                          &dens.release, &dens.wants, &dens.free_pos, &dens.spawn_pos, &dens.free_list,
@@ -286,6 +288,9 @@ struct gs_context {
       dev_alloc(ranges, tiles + 1);
       dev_alloc(tile_loss, (tiles + 1) * 16);
       dev_alloc(tile_count, tiles + 1);
+      dev_alloc(tile_part, (tiles + 1) * gsk::kTileWarpSlots * 16);
+      dev_alloc(tile_done, tiles + 1);
+      GS_CUDA_TRY(cudaMemsetAsync(tile_done, 0, (tiles + 1) * sizeof(uint32_t), stream));  // then each tile resets its own
       tile_cap = tiles + 1;
     }
   }
@@ -522,7 +527,7 @@ struct gs_context {
           t.forward_pixels = fpx;
           consider(t);
         }
-      {  // the forward's round size at the chosen pixels per thread
+      if (best.stage_async) {  // the forward's round size (only its block kernel stages rounds of it)
         gs_tuning t = best;
         t.forward_batch = best.forward_batch == 128u ? 256u : 128u;
         consider(t);
@@ -604,6 +609,8 @@ struct gs_context {
     rb.pixel_dot = pixel_dot;
     rb.tile_loss = tile_loss;
     rb.tile_count = tile_count;
+    rb.tile_part = tile_part;
+    rb.tile_done = tile_done;
     rb.ssim_maps = ssim_maps;
     rb.ssim_last = ssim_last;
     return rb;

@@ -107,11 +107,17 @@ struct RasterBuffers {
   float* pixel_dot = nullptr;
   float* tile_loss = nullptr;               // 16 per global tile
   uint32_t* tile_count = nullptr;
+  // The forward's per-warp tile sums (kTileWarpSlots warps x 16 floats per tile; slot 14
+  // holds the warp's furthest last contributor as bits) and, per tile, how many of its
+  // warps have written theirs (the last one adds them up and resets it to 0).
+  float* tile_part = nullptr;
+  uint32_t* tile_done = nullptr;
   // The SSIM gradient maps w A, w B, w C (rgb each) of every pixel, 36 bytes:
   // ssim_maps[2 p] = (A rgb, B r), ssim_maps[2 p + 1] = (B g, B b, C r, C g), ssim_last[p] = C b.
   float4* ssim_maps = nullptr;
   float* ssim_last = nullptr;
 };
+constexpr uint32_t kTileWarpSlots = 8;  // the most warps a tile has (one pixel per thread)
 // px: pixels per thread (1, 2 or 4); batch: splats staged per round (64, 128, 256);
 // async: stage the next round with cp.async while the current one blends. contributions
 // (non-null): a counting launch that also adds the evaluations that blend into it.

@@ -228,6 +228,121 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue) {
   return item;
 }
 
+// One staged splat blended into a warp's PX pixels at 1-based position `contributor` of the
+// tile's list (train_forward.comp:96-121); returns whether all the lane's pixels are done.
+template <int PX, bool COUNT>
+__device__ __forceinline__ bool splat_blend(const float4 A, const float4 B, const float blue, const uint32_t contributor,
+                                            const float cx, const float (&cy)[PX], bool (&done)[PX], float (&T)[PX],
+                                            float (&C0)[PX], float (&C1)[PX], float (&C2)[PX], uint32_t (&last)[PX],
+                                            uint32_t& blended) {
+  const float dx = __fsub_rn(A.x, cx);
+  const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
+  bool all_done = true;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    // Predicated rather than branched: a pixel that is done, or skips this splat, blends
+    // it with alpha 0, which adds zero weight and keeps T (T (1 - 0) = T) and its last
+    // contributor, bit for bit. Where it blends, T (1 - alpha) is the same product the
+    // stop test formed.
+    const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
+    const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
+    const bool blend = !done[p] && e <= 0.0f && alpha >= kMinAlpha;
+    const bool stop = blend && __fmul_rn(T[p], __fsub_rn(1.0f, alpha)) < kMinTransmittance;
+    const bool ok = blend && !stop;
+    done[p] = done[p] || stop;
+    const float ab = ok ? alpha : 0.0f;
+    const float weight = ab * T[p];
+    C0[p] += B.z * weight;
+    C1[p] += B.w * weight;
+    C2[p] += blue * weight;
+    T[p] = __fmul_rn(T[p], __fsub_rn(1.0f, ab));
+    last[p] = ok ? contributor : last[p];
+    if constexpr (COUNT) blended += ok ? 1u : 0u;
+    all_done = all_done && done[p];
+  }
+  return all_done;
+}
+
+// The forward's per-pixel outputs of a warp's PX pixels (train_forward.comp:123-183): colour over
+// the background, dL/dC of the L1 part and final T, the last contributor, the RGBA8 image and
+// dL/dC . C; and the warp's 14 loss and fit sums in vals (every lane holds the warp's total,
+// summed by a butterfly in a fixed order). Returns the warp's furthest last contributor.
+template <int PX>
+__device__ __forceinline__ uint32_t pixels_out(const RasterArgs& a, const TileLayout<PX>& lay, const gs_frame_data& f,
+                                               const uint32_t lane, const bool (&inside)[PX], const float cx,
+                                               const float (&cy)[PX], const float (&T)[PX], const float (&C0)[PX],
+                                               const float (&C1)[PX], const float (&C2)[PX],
+                                               const uint32_t (&last)[PX], float (&vals)[14]) {
+#pragma unroll
+  for (int k = 0; k < 14; ++k) vals[k] = 0.0f;
+  uint32_t my_max = 0u;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    if (!inside[p]) continue;
+    const uint2 px = lay.pixel(lane, p);
+    const size_t local = size_t(px.y) * lay.W + px.x;
+    const size_t pix = size_t(a.vt->pixel_base[lay.v]) + local;
+    const float o0 = C0[p] + T[p] * f.background[0], o1 = C1[p] + T[p] * f.background[1],
+                o2 = C2[p] + T[p] * f.background[2];
+    float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, w = 1.0f;
+    const uint32_t* target = a.vt->target[lay.v];
+    if (target != nullptr) {
+      const uint32_t u = target[local];
+      const float ta = float(u >> 24) / 255.0f;
+      const float tr[3] = {float(u & 255u) / 255.0f, float((u >> 8) & 255u) / 255.0f, float((u >> 16) & 255u) / 255.0f};
+      const bool masked = (f.model[3] & GS_FLAG_MASKED_TARGET) != 0u;
+      float tc[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float photo = tr[c] * f.exposure[c];
+        tc[c] = masked ? f.background[c] * (1.0f - ta) + photo * ta : photo;
+      }
+      const float e0 = o0 - tc[0], e1 = o1 - tc[1], e2 = o2 - tc[2];
+      w = pixel_weight(make_float4(f.head[0], f.head[1], f.head[2], f.head[3]), cx, cy[p]);
+      const float s = (1.0f - f.loss[0]) * f.background[3] * w;
+      d0 = e0 > 0.0f ? s : (e0 < 0.0f ? -s : 0.0f);
+      d1 = e1 > 0.0f ? s : (e1 < 0.0f ? -s : 0.0f);
+      d2 = e2 > 0.0f ? s : (e2 < 0.0f ? -s : 0.0f);
+      const float l0 = fabsf(e0) + fabsf(e1) + fabsf(e2);
+      const float l1 = e0 * e0 + e1 * e1 + e2 * e2;
+      vals[0] += l0;
+      vals[1] += l1;
+      vals[2] += w * l0;
+      vals[3] += 3.0f * w;
+      const float hx = cx - f.head[0], hy = cy[p] - f.head[1];
+      if (f.head[2] > 0.0f && sqrtf(hx * hx + hy * hy) <= f.head[2]) {
+        vals[4] += l1;
+        vals[5] += 1.0f;
+      }
+      if (ta > 0.95f && T[p] < 0.05f) {
+        vals[6] += C0[p] * C0[p];
+        vals[7] += C1[p] * C1[p];
+        vals[8] += C2[p] * C2[p];
+        vals[9] += 1.0f;
+        vals[10] += C0[p] * tr[0];
+        vals[11] += C1[p] * tr[1];
+        vals[12] += C2[p] * tr[2];
+      }
+      vals[13] += ta > 0.0f ? 1.0f : 0.0f;
+    }
+    a.rb.pixel_out[pix] = make_float4(o0, o1, o2, w);
+    a.rb.pixel_grad[pix] = make_float4(d0, d1, d2, T[p]);
+    a.rb.pixel_count[pix] = last[p];
+    a.rb.image[pix] = pack_unorm(o0) | pack_unorm(o1) << 8 | pack_unorm(o2) << 16 | pack_unorm(1.0f - T[p]) << 24;
+    a.rb.pixel_dot[pix] = d0 * o0 + d1 * o1 + d2 * o2;
+    my_max = max(my_max, last[p]);
+  }
+  // The warp's sums, by a butterfly in a fixed order.
+#pragma unroll
+  for (int k = 0; k < 14; ++k) {
+    float x = vals[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    vals[k] = x;
+  }
+  return __reduce_max_sync(0xffffffffu, my_max);
+}
+
 // COUNT: also add up the evaluations that blend (alpha >= 1/255, in front of the pixel's
 // stop) into *contributions, for the work figure of the pass's roofline.
 // FB splats are staged per round (64, 128 or 256: a tuning knob). With ASYNC the records of
@@ -352,110 +467,15 @@ __device__ __forceinline__ void raster_fwd_tile(const RasterArgs& a, uint32_t gt
         const uint32_t j = uint32_t(w) * 32u + uint32_t(__ffs(m) - 1);
         m &= m - 1u;
         const uint32_t contributor = base + j + 1u;
-        const float4 A = s_a[j];
-        const float4 B = s_b[j];
-        const float blue = s_c[j].x;
-        const float dx = __fsub_rn(A.x, cx);
-        const float e0 = __fmul_rn(__fmul_rn(A.w, dx), dx), e1 = __fmul_rn(B.x, dx);
-        all_done = true;
-#pragma unroll
-        for (int p = 0; p < PX; ++p) {
-          {
-            // Predicated rather than branched: a pixel that is done, or skips this splat,
-            // blends it with alpha 0, which adds zero weight and keeps T (T (1 - 0) = T) and
-            // its last contributor, bit for bit. Where it blends, T (1 - alpha) is the same
-            // product the stop test formed.
-            const float e = splat_exponent(e0, e1, B.y, __fsub_rn(A.y, cy[p]));
-            const float alpha = fminf(kMaxAlpha, __fmul_rn(A.z, exp2_approx(e)));
-            const bool blend = !done[p] && e <= 0.0f && alpha >= kMinAlpha;
-            const bool stop = blend && __fmul_rn(T[p], __fsub_rn(1.0f, alpha)) < kMinTransmittance;
-            const bool ok = blend && !stop;
-            done[p] = done[p] || stop;
-            const float ab = ok ? alpha : 0.0f;
-            const float weight = ab * T[p];
-            C0[p] += B.z * weight;
-            C1[p] += B.w * weight;
-            C2[p] += blue * weight;
-            T[p] = __fmul_rn(T[p], __fsub_rn(1.0f, ab));
-            last[p] = ok ? contributor : last[p];
-            if constexpr (COUNT) blended += ok ? 1u : 0u;
-          }
-          all_done = all_done && done[p];
-        }
+        all_done = splat_blend<PX, COUNT>(s_a[j], s_b[j], s_c[j].x, contributor, cx, cy, done, T, C0, C1, C2, last,
+                                          blended);
       }
     }
   }
   if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
 
   float vals[14];
-#pragma unroll
-  for (int k = 0; k < 14; ++k) vals[k] = 0.0f;
-  uint32_t my_max = 0u;
-#pragma unroll
-  for (int p = 0; p < PX; ++p) {
-    if (!inside[p]) continue;
-    const uint2 px = lay.pixel(lane, p);
-    const size_t local = size_t(px.y) * lay.W + px.x;
-    const size_t pix = size_t(a.vt->pixel_base[lay.v]) + local;
-    const float o0 = C0[p] + T[p] * f.background[0], o1 = C1[p] + T[p] * f.background[1],
-                o2 = C2[p] + T[p] * f.background[2];
-    float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, w = 1.0f;
-    const uint32_t* target = a.vt->target[lay.v];
-    if (target != nullptr) {
-      const uint32_t u = target[local];
-      const float ta = float(u >> 24) / 255.0f;
-      const float tr[3] = {float(u & 255u) / 255.0f, float((u >> 8) & 255u) / 255.0f, float((u >> 16) & 255u) / 255.0f};
-      const bool masked = (f.model[3] & GS_FLAG_MASKED_TARGET) != 0u;
-      float tc[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float photo = tr[c] * f.exposure[c];
-        tc[c] = masked ? f.background[c] * (1.0f - ta) + photo * ta : photo;
-      }
-      const float e0 = o0 - tc[0], e1 = o1 - tc[1], e2 = o2 - tc[2];
-      w = pixel_weight(make_float4(f.head[0], f.head[1], f.head[2], f.head[3]), cx, cy[p]);
-      const float s = (1.0f - f.loss[0]) * f.background[3] * w;
-      d0 = e0 > 0.0f ? s : (e0 < 0.0f ? -s : 0.0f);
-      d1 = e1 > 0.0f ? s : (e1 < 0.0f ? -s : 0.0f);
-      d2 = e2 > 0.0f ? s : (e2 < 0.0f ? -s : 0.0f);
-      const float l0 = fabsf(e0) + fabsf(e1) + fabsf(e2);
-      const float l1 = e0 * e0 + e1 * e1 + e2 * e2;
-      vals[0] += l0;
-      vals[1] += l1;
-      vals[2] += w * l0;
-      vals[3] += 3.0f * w;
-      const float hx = cx - f.head[0], hy = cy[p] - f.head[1];
-      if (f.head[2] > 0.0f && sqrtf(hx * hx + hy * hy) <= f.head[2]) {
-        vals[4] += l1;
-        vals[5] += 1.0f;
-      }
-      if (ta > 0.95f && T[p] < 0.05f) {
-        vals[6] += C0[p] * C0[p];
-        vals[7] += C1[p] * C1[p];
-        vals[8] += C2[p] * C2[p];
-        vals[9] += 1.0f;
-        vals[10] += C0[p] * tr[0];
-        vals[11] += C1[p] * tr[1];
-        vals[12] += C2[p] * tr[2];
-      }
-      vals[13] += ta > 0.0f ? 1.0f : 0.0f;
-    }
-    a.rb.pixel_out[pix] = make_float4(o0, o1, o2, w);
-    a.rb.pixel_grad[pix] = make_float4(d0, d1, d2, T[p]);
-    a.rb.pixel_count[pix] = last[p];
-    a.rb.image[pix] = pack_unorm(o0) | pack_unorm(o1) << 8 | pack_unorm(o2) << 16 | pack_unorm(1.0f - T[p]) << 24;
-    a.rb.pixel_dot[pix] = d0 * o0 + d1 * o1 + d2 * o2;
-    my_max = max(my_max, last[p]);
-  }
-  // Tile sums in a fixed order: a butterfly per warp, then the warps.
-#pragma unroll
-  for (int k = 0; k < 14; ++k) {
-    float x = vals[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    vals[k] = x;
-  }
-  const uint32_t wmax = __reduce_max_sync(0xffffffffu, my_max);
+  const uint32_t wmax = pixels_out<PX>(a, lay, f, lane, inside, cx, cy, T, C0, C1, C2, last, vals);
   if constexpr (COUNT) {
     const uint32_t wsum = __reduce_add_sync(0xffffffffu, blended);
     if (lane == 0 && wsum) atomicAdd(a.contributions, static_cast<unsigned long long>(wsum));
@@ -572,6 +592,120 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
     c[10] *= A.z;
   }
   return true;
+}
+
+// The forward with independent warps (the default without stage_async). A work item is one
+// warp's 8 x 4PX block of a tile (TileLayout<PX>); the warp stages its own rounds of 32
+// splats from the tile's list and stops when all its pixels are done, with no block
+// barrier. Each warp publishes its 14 tile sums and its furthest last contributor; the
+// warp that finishes a tile last (a per-tile counter) adds the warps' sums in warp order,
+// the same order as raster_fwd_tile, so the tile sums are bit-identical to it, writes
+// them, and resets the counter for the next step.
+struct FwdSplitSmem {
+  float4 a[32], b[32], c[32];  // the round's staged splats (stage_splat)
+};
+
+template <int PX, bool COUNT>
+__device__ __forceinline__ void raster_fwd_split(const RasterArgs& a, uint32_t item, uint32_t lane,
+                                                 FwdSplitSmem& sm) {
+  using L = TileLayout<PX>;
+  const uint32_t gt = item / uint32_t(L::kWarps), warp = item - gt * uint32_t(L::kWarps);
+  const L lay(a.vt, a.frames, gt, warp);
+  const gs_frame_data& f = a.frames[lay.v];
+  const uint2 range = a.rb.ranges[gt];
+
+  bool inside[PX], done[PX];
+  float cx = 0.0f, cy[PX], T[PX], C0[PX], C1[PX], C2[PX];
+  uint32_t last[PX];
+  uint32_t blended = 0u;  // COUNT
+  bool all_done = true;
+#pragma unroll
+  for (int p = 0; p < PX; ++p) {
+    const uint2 px = lay.pixel(lane, p);
+    inside[p] = px.x < lay.W && px.y < lay.H;
+    done[p] = !inside[p];
+    all_done = all_done && done[p];
+    cx = float(px.x) + 0.5f;
+    cy[p] = float(px.y) + 0.5f;
+    T[p] = 1.0f;
+    C0[p] = C1[p] = C2[p] = 0.0f;
+    last[p] = 0u;
+  }
+  const float block_h = float(4 * PX);
+  for (uint32_t start = range.x; start < range.y; start += 32u) {
+    if (__all_sync(0xffffffffu, all_done)) break;
+    __syncwarp();  // the previous round's reads of the staging buffers are done
+    const uint32_t k = start + lane;
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
+    if (k < range.y) {
+      const uint32_t g = a.rb.gauss[k];
+      const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
+      stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
+      sm.a[lane] = A;
+      sm.b[lane] = B;
+      sm.c[lane] = C;
+    }
+    __syncwarp();
+    uint32_t m = __ballot_sync(0xffffffffu, k < range.y && block_reached(A, B, C, lay.bx, lay.by, block_h));
+    const uint32_t base = start - range.x;  // position in the tile's list of the round's first splat
+    while (m != 0u && !all_done) {
+      const uint32_t j = uint32_t(__ffs(m) - 1);
+      m &= m - 1u;
+      all_done = splat_blend<PX, COUNT>(sm.a[j], sm.b[j], sm.c[j].x, base + j + 1u, cx, cy, done, T, C0, C1, C2, last,
+                                        blended);
+    }
+  }
+
+  float vals[14];
+  const uint32_t wmax = pixels_out<PX>(a, lay, f, lane, inside, cx, cy, T, C0, C1, C2, last, vals);
+  if constexpr (COUNT) {
+    const uint32_t wsum = __reduce_add_sync(0xffffffffu, blended);
+    if (lane == 0 && wsum) atomicAdd(a.contributions, static_cast<unsigned long long>(wsum));
+  }
+  float* parts = a.rb.tile_part + size_t(gt) * (kTileWarpSlots * 16u);
+  uint32_t last_warp = 0u;
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 14; ++v) parts[warp * 16u + uint32_t(v)] = vals[v];
+    parts[warp * 16u + 14u] = __uint_as_float(wmax);
+    __threadfence();  // the sums are visible before the count says so
+    last_warp = atomicAdd(a.rb.tile_done + gt, 1u) == uint32_t(L::kWarps) - 1u ? 1u : 0u;
+  }
+  if (__shfl_sync(0xffffffffu, last_warp, 0) == 0u) return;
+  __threadfence();
+  if (lane < 16u) {
+    float sum = 0.0f;
+    if (lane < 14u)
+      for (int w8 = 0; w8 < L::kWarps; ++w8) sum += __ldcg(parts + w8 * 16 + int(lane));
+    // Layout of train_forward.comp:18-23 (slots 2 and 4 are the SSIM pass's):
+    // values 0, 1 -> slots 0, 1; value 2 -> slot 3; values 3..13 -> slots 5..15.
+    float* tl = a.rb.tile_loss + size_t(gt) * 16u;
+    if (lane < 14u) tl[lane < 2u ? lane : (lane == 2u ? 3u : lane + 2u)] = sum;
+    if (lane == 14u) tl[2] = 0.0f;
+    if (lane == 15u) tl[4] = 0.0f;
+  }
+  if (lane == 0u) {
+    uint32_t most = 0u;
+    for (int w8 = 0; w8 < L::kWarps; ++w8) most = max(most, __float_as_uint(__ldcg(parts + w8 * 16 + 14)));
+    a.rb.tile_count[gt] = most;
+    a.rb.tile_done[gt] = 0u;
+  }
+}
+
+// Four independent warps a block, each with its own staging buffers (8 blocks per SM; 6 at
+// 4 pixels per thread, whose 64-register cap would spill).
+template <int PX, bool COUNT>
+__global__ void __launch_bounds__(128, PX == 4 ? 6 : 8) k_raster_fwd_split(RasterArgs a) {
+  __shared__ __align__(16) FwdSplitSmem s_warp[4];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t total = a.vt->total_tiles * uint32_t(TileLayout<PX>::kWarps);
+  for (;;) {
+    uint32_t item = 0u;
+    if (lane == 0u) item = atomicAdd(a.queue, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= total) break;
+    raster_fwd_split<PX, COUNT>(a, item, lane, s_warp[warp]);
+  }
 }
 
 // ASYNC: the splat records of round i + 1 are copied with cp.async while round i is
@@ -1114,6 +1248,16 @@ void launch_fwd(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
   k_raster_fwd<PX, FB, ASYNC, COUNT><<<grid, 256 / PX, 0, st>>>(a);
 }
 
+template <int PX, bool COUNT>
+void launch_fwd_split(const RasterArgs& a, const StepPointers& sp, cudaStream_t st) {
+  static uint32_t grid = 0, cap = 0;
+  if (grid == 0 || cap != sp.tile_cap) {
+    grid = persistent_grid(k_raster_fwd_split<PX, COUNT>, 128, sp);
+    cap = sp.tile_cap;
+  }
+  k_raster_fwd_split<PX, COUNT><<<grid, 128, 0, st>>>(a);
+}
+
 template <int PX, bool ASYNC>
 void launch_fwd_batch(const RasterArgs& a, const StepPointers& sp, int batch, cudaStream_t st) {
   if (batch >= 256) launch_fwd<PX, 256, ASYNC>(a, sp, st);
@@ -1135,9 +1279,15 @@ void launch_raster_forward(const StepPointers& sp, const ViewBuffers& vb, const 
   RasterArgs a{sp.frames, sp.vt, sp.queue + kQueueForward, rb, vb.splat, vb.foot, nullptr, nullptr, nullptr, 0u,
                contributions};
   if (contributions != nullptr) {  // the counting variant: same blend, plus the count
-    if (px >= 4) launch_fwd<4, 256, false, true>(a, sp, st);
-    else if (px == 2) launch_fwd<2, 256, false, true>(a, sp, st);
-    else launch_fwd<1, 256, false, true>(a, sp, st);
+    if (px >= 4) launch_fwd_split<4, true>(a, sp, st);
+    else if (px == 2) launch_fwd_split<2, true>(a, sp, st);
+    else launch_fwd_split<1, true>(a, sp, st);
+    return;
+  }
+  if (!async) {  // independent warps (their rounds are 32 splats whatever `batch` says)
+    if (px >= 4) launch_fwd_split<4, false>(a, sp, st);
+    else if (px == 2) launch_fwd_split<2, false>(a, sp, st);
+    else launch_fwd_split<1, false>(a, sp, st);
     return;
   }
   if (px >= 4) launch_fwd_mode<4>(a, sp, batch, async, st);

@@ -117,7 +117,9 @@ def test_async_staging_is_bit_identical(ctx):
     when the records arrive, not what is computed: the forward's outputs, the per-pair
     gradients and the moments equal the plain-load staging bit for bit, at every forward
     batch and both backward batches (the batch changes how a tile's list is cut into rounds,
-    not the order or the sums), on a view whose tiles hold several rounds of splats."""
+    not the order or the sums), on a view whose tiles hold several rounds of splats. Without
+    cp.async the forward runs its independent-warp kernel (each warp staging its own rounds
+    of 32), so this also checks that kernel against the block kernel bit for bit."""
     scene, cam, opt, target = view_and_target(n=60000)
     frozen = F.frozen_options(1, False)
     frozen.lambda_dssim, frozen.lambda_dssim_end = 0.2, -1.0
