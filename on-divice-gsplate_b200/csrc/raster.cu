@@ -1,12 +1,16 @@
 // Tile rasterisation: forward blend (train_forward.comp:59-183) and its adjoint
 // (train_common.glsl:215-253; the front-to-back form of train_backward_bucket.glsl:14-16).
 //
-// Both run one block per 16x16 tile of the flattened (view, tile) space, so a batch of
-// views of uneven resolution is one launch. Each thread owns PX pixels (1, 2 or 4) of the
-// tile, stacked 4 rows apart, so a warp covers an 8 x 4PX block. Splat records are
-// gathered through the sorted pair list into shared memory a batch at a time; each warp
-// then ballots which staged splats' footprint ellipses reach its block and walks only
-// those, in order (a culled splat is one every pixel of the block would skip anyway).
+// Both work on 16x16 tiles of the flattened (view, tile) space, taken from an atomic
+// queue, so a batch of views of uneven resolution is one launch. Each thread owns PX
+// pixels (1, 2 or 4) of a tile, stacked 4 rows apart, so a warp covers an 8 x 4PX block.
+// Splat records are gathered through the sorted pair list into shared memory a round at a
+// time; a warp ballots which staged splats' footprint ellipses reach its block and walks
+// only those, in order (a culled splat is one every pixel of the block would skip anyway).
+// The default kernels (raster_fwd_split, raster_bwd_split) make each warp's block its own
+// work item, staging its own rounds; the block kernels (raster_fwd_tile, raster_bwd_tile)
+// share a round between a tile's warps and serve asynchronous staging and the
+// deterministic backward.
 //
 // The adjoint keeps no per-fragment state: each pixel walks its splats front to back
 // again from T = 1 and R = dL/dC . C_final (pixel_dot, background included), up to its
