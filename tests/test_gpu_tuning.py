@@ -119,7 +119,8 @@ def test_async_staging_is_bit_identical(ctx):
     batch and both backward batches (the batch changes how a tile's list is cut into rounds,
     not the order or the sums), on a view whose tiles hold several rounds of splats. Without
     cp.async the forward runs its independent-warp kernel (each warp staging its own rounds
-    of 32), so this also checks that kernel against the block kernel bit for bit."""
+    of 32, its last warp per tile adding the warps' tile sums), so this also checks that
+    kernel, tile sums included, against the block kernel bit for bit."""
     scene, cam, opt, target = view_and_target(n=60000)
     frozen = F.frozen_options(1, False)
     frozen.lambda_dssim, frozen.lambda_dssim_end = 0.2, -1.0
@@ -130,7 +131,8 @@ def test_async_staging_is_bit_identical(ctx):
         ctx.model_init(scene.params, scene.sh)
         ctx.set_views([fr], [target])
         ctx.step(train=True)
-        outs[(fb, bb, stage)] = {k: ctx.snapshot(k) for k in ("pixel_count", "pixel_out", "pixel_grad", "pair_grads")}
+        outs[(fb, bb, stage)] = {k: ctx.snapshot(k)
+                                 for k in ("pixel_count", "pixel_out", "pixel_grad", "pair_grads", "tile_loss")}
         outs[(fb, bb, stage)]["m"] = ctx.moments()["m"]
     ref = outs[(256, 64, 0)]
     assert (ref["pixel_count"] > 256).any()  # tiles with more than one forward round
