@@ -298,6 +298,19 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
   const uint32_t lid = threadIdx.x;
   const size_t pbase = a.vt->pixel_base[v];
   const int ox = tx * int(kTile) - kR, oy = ty * int(kTile) - kR;
+  // The thread's own pixel's inputs of the last phase, loaded now so that their latency
+  // hides behind the blurs.
+  const uint32_t lx = lid % kTile, ly = lid / kTile;
+  const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
+  const bool mine = lid < kTilePixels && px < W && py < H;
+  const size_t pix = pbase + size_t(py) * W + px;
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f), pg = o;
+  uint32_t own_target = 0u;
+  if (mine) {
+    o = a.rb.pixel_out[pix];
+    pg = a.rb.pixel_grad[pix];
+    own_target = target[size_t(py) * W + px];
+  }
   // Each thread's (up to) three window pixels: every load issued before the first store,
   // so their latencies overlap instead of adding up.
   float4 m0[kWindowLoads], m1[kWindowLoads];
@@ -364,18 +377,13 @@ __global__ void __launch_bounds__(kLossThreads) k_ssim_grad(LossArgs a) {
     for (int o = 0; o < kRun8; ++o) s_g[p * kAbc + (q * kRun8 + o) * kTile + col] = out[o];
   }
   __syncthreads();
-  const uint32_t lx = lid % kTile, ly = lid / kTile;
-  const uint32_t px = uint32_t(tx) * kTile + lx, py = uint32_t(ty) * kTile + ly;
-  if (lid >= kTilePixels || px >= W || py >= H) return;
-  const size_t pix = pbase + size_t(py) * W + px;
-  const float4 o = a.rb.pixel_out[pix];
-  const float3 y = target_colour(f, target[size_t(py) * W + px]);
+  if (!mine) return;
+  const float3 y = target_colour(f, own_target);
   const float xs[3] = {o.x, o.y, o.z}, ys[3] = {y.x, y.y, y.z};
   float ds[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
     ds[c] = s_g[c * kAbc + lid] + 2.0f * xs[c] * s_g[(3 + c) * kAbc + lid] + ys[c] * s_g[(6 + c) * kAbc + lid];
-  float4 pg = a.rb.pixel_grad[pix];
   const float s = f.loss[0] * f.background[3];
   pg.x -= s * ds[0];
   pg.y -= s * ds[1];
