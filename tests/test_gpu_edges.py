@@ -78,9 +78,14 @@ def test_every_gaussian_culled(ctx):
     assert not m["m"].any() and not m["m_sh"].any()
 
 
-def test_sixteen_ragged_views_match_oracle(ctx):
+@pytest.mark.parametrize("tuning", [dict(), dict(deterministic=0), dict(deterministic=0, forward_pixels=1, backward_pixels=2),
+                                    dict(deterministic=0, forward_pixels=4, backward_pixels=8),
+                                    dict(deterministic=1, backward_pixels=8)])
+def test_sixteen_ragged_views_match_oracle(ctx, tuning):
     """GS_MAX_VIEWS views of different sizes (none a multiple of 16) in one step: per-view
-    pair counts and losses, and the summed gradient, against the oracle."""
+    pair counts and losses, and the summed gradient, against the oracle; under the default
+    tuning, the fast mode's independent-warp kernels at each warp layout, and one warp per
+    tile in both modes (work items of ragged edge tiles, views of uneven size in one queue)."""
     scene = S.make_scene(2000, 6, 1, radius=1.0, log_scale_mu=-3.5, log_scale_sigma=0.4)
     rng = np.random.default_rng(13)
     frames, targets = [], []
@@ -92,11 +97,16 @@ def test_sixteen_ragged_views_match_oracle(ctx):
         t = rng.integers(0, 256, size=(h, w, 4), dtype=np.uint8)
         t[..., 3] = 255
         targets.append(t)
-    ctx.model_init(scene.params, scene.sh)
-    ctx.set_views(frames, targets)
-    res = ctx.step(True)
+    default = ctx.tuning()
+    ctx.set_tuning(**tuning)
+    try:
+        ctx.model_init(scene.params, scene.sh)
+        ctx.set_views(frames, targets)
+        res = ctx.step(True)
+        g16, gsh = ctx.first_step_gradients()
+    finally:
+        ctx.set_tuning(**{k: getattr(default, k) for k in ("deterministic", "forward_pixels", "backward_pixels")})
     assert res.n_views == 16
-    g16, gsh = ctx.first_step_gradients()
     model = O.Model.create(scene.params, scene.sh)
     results, ref16, refsh, _ = O.train_step(model, frames, targets)
     for v, r in enumerate(results):
