@@ -5,7 +5,8 @@ oracle/_ref/libgs_ref.so is the reference's FP64 CPU forward + loss
 compiled from a reference checkout by `make -C oracle ref`. These tests check:
 - the oracle's restatement (gso_reference_loss, gso_reference_ssim) reproduces it bit for
   bit: loss, FP64 image and SSIM, on the reference's own test scene (masks, head weight,
-  every lambda) and on BASELINE-shaped scenes (configs 0 and 1 at reduced and full size);
+  every lambda) and on the small workloads' scenes (20k gaussians SH0 at 360x640, 512
+  gaussians SH3 at 128x128, at reduced and full size);
 - the oracle's FP32 training passes (the checker of the CUDA path) render within the
   reference's own bars of its FP64 forward: image within 2.5/255 and loss within 1e-4
   (test_trainer.cpp:34-35);
