@@ -295,12 +295,12 @@ def cpu_baseline(scene, targets, cams, opt, seconds: float = 20.0) -> dict:
 # gaussian against every pixel) at the two small workloads it is tractable at: seeded scenes
 # of N gaussians in a radius-1 ball, SH degree D, log-scales N(mu, sigma), one front view.
 REFERENCE_LOSS_CONFIGS = {
-    "config1": dict(n=512, degree=3, mu=-2.5, sigma=0.3, width=128, height=128, focal=200.0),
-    "config0": dict(n=20000, degree=0, mu=-4.0, sigma=0.5, width=360, height=640, focal=500.0),
+    "512_sh3_128x128": dict(n=512, degree=3, mu=-2.5, sigma=0.3, width=128, height=128, focal=200.0),
+    "20k_sh0_360x640": dict(n=20000, degree=0, mu=-4.0, sigma=0.5, width=360, height=640, focal=500.0),
 }
 
 
-def reference_forward_loss(names=("config1",), repeats: int = 5) -> dict:
+def reference_forward_loss(names=("512_sh3_128x128",), repeats: int = 5) -> dict:
     """Times the reference's own CPU code for the path (engine/src/train_selftest.cpp's
     reference_loss, compiled unchanged into oracle/_ref/libgs_ref.so) on one host thread:
     forward + L1/SSIM loss of one view, no backward. {} when the library was not built."""
@@ -319,7 +319,7 @@ def reference_forward_loss(names=("config1",), repeats: int = 5) -> dict:
         target[..., 3] = 255
         p64, s64 = scene.params.astype(np.float64), scene.sh.astype(np.float64)
         times = []
-        for _ in range(repeats if name == "config1" else 1):
+        for _ in range(repeats if name == "512_sh3_128x128" else 1):
             t0 = time.perf_counter()
             O.ref_reference_loss(cam.as_dict(), c["width"], c["height"], p64, s64, c["degree"], target,
                                  (0.0, 0.0, 0.0), False, 0.2)
@@ -331,7 +331,7 @@ def reference_forward_loss(names=("config1",), repeats: int = 5) -> dict:
     return out
 
 
-def b200_small_configs(names=("config1", "config0"), steps: int = 50) -> dict:
+def b200_small_workloads(names=("512_sh3_128x128", "20k_sh0_360x640"), steps: int = 50) -> dict:
     """This path on the GPU at the same small workloads, for beside reference_forward_loss:
     device time per view of a forward + loss step (no backward, as the reference's CPU code)
     and of a full training step, graph replay, median over `steps` steps."""
@@ -428,15 +428,15 @@ def main() -> None:
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default tuning (profiling runs: timings under ncu would mislead the autotuner)")
     ap.add_argument("--reference-loss", action="store_true",
-                    help="time only the reference's own CPU forward + loss at configs 1 and 0 (about 2 min) "
+                    help="time only the reference's own CPU forward + loss on 512 gaussians at 128x128 and 20k at 360x640 (about 2 min) "
                          "and this path's step at the same workloads on the GPU")
     ap.add_argument("--set", action="append", default=[], metavar="KNOB=VALUE",
                     help="a gs_tuning field to set instead of autotuning it (profiling runs), e.g. deterministic=0")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.reference_loss:
-        line = {"reference_cpu_forward_loss": reference_forward_loss(("config1", "config0"))}
-        line["b200"] = b200_small_configs()
+        line = {"reference_cpu_forward_loss": reference_forward_loss(("512_sh3_128x128", "20k_sh0_360x640"))}
+        line["b200"] = b200_small_workloads()
         print(json.dumps(line), flush=True)
         return
 
