@@ -40,7 +40,7 @@ def ctx():
 
 
 @pytest.fixture(scope="module")
-def config3(ctx):
+def full_view(ctx):
     scene = S.make_scene(N, 0, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
     truth = S.make_scene(N, 1, 3, radius=2.0, log_scale_mu=-5.0, log_scale_sigma=0.5)
     cam = S.front_camera(W, H, FOCAL)
@@ -62,8 +62,8 @@ def config3(ctx):
     return scene, fr, target, res, snap, g16, gsh, r
 
 
-def test_pairs_order_and_ranges_bit_exact(config3):
-    _, _, _, res, snap, _, _, r = config3
+def test_pairs_order_and_ranges_bit_exact(full_view):
+    _, _, _, res, snap, _, _, r = full_view
     assert res.pairs[0] == r.pairs > 3_000_000
     np.testing.assert_array_equal(snap["tiles"], r.tiles)
     np.testing.assert_array_equal(snap["pair_tile"], r.pair_tile[: r.pairs])
@@ -75,8 +75,8 @@ def test_pairs_order_and_ranges_bit_exact(config3):
     np.testing.assert_array_equal(snap["ranges"].reshape(-1), r.ranges[: 2 * ntiles])
 
 
-def test_image_transmittance_and_loss(config3):
-    _, _, _, res, snap, _, _, r = config3
+def test_image_transmittance_and_loss(full_view):
+    _, _, _, res, snap, _, _, r = full_view
     same = snap["pixel_count"] == r.pixel_count
     assert same.mean() >= 0.9995, same.mean()
     colour = np.abs(snap["pixel_out"][same, :3] - r.ssim_input[same, :3]).max(axis=1)
@@ -90,16 +90,16 @@ def test_image_transmittance_and_loss(config3):
         assert abs(sums[k] - r.sums[k]) <= 1e-4 * abs(r.sums[k]) + 1e-6, k
 
 
-def test_pair_gradients(config3):
-    _, _, _, _, snap, _, _, r = config3
+def test_pair_gradients(full_view):
+    _, _, _, _, snap, _, _, r = full_view
     got, ref = snap["pair_grads"], r.pair_grads[: r.pairs]
     for name, cols in {"mean2d": [0, 1], "conic": [2, 3, 4], "opacity": [5], "colour": [6, 7, 8],
                        "abs_mean": [9, 10]}.items():
         assert rel_l2(got[:, cols], ref[:, cols]) < 1e-3, name
 
 
-def test_parameter_gradients(config3):
-    scene, fr, target, _, _, g16, gsh, _ = config3
+def test_parameter_gradients(full_view):
+    scene, fr, target, _, _, g16, gsh, _ = full_view
     model = O.Model.create(scene.params, scene.sh)
     _, ref16, refsh, _ = O.train_step(model, [fr], [target])
     for name, cols in GROUPS.items():
