@@ -29,7 +29,7 @@ def ctx():
     c.close()
 
 
-def cfg0_view():
+def small_view():
     """20k gaussians, SH 0, one 360x640 view at (0, 0, 3), f = 500; target rendered from an
     independent seed-1 set (the plain single-view configuration)."""
     scene = S.make_scene(20000, 0, 0, radius=1.0, log_scale_mu=-4.0, log_scale_sigma=0.5)
@@ -51,7 +51,7 @@ def gpu_step(ctx, scene, frames, targets, train=True, capacity=None):
 
 
 def test_projection_and_pairs_match_oracle(ctx):
-    scene, cam, opt, target = cfg0_view()
+    scene, cam, opt, target = small_view()
     fr = frame_for(scene, cam, opt, (0, 0, 0))
     res = gpu_step(ctx, scene, [fr], [target], train=False)
     assert res.overflow == 0 and res.tile_mismatch == 0
@@ -97,7 +97,7 @@ def _stage_oracle(ctx, fr, scene, target, ssim=True):
 @pytest.mark.parametrize("backward_pixels", [4, 8])
 def test_forward_loss_backward_match_oracle(ctx, backward_pixels):
     """Backward at 4 pixels per thread (two warps per tile) and at 8 (one warp per tile)."""
-    scene, cam, opt, target = cfg0_view()
+    scene, cam, opt, target = small_view()
     fr = frame_for(scene, cam, opt, (0.1, 0.2, 0.3))
     ctx.set_tuning(backward_pixels=backward_pixels)
     try:
@@ -129,7 +129,7 @@ def test_forward_loss_backward_match_oracle(ctx, backward_pixels):
 
 def test_gradients_end_to_end_match_oracle(ctx):
     """First-step gradients (m / (1 - beta1)) of a plain step vs the oracle's own full step."""
-    scene, cam, opt, target = cfg0_view()
+    scene, cam, opt, target = small_view()
     fr = frame_for(scene, cam, opt, (0.1, 0.2, 0.3))
     gpu_step(ctx, scene, [fr], [target], train=True)
     g16, gsh = ctx.first_step_gradients()
@@ -198,7 +198,7 @@ def test_adjoint_sh3_against_oracle_and_fd(ctx):
 
 @pytest.mark.parametrize("backward_pixels", [4, 8])
 def test_deterministic_mode_is_bit_stable(ctx, backward_pixels):
-    scene, cam, opt, target = cfg0_view()
+    scene, cam, opt, target = small_view()
     fr = frame_for(scene, cam, opt, (0.1, 0.2, 0.3))
     ctx.set_tuning(backward_pixels=backward_pixels)
     try:
@@ -315,7 +315,7 @@ def test_render_matches_forward(ctx):
     """gs_render's RGBA8 image against the oracle's forward on the GPU's projection: within
     one RGBA8 step (the colour is within 1e-4, the alpha within 1e-5, before rounding) on
     every pixel whose contributor count agrees, and those are at least 99.95% of the image."""
-    scene, cam, opt, target = cfg0_view()
+    scene, cam, opt, target = small_view()
     fr = frame_for(scene, cam, opt, (0, 0, 0), ssim=False)
     ctx.model_init(scene.params, scene.sh)
     img = ctx.render(fr)

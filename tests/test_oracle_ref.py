@@ -47,9 +47,9 @@ def test_restatement_equals_reference_on_its_test_scene(masked, lam, head):
 
 
 @pytest.mark.parametrize("name,n,degree,W,H,focal,mu,sigma", [
-    ("config 1 (512 gaussians SH3, 128x128)", 512, 3, 128, 128, 200.0, -2.5, 0.3),
-    ("config 0 at 1/16 the pixels and 1/10 the gaussians", 2000, 0, 90, 160, 125.0, -4.0, 0.5),
-    ("config 0 shapes with SH3, 1/16 the pixels", 2000, 3, 90, 160, 125.0, -3.5, 0.5),
+    ("512 gaussians SH3, 128x128", 512, 3, 128, 128, 200.0, -2.5, 0.3),
+    ("the 20k-gaussian 360x640 workload at 1/16 the pixels and 1/10 the gaussians", 2000, 0, 90, 160, 125.0, -4.0, 0.5),
+    ("the 20k-gaussian workload's shapes with SH3, 1/16 the pixels", 2000, 3, 90, 160, 125.0, -3.5, 0.5),
 ])
 def test_restatement_equals_reference_on_workload_scenes(name, n, degree, W, H, focal, mu, sigma):
     scene = S.make_scene(n, 0, degree, radius=1.0, log_scale_mu=mu, log_scale_sigma=sigma)
