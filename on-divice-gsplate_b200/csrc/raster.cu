@@ -26,7 +26,9 @@
 // - Fast mode (raster_bwd_split): each warp works on its own block of a tile, stages its
 //   own rounds and stops at its own last contributor; it sums 9 values through shared
 //   memory and adds them to the gaussian's accumulator with three 16-byte vector atomics
-//   (red.global.add.v4.f32). It leaves out the |dL/dmean2d| sums (pair values 9 and 10):
+//   (red.global.add.v4.f32). The 9 values a lane contributes are its raw sums, before the
+//   splat's opacity and conic factors, which are applied once per splat after the warp sum
+//   (raw_to_grads) instead of once per lane and visit. It leaves out the |dL/dmean2d| sums (pair values 9 and 10):
 //   they feed only the densify statistic stats.w, which no densify decision reads
 //   (train_densify_mark.comp:22-57 uses x, y, z).
 // - backward_pixels = 8 (raster_bwd_warp_tile): one warp per whole tile, either mode.
@@ -519,8 +521,12 @@ __global__ void __launch_bounds__(256 / PX) k_raster_fwd(RasterArgs a) {
 // front-to-back form described at the top of the file), at 1-based position `pos` of the
 // tile's list: updates each lane's T and R and, when some lane of the warp blends the
 // splat, forms the splat's gradient values over the lane's pixels in c (11 with the
-// |dmean| sums (ABS), else 9) and returns true.
-template <int PX, bool ABS>
+// |dmean| sums (ABS), else 9) and returns true. With RAW c holds the lane's sums before
+// the splat's own factors instead, (u, dx u, dx^2 u, st, dx st, sty, the three colour
+// weights, and with ABS the |dmean| sums without the opacity), linear in the lane's
+// values, so the warp sums them first and raw_to_grads applies the opacity and the conic
+// once per splat.
+template <int PX, bool ABS, bool RAW = false>
 __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, const float blue, const uint32_t pos,
                                               const float cx, const float (&cy)[PX], const float (&dl0)[PX],
                                               const float (&dl1)[PX], const float (&dl2)[PX],
@@ -582,6 +588,15 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
     R[p] = rest;
   }
   if (!__any_sync(0xffffffffu, has)) return false;
+  if constexpr (RAW) {
+    c[0] = u;
+    c[1] = dx * u;
+    c[2] = dx * c[1];
+    c[3] = st;
+    c[4] = dx * st;
+    c[5] = sty;
+    return true;
+  }
   const float sd = A.z * u;
   st *= A.z;
   sty *= A.z;
@@ -596,6 +611,28 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
     c[10] *= A.z;
   }
   return true;
+}
+
+// The splat's gradient values from the warp sums of splat_adjoint's raw terms r (in
+// place): with op the opacity and the conic (ca, cb, cc) back from the staged exponent
+// terms, dmean = -op (ca S(dx u) + cb S(st), cb S(dx u) + cc S(st)), dconic = -op
+// (S(dx^2 u) / 2, S(dx st), S(sty) / 2), dopacity = S(u), |dmean| (ABS) = op S(|.|); the
+// colour weights are unchanged.
+template <bool ABS>
+__device__ __forceinline__ void raw_to_grads(const float4 A, const float4 B, float (&r)[12]) {
+  const float ca = A.w * (-2.0f / kLog2e), cb = B.x * (-1.0f / kLog2e), cc = B.y * (-2.0f / kLog2e);
+  const float op = A.z;
+  const float u = r[0], dxu = r[1], dx2u = r[2], st = r[3], dxst = r[4], sty = r[5];
+  r[0] = -op * fmaf(ca, dxu, cb * st);
+  r[1] = -op * fmaf(cb, dxu, cc * st);
+  r[2] = (-0.5f * op) * dx2u;
+  r[3] = -op * dxst;
+  r[4] = (-0.5f * op) * sty;
+  r[5] = u;
+  if constexpr (ABS) {
+    r[9] *= op;
+    r[10] *= op;
+  }
 }
 
 // The forward with independent warps (the default without stage_async). A work item is one
@@ -725,7 +762,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
   __shared__ float4 s_c[BATCH];  // staged splats (stage_splat): s_a, s_b, s_c
   __shared__ RawRound<ASYNC ? BATCH : 1> s_raw[ASYNC ? 2 : 1];
   __shared__ uint32_t s_dst[BATCH];
-  __shared__ float s_part[L::kWarps][BATCH][12];
+  __shared__ __align__(16) float s_part[L::kWarps][BATCH][12];
   __shared__ uint32_t s_wrote[L::kWarps][BATCH / 32];  // per warp: the splats whose partial it wrote
 
   const uint32_t lid = threadIdx.x, lane = lid & 31u, warp = lid >> 5;
@@ -840,7 +877,7 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
         m &= m - 1u;
         const uint32_t pos = start + j + 1u;  // 1-based position in the tile's list
         float c[12];
-        if (splat_adjoint<PX, ABS>(s_a[j], s_b[j], s_c[j].x, pos, cx, cy, dl0, dl1, dl2, last, T, R, c)) {
+        if (splat_adjoint<PX, ABS, true>(s_a[j], s_b[j], s_c[j].x, pos, cx, cy, dl0, dl1, dl2, last, T, R, c)) {
           const uint32_t slot = warp_reduce_scatter12(c, lane);
           if (slot < 12u) s_part[warp][j][slot] = c[0];
           wrote |= 1u << (j & 31u);
@@ -849,15 +886,33 @@ __device__ __forceinline__ void raster_bwd_tile(const RasterArgs& a, uint32_t gt
       if (lane == 0) s_wrote[warp][w] = wrote;
     }
     __syncthreads();
-    // The pair's gradient at its pre-sort index: the warps' partials added in order (zero
-    // for a splat no warp drew), for train_pair_sum's fixed-order sum per gaussian.
-    for (uint32_t idx = lid; idx < nb * 12u; idx += L::kThreads) {
-      const uint32_t j = idx / 12u, k = idx - j * 12u;
-      float s = 0.0f;
+    // The pair's gradient at its pre-sort index: the warps' raw partials added in order,
+    // then the splat's factors applied (zero for a splat no warp drew), for
+    // train_pair_sum's fixed-order sum per gaussian.
+    for (uint32_t j = lid; j < nb; j += L::kThreads) {
+      float r[12];
 #pragma unroll
-      for (int w8 = 0; w8 < L::kWarps; ++w8)
-        if ((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) s += s_part[w8][j][k];
-      a.pair_grads[size_t(s_dst[j]) * 12u + k] = s;
+      for (int k = 0; k < 12; ++k) r[k] = 0.0f;
+      bool drawn = false;
+#pragma unroll
+      for (int w8 = 0; w8 < L::kWarps; ++w8) {
+        if (((s_wrote[w8][j >> 5] >> (j & 31u)) & 1u) == 0u) continue;
+        drawn = true;
+        const float4* part = reinterpret_cast<const float4*>(&s_part[w8][j][0]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float4 v = part[q];
+          r[4 * q] += v.x;
+          r[4 * q + 1] += v.y;
+          r[4 * q + 2] += v.z;
+          r[4 * q + 3] += v.w;
+        }
+      }
+      if (drawn) raw_to_grads<ABS>(s_a[j], s_b[j], r);
+      float4* o = reinterpret_cast<float4*>(a.pair_grads + size_t(s_dst[j]) * 12u);
+      o[0] = make_float4(r[0], r[1], r[2], r[3]);
+      o[1] = make_float4(r[4], r[5], r[6], r[7]);
+      o[2] = make_float4(r[8], r[9], r[10], r[11]);
     }
   }
   if constexpr (ASYNC) copy_async_wait<0>();  // no copy may land in the next tile's buffers
@@ -1128,12 +1183,21 @@ __device__ __forceinline__ void raster_bwd_split(const RasterArgs& a, uint32_t i
       const uint32_t j = uint32_t(__ffs(m) - 1);
       m &= m - 1u;
       float c[12];
-      if (splat_adjoint<PX, false>(sm.a[j], sm.b[j], sm.c[j].x, start + j + 1u, cx, cy, dl0, dl1, dl2, last, T, R,
-                                   c)) {
+      if (splat_adjoint<PX, false, true>(sm.a[j], sm.b[j], sm.c[j].x, start + j + 1u, cx, cy, dl0, dl1, dl2, last, T,
+                                         R, c)) {
         const float sum = warp_sum9_rows(sm.lanes, c, lane);
         if (lane < 12u) sm.part[j][lane] = lane < 9u ? sum : 0.0f;
         wrote |= 1u << j;
       }
+    }
+    __syncwarp();
+    if ((wrote >> lane) & 1u) {  // lane j staged splat j: its factors are this lane's A and B
+      float4* row = reinterpret_cast<float4*>(&sm.part[lane][0]);
+      const float4 r0 = row[0], r1 = row[1];
+      float r[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+      raw_to_grads<false>(A, B, r);
+      row[0] = make_float4(r[0], r[1], r[2], r[3]);
+      row[1] = make_float4(r[4], r[5], r[6], r[7]);
     }
     __syncwarp();
     for (uint32_t idx = lane; idx < nb * 3u; idx += 32u) {
