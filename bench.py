@@ -70,6 +70,13 @@ def frame(scene, cam, opt, step):
     return F.make_frame(cam, scene.count, scene.sh.shape[1], step, opt, (0.0, 0.0, 0.0), 3.3)
 
 
+def frames(scene, cams, opt, step):
+    """The step's frames in one array (make_frames: the same bytes as frame() per camera)."""
+    from gs_b200 import frame as F
+
+    return F.make_frames(cams, scene.count, scene.sh.shape[1], step, opt, (0.0, 0.0, 0.0), 3.3)
+
+
 class ViewOrder:
     """Shuffled epochs over the cameras (Trainer::next_view, trainer.cpp:911-924)."""
 
@@ -517,7 +524,7 @@ def main() -> None:
     t0 = time.perf_counter()
     for _ in range(args.steps):
         idx = order.next(VIEWS_PER_STEP)
-        ctx.set_views([frame(scene, cams[i], opt, step) for i in idx], [host_targets[i] for i in idx])
+        ctx.set_views(frames(scene, [cams[i] for i in idx], opt, step), [host_targets[i] for i in idx])
         ctx.step(True)
         step += 1
     torch.cuda.synchronize()

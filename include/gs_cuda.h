@@ -130,7 +130,7 @@ typedef enum gs_snapshot_kind {
   GS_SNAP_TILE_LOSS = 11,   /* 16 floats per tile */
   GS_SNAP_PIXEL_DOT = 12,   /* float per pixel: dL/dC . colour */
   GS_SNAP_STATS = 13,       /* 4 floats per slot: densification statistics */
-  GS_SNAP_PAIR_GAUSSIAN = 14, /* uint32 per pair, pre-sort order: the slot */
+  GS_SNAP_PAIR_GAUSSIAN = 14, /* uint32 per pair, pre-sort order: the slot (not after an atomic training step) */
   GS_SNAP_PIXEL_OUT = 15,     /* 4 floats per pixel: rendered rgb over the background, loss weight */
   GS_SNAP_SPAWN = 16,         /* uint32 per slot after gs_densify: 0 none, 1 clone, 2 split */
   GS_SNAP_MOTION_BIND = 17,   /* 8 uint32 per slot: 4 motion nodes, their 4 weights (float bits) */

@@ -601,7 +601,6 @@ struct gs_context {
     rb.ranges = ranges;
     rb.values = sorted_values;
     rb.gauss = payload_gaussian ? sorted_values : sorted_g;
-    rb.pair_gaussian = pair_gaussian;
     rb.pixel_grad = pixel_grad;
     rb.pixel_out = pixel_out;
     rb.pixel_count = pixel_count;
@@ -688,8 +687,10 @@ struct gs_context {
     depth_sorted_vals = in_alt ? dvals_alt : dvals;
     // Offsets of each item's pairs in depth order; the total is the step's pair count.
     gsk::exclusive_scan(sort, vb.tiles, depth_sorted_vals, sorted_offsets, items, d_scalars, stream, &launches);
+    // With the gaussian as the payload nothing reads the per-pair gaussian: not written.
     gsk::launch_emit(sp, vb, model.cap, items, depth_sorted_vals, sorted_offsets, d_scalars, uint32_t(pair_cap), keys,
-                     values, pair_gaussian, pair_grads, d_scalars + 1, payload_gaussian, stream);
+                     values, payload_gaussian ? nullptr : pair_gaussian, pair_grads, d_scalars + 1, payload_gaussian,
+                     stream);
     launches += items ? 1 : 0;
     const uint32_t max_tiles = uint32_t(tile_cap - 1);
     const int tile_bits = int(bits_for(max_tiles + 1));
@@ -1262,6 +1263,9 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_TILE_LOSS: d2h(host, c->tile_loss + tb * 16, size); break;
       case GS_SNAP_PAIR_GRADS: d2h(host, c->pair_grads, size); break;
       case GS_SNAP_PAIR_GAUSSIAN: {
+        if (c->payload_gaussian)
+          fail(GS_ERR_INVALID, "gs_snapshot: an atomic training step sorts gaussians and keeps no per-pair gaussian: "
+                               "deterministic or forward-only steps keep it");
         std::vector<uint32_t> g(pairs);
         d2h(g.data(), c->pair_gaussian, pairs * 4);
         for (auto& x : g) x -= view * cap;  // slots of this view

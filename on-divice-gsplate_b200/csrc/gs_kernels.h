@@ -99,7 +99,6 @@ struct RasterBuffers {
   const uint2* ranges = nullptr;
   const uint32_t* values = nullptr;         // per sorted pair: its pre-sort index (or g, see launch_emit)
   const uint32_t* gauss = nullptr;          // per sorted pair: its gaussian g (render order)
-  const uint32_t* pair_gaussian = nullptr;  // g per pre-sort pair
   float4* pixel_grad = nullptr;             // dL/dC rgb, final T
   float4* pixel_out = nullptr;              // rendered colour rgb (over the background), loss weight
   uint32_t* pixel_count = nullptr;

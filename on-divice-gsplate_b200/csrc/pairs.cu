@@ -26,7 +26,7 @@ struct EmitArgs {
   uint32_t* offsets;
   uint32_t* keys;
   uint32_t* values;
-  uint32_t* pair_gaussian;
+  uint32_t* pair_gaussian;  // g per pre-sort pair; null when the values carry g (nothing reads it then)
   float4* pair_grads;
   uint32_t* mismatch;
   bool payload_gaussian;  // values carry g instead of the pre-sort index
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
       } else {
         a.keys[q] = tile;
         a.values[q] = a.payload_gaussian ? g : q;
-        a.pair_gaussian[q] = g;
+        if (a.pair_gaussian != nullptr) a.pair_gaussian[q] = g;
       }
     };
     uint32_t wanted = 0u;
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
     const uint32_t owner = st_owner[q - wfirst];
     a.keys[q] = st_tile[q - wfirst];
     a.values[q] = a.payload_gaussian ? owner : q;
-    a.pair_gaussian[q] = owner;
+    if (a.pair_gaussian != nullptr) a.pair_gaussian[q] = owner;
   }
 }
 

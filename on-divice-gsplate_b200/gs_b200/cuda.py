@@ -116,7 +116,9 @@ def _check(code: int) -> None:
 
 def _frames(frames) -> np.ndarray:
     """The views' FrameData as one contiguous array (no copies beyond the concatenation when
-    they already are FRAME_DTYPE records)."""
+    they already are FRAME_DTYPE records; none for an array of them, as make_frames gives)."""
+    if isinstance(frames, np.ndarray) and frames.dtype == FRAME_DTYPE:
+        return np.ascontiguousarray(frames.reshape(-1))
     if all(isinstance(f, np.ndarray) and f.dtype == FRAME_DTYPE for f in frames):
         return np.concatenate([f.reshape(1) for f in frames])
     return np.ascontiguousarray(np.concatenate([np.asarray(f, FRAME_DTYPE).reshape(1) for f in frames]))
@@ -200,7 +202,7 @@ class Context:
             keep += arrs
             tptr = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
         self._keep = keep  # the library may read the targets until the next step returns
-        _check(self.lib.gs_set_views(self.h, len(frames), _ptr(fr), tptr))
+        _check(self.lib.gs_set_views(self.h, len(fr), _ptr(fr), tptr))
 
     def set_dataset(self, images: list[np.ndarray]) -> None:
         """Keeps RGBA8 target images (H x W x 4 uint8) in HBM across steps."""
@@ -214,7 +216,7 @@ class Context:
         fr = _frames(frames)
         idx = np.ascontiguousarray(images, np.uint32)
         self._keep = [fr]
-        _check(self.lib.gs_set_views_dataset(self.h, len(frames), _ptr(fr), _ptr(idx)))
+        _check(self.lib.gs_set_views_dataset(self.h, len(fr), _ptr(fr), _ptr(idx)))
 
     def step(self, train: bool = True, profile: bool = False, count: bool = False) -> StepResult:
         """One step; `profile`: per-pass device times; `count`: the forward also counts its

@@ -214,3 +214,24 @@ def make_frame(camera: Camera, slots: int, sh_stride: int, step: int, options: T
     f["head"][0, 3] = 1.0
     f["exposure"][0, :3] = 1.0
     return f
+
+
+def make_frames(cameras: list[Camera], slots: int, sh_stride: int, step: int, options: TrainOptions, background,
+                camera_extent: float, masked_target: bool = False, ssim: bool = True,
+                pair_capacity: int = 0) -> np.ndarray:
+    """The frames of one step's views, as make_frame gives them one by one (the same bytes),
+    in one FRAME_DTYPE array: the step's schedule is worked out once and the camera fields
+    are filled for all views together."""
+    if not cameras:
+        return np.zeros(0, FRAME_DTYPE)
+    f = np.repeat(make_frame(cameras[0], slots, sh_stride, step, options, background, camera_extent, masked_target,
+                             ssim, pair_capacity), len(cameras))
+    W = np.array([c.width for c in cameras], np.uint32)
+    H = np.array([c.height for c in cameras], np.uint32)
+    f["rot"][:, :, :3] = np.stack([np.asarray(c.rotation, np.float32).reshape(3, 3) for c in cameras])
+    f["rot"][:, :, 3] = np.stack([np.asarray(c.translation, np.float32).reshape(3) for c in cameras])
+    f["cam_pos"][:, :3] = np.stack([np.asarray(c.position, np.float32).reshape(3) for c in cameras])
+    f["intrinsics"] = np.array([(c.fx, c.fy, c.cx, c.cy) for c in cameras], np.float32)
+    f["image"] = np.stack([W, H, (W + TILE - 1) // TILE, (H + TILE - 1) // TILE], axis=1)
+    f["background"][:, 3] = np.float32(1.0) / (np.float32(3.0) * W.astype(np.float32) * H.astype(np.float32))
+    return f

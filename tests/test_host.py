@@ -47,6 +47,22 @@ def test_camera_matches_python_mirror():
     np.testing.assert_allclose(vals[9:], cam.translation, atol=1e-6)
 
 
+@pytest.mark.parametrize("step", [0, 7, 4000])
+def test_batch_frames_equal_single_frames(step):
+    """make_frames gives the same bytes as make_frame per camera, for views of mixed sizes."""
+    cams = S.orbit_cameras(5, 3.0, 0.5, 1920, 1080, 1400.0) + [S.front_camera(37, 23, 50.0),
+                                                               S.front_camera(360, 640, 500.0)]
+    opt = F.TrainOptions(iterations=30000, sh_degree=3, sh_degree_interval=1000, lambda_dssim=0.2,
+                         lambda_dssim_end=0.1, opacity_reset_interval=3000)
+    for masked, ssim, cap in [(False, True, 0), (True, False, 12345)]:
+        want = np.concatenate([F.make_frame(c, 70000, 45, step, opt, (0.1, 0.2, 0.3), 3.3, masked, ssim, cap)
+                               for c in cams])
+        got = F.make_frames(cams, 70000, 45, step, opt, (0.1, 0.2, 0.3), 3.3, masked, ssim, cap)
+        assert got.dtype == F.FRAME_DTYPE and got.shape == (len(cams),)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert F.make_frames([], 1, 0, 0, opt, (0.0, 0.0, 0.0), 1.0).shape == (0,)
+
+
 def test_frame_matches_python_mirror():
     words = np.array([int(w, 16) for w in run("frame").split()], np.uint32)
     assert words.size == 72
