@@ -25,11 +25,12 @@
 //   index (pair_grads, summed per gaussian by train_pair_sum's fixed order): bit-stable.
 // - Fast mode (raster_bwd_split): each warp works on its own block of a tile, stages its
 //   own rounds and stops at its own last contributor; it sums 9 values through shared
-//   memory and adds them to the gaussian's accumulator with three 16-byte vector atomics
-//   (red.global.add.v4.f32). The 9 values a lane contributes are its raw sums, before the
-//   splat's opacity and conic factors, which are applied once per splat after the warp sum
-//   (raw_to_grads) instead of once per lane and visit. It leaves out the |dL/dmean2d| sums (pair values 9 and 10):
-//   they feed only the densify statistic stats.w, which no densify decision reads
+//   memory, and the lane that staged the splat adds them to the gaussian's accumulator with
+//   two 16-byte vector atomics (red.global.add.v4.f32) and one scalar. The 9 values a lane
+//   contributes are its raw sums, before the splat's opacity and conic factors, which are
+//   applied once per splat after the warp sum (raw_to_grads) instead of once per lane and
+//   visit. It leaves out the |dL/dmean2d| sums (pair values 9 and 10): they feed only the
+//   densify statistic stats.w, which no densify decision reads
 //   (train_densify_mark.comp:22-57 uses x, y, z).
 // - backward_pixels = 8 (raster_bwd_warp_tile): one warp per whole tile, either mode.
 #include "gs_kernels.h"
@@ -546,6 +547,9 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
   float u = 0.0f, st = 0.0f, sty = 0.0f;
 #pragma unroll
   for (int k = 6; k < 12; ++k) c[k] = 0.0f;
+  // Whether some lane of the warp blends in some group. Without ABS it is set, warp-uniform,
+  // by the groups' votes below; with ABS from each lane's tests and one more vote, which
+  // measured faster in the deterministic kernel.
   bool has = false;
   float dy[PX], G[PX], raw[PX], alpha[PX];
   bool blend[PX];
@@ -557,7 +561,7 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
     raw[p] = __fmul_rn(A.z, G[p]);
     alpha[p] = fminf(kMaxAlpha, raw[p]);
     blend[p] = pos <= last[p] && e <= 0.0f && alpha[p] >= kMinAlpha;
-    has = has || blend[p];
+    if constexpr (ABS) has = has || blend[p];
   }
   // Then the groups' adjoints, each skipped by the whole warp when no lane blends; a
   // lane that does not blend takes alpha 0, which leaves its T and R as they are and
@@ -565,6 +569,7 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
 #pragma unroll
   for (int p = 0; p < PX; ++p) {
     if (!__any_sync(0xffffffffu, blend[p])) continue;
+    if constexpr (!ABS) has = true;
     const float ab = blend[p] ? alpha[p] : 0.0f;
     const float gc = dl0[p] * B.z + dl1[p] * B.w + dl2[p] * blue;
     const float weight = ab * T[p];
@@ -587,7 +592,8 @@ __device__ __forceinline__ bool splat_adjoint(const float4 A, const float4 B, co
     T[p] = __fmul_rn(T[p], one_minus);
     R[p] = rest;
   }
-  if (!__any_sync(0xffffffffu, has)) return false;
+  if constexpr (ABS) has = __any_sync(0xffffffffu, has);
+  if (!has) return false;
   if constexpr (RAW) {
     c[0] = u;
     c[1] = dx * u;
@@ -1120,14 +1126,13 @@ __global__ void __launch_bounds__(128, 5) k_raster_bwd_warp(RasterArgs a) {
 // raster_bwd_tile (TileLayout<PX>: an 8 x 4PX block, 8 / PX of them a tile). The warp
 // stages its own rounds of 32 splats from the tile's list, stops at its block's own
 // furthest last contributor, and adds each splat's sums into the gaussian's accumulator
-// with three 16-byte vector atomics, so no warp waits at a block barrier for another
-// warp's pixels or round. Staging the tile's list once per warp instead of once per tile
+// with vector atomics, so no warp waits at a block barrier for another warp's pixels or
+// round. Staging the tile's list once per warp instead of once per tile
 // costs about 2% more instructions. (The deterministic mode adds the warps of a tile in a
 // fixed order instead, in raster_bwd_tile.)
 struct SplitSmem {
   float4 a[32], b[32], c[32];  // the round's staged splats (stage_splat)
-  uint32_t dst[32];            // their gaussians
-  float part[32][12];          // the round's per-splat warp sums
+  float part[32][12];          // the round's per-splat warp sums (9 used)
   float lanes[32][12];         // the lanes' values of the splat being summed (warp_sum9_rows)
 };
 
@@ -1165,14 +1170,14 @@ __device__ __forceinline__ void raster_bwd_split(const RasterArgs& a, uint32_t i
   for (uint32_t start = 0; start < stop; start += 32u) {
     __syncwarp();  // the previous round's reads of the staging buffers are done
     float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
+    uint32_t g = 0u;  // the gaussian of the splat this lane stages
     if (start + lane < stop) {
-      const uint32_t g = a.rb.gauss[range.x + start + lane];
+      g = a.rb.gauss[range.x + start + lane];
       const float4 q0 = a.splat[size_t(g) * 3u], q1 = a.splat[size_t(g) * 3u + 1u], q2 = a.splat[size_t(g) * 3u + 2u];
       stage_splat(q0, q1, q2, a.foot[g].w, A, B, C);
       sm.a[lane] = A;
       sm.b[lane] = B;
       sm.c[lane] = C;
-      sm.dst[lane] = g;
     }
     __syncwarp();
     const uint32_t nb = min(32u, stop - start);
@@ -1186,25 +1191,23 @@ __device__ __forceinline__ void raster_bwd_split(const RasterArgs& a, uint32_t i
       if (splat_adjoint<PX, false, true>(sm.a[j], sm.b[j], sm.c[j].x, start + j + 1u, cx, cy, dl0, dl1, dl2, last, T,
                                          R, c)) {
         const float sum = warp_sum9_rows(sm.lanes, c, lane);
-        if (lane < 12u) sm.part[j][lane] = lane < 9u ? sum : 0.0f;
+        if (lane < 9u) sm.part[j][lane] = sum;
         wrote |= 1u << j;
       }
     }
     __syncwarp();
-    if ((wrote >> lane) & 1u) {  // lane j staged splat j: its factors are this lane's A and B
-      float4* row = reinterpret_cast<float4*>(&sm.part[lane][0]);
+    // Lane j staged splat j: it applies the splat's factors (its own A and B) to the warp
+    // sums and adds them into the gaussian's accumulator, two 16-byte atomics and one for
+    // the ninth value.
+    if ((wrote >> lane) & 1u) {
+      const float4* row = reinterpret_cast<const float4*>(&sm.part[lane][0]);
       const float4 r0 = row[0], r1 = row[1];
       float r[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
       raw_to_grads<false>(A, B, r);
-      row[0] = make_float4(r[0], r[1], r[2], r[3]);
-      row[1] = make_float4(r[4], r[5], r[6], r[7]);
-    }
-    __syncwarp();
-    for (uint32_t idx = lane; idx < nb * 3u; idx += 32u) {
-      const uint32_t j = idx / 3u, q = idx - 3u * j;
-      if ((wrote >> j) & 1u)
-        atomicAdd(reinterpret_cast<float4*>(a.grad2d) + size_t(sm.dst[j]) * 3u + q,
-                  *reinterpret_cast<const float4*>(&sm.part[j][4u * q]));
+      float4* acc = reinterpret_cast<float4*>(a.grad2d) + size_t(g) * 3u;
+      atomicAdd(acc, make_float4(r[0], r[1], r[2], r[3]));
+      atomicAdd(acc + 1, make_float4(r[4], r[5], r[6], r[7]));
+      atomicAdd(reinterpret_cast<float*>(acc + 2), sm.part[lane][8]);
     }
   }
 }
