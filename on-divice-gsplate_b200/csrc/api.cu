@@ -670,6 +670,7 @@ struct gs_context {
     // gaussian, which the raster passes stage from directly (no gather). Deterministic and
     // forward-only steps keep the index (per-pair gradients, the render-order snapshots).
     payload_gaussian = train && !det;
+    vb.view_word = train && !det;  // the projection zeroes grad2d for the atomics and leaves the view word
     GS_CUDA_TRY(cudaMemsetAsync(d_scalars, 0, sizeof(uint32_t), stream));  // [0] pairs; [1] mismatches accumulate
     const uint32_t motion = motion_mode();
     const gsk::Motion mo = motion_state();

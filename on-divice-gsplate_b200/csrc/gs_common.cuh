@@ -175,6 +175,16 @@ __device__ __forceinline__ uint2 footprint_row_tiles(float mx, float my, float a
   return make_uint2(uint32_t(cols.x) / kTile, uint32_t(cols.y) / kTile + 1u);
 }
 
+// The view word of a drawn (view, slot) in fast mode: the footprint radius (an
+// integer-valued float; saturated at 2^29 - 1 pixels, far above any pruning threshold)
+// above the three clamped-colour bits. Integers below 2^29 convert both ways exactly.
+__device__ __forceinline__ float pack_view_word(float radius, uint32_t clamped) {
+  const uint32_t r = radius >= 536870911.0f ? 536870911u : uint32_t(radius);
+  return __uint_as_float(r << 3 | (clamped & 7u));
+}
+__device__ __forceinline__ uint32_t view_word_clamped(float w) { return __float_as_uint(w) & 7u; }
+__device__ __forceinline__ float view_word_radius(float w) { return float(__float_as_uint(w) >> 3); }
+
 // Tile count of the ellipse, and its tile-row spans packed for the pair emission:
 // x = first tile row | rows << 16 | bit 31 when the spans below are complete; y, z, w hold
 // rows 0-5 as 16 bits each, first tile (10 bits) | tiles in the row (6 bits) << 10. More

@@ -34,6 +34,10 @@ struct ViewBuffers {
   uint32_t* tiles = nullptr; // tiles touched
   uint32_t* offsets = nullptr;  // first pair, pre-sort order
   float4* grad2d = nullptr;  // 3 per g: summed pair gradients (train_pair_sum layout)
+  // Atomic training steps: the projection leaves each drawn (view, slot)'s view word
+  // (pack_view_word: radius and clamped-colour bits) in grad2d's unused 12th float, and the
+  // optimizer reads it there instead of from the splat records.
+  bool view_word = false;
   float4* dir_grad = nullptr; // 1 per slot: position gradient through the SH view direction, summed over views
 };
 

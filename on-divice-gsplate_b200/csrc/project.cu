@@ -33,7 +33,7 @@ struct ProjectArgs {
   uint32_t* tiles;
   uint32_t* dkeys;
   uint32_t* dvals;
-  float4* grad2d;  // zeroed when non-null (atomic backward)
+  float4* grad2d;  // zeroed when non-null (atomic backward), the view word in its 12th float
   Motion motion;
 };
 
@@ -189,11 +189,12 @@ __global__ void __launch_bounds__(128, 7) k_project(ProjectArgs a) {
     const size_t e = size_t(v) * a.slots + i;
     a.dkeys[e] = (v << 16) | key;
     a.dvals[e] = uint32_t(g);
-    if (a.grad2d != nullptr) {
+    if (a.grad2d != nullptr) {  // zeroed for the backward's atomics, with the view word
       const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
       a.grad2d[g * 3u] = z;
       a.grad2d[g * 3u + 1u] = z;
-      a.grad2d[g * 3u + 2u] = z;
+      const float word = tiles > 0u ? pack_view_word(o1.w, __float_as_uint(o2.w)) : 0.f;
+      a.grad2d[g * 3u + 2u] = make_float4(0.f, 0.f, 0.f, word);
     }
   }
 }

@@ -175,11 +175,13 @@ __device__ __forceinline__ uint32_t warp_reduce_scatter12(float c[12], uint32_t 
 // The fast mode's sum of a splat's 9 gradient values (without the |dmean| sums) over a
 // warp's 32 lanes, through shared memory: each lane stores its values as a row of 12 floats
 // (three conflict-free 16-byte stores); lane v + 9h (v < 9, h < 3) adds value v down the
-// rows h, h + 3, h + 6, ... in two interleaved chains (the three groups' banks meet once);
-// lane v then adds the three groups. Fewer instructions than a shuffle butterfly, which
-// spends two selects per shuffle. Returns the warp sum of value `lane` for lanes below 9.
+// rows h, h + 3, h + 6, ... in two interleaved chains (the three groups' banks meet once)
+// and returns that third of the sum (lanes 27-31 return 0). The warp sum of value v is
+// third(v) + third(v + 9) + third(v + 18), in that order: warp_sum9_rows adds them with
+// two shuffles; the split backward stores the thirds and lets one lane add them per round.
+// Fewer instructions than a shuffle butterfly, which spends two selects per shuffle.
 // `rows` is the warp's own 32 x 12 scratch.
-__device__ __forceinline__ float warp_sum9_rows(float (*rows)[12], const float c[12], uint32_t lane) {
+__device__ __forceinline__ float warp_sum9_thirds(float (*rows)[12], const float c[12], uint32_t lane) {
   __syncwarp();  // the previous splat's rows have been read
   float4* row = reinterpret_cast<float4*>(&rows[lane][0]);
   row[0] = make_float4(c[0], c[1], c[2], c[3]);
@@ -196,7 +198,12 @@ __device__ __forceinline__ float warp_sum9_rows(float (*rows)[12], const float c
     }
     if (30u + h < 32u) even += rows[30u + h][v];
   }
-  const float sum = even + odd;
+  return even + odd;
+}
+
+// The warp sum of value `lane` for lanes below 9 (warp_sum9_thirds).
+__device__ __forceinline__ float warp_sum9_rows(float (*rows)[12], const float c[12], uint32_t lane) {
+  const float sum = warp_sum9_thirds(rows, c, lane);
   return sum + __shfl_down_sync(0xffffffffu, sum, 9) + __shfl_down_sync(0xffffffffu, sum, 18);
 }
 
@@ -1132,7 +1139,7 @@ __global__ void __launch_bounds__(128, 5) k_raster_bwd_warp(RasterArgs a) {
 // fixed order instead, in raster_bwd_tile.)
 struct SplitSmem {
   float4 a[32], b[32], c[32];  // the round's staged splats (stage_splat)
-  float part[32][12];          // the round's per-splat warp sums (9 used)
+  float part[32][28];          // the round's per-splat partial sums: value v of third h at v + 9h
   float lanes[32][12];         // the lanes' values of the splat being summed (warp_sum9_rows)
 };
 
@@ -1190,24 +1197,34 @@ __device__ __forceinline__ void raster_bwd_split(const RasterArgs& a, uint32_t i
       float c[12];
       if (splat_adjoint<PX, false, true>(sm.a[j], sm.b[j], sm.c[j].x, start + j + 1u, cx, cy, dl0, dl1, dl2, last, T,
                                          R, c)) {
-        const float sum = warp_sum9_rows(sm.lanes, c, lane);
-        if (lane < 9u) sm.part[j][lane] = sum;
+        const float third = warp_sum9_thirds(sm.lanes, c, lane);
+        if (lane < 27u) sm.part[j][lane] = third;
         wrote |= 1u << j;
       }
     }
     __syncwarp();
-    // Lane j staged splat j: it applies the splat's factors (its own A and B) to the warp
-    // sums and adds them into the gaussian's accumulator, two 16-byte atomics and one for
-    // the ninth value.
+    // Lane j staged splat j: it adds the three thirds of each warp sum, applies the splat's
+    // factors (its own A and B) and adds the result into the gaussian's accumulator, two
+    // 16-byte atomics and one for the ninth value.
     if ((wrote >> lane) & 1u) {
       const float4* row = reinterpret_cast<const float4*>(&sm.part[lane][0]);
-      const float4 r0 = row[0], r1 = row[1];
-      float r[12] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+      float t[28];
+#pragma unroll
+      for (int q = 0; q < 7; ++q) {
+        const float4 x = row[q];
+        t[4 * q] = x.x;
+        t[4 * q + 1] = x.y;
+        t[4 * q + 2] = x.z;
+        t[4 * q + 3] = x.w;
+      }
+      float r[12];
+#pragma unroll
+      for (int v = 0; v < 9; ++v) r[v] = t[v] + t[v + 9] + t[v + 18];  // the thirds in lane order
       raw_to_grads<false>(A, B, r);
       float4* acc = reinterpret_cast<float4*>(a.grad2d) + size_t(g) * 3u;
       atomicAdd(acc, make_float4(r[0], r[1], r[2], r[3]));
       atomicAdd(acc + 1, make_float4(r[4], r[5], r[6], r[7]));
-      atomicAdd(reinterpret_cast<float*>(acc + 2), sm.part[lane][8]);
+      atomicAdd(reinterpret_cast<float*>(acc + 2), r[8]);
     }
   }
 }

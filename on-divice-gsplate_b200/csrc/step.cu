@@ -100,10 +100,17 @@ struct StepArgs {
   const uint32_t* tiles;
   const float4* grad2d;
   float4* dir_grad;  // per slot: position gradient through the SH view direction (k_step_sh -> k_step_geometry)
+  bool view_word;    // grad2d's 12th float holds the view word (ViewBuffers::view_word), not zero
   const uint32_t* d_pairs;
   uint32_t accept;
   Motion motion;  // nodes == 0: no view moves
 };
+
+// A (view, slot)'s third grad2d float4 as the pair sums: without the view word.
+__device__ __forceinline__ float4 grad_tail(const StepArgs& a, float4 v) {
+  if (a.view_word) v.w = 0.0f;
+  return v;
+}
 
 // Adam (train_step.glsl:62-67). The square root and the division use the hardware's
 // approximate forms (PTX sqrt.approx.f32, relative error within 2^-23; div.full.f32,
@@ -532,7 +539,7 @@ __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
     const size_t gv = size_t(nv) * a.cap + i;
     n1 = a.grad2d[gv * 3u + 1u];
     n2 = a.grad2d[gv * 3u + 2u];
-    nw = a.splat[gv * 3u + 2u].w;
+    if (!a.view_word) nw = a.splat[gv * 3u + 2u].w;
   }
   while (mask) {
     const uint32_t v = nv;
@@ -544,10 +551,10 @@ __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
       const size_t gv = size_t(nv) * a.cap + i;
       n1 = a.grad2d[gv * 3u + 1u];
       n2 = a.grad2d[gv * 3u + 2u];
-      nw = a.splat[gv * 3u + 2u].w;
+      if (!a.view_word) nw = a.splat[gv * 3u + 2u].w;
     }
     float dcol[3];
-    view_colour_grad(a1, a2, __float_as_uint(cw), dcol);
+    view_colour_grad(a1, a2, a.view_word ? view_word_clamped(a2.w) : __float_as_uint(cw), dcol);
     colour |= dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f;
     const gs_frame_data& f = s_frames[v];
     float dr[3] = {p0.x - f.cam_pos[0], p0.y - f.cam_pos[1], p0.z - f.cam_pos[2]};
@@ -652,13 +659,16 @@ __global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
     n0 = a.grad2d[g * 3u];
     n1 = a.grad2d[g * 3u + 1u];
     n2 = a.grad2d[g * 3u + 2u];
-    nw = a.splat[g * 3u + 2u].w;
-    nr = a.splat[g * 3u + 1u].w;
+    if (!a.view_word) {
+      nw = a.splat[g * 3u + 2u].w;
+      nr = a.splat[g * 3u + 1u].w;
+    }
   }
   while (mask) {
     const uint32_t v = nv;
-    const float4 a0 = n0, a1 = n1, a2 = n2;
-    const float cw = nw, radius = nr;
+    const float4 a0 = n0, a1 = n1, a2 = grad_tail(a, n2);
+    const float cw = a.view_word ? __uint_as_float(view_word_clamped(n2.w)) : nw;
+    const float radius = a.view_word ? view_word_radius(n2.w) : nr;
     mask &= mask - 1u;
     if (mask) {
       nv = uint32_t(__ffs(mask) - 1);
@@ -666,8 +676,10 @@ __global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
       n0 = a.grad2d[g * 3u];
       n1 = a.grad2d[g * 3u + 1u];
       n2 = a.grad2d[g * 3u + 2u];
-      nw = a.splat[g * 3u + 2u].w;
-      nr = a.splat[g * 3u + 1u].w;
+      if (!a.view_word) {
+        nw = a.splat[g * 3u + 2u].w;
+        nr = a.splat[g * 3u + 1u].w;
+      }
     }
     float dcol[3], dir[3], dir_len;
     if constexpr (MOTION) {
@@ -726,7 +738,7 @@ __global__ void __launch_bounds__(128) k_pose_grad(StepArgs a, float* __restrict
       float4 st = make_float4(0.f, 0.f, 0.f, 0.f);
       float dcol[3], dir[3], dir_len;
       uint32_t drew = 0u;
-      const float4 a0 = a.grad2d[g * 3u], a1 = a.grad2d[g * 3u + 1u], a2 = a.grad2d[g * 3u + 2u];
+      const float4 a0 = a.grad2d[g * 3u], a1 = a.grad2d[g * 3u + 1u], a2 = grad_tail(a, a.grad2d[g * 3u + 2u]);
       const uint32_t clamped = __float_as_uint(a.splat[g * 3u + 2u].w);
       bool done = false;
       if constexpr (MOTION) {
@@ -839,8 +851,8 @@ __global__ void __launch_bounds__(128) k_motion_grad(StepArgs a, float* __restri
         float dcol[3], dir[3], dir_len;
         uint32_t drew = 0u;
         view_backward<DEG, false, true>(s_frame, p0, G, a.grad2d[g * 3u], a.grad2d[g * 3u + 1u],
-                                        a.grad2d[g * 3u + 2u], __float_as_uint(a.splat[g * 3u + 2u].w), 0.0f, g16,
-                                        nullptr, st, dcol, dir, dir_len, drew, nullptr, &dm, share);
+                                        grad_tail(a, a.grad2d[g * 3u + 2u]), __float_as_uint(a.splat[g * 3u + 2u].w),
+                                        0.0f, g16, nullptr, st, dcol, dir, dir_len, drew, nullptr, &dm, share);
         if constexpr (K > 0) {
           // The SH view-direction term of dL/dx: U (dd - dir (dir . dd)) / |x - c|.
           float dd[3] = {0.f, 0.f, 0.f};
@@ -1197,7 +1209,7 @@ StepArgs step_args(const StepPointers& sp, const Model& m, const ViewBuffers& vb
                    uint32_t accept, const Motion* motion) {
   return StepArgs{sp.frames, sp.n_views, m.cap,    m.slots,     m.P,     m.M,    m.V,
                   m.SH,      m.MSH,      m.VSH,    m.stats,     vb.splat, vb.tiles, vb.grad2d,
-                  vb.dir_grad, d_pairs,  accept,   motion ? *motion : Motion{}};
+                  vb.dir_grad, vb.view_word, d_pairs, accept, motion ? *motion : Motion{}};
 }
 
 void launch_step(const StepPointers& sp, const Model& m, uint32_t degree, const ViewBuffers& vb,
