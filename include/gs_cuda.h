@@ -120,7 +120,7 @@ typedef enum gs_snapshot_kind {
   GS_SNAP_PIXEL_GRAD = 1,   /* 4 floats per pixel: dL/dC rgb, final transmittance */
   GS_SNAP_PROJECTED = 2,    /* 16 floats per slot (train_common.glsl:9-13) */
   GS_SNAP_TILES = 3,        /* uint32 per slot: tiles touched */
-  GS_SNAP_OFFSETS = 4,      /* uint32 per slot: first pair (pre-sort order) */
+  GS_SNAP_OFFSETS = 4,      /* uint32 per slot: first pair, pre-sort order (not after an atomic training step) */
   GS_SNAP_PAIR_GRADS = 5,   /* 12 floats per pair, pre-sort order (deterministic mode) */
   GS_SNAP_PAIR_TILE = 6,    /* uint32 per pair, pre-sort order: the view's tile (not after an atomic training step) */
   GS_SNAP_RENDER_ORDER = 7, /* uint32 per pair: pre-sort index in render order (not after an atomic training step) */

@@ -1257,7 +1257,12 @@ int gs_snapshot(gs_context* c, uint32_t view, gs_snapshot_kind which, void* host
       case GS_SNAP_PIXEL_OUT: d2h(host, c->pixel_out + pb, size); break;
       case GS_SNAP_SPAWN: d2h(host, c->dens.spawn, size); break;
       case GS_SNAP_TILES: d2h(host, c->vb.tiles + size_t(view) * cap, size); break;
-      case GS_SNAP_OFFSETS: d2h(host, c->vb.offsets + size_t(view) * cap, size); break;
+      case GS_SNAP_OFFSETS:
+        if (c->payload_gaussian)
+          fail(GS_ERR_INVALID, "gs_snapshot: an atomic training step keeps no first-pair offsets: deterministic or "
+                               "forward-only steps keep them");
+        d2h(host, c->vb.offsets + size_t(view) * cap, size);
+        break;
       case GS_SNAP_STATS: d2h(host, c->model.stats, size); break;
       case GS_SNAP_MOTION_BIND: d2h(host, c->motion_bind, size); break;
       case GS_SNAP_CONTRIBUTIONS: std::memcpy(host, &c->last_contributions, size); break;

@@ -23,7 +23,7 @@ struct EmitArgs {
   const float4* splat;
   const float4* foot;
   const uint4* spans;
-  uint32_t* offsets;
+  uint32_t* offsets;  // first pair per g; null in atomic training steps (only snapshots read it)
   uint32_t* keys;
   uint32_t* values;
   uint32_t* pair_gaussian;  // g per pre-sort pair; null when the values carry g (nothing reads it then)
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
   const uint32_t wfirst = __shfl_sync(0xffffffffu, p, 0);
   const uint32_t wend = min(__reduce_max_sync(0xffffffffu, count ? p + count : 0u), a.pair_capacity);
   if (wend <= wfirst) {
-    if (count != 0u) a.offsets[a.sorted_vals[k]] = p;  // all past the capacity
+    if (count != 0u && a.offsets != nullptr) a.offsets[a.sorted_vals[k]] = p;  // all past the capacity
     return;
   }
   const bool staged = wend - wfirst <= kEmitStage;
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(128) k_emit(EmitArgs a) {
     const uint32_t v = g / a.cap;
     const gs_frame_data& f = a.frames[v];
     const uint4 packed = a.spans[g];
-    a.offsets[g] = p;
+    if (a.offsets != nullptr) a.offsets[g] = p;
     const uint32_t end = min(p + count, a.pair_capacity);
     const uint32_t tile_base = a.vt->tile_base[v];
     const uint32_t width = f.image[0], height = f.image[1], tiles_x = f.image[2];
@@ -199,9 +199,11 @@ void launch_emit(const StepPointers& sp, const ViewBuffers& vb, uint32_t cap, ui
                  uint32_t pair_capacity, uint32_t* keys, uint32_t* values, uint32_t* pair_gaussian, float4* pair_grads,
                  uint32_t* mismatch, bool payload_gaussian, cudaStream_t st) {
   if (n_items == 0u) return;
-  EmitArgs a{sp.frames, sp.vt,    cap,        n_items, pair_capacity, sorted_vals, sorted_offsets,
-             total,     vb.splat, vb.foot,    vb.spans, vb.offsets, keys,  values,       pair_gaussian,
-             pair_grads, mismatch, payload_gaussian};
+  // An atomic training step (the gaussian as the payload) writes no first-pair offsets.
+  uint32_t* offsets = payload_gaussian ? nullptr : vb.offsets;
+  EmitArgs a{sp.frames, sp.vt,    cap,        n_items,  pair_capacity, sorted_vals, sorted_offsets,
+             total,     vb.splat, vb.foot,    vb.spans, offsets,       keys,        values,
+             pair_gaussian, pair_grads, mismatch, payload_gaussian};
   k_emit<<<(n_items + 127u) / 128u, 128, 0, st>>>(a);
 }
 
