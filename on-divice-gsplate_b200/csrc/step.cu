@@ -510,7 +510,7 @@ __device__ __forceinline__ void copy_frames(const StepArgs& a, gs_frame_data* s_
 // together so each thread keeps 18 loads in flight (the SH values are already loaded).
 // Capped at 128 registers (4 blocks per SM, a few spills): 55 us faster on 8 views of 1M
 // slots than 3 blocks at 168 registers; at 5 blocks (96 registers) the spills cost more.
-template <int DEG, bool MOTION>
+template <int DEG, bool MOTION, bool WORD>
 __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
     const size_t gv = size_t(nv) * a.cap + i;
     n1 = a.grad2d[gv * 3u + 1u];
     n2 = a.grad2d[gv * 3u + 2u];
-    if (!a.view_word) nw = a.splat[gv * 3u + 2u].w;
+    if (!WORD) nw = a.splat[gv * 3u + 2u].w;
   }
   while (mask) {
     const uint32_t v = nv;
@@ -551,10 +551,10 @@ __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
       const size_t gv = size_t(nv) * a.cap + i;
       n1 = a.grad2d[gv * 3u + 1u];
       n2 = a.grad2d[gv * 3u + 2u];
-      if (!a.view_word) nw = a.splat[gv * 3u + 2u].w;
+      if (!WORD) nw = a.splat[gv * 3u + 2u].w;
     }
     float dcol[3];
-    view_colour_grad(a1, a2, a.view_word ? view_word_clamped(a2.w) : __float_as_uint(cw), dcol);
+    view_colour_grad(a1, a2, WORD ? view_word_clamped(a2.w) : __float_as_uint(cw), dcol);
     colour |= dcol[0] != 0.0f || dcol[1] != 0.0f || dcol[2] != 0.0f;
     const gs_frame_data& f = s_frames[v];
     float dr[3] = {p0.x - f.cam_pos[0], p0.y - f.cam_pos[1], p0.z - f.cam_pos[2]};
@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(128, 4) k_step_sh(StepArgs a) {
 
 // Part 2 (train_step.glsl:72-240): every view's projection backward summed, plus the SH
 // view-direction term from part 1, then Adam on the 16 parameters.
-template <int DEG, bool MOTION>
+template <int DEG, bool MOTION, bool WORD>
 __global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
   __shared__ gs_frame_data s_frames[kMaxViews];
   copy_frames(a, s_frames, a.n_views);
@@ -659,16 +659,16 @@ __global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
     n0 = a.grad2d[g * 3u];
     n1 = a.grad2d[g * 3u + 1u];
     n2 = a.grad2d[g * 3u + 2u];
-    if (!a.view_word) {
+    if (!WORD) {
       nw = a.splat[g * 3u + 2u].w;
       nr = a.splat[g * 3u + 1u].w;
     }
   }
   while (mask) {
     const uint32_t v = nv;
-    const float4 a0 = n0, a1 = n1, a2 = grad_tail(a, n2);
-    const float cw = a.view_word ? __uint_as_float(view_word_clamped(n2.w)) : nw;
-    const float radius = a.view_word ? view_word_radius(n2.w) : nr;
+    const float4 a0 = n0, a1 = n1, a2 = WORD ? make_float4(n2.x, n2.y, n2.z, 0.0f) : n2;
+    const float cw = WORD ? __uint_as_float(view_word_clamped(n2.w)) : nw;
+    const float radius = WORD ? view_word_radius(n2.w) : nr;
     mask &= mask - 1u;
     if (mask) {
       nv = uint32_t(__ffs(mask) - 1);
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(128, 5) k_step_geometry(StepArgs a) {
       n0 = a.grad2d[g * 3u];
       n1 = a.grad2d[g * 3u + 1u];
       n2 = a.grad2d[g * 3u + 2u];
-      if (!a.view_word) {
+      if (!WORD) {
         nw = a.splat[g * 3u + 2u].w;
         nr = a.splat[g * 3u + 1u].w;
       }
@@ -1186,23 +1186,30 @@ void launch_pair_sum(const ViewBuffers& vb, uint32_t n_items, const uint32_t* de
   k_pair_sum<<<(n_items + per_block - 1u) / per_block, per_block, 0, st>>>(a);
 }
 
-template <bool MOTION>
-void step_degree(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const StepArgs& a) {
+template <bool MOTION, bool WORD>
+void step_degree_word(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const StepArgs& a) {
   switch (degree) {
-    case 0: k_step_geometry<0, MOTION><<<grid, block, 0, st>>>(a); break;
+    case 0: k_step_geometry<0, MOTION, WORD><<<grid, block, 0, st>>>(a); break;
     case 1:
-      k_step_sh<1, MOTION><<<grid, block, 0, st>>>(a);
-      k_step_geometry<1, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_sh<1, MOTION, WORD><<<grid, block, 0, st>>>(a);
+      k_step_geometry<1, MOTION, WORD><<<grid, block, 0, st>>>(a);
       break;
     case 2:
-      k_step_sh<2, MOTION><<<grid, block, 0, st>>>(a);
-      k_step_geometry<2, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_sh<2, MOTION, WORD><<<grid, block, 0, st>>>(a);
+      k_step_geometry<2, MOTION, WORD><<<grid, block, 0, st>>>(a);
       break;
     default:
-      k_step_sh<3, MOTION><<<grid, block, 0, st>>>(a);
-      k_step_geometry<3, MOTION><<<grid, block, 0, st>>>(a);
+      k_step_sh<3, MOTION, WORD><<<grid, block, 0, st>>>(a);
+      k_step_geometry<3, MOTION, WORD><<<grid, block, 0, st>>>(a);
       break;
   }
+}
+
+// The view word's reads are compiled in or out (WORD), so neither mode branches on it.
+template <bool MOTION>
+void step_degree(uint32_t degree, dim3 grid, dim3 block, cudaStream_t st, const StepArgs& a) {
+  if (a.view_word) step_degree_word<MOTION, true>(degree, grid, block, st, a);
+  else step_degree_word<MOTION, false>(degree, grid, block, st, a);
 }
 
 StepArgs step_args(const StepPointers& sp, const Model& m, const ViewBuffers& vb, const uint32_t* d_pairs,
