@@ -138,6 +138,7 @@ struct gs_context {
   uint32_t *keys = nullptr, *values = nullptr, *keys_alt = nullptr, *values_alt = nullptr, *pair_gaussian = nullptr;
   uint32_t* sorted_g = nullptr;  // each sorted pair's gaussian, in render order (gathered by the ranges pass)
   bool payload_gaussian = false;  // the latest step sorted each pair's gaussian instead of its pre-sort index
+  bool graph_payload = false;     // payload_gaussian of the captured graph's steps
   float4* pair_grads = nullptr;
   const uint32_t* sorted_keys = nullptr;
   const uint32_t* sorted_values = nullptr;
@@ -376,8 +377,10 @@ struct gs_context {
       GS_CUDA_TRY(e);
       graph_key = key;
       graph_launches = launches;
+      graph_payload = payload_gaussian;
     }
     launches = graph_launches;
+    payload_gaussian = graph_payload;  // a step recorded since (without the graph) may have changed it
     GS_CUDA_TRY(cudaGraphLaunch(graph_exec, stream));
   }
 
