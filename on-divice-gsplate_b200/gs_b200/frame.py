@@ -226,12 +226,21 @@ def make_frames(cameras: list[Camera], slots: int, sh_stride: int, step: int, op
         return np.zeros(0, FRAME_DTYPE)
     f = np.repeat(make_frame(cameras[0], slots, sh_stride, step, options, background, camera_extent, masked_target,
                              ssim, pair_capacity), len(cameras))
-    W = np.array([c.width for c in cameras], np.uint32)
-    H = np.array([c.height for c in cameras], np.uint32)
-    f["rot"][:, :, :3] = np.stack([np.asarray(c.rotation, np.float32).reshape(3, 3) for c in cameras])
-    f["rot"][:, :, 3] = np.stack([np.asarray(c.translation, np.float32).reshape(3) for c in cameras])
-    f["cam_pos"][:, :3] = np.stack([np.asarray(c.position, np.float32).reshape(3) for c in cameras])
-    f["intrinsics"] = np.array([(c.fx, c.fy, c.cx, c.cy) for c in cameras], np.float32)
-    f["image"] = np.stack([W, H, (W + TILE - 1) // TILE, (H + TILE - 1) // TILE], axis=1)
-    f["background"][:, 3] = np.float32(1.0) / (np.float32(3.0) * W.astype(np.float32) * H.astype(np.float32))
+    n = len(cameras)
+    rot = np.empty((n, 3, 4), np.float32)
+    pos = np.empty((n, 3), np.float32)
+    intr = np.empty((n, 4), np.float32)
+    image = np.empty((n, 4), np.uint32)
+    for k, c in enumerate(cameras):
+        rot[k, :, :3] = np.asarray(c.rotation).reshape(3, 3)
+        rot[k, :, 3] = c.translation
+        pos[k] = c.position
+        intr[k] = (c.fx, c.fy, c.cx, c.cy)
+        image[k] = (c.width, c.height, (c.width + TILE - 1) // TILE, (c.height + TILE - 1) // TILE)
+    f["rot"] = rot
+    f["cam_pos"][:, :3] = pos
+    f["intrinsics"] = intr
+    f["image"] = image
+    W, H = image[:, 0].astype(np.float32), image[:, 1].astype(np.float32)
+    f["background"][:, 3] = np.float32(1.0) / (np.float32(3.0) * W * H)
     return f
