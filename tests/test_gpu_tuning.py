@@ -143,9 +143,11 @@ def test_async_staging_is_bit_identical(ctx):
 
 
 def test_atomic_steps_sort_gaussians(ctx):
-    """An atomic training step sorts each pair's gaussian (no pre-sort index): the pair-order
-    snapshots are refused with a message, the tile ranges and gradients are those of the
-    deterministic step, and a forward-only step afterwards has the pair order again."""
+    """An atomic training step sorts each pair's gaussian (no pre-sort index): the pair-order,
+    per-pair gaussian and first-pair offset snapshots are refused with a message, also after
+    a graph replay that follows a step run without the graph; the tile ranges and gradients
+    are those of the deterministic step, and a forward-only step afterwards has the pair
+    order again."""
     from gs_b200.cuda import GsError
 
     scene, cam, opt, target = view_and_target()
@@ -163,10 +165,19 @@ def test_atomic_steps_sort_gaussians(ctx):
     ctx.step(train=True)
     np.testing.assert_array_equal(ctx.snapshot("ranges"), ref_ranges)
     assert rel_l2(ctx.first_step_gradients()[0], ref_g) < 1e-5
+    for kind in ("render_order", "pair_gaussian", "offsets"):  # an atomic step keeps none of them
+        with pytest.raises(GsError, match="atomic training step"):
+            ctx.snapshot(kind)
+    # A counting forward between two replays of the training graph runs without the graph;
+    # the replay after it is an atomic step again.
+    ctx.step(train=False, count=True)
+    ctx.snapshot("offsets")
+    ctx.step(train=True)
     with pytest.raises(GsError, match="atomic training step"):
-        ctx.snapshot("render_order")
+        ctx.snapshot("offsets")
     ctx.step(train=False)
     np.testing.assert_array_equal(ctx.snapshot("render_order"), ref_order)
+    ctx.snapshot("pair_gaussian")
     ctx.set_tuning(deterministic=1)
 
 
